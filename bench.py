@@ -1,0 +1,286 @@
+#!/usr/bin/env python
+"""Throughput of Canard's full time step on B200, in Mpoint-steps/s.
+
+Workload (default): Taylor-Green vortex on a single 256^3-cell block (257^3
+stored points, the reference's point count including the periodic shared
+points), viscous, plain FP64, the full reference time step: 15 compact filter
+passes, then 4 Runge-Kutta stages (primitives, viscous stresses, fluxes, 27
+compact line solves per stage, GCBC/sponge where present, RK update, junction
+averaging), with the reference's dt schedule. Synthetic, seeded input.
+
+One step = one call of the reference's time-loop body. `value` is device time
+(CUDA events on the launching stream, max over ranks) with the state resident
+in HBM; `e2e` goes through the public C ABI with the state in pinned host
+memory copied in and out every step. Multi-GPU runs are independent replicas
+(the single-block case has no partition on this path), so scaling is weak.
+
+`--impl reference` times the reference algorithm on the host CPU cores (the
+oracle restatement: the Fortran reference cannot be compiled in this image).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = None
+try:
+    METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
+except Exception:
+    METRIC = "Mpoint-steps/s on 1 B200"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256, help="cells per direction of the TGV block")
+    p.add_argument("--cpu-n", type=int, default=128, help="cells per direction of the CPU sample")
+    p.add_argument("--cpu-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_arm(n, steps, warmup=0):
+    """Oracle (CPU restatement of the reference) on a TGV sample; returns
+    Mpoint-steps/s, thread count, sample description."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from canard_b200 import cases
+    threads = os.cpu_count() or 1
+    cs = cases.tgv(n)
+    o = po.Oracle(cs, threads=threads)
+    if warmup:
+        o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    v = cs.npts * steps / dt / 1e6
+    sample = (f"TGV {n}^3 cells ({n + 1}^3 points), viscous FP64, {steps} full steps after set-up"
+              f"{' and ' + str(warmup) + ' warm-up steps' if warmup else ''}, OpenMP over lines")
+    return v, threads, sample, dt
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except Exception:
+                continue
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v_steps = []
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        from canard_b200 import cases
+        threads = os.cpu_count() or 1
+        cs = cases.tgv(args.cpu_n)
+        o = po.Oracle(cs, threads=threads)
+        o.step(args.warmup)
+        t0 = time.perf_counter()
+        o.step(args.steps)
+        dt = time.perf_counter() - t0
+        v = cs.npts * args.steps / dt / 1e6
+        sample = (f"each step = one full reference time step of TGV {args.cpu_n}^3 cells "
+                  f"({args.cpu_n + 1}^3 points), viscous FP64, on the host CPU")
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpoint-steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded TGV initial condition)",
+                "config": {"workload": f"tgv{args.n}: Taylor-Green vortex, viscous, FP64 plain, full step",
+                           "cpu_sample": f"tgv{args.cpu_n}"},
+                "cpu_baseline": {"value": v, "unit": "Mpoint-steps/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        del v_steps
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from canard_b200 import api, cases
+
+    if args.warmup < 3:
+        raise SystemExit("at least 3 warm-up steps")
+    cs = cases.tgv(args.n)
+    ctx = api.Context(cs)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    npts = cs.npts
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    ctx.step(args.warmup)
+    barrier()
+    torch.cuda.synchronize()
+    n0 = ctx.launch_count()
+    clk = Clocks(local) if rank == 0 else None
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop() if clk else None
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launch_count() - n0
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * npts * args.steps / (ms / 1e3) / 1e6
+
+    # per-family device time (the reference's timers as CUDA events), one step
+    ctx.set_timers(True)
+    ctx.step(1)
+    fam = ctx.timers()
+    ctx.set_timers(False)
+    tot = sum(f["ms"] for f in fam.values())
+    dom_name, dom = max(((k, v) for k, v in fam.items() if k.startswith(("deriv", "filter"))),
+                        key=lambda kv: kv[1]["ms"])
+    line_fams = {k: v for k, v in fam.items() if k.startswith(("deriv", "filter"))}
+    lb = sum(v["bytes"] for v in line_fams.values())
+    lms = sum(v["ms"] for v in line_fams.values())
+    peak, peak_kind = peaks()
+    achieved = dom["bytes"] / dom["launches"] / (dom["ms"] / dom["launches"] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom_name)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": f"k_line ({dom_name})", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": dom["bytes"] / dom["launches"],
+                "all_line_solves_gbs": lb / (lms / 1e3) / 1e9}
+
+    # end to end through the C ABI: pinned host state in and out every step
+    qh = torch.empty((5,) + cs.blocks[0].shape, dtype=torch.float64, pin_memory=True)
+    qh.copy_(torch.from_numpy(ctx.state(0)))
+    qn = qh.numpy()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_steps):
+        ctx.set_state(0, qn)
+        ctx.step(1)
+        ctx.get_state_into(0, qn)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ems = max(f0.elapsed_time(f1), wall * 1e3)
+    if dist is not None:
+        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = {"value": world * npts * args.e2e_steps / (ems / 1e3) / 1e6, "unit": "Mpoint-steps/s",
+           "h2d_bytes_per_step": int(qh.numel() * 8), "d2h_bytes_per_step": int(qh.numel() * 8),
+           "steps": args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ctx.close()
+        torch.cuda.empty_cache()
+        v, th, sample, _ = cpu_arm(args.cpu_n, args.cpu_steps)
+        cpu = {"value": v, "unit": "Mpoint-steps/s", "cores": th, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Taylor-Green vortex initial condition)",
+                "config": {"workload": f"tgv{args.n}: Taylor-Green vortex {args.n}^3 cells ({args.n + 1}^3 points),"
+                                       " Re 1600, Mach 0.1, viscous, FP64 plain, full time step",
+                           "points": npts, "precision": "fp64",
+                           "l2": "inputs larger than L2 (state, metrics and work fields ~"
+                                 f"{54 * 8 * npts / 1e9:.1f} GB resident)",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks,
+                "families": {k: {"ms_per_step": v["ms"], "share": v["ms"] / tot if tot else 0.0,
+                                 "launches": v["launches"]} for k, v in fam.items() if v["launches"]}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,257 @@
+"""Python host side of the C ABI (include/canard_gpu.h).
+
+Mirrors the reference's interfaces for the time-step path:
+
+* ``Context.mpigo / deriv / filte``      -> t_numerics (src/mo_numerics.f90:429-987)
+* ``Context.phase(PH_FLUXES, nk)`` etc.  -> t_physics / mo_gcbc / mo_sponge routines
+* ``Context.step(n)``                    -> the time loop body (src/mo_canard_driver.f90:226-431)
+
+Arrays cross the boundary as host float64 arrays in the reference layout
+``q(0:lmx, ncols)`` (NumPy shape ``(ncols, lze+1, let+1, lxi+1)``).
+Errors come back as ``CanardError`` carrying the library's code and message,
+the way the reference stops with a message.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Sequence
+
+import numpy as np
+
+from . import cases as _cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libcanard_b200.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(7)
+FP64, FP32_MIXED = 0, 1
+
+F_QA, F_QO, F_DE, F_P, F_SS1, F_XIM, F_ETM, F_ZEM, F_YACO, F_TAU = range(10)
+F_DRVA = (10, 11, 12)
+F_CM = (13, 14, 15)
+NCOLS = {F_QA: 5, F_QO: 5, F_DE: 5, F_P: 1, F_SS1: 1, F_XIM: 3, F_ETM: 3, F_ZEM: 3, F_YACO: 1, F_TAU: 9}
+
+(PH_FILTER, PH_COPYQO, PH_PRIM, PH_TIMESTEP, PH_VISCOUS, PH_FLUXES, PH_GCBC, PH_SPONGE,
+ PH_RKUPDATE, PH_WALL, PH_AVERAGE, PH_ADVANCE, PH_MOVEF_A) = range(13)
+
+
+class CanardError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"canard error {code}: {msg}")
+        self.code = code
+
+
+class _Block(ctypes.Structure):
+    _fields_ = [("lxi", ctypes.c_int32), ("let", ctypes.c_int32), ("lze", ctypes.c_int32),
+                ("nbc", (ctypes.c_int32 * 2) * 3), ("mbcd", (ctypes.c_int32 * 2) * 3)]
+
+
+class _Case(ctypes.Structure):
+    _fields_ = [("nblocks", ctypes.c_int32), ("viscous", ctypes.c_int32),
+                ("fltk", ctypes.c_double), ("fltrbc", ctypes.c_double),
+                ("reoo", ctypes.c_double), ("tempoo", ctypes.c_double),
+                ("amach1", ctypes.c_double), ("amach2", ctypes.c_double), ("amach3", ctypes.c_double),
+                ("timf", ctypes.c_double), ("nsmf", ctypes.c_int32), ("cfl", ctypes.c_double),
+                ("szco", ctypes.c_double), ("szth0", ctypes.c_double), ("szth1", ctypes.c_double),
+                ("doml0", ctypes.c_double), ("doml1", ctypes.c_double)]
+
+
+_lib = None
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"{LIBPATH} is missing: build it with canard_b200/csrc/build.py")
+        L = ctypes.CDLL(LIBPATH)
+        vp = ctypes.c_void_p
+        i32 = ctypes.c_int32
+        L.canard_ctx_create.argtypes = [ctypes.POINTER(_Case), i32, ctypes.POINTER(_Block), i32,
+                                        ctypes.POINTER(vp)]
+        L.canard_ctx_destroy.argtypes = [vp]
+        L.canard_last_error.restype = ctypes.c_char_p
+        L.canard_last_error.argtypes = [vp]
+        L.canard_set_stream.argtypes = [vp, vp]
+        L.canard_upload_grid.argtypes = [vp, i32, i32, _DP]
+        L.canard_setup.argtypes = [vp]
+        L.canard_set_state.argtypes = [vp, i32, i32, _DP]
+        L.canard_get_state.argtypes = [vp, i32, i32, _DP]
+        L.canard_get_field.argtypes = [vp, i32, i32, i32, _DP, ctypes.c_int64]
+        L.canard_set_field.argtypes = [vp, i32, i32, i32, _DP, ctypes.c_int64]
+        L.canard_step.argtypes = [vp, i32]
+        L.canard_phase.argtypes = [vp, i32, i32]
+        L.canard_get_time.argtypes = [vp, i32, _DP]
+        L.canard_set_time.argtypes = [vp, i32, _DP]
+        L.canard_mpigo.argtypes = [vp, ctypes.POINTER(_DP), i32, i32, i32, i32, i32, i32]
+        L.canard_deriv.argtypes = [vp, i32, _DP, _DP, i32, i32]
+        L.canard_filte.argtypes = [vp, i32, _DP, i32, i32]
+        L.canard_set_timers.argtypes = [vp, i32]
+        L.canard_get_timers.argtypes = [vp, _DP, _DP, _DP, i32]
+        L.canard_timer_name.restype = ctypes.c_char_p
+        L.canard_timer_name.argtypes = [i32]
+        L.canard_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.canard_coeffs.argtypes = [ctypes.c_double, ctypes.c_double, _DP]
+        L.canard_penta.argtypes = [ctypes.c_double, ctypes.c_double, i32, i32, i32, i32, _DP, _DP]
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_DP)
+
+
+def coeffs(fltk: float, fltrbc: float) -> np.ndarray:
+    out = np.zeros(150)
+    rc = lib().canard_coeffs(fltk, fltrbc, _dp(out))
+    if rc:
+        raise CanardError(rc, "canard_coeffs")
+    return out
+
+
+def penta(fltk, fltrbc, n, ns, ne, nt):
+    xu = np.zeros(3 * n)
+    xl = np.zeros(2 * n)
+    rc = lib().canard_penta(fltk, fltrbc, n, ns, ne, nt, _dp(xu), _dp(xl))
+    if rc:
+        raise CanardError(rc, "canard_penta")
+    return xu.reshape(3, n), xl.reshape(2, n)
+
+
+def _structs(case_list: Sequence[_cases.CaseSpec]):
+    cs_arr = (_Case * len(case_list))()
+    blocks = [b for cs in case_list for b in cs.blocks]
+    b_arr = (_Block * len(blocks))()
+    for i, cs in enumerate(case_list):
+        c = cs_arr[i]
+        c.nblocks = len(cs.blocks)
+        c.viscous = int(cs.viscous)
+        c.fltk, c.fltrbc, c.reoo, c.tempoo = cs.fltk, cs.fltrbc, cs.reoo, cs.tempoo
+        c.amach1, c.amach2, c.amach3 = (float(v) for v in cs.amach)
+        c.timf, c.nsmf, c.cfl = cs.timf, int(cs.nsmf), cs.cfl
+        c.szco, c.szth0, c.szth1, c.doml0, c.doml1 = cs.szco, cs.szth0, cs.szth1, cs.doml0, cs.doml1
+    for i, b in enumerate(blocks):
+        b_arr[i].lxi, b_arr[i].let, b_arr[i].lze = b.lxi, b.let, b.lze
+        for d in range(3):
+            for s in range(2):
+                b_arr[i].nbc[d][s] = int(b.nbc[d][s])
+                b_arr[i].mbcd[d][s] = int(b.mbcd[d][s])
+    return cs_arr, b_arr
+
+
+class Context:
+    """A device context holding one or more cases (several = batched)."""
+
+    def __init__(self, case_list, precision: int = FP64, setup: bool = True, upload_state: bool = True):
+        if isinstance(case_list, _cases.CaseSpec):
+            case_list = [case_list]
+        self.cases: List[_cases.CaseSpec] = list(case_list)
+        self._c, self._b = _structs(self.cases)
+        h = ctypes.c_void_p()
+        rc = lib().canard_ctx_create(self._c, len(self.cases), self._b, int(precision), ctypes.byref(h))
+        if rc:
+            raise CanardError(rc, "canard_ctx_create failed")
+        self.h = h
+        if setup:
+            for ci, cs in enumerate(self.cases):
+                for bi, x in enumerate(cs.xyz):
+                    self._check(lib().canard_upload_grid(self.h, ci, bi, _dp(np.ascontiguousarray(x, np.float64))))
+            self._check(lib().canard_setup(self.h))
+        if upload_state:
+            for ci, cs in enumerate(self.cases):
+                if cs.qa is not None:
+                    for bi, q in enumerate(cs.qa):
+                        self.set_state(bi, q, ci)
+
+    def _check(self, rc):
+        if rc:
+            raise CanardError(rc, lib().canard_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().canard_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int):
+        self._check(lib().canard_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def set_state(self, b, qa, case=0):
+        self._check(lib().canard_set_state(self.h, case, b, _dp(np.ascontiguousarray(qa, np.float64))))
+
+    def state(self, b=0, case=0):
+        blk = self.cases[case].blocks[b]
+        out = np.zeros((5,) + blk.shape)
+        self._check(lib().canard_get_state(self.h, case, b, _dp(out)))
+        return out
+
+    def get_state_into(self, b, out, case=0):
+        self._check(lib().canard_get_state(self.h, case, b, _dp(out)))
+
+    def set_timers(self, on):
+        self._check(lib().canard_set_timers(self.h, 1 if on else 0))
+
+    def timers(self):
+        """Per kernel family: device ms, launches, algorithmic bytes since set_timers(True)."""
+        n = 32
+        ms, la, by = np.zeros(n), np.zeros(n), np.zeros(n)
+        k = lib().canard_get_timers(self.h, _dp(ms), _dp(la), _dp(by), n)
+        if k < 0:
+            self._check(-k)
+        return {lib().canard_timer_name(i).decode(): {"ms": ms[i], "launches": int(la[i]), "bytes": by[i]}
+                for i in range(k)}
+
+    def launch_count(self):
+        v = ctypes.c_int64()
+        self._check(lib().canard_launch_count(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def field(self, which, b=0, case=0):
+        blk = self.cases[case].blocks[b]
+        if which in NCOLS:
+            out = np.zeros((NCOLS[which],) + blk.shape)
+        else:
+            nbs = [(blk.let + 1) * (blk.lze + 1), (blk.lze + 1) * (blk.lxi + 1), (blk.lxi + 1) * (blk.let + 1)]
+            d = (which - 10) % 3
+            out = np.zeros((10 if which < 13 else 6) * nbs[d])
+        self._check(lib().canard_get_field(self.h, case, b, which, _dp(out), out.size))
+        return out
+
+    def set_field(self, which, arr, b=0, case=0):
+        a = np.ascontiguousarray(arr, np.float64)
+        self._check(lib().canard_set_field(self.h, case, b, which, _dp(a), a.size))
+
+    def step(self, n=1):
+        self._check(lib().canard_step(self.h, n))
+
+    def phase(self, ph, nk=0):
+        self._check(lib().canard_phase(self.h, ph, nk))
+
+    def time(self, case=0):
+        out = np.zeros(6)
+        self._check(lib().canard_get_time(self.h, case, _dp(out)))
+        return out
+
+    def set_time(self, t6, case=0):
+        self._check(lib().canard_set_time(self.h, case, _dp(np.asarray(t6, np.float64))))
+
+    # t_numerics
+    def mpigo(self, fields, nt, nrt, n45, itag, m, ncols=1):
+        arr = (_DP * len(fields))(*[_dp(f) for f in fields])
+        self._check(lib().canard_mpigo(self.h, arr, ncols, nt, nrt, n45, itag, m))
+
+    def deriv(self, b, fin, fout, nn, m):
+        self._check(lib().canard_deriv(self.h, b, _dp(fin), _dp(fout), nn, m))
+
+    def filte(self, b, f, inn, m):
+        self._check(lib().canard_filte(self.h, b, _dp(f), inn, m))

@@ -1,0 +1,265 @@
+"""Case descriptions and synthetic inputs for the Canard per-step hot path.
+
+A case is the content of the reference's ``input.canard`` namelists for one run
+(``nml_domdcomp``, ``nml_numerics``, ``nml_physics``, ``nml_canard``,
+``nml_sponge``; see src/mo_io.f90:35-66, src/mo_physics.f90:86-111,
+src/mo_numerics.f90:97-110, src/mo_sponge.f90:210-220, src/mo_gridgen.f90:49-71)
+plus the grid coordinates and the initial conserved state of every block.
+
+Every block is one sub-domain with ``nbpc = 1`` (one rank per block in the
+reference). Field arrays use the reference layout: a NumPy array of shape
+``(ncols, lze+1, let+1, lxi+1)`` in C order is exactly the Fortran array
+``q(0:lmx, ncols)`` with ``l = (k*(let+1)+j)*(lxi+1)+i`` (src/mo_utils.f90:54-69).
+
+The workloads are seeded synthetic stand-ins for the configurations the
+throughput metric is quoted on (the reference ships no data sets):
+
+* ``tgv``: Taylor-Green vortex on [0, 2pi]^3, periodic on all faces.
+* ``curvilinear_4block``: 4 blocks tiled 2x2 in (xi, eta) on a sine-perturbed
+  grid, non-reflecting GCBC in/outflow, sponge, periodic in zeta.
+* ``vortex``: isentropic vortex advected through a GCBC outflow.
+* ``batched``: many independent single-block TGV / vortex cases.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+# boundary codes, src/mo_parameters.f90:34-40
+BC_NON_REFLECTIVE = 10
+BC_WALL_INVISCID = 20
+BC_WALL_VISCOUS = 25
+BC_INTER_CURV = 30
+BC_INTER_STRAIGHT = 35
+BC_INTER_SUBDOMAINS = 40
+BC_PERIODIC = 45
+
+GAM = 1.4
+
+
+@dataclasses.dataclass
+class BlockSpec:
+    lxi: int
+    let: int
+    lze: int
+    nbc: Sequence[Sequence[int]]   # [direction][side]
+    mbcd: Sequence[Sequence[int]]  # [direction][side], neighbour block or -1
+
+    @property
+    def shape(self):
+        return (self.lze + 1, self.let + 1, self.lxi + 1)
+
+    @property
+    def npts(self) -> int:
+        return (self.lxi + 1) * (self.let + 1) * (self.lze + 1)
+
+
+@dataclasses.dataclass
+class CaseSpec:
+    blocks: List[BlockSpec]
+    viscous: int = 1
+    fltk: float = 0.85          # namelist value; the code uses pi*fltk
+    fltrbc: float = 0.85
+    reoo: float = 16000.0
+    tempoo: float = 300.0
+    amach: Sequence[float] = (0.0, 0.0, 0.0)
+    timf: float = 0.0
+    nsmf: int = 1
+    cfl: float = 0.8
+    szco: float = 0.0
+    szth0: float = 0.0
+    szth1: float = 0.0
+    doml0: float = 0.0
+    doml1: float = 0.0
+    xyz: Optional[List[np.ndarray]] = None   # per block (3, Z, Y, X)
+    qa: Optional[List[np.ndarray]] = None    # per block (5, Z, Y, X)
+    name: str = ""
+
+    @property
+    def npts(self) -> int:
+        return sum(b.npts for b in self.blocks)
+
+
+def _conserved(rho, u, v, w, p):
+    q = np.empty((5,) + rho.shape)
+    q[0] = rho
+    q[1] = rho * u
+    q[2] = rho * v
+    q[3] = rho * w
+    q[4] = p / (GAM - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return q
+
+
+def tgv(n: int = 64, mach: float = 0.1, re: float = 1600.0, viscous: int = 1,
+        nx: Optional[int] = None, ny: Optional[int] = None, nz: Optional[int] = None) -> CaseSpec:
+    """Taylor-Green vortex: u = V0 sin x cos y cos z, v = -V0 cos x sin y cos z,
+    w = 0, p = 1/gamma + V0^2/16 (cos 2x + cos 2y)(cos 2z + 2), isothermal start
+    (T = gamma p / rho = 1), V0 = Mach in units of the sound speed.
+
+    The flow is at rest in the frame (amach = 0), so the reference uses reoo
+    unscaled (src/mo_physics.f90:104-106): reoo = Re / M."""
+    nx = nx or n
+    ny = ny or n
+    nz = nz or n
+    per = [[BC_PERIODIC, BC_PERIODIC]] * 3
+    blk = BlockSpec(nx, ny, nz, [list(p) for p in per], [[0, 0], [0, 0], [0, 0]])
+    x = 2 * np.pi * np.arange(nx + 1) / nx
+    y = 2 * np.pi * np.arange(ny + 1) / ny
+    z = 2 * np.pi * np.arange(nz + 1) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    xyz = np.stack([X, Y, Z])
+    v0 = mach
+    u = v0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    v = -v0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    w = np.zeros_like(u)
+    p = 1.0 / GAM + v0 * v0 / 16.0 * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    rho = GAM * p
+    return CaseSpec([blk], viscous=viscous, reoo=re / mach, xyz=[xyz], qa=[_conserved(rho, u, v, w, p)],
+                    name=f"tgv{nx}x{ny}x{nz}")
+
+
+def vortex_state(X, Y, mach, strength=5.0, radius=1.0, xc=0.0, yc=0.0):
+    """Isentropic vortex (strength in units of the sound speed) in a uniform
+    stream of Mach ``mach`` along x; returns rho, u, v, w, p."""
+    r2 = ((X - xc) ** 2 + (Y - yc) ** 2) / radius ** 2
+    eps = strength * mach / (2 * np.pi)   # peak swirl, Yee's beta scaled by the stream speed
+    du = -eps * (Y - yc) / radius * np.exp(0.5 * (1 - r2))
+    dv = eps * (X - xc) / radius * np.exp(0.5 * (1 - r2))
+    T = 1.0 - 0.5 * (GAM - 1) * eps * eps * np.exp(1 - r2)   # cyclostrophic, isentropic
+    rho = T ** (1.0 / (GAM - 1))
+    p = rho * T / GAM
+    return rho, mach + du, dv, np.zeros_like(du), p
+
+
+def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, viscous=1) -> CaseSpec:
+    """Isentropic vortex advected through a non-reflecting (GCBC) outflow.
+
+    Domain [-8, 8] x [-16/3, 16/3] x [0, 4], xi faces BC 10, eta faces BC 10,
+    zeta periodic. The vortex is moved by the uniform stream in the lab frame
+    (amach = 0), so ``reoo = Re / M``."""
+    bc = [[BC_NON_REFLECTIVE, BC_NON_REFLECTIVE], [BC_NON_REFLECTIVE, BC_NON_REFLECTIVE],
+          [BC_PERIODIC, BC_PERIODIC]]
+    mb = [[-1, -1], [-1, -1], [0, 0]]
+    blk = BlockSpec(nx, ny, nz, bc, mb)
+    lx = 16.0
+    dx = lx / nx
+    x = -8.0 + dx * np.arange(nx + 1)
+    y = -0.5 * ny * dx + dx * np.arange(ny + 1)
+    z = dx * np.arange(nz + 1)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    rho, u, v, w, p = vortex_state(X, Y, mach, strength, radius)
+    return CaseSpec([blk], viscous=viscous, reoo=re / mach, xyz=[np.stack([X, Y, Z])],
+                    qa=[_conserved(rho, u, v, w, p)], name=f"vortex{nx}x{ny}x{nz}")
+
+
+def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, seed=7,
+                       viscous=1, sponge_cells=20) -> CaseSpec:
+    """Four blocks tiled 2x2 in (xi, eta) on x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta),
+    y = eta + 0.05 sin(2 pi xi), z = zeta with unit index spacing h = 1/128.
+
+    Block numbering: 0 (lower left), 1 (lower right), 2 (upper left), 3 (upper
+    right). Faces: xi-min of 0/2 and xi-max of 1/3 are non-reflecting (10);
+    the xi interface is a straight interface (35); the eta interface is a
+    curved interface (30); the outer eta faces are periodic between the lower
+    and the upper row (45); zeta is periodic on each block (45).
+
+    The uniform stream (Mach ``mach`` along x) is carried by the moving frame
+    (amach1 = mach, nsmf = 1), with 1% seeded velocity noise. The sponge covers
+    the last ``sponge_cells`` cells before the outflow (szth1 = half of it,
+    src/mo_sponge.f90:238-249)."""
+    h = 1.0 / 128.0
+    NX, NY, NZ = 2 * nxb, 2 * nyb, nzb
+    blocks = []
+    for bj in range(2):
+        for bi in range(2):
+            nbc = [[0, 0], [0, 0], [BC_PERIODIC, BC_PERIODIC]]
+            mb = [[-1, -1], [-1, -1], [-1, -1]]
+            me = 2 * bj + bi
+            mb[2] = [me, me]
+            if bi == 0:
+                nbc[0] = [BC_NON_REFLECTIVE, BC_INTER_STRAIGHT]
+                mb[0] = [-1, me + 1]
+            else:
+                nbc[0] = [BC_INTER_STRAIGHT, BC_NON_REFLECTIVE]
+                mb[0] = [me - 1, -1]
+            other = 2 * (1 - bj) + bi
+            if bj == 0:
+                nbc[1] = [BC_PERIODIC, BC_INTER_CURV]
+            else:
+                nbc[1] = [BC_INTER_CURV, BC_PERIODIC]
+            mb[1] = [other, other]
+            blocks.append(BlockSpec(nxb, nyb, nzb, nbc, mb))
+    rng = np.random.default_rng(seed)
+    xyz, qa = [], []
+    for bj in range(2):
+        for bi in range(2):
+            i = bi * nxb + np.arange(nxb + 1)
+            j = bj * nyb + np.arange(nyb + 1)
+            k = np.arange(nzb + 1)
+            Kz, Jy, Ix = np.meshgrid(k, j, i, indexing="ij")
+            xi, eta, zeta = Ix * h, Jy * h, Kz * h
+            X = xi + 0.05 * np.sin(2 * np.pi * eta) * np.sin(2 * np.pi * zeta)
+            Y = eta + 0.05 * np.sin(2 * np.pi * xi)
+            Z = zeta
+            xyz.append(np.stack([X, Y, Z]))
+            shape = X.shape
+            rho = np.ones(shape)
+            p = np.full(shape, 1.0 / GAM)
+            u = noise * mach * rng.standard_normal(shape)
+            v = noise * mach * rng.standard_normal(shape)
+            w = noise * mach * rng.standard_normal(shape)
+            qa.append(_conserved(rho, u, v, w, p))
+    xmax = NX * h
+    return CaseSpec(blocks, viscous=viscous, reoo=re, amach=(mach, 0.0, 0.0), nsmf=1,
+                    szco=1.0, szth0=0.0, szth1=0.5 * sponge_cells * h, doml0=0.0, doml1=xmax,
+                    xyz=xyz, qa=qa, name=f"curv4x{nxb}x{nyb}x{nzb}")
+
+
+def batched(ncases=64, seed=11, lo=32, hi=96) -> List[CaseSpec]:
+    """Independent single-block cases with seeded uneven sides in [lo, hi],
+    alternating TGV and isentropic vortex, Mach in [0.1, 0.5], Re in [400, 3200]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(ncases):
+        nx, ny, nz = (int(v) for v in rng.integers(lo, hi + 1, size=3))
+        mach = float(rng.uniform(0.1, 0.5))
+        re = float(rng.uniform(400.0, 3200.0))
+        if c % 2 == 0:
+            cs = tgv(nx=nx, ny=ny, nz=nz, mach=mach, re=re)
+        else:
+            cs = _periodic_vortex(nx, ny, nz, mach, re)
+        cs.name = f"b{c}:" + cs.name
+        out.append(cs)
+    return out
+
+
+def _periodic_vortex(nx, ny, nz, mach, re):
+    per = [[BC_PERIODIC, BC_PERIODIC]] * 3
+    blk = BlockSpec(nx, ny, nz, [list(p) for p in per], [[0, 0], [0, 0], [0, 0]])
+    L = 10.0
+    x = -L / 2 + L * np.arange(nx + 1) / nx
+    y = -L / 2 + L * np.arange(ny + 1) / ny
+    z = L * np.arange(nz + 1) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    rho, u, v, w, p = vortex_state(X, Y, mach, 5.0, 1.0)
+    return CaseSpec([blk], viscous=1, reoo=re / mach, xyz=[np.stack([X, Y, Z])],
+                    qa=[_conserved(rho, u, v, w, p)], name=f"pvortex{nx}x{ny}x{nz}")
+
+
+def noise_fields(blk: BlockSpec, nfields: int = 5, seed: int = 20261203, kmax: int = 32) -> np.ndarray:
+    """Seeded N(0,1) noise plus sum_{k=1..kmax} sin(k 2 pi i / N) along each
+    direction, for the isolated derivative / filter benches."""
+    rng = np.random.default_rng(seed)
+    Z, Y, X = blk.shape
+    out = rng.standard_normal((nfields,) + blk.shape)
+    i = np.arange(X)[None, None, :]
+    j = np.arange(Y)[None, :, None]
+    k = np.arange(Z)[:, None, None]
+    modes = np.zeros(blk.shape)
+    for kk in range(1, kmax + 1):
+        modes = modes + np.sin(kk * 2 * np.pi * i / max(X - 1, 1)) + np.sin(kk * 2 * np.pi * j / max(Y - 1, 1)) \
+            + np.sin(kk * 2 * np.pi * k / max(Z - 1, 1))
+    return out + modes[None]

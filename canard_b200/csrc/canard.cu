@@ -1,0 +1,1366 @@
+// Context, set-up and time-loop orchestration of the Canard hot path, behind
+// the C ABI of include/canard_gpu.h. One context = one CUDA stream; all device
+// memory is allocated at canard_ctx_create / canard_setup, never on the step
+// path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "canard_gpu.h"
+#include "host.h"
+#include "kernels.cuh"
+
+using namespace canard;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct ApiError : std::runtime_error {
+  int code;
+  ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess)                                                                      \
+      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+template <class T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc(&p, n * sizeof(T)));
+  CK(cudaMemset(p, 0, n * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+template <class T>
+T* dupload(const std::vector<T>& v, cudaStream_t st) {
+  T* p = dalloc<T>(v.size());
+  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return p;
+}
+
+const int kNnf[3] = {2, 3, 1};  // filter direction order (src/mo_numerics.f90:22)
+
+// A task table resident on the device.
+template <class T>
+struct Table {
+  T* tasks = nullptr;
+  int* first = nullptr;
+  int ntasks = 0;
+  int total = 0;  // tiles or lines
+  size_t smem = 0;
+  double bytes = 0;  // algorithmic bytes of one launch
+};
+
+struct CaseState {
+  canard_case_desc d;
+  Scheme sch;
+  DevScheme* dsch = nullptr;
+  int b0 = 0, nb = 0;
+  double reoo, srefoo, srefp1dre, uoo[3];
+  int n = 0, ndt = 0;
+  double dt = 0, dts = 0, dte = 0, timo = 0;
+};
+
+struct BlockState {
+  BlockGeom g;
+  double* arena = nullptr;
+  BlockDev dev;  // host copy of the device descriptor
+  double *lu[2][3] = {};       // [nt][dir]: 5 * L
+  double *recv[2][3] = {};     // [nt][dir]: 5 fields x 2 sides x ncomp x nbs
+  double* chain[3] = {};       // [dir]: 2 sides x nbs
+  double* drva[3] = {};        // (nbs,5,0:1)
+  double* drvb[3] = {};
+  double* cm[3] = {};          // (nbs,3,0:1)
+  long long* gc_pts = nullptr;
+  double* gc_w = nullptr;
+  std::vector<GcbcFace> gc_faces;
+  long long* sp_pts = nullptr;
+  double *sp_a = nullptr, *sp_b = nullptr;
+  int sp_n = 0;
+  std::vector<double> xyz_host;  // reference layout, kept for the sponge set-up
+  double* recv_ptr(int nt, int dir, int m, int side) const {
+    const int nc = nt == 0 ? 2 : 3;
+    return recv[nt][dir] + ((size_t)(m - 1) * 2 + side) * nc * g.nbs[dir];
+  }
+};
+
+// field offsets inside a block arena (in units of npad)
+enum { F_QA = 0, F_QO = 5, F_DE = 10, F_P = 15, F_MU = 16, F_XIM = 17, F_ETM = 20, F_ZEM = 23, F_YACO = 26,
+       F_TAU = 27, F_SCR = 36, F_XYZ = 51, F_COUNT = 54 };
+
+enum TimerFamily {
+  T_DERIV_XI = 0, T_DERIV_ETA, T_DERIV_ZETA, T_FILTER_XI, T_FILTER_ETA, T_FILTER_ZETA, T_MPIGO, T_PRIM,
+  T_FLUXCOMP, T_VISCASM, T_FLUXSUM, T_RK, T_GCBC, T_SPONGE, T_AVERAGE, T_TIMESTEP, T_COPY, T_NFAM
+};
+const char* kTimerNames[T_NFAM] = {"deriv_xi", "deriv_eta", "deriv_zeta", "filter_xi", "filter_eta", "filter_zeta",
+                                   "mpigo", "primitives", "flux_components", "viscous_assemble", "flux_sum",
+                                   "rk_update", "gcbc", "sponge", "averaging", "timestep", "copy_qo"};
+
+struct AvgDev {
+  int ntg = 0, nsrc = 0;
+  int *tb = nullptr, *tfirst = nullptr, *tcount = nullptr, *sb = nullptr;
+  long long *tl = nullptr, *sl = nullptr;
+  double* snap = nullptr;
+};
+
+}  // namespace
+
+struct canard_ctx {
+  std::string err;
+  int precision = CANARD_FP64;
+  cudaStream_t own = nullptr, st = nullptr;
+  std::vector<CaseState> cases;
+  std::vector<BlockState> blocks;
+  std::vector<FaceLink> links;  // global block indices
+  BlockDev* dbd = nullptr;
+  CaseConst* dcc = nullptr;
+  StageParams* dsp = nullptr;       // [2 ring][5 slots][ncases]
+  StageParams* hsp = nullptr;       // pinned, same shape
+  cudaEvent_t ring_ev[2] = {nullptr, nullptr};
+  int ring = 0;
+  unsigned long long* ddt = nullptr;  // [ncases][2]
+  unsigned long long* hdt = nullptr;  // pinned
+  int* derr = nullptr;
+  bool setup_done = false;
+  // hot-path tables
+  Table<LineTask> filt[5][3], visc[3], flux[3];
+  Table<FaceTask> mp_filt[5][3], mp_visc, mp_flux;
+  Table<GcbcTask> gc_setup, gc_upd[3][2];
+  std::vector<const double*> fc_src_h;
+  double** fc_src = nullptr;
+  double** fc_dst = nullptr;
+  int* fc_cnt = nullptr;
+  int fc_n = 0, fc_max = 0;
+  Table<SpongeTask> sponge;
+  AvgDev avg_pt, avg_ln, avg_sf;
+  // timers (mo_timer equivalent) and launch counter
+  bool timers = false;
+  long long launches = 0;
+  double t_ms[T_NFAM] = {}, t_n[T_NFAM] = {}, t_bytes[T_NFAM] = {};
+  struct Pending { int fam; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double ew_bytes_per_pt = 0;  // sum over blocks of valid points (for element-wise bytes)
+  // scratch for set-up / unit calls
+  std::vector<void*> transient;
+  int cur_slot_base = 0;
+  size_t max_smem_line = 0;
+};
+
+namespace {
+
+void set_err(canard_ctx* c, const std::string& m) {
+  if (c) c->err = m;
+}
+
+int nblk(const canard_ctx* c) { return (int)c->blocks.size(); }
+
+cudaEvent_t pool_event(canard_ctx* c) {
+  if (c->ev_pool.empty()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    return e;
+  }
+  cudaEvent_t e = c->ev_pool.back();
+  c->ev_pool.pop_back();
+  return e;
+}
+
+// Brackets one launch of family `fam`; `bytes` = algorithmic bytes moved.
+struct Timed {
+  canard_ctx* c;
+  int fam;
+  cudaEvent_t b = nullptr;
+  Timed(canard_ctx* c_, int fam_, double bytes) : c(c_), fam(fam_) {
+    c->launches += 1;
+    c->t_n[fam] += 1;
+    c->t_bytes[fam] += bytes;
+    if (c->timers) {
+      cudaEvent_t a = pool_event(c);
+      b = pool_event(c);
+      CK(cudaEventRecord(a, c->st));
+      c->pending.push_back({fam, a, b});
+    }
+  }
+  ~Timed() noexcept(false) {
+    if (b) CK(cudaEventRecord(b, c->st));
+  }
+};
+
+void collect_timers(canard_ctx* c) {
+  for (auto& p : c->pending) {
+    float ms = 0;
+    CK(cudaEventSynchronize(p.b));
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    c->t_ms[p.fam] += ms;
+    c->ev_pool.push_back(p.a);
+    c->ev_pool.push_back(p.b);
+  }
+  c->pending.clear();
+}
+
+double valid_points(const canard_ctx* c) {
+  double s = 0;
+  for (auto& b : c->blocks) s += (double)b.g.X * b.g.Y * b.g.Z;
+  return s;
+}
+
+double* fptr(const BlockState& b, int f) { return b.arena + (size_t)f * b.g.npad; }
+
+// ---- line task construction ----------------------------------------------------
+void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const double* in,
+                    double* out, int m, bool with_drva, LineTask& t) {
+  const BlockGeom& g = B.g;
+  t.in = in;
+  t.out = out;
+  t.lu = B.lu[nt][dir];
+  t.recv = B.recv_ptr(nt, dir, m, 0);
+  t.drva = with_drva ? B.drva[dir] : nullptr;
+  t.sc = c->cases[g.case_id].dsch;
+  t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp;
+  t.L = g.ijk[0][dir] + 1;
+  t.nbs = g.nbs[dir];
+  t.m = m;
+  t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
+  t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
+  if (dir == 0) {
+    t.ntx = 1;
+    t.ntiles = (g.Y * g.Z + kLanes - 1) / kLanes;
+  } else {
+    t.ntx = (g.X + kLanes - 1) / kLanes;
+    t.ntiles = t.ntx * (dir == 1 ? g.Z : g.Y);
+  }
+}
+
+size_t line_smem(int dir, int L) {
+  if (dir == 0) return 128 + (size_t)kLanes * dir1_pitch(L) * sizeof(double);
+  return 128 + (size_t)L * kLanes * sizeof(double);
+}
+
+Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir, bool transient) {
+  Table<LineTask> T;
+  std::vector<int> first;
+  int tot = 0;
+  size_t sm = 0;
+  for (auto& t : v) {
+    t.tile0 = tot;
+    first.push_back(tot);
+    tot += t.ntiles;
+    sm = std::max(sm, line_smem(dir, t.L));
+    T.bytes += 2.0 * sizeof(double) * t.X * t.Y * t.Z;  // read the field, write the result
+  }
+  T.ntasks = (int)v.size();
+  T.total = tot;
+  T.smem = sm;
+  T.tasks = dupload(v, c->st);
+  T.first = dupload(first, c->st);
+  if (transient) {
+    c->transient.push_back(T.tasks);
+    c->transient.push_back(T.first);
+  }
+  return T;
+}
+
+template <class T>
+Table<T> make_lines_table(canard_ctx* c, std::vector<T> v, bool transient, int T::*count_field,
+                          int T::*first_field) {
+  Table<T> Tb;
+  std::vector<int> first;
+  int tot = 0;
+  for (auto& t : v) {
+    t.*first_field = tot;
+    first.push_back(tot);
+    tot += t.*count_field;
+  }
+  Tb.ntasks = (int)v.size();
+  Tb.total = tot;
+  Tb.tasks = dupload(v, c->st);
+  Tb.first = dupload(first, c->st);
+  if (transient) {
+    c->transient.push_back(Tb.tasks);
+    c->transient.push_back(Tb.first);
+  }
+  return Tb;
+}
+
+template <int DIR, int OP>
+void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
+  k_line<DIR, OP><<<T.total, kLanes, T.smem, c->st>>>(T.tasks, T.first, T.ntasks, c->derr);
+  CK(cudaGetLastError());
+}
+
+void launch_line(canard_ctx* c, const Table<LineTask>& T, int dir, int op) {
+  if (op == 0) {
+    if (dir == 0) launch_line_dir<1, 0>(c, T);
+    else if (dir == 1) launch_line_dir<2, 0>(c, T);
+    else launch_line_dir<3, 0>(c, T);
+  } else {
+    if (dir == 0) launch_line_dir<1, 1>(c, T);
+    else if (dir == 1) launch_line_dir<2, 1>(c, T);
+    else launch_line_dir<3, 1>(c, T);
+  }
+}
+
+void set_line_smem_limits() {
+  static bool done = false;
+  if (done) return;
+  const int lim = 227 * 1024;
+  CK(cudaFuncSetAttribute(k_line<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK(cudaFuncSetAttribute(k_line<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK(cudaFuncSetAttribute(k_line<3, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK(cudaFuncSetAttribute(k_line<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK(cudaFuncSetAttribute(k_line<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK(cudaFuncSetAttribute(k_line<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  done = true;
+}
+
+// ---- mpigo face tasks ----------------------------------------------------------
+// One task per sending face (block, dir, side) with ndf = 1. `col(b, dir)`
+// gives the field column the block uses for that direction.
+template <class ColFn>
+std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, int exch_dir, ColFn col,
+                                 int only_case = -1) {
+  std::vector<FaceTask> out;
+  int line0 = 0;
+  for (const FaceLink& L : c->links) {
+    if (only_case >= 0 && c->blocks[L.src_b].g.case_id != only_case) continue;
+    const BlockState& S = c->blocks[L.src_b];
+    const BlockState& R = c->blocks[L.dst_b];
+    const int d = L.nn;
+    if (!bc_interface(S.g.nbc[d][L.src_side])) continue;
+    FaceTask t{};
+    t.src = col(L.src_b, d);
+    t.dstf = col(L.dst_b, d);
+    t.recv = R.recv_ptr(nt, d, m, L.dst_side);
+    t.chain = S.chain[d] + (size_t)L.src_side * S.g.nbs[d];
+    t.sc = c->cases[S.g.case_id].dsch;
+    t.nn = d + 1;
+    t.sb = L.src_side;
+    t.nt = nt;
+    t.exch = (exch_dir < 0 || exch_dir == d) ? 1 : 0;
+    const int np = S.g.nbc[d][L.src_side];
+    t.iik = (np == BC_SUBDOM) ? 0 : 1;
+    t.ra0k = (np == BC_PERIODIC) ? (double)n45 : 0.0;
+    t.corr = (n45 == 1 && R.g.nbc[d][L.dst_side] == BC_PERIODIC) ? 1 : 0;
+    t.X = S.g.X; t.Y = S.g.Y; t.Z = S.g.Z; t.Xp = S.g.Xp; t.N = S.g.ijk[0][d];
+    t.XA = R.g.X; t.YA = R.g.Y; t.ZA = R.g.Z; t.XpA = R.g.Xp; t.NA = R.g.ijk[0][d];
+    t.nbs = S.g.nbs[d];
+    t.nj = S.g.ijk[1][d] + 1;
+    t.line0 = line0;
+    line0 += t.nbs;
+    out.push_back(t);
+  }
+  return out;
+}
+
+Table<FaceTask> make_face_table(canard_ctx* c, std::vector<FaceTask> v, bool transient) {
+  Table<FaceTask> T;
+  std::vector<int> first;
+  int tot = 0;
+  for (auto& t : v) { t.line0 = tot; first.push_back(tot); tot += t.nbs; }
+  T.ntasks = (int)v.size();
+  T.total = tot;
+  T.bytes = (double)tot * (12 + (v.empty() ? 0 : (v[0].nt ? 3 : 2))) * sizeof(double);
+  T.tasks = dupload(v, c->st);
+  T.first = dupload(first, c->st);
+  if (transient) { c->transient.push_back(T.tasks); c->transient.push_back(T.first); }
+  return T;
+}
+
+void launch_mpigo(canard_ctx* c, const Table<FaceTask>& T) {
+  if (T.ntasks == 0) return;
+  const int thr = 128;
+  const int grid = std::min((T.total + thr - 1) / thr, 148 * 16);
+  Timed tm(c, T_MPIGO, T.bytes);
+  k_mpigo<<<grid, thr, 0, c->st>>>(T.tasks, T.first, T.ntasks, T.total);
+  CK(cudaGetLastError());
+}
+
+dim3 ew_grid(const canard_ctx* c) {
+  long long mx = 0;
+  for (auto& b : c->blocks) mx = std::max<long long>(mx, (long long)b.g.npad);
+  long long gx = std::min<long long>((mx + 255) / 256, 148 * 8);
+  return dim3((unsigned)std::max<long long>(gx, 1), (unsigned)c->blocks.size());
+}
+
+void free_transient(canard_ctx* c) {
+  for (void* p : c->transient) cudaFree(p);
+  c->transient.clear();
+}
+
+void collect_timers(canard_ctx* c);
+void sync_check(canard_ctx* c) {
+  CK(cudaStreamSynchronize(c->st));
+  collect_timers(c);
+  int e = 0;
+  CK(cudaMemcpy(&e, c->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(c->derr, 0, sizeof(int)));
+    throw ApiError(CANARD_ERR_TIMEOUT, "a bounded device wait gave up (error flag set by a kernel)");
+  }
+}
+
+// ---- moving frame, src/mo_physics.f90:144-169 (host arithmetic) ----------------
+void movef(const CaseState& cs, double dtko, double dtk, double umf[3], double dudtmf[3]) {
+  const double pi = std::acos(-1.0);
+  if (cs.d.nsmf == 0) {
+    const double ra0 = pi / cs.d.timf;
+    const double ra1 = ra0 * std::min(cs.timo, cs.d.timf);
+    const double ra2 = ra0 * std::min(cs.timo + dtko, cs.d.timf);
+    double fctr = 1.0 - std::cos(ra1);
+    double dfdt = ra0 * std::sin(ra2);
+    double progmf = 0.5 * (fctr + dtk * dfdt);
+    for (int d = 0; d < 3; ++d) umf[d] = progmf * cs.uoo[d];
+    fctr = std::sin(ra1);
+    dfdt = ra0 * std::cos(ra2);
+    progmf = (0.5 * ra0) * (fctr + dtk * dfdt);
+    for (int d = 0; d < 3; ++d) dudtmf[d] = progmf * cs.uoo[d];
+  } else {
+    for (int d = 0; d < 3; ++d) { umf[d] = cs.uoo[d]; dudtmf[d] = 0.0; }
+  }
+}
+
+// stage parameters of stage nk (1..4) for the case's current dt, timo
+void stage_params(const CaseState& cs, int nk, StageParams& p) {
+  const int nkrk = 4;
+  double dtko = (cs.dt * std::min(std::max(nk - 2, 0), 1)) / (nkrk - nk + 3);
+  double dtk = (cs.dt * std::min(nk - 1, 1)) / (nkrk - nk + 2);
+  movef(cs, dtko, dtk, p.umf, p.dudtmf);
+  dtko = (cs.dt * std::min(nk - 1, 1)) / (nkrk - nk + 2);
+  dtk = cs.dt / (nkrk - nk + 1);
+  double dud[3];
+  movef(cs, dtko, dtk, p.umfb, dud);
+  p.dtk = dtk;
+  p.dt = cs.dt;
+}
+
+StageParams* dev_slot(canard_ctx* c, int slot) {  // slot 0..3 = stages, 4 = time step
+  return c->dsp + ((size_t)c->ring * 5 + slot) * c->cases.size();
+}
+StageParams* host_slot(canard_ctx* c, int slot) {
+  return c->hsp + ((size_t)c->ring * 5 + slot) * c->cases.size();
+}
+
+// writes the stage parameters of all cases for all 4 stages into the ring
+// slot and uploads them
+void upload_stage_params(canard_ctx* c) {
+  for (int nk = 1; nk <= 4; ++nk)
+    for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], nk, host_slot(c, nk - 1)[i]);
+  CK(cudaMemcpyAsync(dev_slot(c, 0), host_slot(c, 0), 4 * c->cases.size() * sizeof(StageParams),
+                     cudaMemcpyHostToDevice, c->st));
+}
+
+// ---- phases --------------------------------------------------------------------
+void ph_filter(canard_ctx* c) {
+  for (int m = 1; m <= 5; ++m)
+    for (int inn = 1; inn <= 3; ++inn) {
+      launch_mpigo(c, c->mp_filt[m - 1][inn - 1]);
+      launch_line(c, c->filt[m - 1][inn - 1], kNnf[inn - 1] - 1, 1);
+    }
+}
+
+void ph_copyqo(canard_ctx* c) {
+  Timed tm(c, T_COPY, 80.0 * valid_points(c));
+  k_copy5<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  CK(cudaGetLastError());
+}
+
+void ph_prim(canard_ctx* c) {
+  Timed tm(c, T_PRIM, 96.0 * valid_points(c));
+  k_prim<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, c->dcc);
+  CK(cudaGetLastError());
+}
+
+void ph_viscous(canard_ctx* c) {
+  bool any = false;
+  for (auto& cs : c->cases) any = any || cs.d.viscous;
+  if (!any) return;
+  {
+    Timed tm(c, T_COPY, 16.0 * valid_points(c));
+    k_copy_mu<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+    CK(cudaGetLastError());
+  }
+  launch_mpigo(c, c->mp_visc);
+  launch_line(c, c->visc[2], 2, 0);
+  launch_line(c, c->visc[1], 1, 0);
+  launch_line(c, c->visc[0], 0, 0);
+  Timed tm(c, T_VISCASM, 8.0 * (12 + 9 + 1 + 4 + 9 + 1) * valid_points(c));
+  k_viscous_assemble<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  CK(cudaGetLastError());
+}
+
+void ph_fluxes(canard_ctx* c, const StageParams* sp) {
+  {
+    Timed tm(c, T_FLUXCOMP, 8.0 * (5 + 1 + 3 + 9 + 9 + 15 + 1) * valid_points(c));
+    k_flux<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, sp, c->dcc);
+    CK(cudaGetLastError());
+  }
+  launch_mpigo(c, c->mp_flux);
+  launch_line(c, c->flux[0], 0, 0);
+  launch_line(c, c->flux[1], 1, 0);
+  launch_line(c, c->flux[2], 2, 0);
+  Timed tm(c, T_FLUXSUM, 8.0 * 20 * valid_points(c));
+  k_flux_sum<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  CK(cudaGetLastError());
+}
+
+void ph_gcbc(canard_ctx* c, const StageParams* sp) {
+  if (c->gc_setup.ntasks == 0) return;
+  const int thr = 128;
+  auto grid = [](int n) { return std::max(1, std::min((n + 127) / 128, 148 * 8)); };
+  Timed tm(c, T_GCBC, 0.0);
+  k_gcbc_setup<<<grid(c->gc_setup.total), thr, 0, c->st>>>(c->dbd, c->gc_setup.tasks, c->gc_setup.first,
+                                                           c->gc_setup.ntasks, c->gc_setup.total, sp);
+  CK(cudaGetLastError());
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s) c->launches += c->gc_upd[d][s].ntasks > 0 ? 1 : 0;
+  if (c->fc_n > 0) {
+    c->launches += 1;
+    k_face_copy<<<dim3(std::max(1, std::min((c->fc_max + 255) / 256, 1024)), c->fc_n), 256, 0, c->st>>>(
+        c->fc_src, c->fc_dst, c->fc_cnt, c->fc_n);
+    CK(cudaGetLastError());
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s) {
+      const auto& T = c->gc_upd[d][s];
+      if (T.ntasks == 0) continue;
+      k_gcbc_update<<<grid(T.total), thr, 0, c->st>>>(c->dbd, T.tasks, T.first, T.ntasks, T.total, sp);
+      CK(cudaGetLastError());
+    }
+}
+
+void ph_sponge(canard_ctx* c) {
+  if (c->sponge.ntasks == 0 || c->sponge.total == 0) return;
+  const int grid = std::max(1, std::min((c->sponge.total + 255) / 256, 148 * 8));
+  Timed tm(c, T_SPONGE, 8.0 * 22 * c->sponge.total);
+  k_sponge<<<grid, 256, 0, c->st>>>(c->dbd, c->sponge.tasks, c->sponge.first, c->sponge.ntasks, c->sponge.total);
+  CK(cudaGetLastError());
+}
+
+void ph_rk(canard_ctx* c, const StageParams* sp) {
+  Timed tm(c, T_RK, 8.0 * 16 * valid_points(c));
+  k_rk<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, sp);
+  CK(cudaGetLastError());
+}
+
+void run_avg(canard_ctx* c, const AvgDev& A, int mode) {
+  if (A.ntg == 0) return;
+  Timed tm(c, T_AVERAGE, 8.0 * 5 * (A.nsrc + A.ntg));
+  c->launches += 1;  // snapshot + combine
+  k_avg_snapshot<<<std::max(1, std::min((A.nsrc + 255) / 256, 1184)), 256, 0, c->st>>>(c->dbd, A.sb, A.sl,
+                                                                                       A.nsrc, A.snap);
+  CK(cudaGetLastError());
+  k_avg_combine<<<std::max(1, std::min((A.ntg + 255) / 256, 1184)), 256, 0, c->st>>>(
+      c->dbd, A.tb, A.tl, A.tfirst, A.tcount, A.ntg, A.snap, mode);
+  CK(cudaGetLastError());
+}
+
+void ph_average(canard_ctx* c) {
+  run_avg(c, c->avg_pt, 0);
+  run_avg(c, c->avg_ln, 0);
+  run_avg(c, c->avg_sf, 1);
+}
+
+// time step reduction (src/mo_physics.f90:171-211) + dt ramp
+// (src/mo_canard_driver.f90:278-294) for the cases that need it this step.
+void timestep(canard_ctx* c) {
+  bool need = false;
+  for (auto& cs : c->cases) need = need || (cs.n % 10 == 1);
+  if (need) {
+    // stage-1 moving-frame velocity (dtko = dtk = 0 at nk = 1)
+    StageParams* hp = host_slot(c, 4);
+    for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], 1, hp[i]);
+    CK(cudaMemcpyAsync(dev_slot(c, 4), hp, c->cases.size() * sizeof(StageParams), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->ddt, 0, 2 * c->cases.size() * sizeof(unsigned long long), c->st));
+    Timed tm(c, T_TIMESTEP, 8.0 * 17 * valid_points(c));
+    k_dtmax<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->hdt, c->ddt, 2 * c->cases.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  for (size_t i = 0; i < c->cases.size(); ++i) {
+    CaseState& cs = c->cases[i];
+    if (cs.n % 10 == 1) {
+      cs.ndt = cs.n;
+      cs.dts = cs.dte;
+      double r1, r2;
+      std::memcpy(&r1, &c->hdt[2 * i], 8);
+      std::memcpy(&r2, &c->hdt[2 * i + 1], 8);
+      const double ra0 = cs.d.cfl / r1;
+      double ra1 = ra0;
+      if (cs.d.viscous) ra1 = 0.5 / r2;
+      cs.dte = std::min(ra0, ra1);
+    }
+    const double pi = std::acos(-1.0);
+    const double sn = std::sin((0.05 * pi) * (cs.n - cs.ndt));
+    cs.dt = cs.dts + (cs.dte - cs.dts) * (sn * sn);
+  }
+}
+
+void wait_ring(canard_ctx* c) {
+  c->ring ^= 1;
+  CK(cudaEventSynchronize(c->ring_ev[c->ring]));
+}
+
+void one_step(canard_ctx* c) {
+  for (auto& cs : c->cases)
+    if (cs.dt == 0.0 && cs.n > 2) throw ApiError(CANARD_ERR_NAN, "Canard: Overflow. (dt == 0 after step 2)");
+  wait_ring(c);
+  ph_filter(c);
+  ph_copyqo(c);
+  ph_prim(c);
+  timestep(c);
+  upload_stage_params(c);
+  for (int nk = 1; nk <= 4; ++nk) {
+    const StageParams* sp = dev_slot(c, nk - 1);
+    if (nk > 1) ph_prim(c);
+    ph_viscous(c);
+    ph_fluxes(c, sp);
+    ph_gcbc(c, sp);
+    ph_sponge(c);
+    ph_rk(c, sp);
+    ph_average(c);
+  }
+  CK(cudaEventRecord(c->ring_ev[c->ring], c->st));
+  for (auto& cs : c->cases) {
+    cs.n = cs.n + 1;
+    cs.timo = cs.timo + cs.dt;
+  }
+}
+
+// ---- set-up ------------------------------------------------------------------------
+void build_tables(canard_ctx* c) {
+  const int nb = nblk(c);
+  // filter passes
+  for (int m = 1; m <= 5; ++m)
+    for (int inn = 1; inn <= 3; ++inn) {
+      const int dir = kNnf[inn - 1] - 1;
+      std::vector<LineTask> v;
+      for (int b = 0; b < nb; ++b) {
+        LineTask t;
+        double* f = fptr(c->blocks[b], F_QA + m - 1);
+        fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t);
+        v.push_back(t);
+      }
+      c->filt[m - 1][inn - 1] = make_line_table(c, v, dir, false);
+      c->mp_filt[m - 1][inn - 1] = make_face_table(
+          c, face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }), false);
+    }
+  // viscous gradients: de(:,m) m = 2..5 -> scr 3*(m-2) + dir
+  for (int dir = 0; dir < 3; ++dir) {
+    std::vector<LineTask> v;
+    for (int b = 0; b < nb; ++b) {
+      if (!c->cases[c->blocks[b].g.case_id].d.viscous) continue;
+      for (int m = 2; m <= 5; ++m) {
+        LineTask t;
+        fill_line_task(c, c->blocks[b], dir, 0, fptr(c->blocks[b], F_DE + m - 1),
+                       fptr(c->blocks[b], F_SCR + 3 * (m - 2) + dir), m, false, t);
+        v.push_back(t);
+      }
+    }
+    c->visc[dir] = make_line_table(c, v, dir, false);
+  }
+  {
+    std::vector<FaceTask> all;
+    for (int m = 2; m <= 5; ++m) {
+      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int) { return fptr(c->blocks[b], F_DE + m - 1); });
+      all.insert(all.end(), v.begin(), v.end());
+    }
+    c->mp_visc = make_face_table(c, all, false);
+  }
+  // fluxes: scr 3*(m-1) + dir, in place
+  for (int dir = 0; dir < 3; ++dir) {
+    std::vector<LineTask> v;
+    for (int b = 0; b < nb; ++b)
+      for (int m = 1; m <= 5; ++m) {
+        LineTask t;
+        double* f = fptr(c->blocks[b], F_SCR + 3 * (m - 1) + dir);
+        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t);
+        v.push_back(t);
+      }
+    c->flux[dir] = make_line_table(c, v, dir, false);
+  }
+  {
+    std::vector<FaceTask> all;
+    for (int m = 1; m <= 5; ++m) {
+      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int d) { return fptr(c->blocks[b], F_SCR + 3 * (m - 1) + d); });
+      all.insert(all.end(), v.begin(), v.end());
+    }
+    c->mp_flux = make_face_table(c, all, false);
+  }
+}
+
+void build_gcbc_sponge_avg(canard_ctx* c) {
+  const int nb = nblk(c);
+  // GCBC tables need yaco (reference layout) on the host
+  std::vector<GcbcTask> setup_tasks;
+  std::vector<GcbcTask> upd[3][2];
+  std::vector<const double*> fsrc;
+  std::vector<double*> fdst;
+  std::vector<int> fcnt;
+  std::vector<SpongeTask> sp_tasks;
+  for (int b = 0; b < nb; ++b) {
+    BlockState& B = c->blocks[b];
+    const BlockGeom& g = B.g;
+    const CaseState& cs = c->cases[g.case_id];
+    const size_t Lr = (size_t)g.X * g.Y * g.Z;
+    std::vector<double> ypad((size_t)g.npad), yref(Lr);
+    CK(cudaMemcpyAsync(ypad.data(), fptr(B, F_YACO), g.npad * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int z = 0; z < g.Z; ++z)
+      for (int y = 0; y < g.Y; ++y)
+        for (int x = 0; x < g.X; ++x) yref[g.ref_index(x, y, z)] = ypad[g.dev(x, y, z)];
+    std::vector<int64_t> pts;
+    std::vector<double> w;
+    gcbc_tables(g, yref.data(), B.gc_faces, pts, w);
+    if (!pts.empty()) {
+      std::vector<long long> p2(pts.begin(), pts.end());
+      B.gc_pts = dupload(p2, c->st);
+      B.gc_w = dupload(w, c->st);
+    }
+    for (const GcbcFace& f : B.gc_faces) {
+      const int d = f.nn - 1;
+      GcbcTask t{};
+      t.b = b; t.nn = f.nn; t.side = f.side; t.bc = f.bc;
+      t.cm = B.cm[d] + (size_t)3 * f.side * g.nbs[d];
+      t.drva = B.drva[d] + (size_t)5 * f.side * g.nbs[d];
+      t.drvb = (f.bc == BC_CURV) ? B.drvb[d] + (size_t)5 * f.side * g.nbs[d] : nullptr;
+      t.pts = B.gc_pts + f.first;
+      t.w = B.gc_w + f.first;
+      t.nbs = g.nbs[d];
+      t.nj = g.ijk[1][d] + 1;
+      t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp; t.N = g.ijk[0][d];
+      setup_tasks.push_back(t);
+      upd[d][f.side].push_back(t);
+    }
+    // sponge
+    if (cs.d.szco != 0.0) {
+      std::vector<int64_t> sp;
+      std::vector<double> a, bb;
+      sponge_list(g, cs.d, B.xyz_host.data(), yref.data(), sp, a, bb);
+      if (!sp.empty()) {
+        std::vector<long long> s2(sp.begin(), sp.end());
+        B.sp_pts = dupload(s2, c->st);
+        B.sp_a = dupload(a, c->st);
+        B.sp_b = dupload(bb, c->st);
+        B.sp_n = (int)sp.size();
+        SpongeTask st{b, B.sp_pts, B.sp_a, B.sp_b, B.sp_n, 0};
+        sp_tasks.push_back(st);
+      }
+    }
+  }
+  for (const FaceLink& L : c->links) {  // gcbc_comm: BC_INTER_CURV faces only
+    const BlockState& R = c->blocks[L.dst_b];
+    const BlockState& S = c->blocks[L.src_b];
+    const int d = L.nn;
+    if (R.g.nbc[d][L.dst_side] != BC_CURV) continue;
+    fsrc.push_back(S.drva[d] + (size_t)5 * L.src_side * S.g.nbs[d]);
+    fdst.push_back(R.drvb[d] + (size_t)5 * L.dst_side * R.g.nbs[d]);
+    fcnt.push_back(5 * R.g.nbs[d]);
+  }
+  c->gc_setup = make_lines_table(c, setup_tasks, false, &GcbcTask::nbs, &GcbcTask::line0);
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s)
+      c->gc_upd[d][s] = make_lines_table(c, upd[d][s], false, &GcbcTask::nbs, &GcbcTask::line0);
+  c->fc_n = (int)fsrc.size();
+  if (c->fc_n) {
+    std::vector<double*> s2;
+    for (auto p : fsrc) s2.push_back(const_cast<double*>(p));
+    c->fc_src = dupload(s2, c->st);
+    c->fc_dst = dupload(fdst, c->st);
+    c->fc_cnt = dupload(fcnt, c->st);
+    c->fc_max = *std::max_element(fcnt.begin(), fcnt.end());
+  }
+  c->sponge = make_lines_table(c, sp_tasks, false, &SpongeTask::count, &SpongeTask::first);
+  // junction averaging plans (per case: blocks of one case only see each other)
+  AvgPlan P, Lp, Sf;
+  for (const CaseState& cs : c->cases) {
+    std::vector<BlockGeom> gs;
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) gs.push_back(c->blocks[b].g);
+    std::vector<FaceLink> lk;
+    std::string e = face_links(gs, lk);
+    if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
+    AvgPlan p1, l1, s1;
+    e = junction_plans(gs, p1, l1);
+    if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
+    e = surface_plan(gs, lk, s1);
+    if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
+    auto append = [&](AvgPlan& dst, const AvgPlan& src) {
+      const int off = (int)dst.src_b.size();
+      for (AvgTarget t : src.targets) { t.b += cs.b0; t.first += off; dst.targets.push_back(t); }
+      for (int b : src.src_b) dst.src_b.push_back(b + cs.b0);
+      dst.src_l.insert(dst.src_l.end(), src.src_l.begin(), src.src_l.end());
+    };
+    append(P, p1); append(Lp, l1); append(Sf, s1);
+  }
+  auto upload_avg = [&](const AvgPlan& p, AvgDev& A) {
+    A.ntg = (int)p.targets.size();
+    A.nsrc = (int)p.src_b.size();
+    if (A.ntg == 0) return;
+    std::vector<int> tb, tf, tc;
+    std::vector<long long> tl, sl(p.src_l.begin(), p.src_l.end());
+    for (const auto& t : p.targets) { tb.push_back(t.b); tl.push_back(t.l); tf.push_back(t.first); tc.push_back(t.count); }
+    A.tb = dupload(tb, c->st); A.tl = dupload(tl, c->st); A.tfirst = dupload(tf, c->st); A.tcount = dupload(tc, c->st);
+    A.sb = dupload(p.src_b, c->st); A.sl = dupload(sl, c->st);
+    A.snap = dalloc<double>((size_t)A.nsrc * 5);
+  };
+  upload_avg(P, c->avg_pt);
+  upload_avg(Lp, c->avg_ln);
+  upload_avg(Sf, c->avg_sf);
+}
+
+// t_grid%grid_metrics on the device (src/mo_grid.f90:52-189)
+void grid_metrics(canard_ctx* c) {
+  const int nb = nblk(c);
+  // coordinate derivatives: scr 3*(m-1) + dir
+  for (int m = 1; m <= 3; ++m) {
+    auto ft = face_tasks(c, 0, 1, m, -1, [&](int b, int) { return fptr(c->blocks[b], F_XYZ + m - 1); });
+    launch_mpigo(c, make_face_table(c, ft, true));
+    for (int dir = 2; dir >= 0; --dir) {
+      std::vector<LineTask> v;
+      for (int b = 0; b < nb; ++b) {
+        LineTask t;
+        fill_line_task(c, c->blocks[b], dir, 0, fptr(c->blocks[b], F_XYZ + m - 1),
+                       fptr(c->blocks[b], F_SCR + 3 * (m - 1) + dir), m, true, t);
+        v.push_back(t);
+      }
+      launch_line(c, make_line_table(c, v, dir, true), dir, 0);
+    }
+  }
+  k_cofactors<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  CK(cudaGetLastError());
+  const int mets[3] = {F_XIM, F_ETM, F_ZEM};
+  for (int m = 1; m <= 3; ++m)
+    for (int w = 0; w < 3; ++w)
+      for (int inn = 1; inn <= 3; ++inn) {
+        const int dir = kNnf[inn - 1] - 1;
+        auto col = [&](int b, int) { return fptr(c->blocks[b], mets[w] + m - 1); };
+        launch_mpigo(c, make_face_table(c, face_tasks(c, 1, 0, m, dir, col), true));
+        std::vector<LineTask> v;
+        for (int b = 0; b < nb; ++b) {
+          LineTask t;
+          double* f = fptr(c->blocks[b], mets[w] + m - 1);
+          fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t);
+          v.push_back(t);
+        }
+        launch_line(c, make_line_table(c, v, dir, true), dir, 1);
+      }
+  k_jacobian<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  CK(cudaGetLastError());
+  // face normals of all six faces
+  std::vector<CmTask> cmt;
+  std::vector<int> first;
+  int tot = 0;
+  for (int b = 0; b < nb; ++b)
+    for (int d = 0; d < 3; ++d)
+      for (int s = 0; s < 2; ++s) {
+        const BlockState& B = c->blocks[b];
+        CmTask t{b, d + 1, s, B.g.nbs[d], B.g.ijk[1][d] + 1, B.g.ijk[0][d], tot,
+                 B.cm[d] + (size_t)3 * s * B.g.nbs[d]};
+        first.push_back(tot);
+        tot += t.nbs;
+        cmt.push_back(t);
+      }
+  CmTask* dt = dupload(cmt, c->st);
+  int* df = dupload(first, c->st);
+  c->transient.push_back(dt);
+  c->transient.push_back(df);
+  k_face_normals<<<std::max(1, std::min((tot + 127) / 128, 1184)), 128, 0, c->st>>>(c->dbd, dt, df,
+                                                                                     (int)cmt.size(), tot);
+  CK(cudaGetLastError());
+  sync_check(c);
+  free_transient(c);
+}
+
+// copy between a host array in the reference layout (ncols x X*Y*Z) and a
+// padded device field
+void h2d_field(canard_ctx* c, const BlockState& B, double* dst, const double* src, int ncols) {
+  const BlockGeom& g = B.g;
+  CK(cudaMemcpy2DAsync(dst, g.Xp * sizeof(double), src, g.X * sizeof(double), g.X * sizeof(double),
+                       (size_t)g.Y * g.Z * ncols, cudaMemcpyHostToDevice, c->st));
+}
+void d2h_field(canard_ctx* c, const BlockState& B, double* dst, const double* src, int ncols) {
+  const BlockGeom& g = B.g;
+  CK(cudaMemcpy2DAsync(dst, g.X * sizeof(double), src, g.Xp * sizeof(double), g.X * sizeof(double),
+                       (size_t)g.Y * g.Z * ncols, cudaMemcpyDeviceToHost, c->st));
+}
+
+int block_index(const canard_ctx* c, int icase, int iblock) {
+  if (icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "case index out of range");
+  const CaseState& cs = c->cases[icase];
+  if (iblock < 0 || iblock >= cs.nb) throw ApiError(CANARD_ERR_ARG, "block index out of range");
+  return cs.b0 + iblock;
+}
+
+template <class F>
+int guarded(canard_ctx* c, F&& f) {
+  if (!c) return CANARD_ERR_ARG;
+  try {
+    f();
+    return CANARD_OK;
+  } catch (const ApiError& e) {
+    set_err(c, e.what());
+    return e.code;
+  } catch (const CudaError& e) {
+    set_err(c, e.what());
+    return CANARD_ERR_CUDA;
+  } catch (const std::exception& e) {
+    set_err(c, e.what());
+    return CANARD_ERR_ARG;
+  }
+}
+
+void destroy(canard_ctx* c) {
+  for (auto& b : c->blocks) {
+    cudaFree(b.arena);
+    for (int nt = 0; nt < 2; ++nt)
+      for (int d = 0; d < 3; ++d) { cudaFree(b.lu[nt][d]); cudaFree(b.recv[nt][d]); }
+    for (int d = 0; d < 3; ++d) { cudaFree(b.chain[d]); cudaFree(b.drva[d]); cudaFree(b.drvb[d]); cudaFree(b.cm[d]); }
+    cudaFree(b.gc_pts); cudaFree(b.gc_w); cudaFree(b.sp_pts); cudaFree(b.sp_a); cudaFree(b.sp_b);
+  }
+  for (auto& cs : c->cases) cudaFree(cs.dsch);
+  cudaFree(c->dbd); cudaFree(c->dcc); cudaFree(c->dsp); cudaFree(c->ddt); cudaFree(c->derr);
+  if (c->hsp) cudaFreeHost(c->hsp);
+  if (c->hdt) cudaFreeHost(c->hdt);
+  for (auto e : c->ring_ev) if (e) cudaEventDestroy(e);
+  for (auto& p : c->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  auto ft = [](auto& T) { cudaFree(T.tasks); cudaFree(T.first); };
+  for (int m = 0; m < 5; ++m) for (int i = 0; i < 3; ++i) { ft(c->filt[m][i]); ft(c->mp_filt[m][i]); }
+  for (int d = 0; d < 3; ++d) { ft(c->visc[d]); ft(c->flux[d]); }
+  ft(c->mp_visc); ft(c->mp_flux); ft(c->gc_setup); ft(c->sponge);
+  for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) ft(c->gc_upd[d][s]);
+  cudaFree(c->fc_src); cudaFree(c->fc_dst); cudaFree(c->fc_cnt);
+  for (AvgDev* A : {&c->avg_pt, &c->avg_ln, &c->avg_sf}) {
+    cudaFree(A->tb); cudaFree(A->tl); cudaFree(A->tfirst); cudaFree(A->tcount); cudaFree(A->sb); cudaFree(A->sl);
+    cudaFree(A->snap);
+  }
+  free_transient(c);
+  if (c->own) cudaStreamDestroy(c->own);
+}
+
+void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const canard_block_desc* blocks) {
+  if (!cases || !blocks || ncases <= 0) throw ApiError(CANARD_ERR_ARG, "null or empty case list");
+  CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  c->st = c->own;
+  int b0 = 0;
+  for (int i = 0; i < ncases; ++i) {
+    CaseState cs;
+    cs.d = cases[i];
+    if (cs.d.nblocks <= 0) throw ApiError(CANARD_ERR_ARG, "case without blocks");
+    if (!(cs.d.fltrbc > 0.0)) throw ApiError(CANARD_ERR_ARG, "fltrbc must be positive");
+    cs.sch.build(cs.d.fltk, cs.d.fltrbc);
+    // src/mo_physics.f90:101-111
+    const double am = std::sqrt((cs.d.amach1 * cs.d.amach1 + cs.d.amach2 * cs.d.amach2) + cs.d.amach3 * cs.d.amach3);
+    cs.reoo = cs.d.reoo;
+    if (am > 1.0e-8) cs.reoo = cs.reoo / am;
+    cs.srefoo = 111 / cs.d.tempoo;
+    cs.srefp1dre = (cs.srefoo + 1.0) / cs.reoo;
+    cs.uoo[0] = cs.d.amach1; cs.uoo[1] = cs.d.amach2; cs.uoo[2] = cs.d.amach3;
+    cs.b0 = b0;
+    cs.nb = cs.d.nblocks;
+    for (int k = 0; k < cs.nb; ++k) {
+      BlockState B;
+      const canard_block_desc& bd = blocks[b0 + k];
+      if (bd.lxi < 12 || bd.let < 12 || bd.lze < 12)
+        throw ApiError(CANARD_ERR_ARG, "every direction needs at least 13 points (interface closures read 13)");
+      for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < 2; ++s) {
+          const int np = bd.nbc[d][s];
+          if (np == BC_WALLI || np == BC_WALLV)
+            throw ApiError(CANARD_ERR_UNSUPPORTED, "wall boundaries (20/25) are not on this path yet");
+          if (np == BC_SUBDOM)
+            throw ApiError(CANARD_ERR_UNSUPPORTED, "BC 40 needs nbpc > 1; every block here is one sub-domain");
+          if (!(np == BC_NR || np == BC_CURV || np == BC_STRAIGHT || np == BC_PERIODIC))
+            throw ApiError(CANARD_ERR_ARG, "unknown boundary code " + std::to_string(np));
+          if (np != BC_NR && (bd.mbcd[d][s] < 0 || bd.mbcd[d][s] >= cs.nb))
+            throw ApiError(CANARD_ERR_ARG, "interface face without a neighbour block in the case");
+        }
+      make_geom(bd, i, k, B.g);
+      // remap neighbours to global indices for the links
+      c->blocks.push_back(B);
+    }
+    b0 += cs.nb;
+    c->cases.push_back(cs);
+  }
+  // face links per case
+  for (const CaseState& cs : c->cases) {
+    std::vector<BlockGeom> gs;
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) gs.push_back(c->blocks[b].g);
+    std::vector<FaceLink> lk;
+    std::string e = face_links(gs, lk);
+    if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
+    for (FaceLink L : lk) { L.dst_b += cs.b0; L.src_b += cs.b0; c->links.push_back(L); }
+  }
+  // device memory
+  std::vector<BlockDev> bdv;
+  for (auto& B : c->blocks) {
+    const BlockGeom& g = B.g;
+    B.arena = dalloc<double>((size_t)F_COUNT * g.npad);
+    BlockDev& d = B.dev;
+    d.X = g.X; d.Y = g.Y; d.Z = g.Z; d.Xp = g.Xp; d.npad = g.npad; d.case_id = g.case_id;
+    d.qa = fptr(B, F_QA); d.qo = fptr(B, F_QO); d.de = fptr(B, F_DE); d.p = fptr(B, F_P); d.mu = fptr(B, F_MU);
+    d.xim = fptr(B, F_XIM); d.etm = fptr(B, F_ETM); d.zem = fptr(B, F_ZEM); d.yaco = fptr(B, F_YACO);
+    d.tau = fptr(B, F_TAU); d.scr = fptr(B, F_SCR); d.xyz = fptr(B, F_XYZ);
+    const Scheme& sch = c->cases[g.case_id].sch;
+    for (int dir = 0; dir < 3; ++dir) {
+      const int L = g.ijk[0][dir] + 1, nbs = g.nbs[dir];
+      const int n0 = bc_interface(g.nbc[dir][0]) ? 1 : 0, n1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
+      for (int nt = 0; nt < 2; ++nt) {
+        std::vector<double> lu((size_t)5 * L);
+        sch.lu(L, n0, n1, nt, lu.data());
+        B.lu[nt][dir] = dupload(lu, c->st);
+        B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs);
+      }
+      B.chain[dir] = dalloc<double>((size_t)2 * nbs);
+      B.drva[dir] = dalloc<double>((size_t)10 * nbs);
+      B.drvb[dir] = dalloc<double>((size_t)10 * nbs);
+      B.cm[dir] = dalloc<double>((size_t)6 * nbs);
+    }
+    bdv.push_back(d);
+  }
+  c->dbd = dupload(bdv, c->st);
+  std::vector<CaseConst> ccv;
+  for (auto& cs : c->cases) {
+    CaseConst k{cs.srefoo, cs.srefp1dre, cs.d.viscous};
+    ccv.push_back(k);
+    DevScheme ds{};
+    std::memcpy(ds.pbci, cs.sch.pbci, sizeof(ds.pbci));
+    std::memcpy(ds.pbco, cs.sch.pbco, sizeof(ds.pbco));
+    std::memcpy(ds.pbcot, cs.sch.pbcot, sizeof(ds.pbcot));
+    ds.fa = cs.sch.fa; ds.fb = cs.sch.fb; ds.fc = cs.sch.fc;
+    std::memcpy(ds.fbc, cs.sch.fbc, sizeof(ds.fbc));
+    cs.dsch = dupload(std::vector<DevScheme>{ds}, c->st);
+  }
+  c->dcc = dupload(ccv, c->st);
+  const size_t nslots = 2 * 5 * c->cases.size();
+  c->dsp = dalloc<StageParams>(nslots);
+  CK(cudaMallocHost(&c->hsp, nslots * sizeof(StageParams)));
+  std::memset(c->hsp, 0, nslots * sizeof(StageParams));
+  c->ddt = dalloc<unsigned long long>(2 * c->cases.size());
+  CK(cudaMallocHost(&c->hdt, 2 * c->cases.size() * sizeof(unsigned long long)));
+  c->derr = dalloc<int>(1);
+  for (auto& e : c->ring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : c->ring_ev) CK(cudaEventRecord(e, c->st));
+  set_line_smem_limits();
+  build_tables(c);
+  CK(cudaStreamSynchronize(c->st));
+}
+
+}  // namespace
+
+// ==================================================================================
+extern "C" {
+
+int canard_version(void) { return 1; }
+
+int canard_coeffs(double fltk, double fltrbc, double* out150) {
+  if (!out150 || !(fltrbc > 0.0)) return CANARD_ERR_ARG;
+  Scheme s;
+  s.build(fltk, fltrbc);
+  s.pack150(out150);
+  return CANARD_OK;
+}
+
+int canard_penta(double fltk, double fltrbc, int32_t n, int32_t ns, int32_t ne, int32_t nt, double* xu,
+                 double* xl) {
+  if (!xu || !xl || n < 8 || ns < 0 || ns > 1 || ne < 0 || ne > 1 || nt < 0 || nt > 1) return CANARD_ERR_ARG;
+  Scheme s;
+  s.build(fltk, fltrbc);
+  std::vector<double> o((size_t)5 * n);
+  s.lu(n, ns, ne, nt, o.data());
+  // xu (n,3) = u1,u2,u3 ; xl (n,2) = l1,l2 (column-major)
+  for (int i = 0; i < n; ++i) {
+    xl[i] = o[i]; xl[n + i] = o[n + i];
+    xu[i] = o[2 * n + i]; xu[n + i] = o[3 * n + i]; xu[2 * n + i] = o[4 * n + i];
+  }
+  return CANARD_OK;
+}
+
+int canard_ctx_create(const canard_case_desc* cases, int32_t ncases, const canard_block_desc* blocks,
+                      int32_t precision, canard_ctx** out) {
+  if (!out) return CANARD_ERR_ARG;
+  *out = nullptr;
+  if (precision != CANARD_FP64) return CANARD_ERR_UNSUPPORTED;
+  canard_ctx* c = new canard_ctx();
+  c->precision = precision;
+  int rc = guarded(c, [&] { create(c, cases, ncases, blocks); });
+  if (rc != CANARD_OK) {
+    std::fprintf(stderr, "canard_ctx_create: %s\n", c->err.c_str());
+    destroy(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return CANARD_OK;
+}
+
+void canard_ctx_destroy(canard_ctx* c) {
+  if (!c) return;
+  cudaStreamSynchronize(c->st);
+  destroy(c);
+  delete c;
+}
+
+const char* canard_last_error(const canard_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int canard_set_stream(canard_ctx* c, void* stream) {
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    c->st = stream ? static_cast<cudaStream_t>(stream) : c->own;
+  });
+}
+
+int canard_upload_grid(canard_ctx* c, int32_t icase, int32_t iblock, const double* xyz) {
+  return guarded(c, [&] {
+    if (!xyz) throw ApiError(CANARD_ERR_ARG, "null grid");
+    BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    const size_t L = (size_t)B.g.X * B.g.Y * B.g.Z;
+    B.xyz_host.assign(xyz, xyz + 3 * L);
+    h2d_field(c, B, fptr(B, F_XYZ), xyz, 3);
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_setup(canard_ctx* c) {
+  return guarded(c, [&] {
+    for (auto& B : c->blocks)
+      if (B.xyz_host.empty()) throw ApiError(CANARD_ERR_STATE, "canard_setup before every grid is uploaded");
+    grid_metrics(c);
+    build_gcbc_sponge_avg(c);
+    CK(cudaStreamSynchronize(c->st));
+    c->setup_done = true;
+  });
+}
+
+int canard_set_state(canard_ctx* c, int32_t icase, int32_t iblock, const double* qa) {
+  return guarded(c, [&] {
+    if (!qa) throw ApiError(CANARD_ERR_ARG, "null state");
+    BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    h2d_field(c, B, fptr(B, F_QA), qa, 5);
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_get_state(canard_ctx* c, int32_t icase, int32_t iblock, double* qa) {
+  return guarded(c, [&] {
+    if (!qa) throw ApiError(CANARD_ERR_ARG, "null state");
+    BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    d2h_field(c, B, qa, fptr(B, F_QA), 5);
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+static void field_info(const BlockState& B, int field, const double*& dptr, int& ncols, bool& face,
+                       size_t& count) {
+  face = false;
+  switch (field) {
+    case CANARD_F_QA: dptr = fptr(B, F_QA); ncols = 5; break;
+    case CANARD_F_QO: dptr = fptr(B, F_QO); ncols = 5; break;
+    case CANARD_F_DE: dptr = fptr(B, F_DE); ncols = 5; break;
+    case CANARD_F_P: dptr = fptr(B, F_P); ncols = 1; break;
+    case CANARD_F_SS1: dptr = fptr(B, F_MU); ncols = 1; break;
+    case CANARD_F_XIM: dptr = fptr(B, F_XIM); ncols = 3; break;
+    case CANARD_F_ETM: dptr = fptr(B, F_ETM); ncols = 3; break;
+    case CANARD_F_ZEM: dptr = fptr(B, F_ZEM); ncols = 3; break;
+    case CANARD_F_YACO: dptr = fptr(B, F_YACO); ncols = 1; break;
+    case CANARD_F_TAU: dptr = fptr(B, F_TAU); ncols = 9; break;
+    case CANARD_F_DRVA1: case CANARD_F_DRVA2: case CANARD_F_DRVA3: {
+      const int d = field - CANARD_F_DRVA1;
+      dptr = B.drva[d]; face = true; count = (size_t)10 * B.g.nbs[d]; ncols = 0;
+      return;
+    }
+    case CANARD_F_CM1: case CANARD_F_CM2: case CANARD_F_CM3: {
+      const int d = field - CANARD_F_CM1;
+      dptr = B.cm[d]; face = true; count = (size_t)6 * B.g.nbs[d]; ncols = 0;
+      return;
+    }
+    default: throw ApiError(CANARD_ERR_ARG, "unknown field id");
+  }
+  count = (size_t)ncols * B.g.X * B.g.Y * B.g.Z;
+}
+
+int canard_get_field(canard_ctx* c, int32_t icase, int32_t iblock, int32_t field, double* out, int64_t count) {
+  return guarded(c, [&] {
+    BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    const double* dp; int nc; bool face; size_t n;
+    field_info(B, field, dp, nc, face, n);
+    if (!out || count != (int64_t)n) throw ApiError(CANARD_ERR_ARG, "count does not match the field size");
+    if (face) CK(cudaMemcpyAsync(out, dp, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    else d2h_field(c, B, out, dp, nc);
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_set_field(canard_ctx* c, int32_t icase, int32_t iblock, int32_t field, const double* in, int64_t count) {
+  return guarded(c, [&] {
+    BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    const double* dp; int nc; bool face; size_t n;
+    field_info(B, field, dp, nc, face, n);
+    if (!in || count != (int64_t)n) throw ApiError(CANARD_ERR_ARG, "count does not match the field size");
+    if (face) CK(cudaMemcpyAsync(const_cast<double*>(dp), in, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    else h2d_field(c, B, const_cast<double*>(dp), in, nc);
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_step(canard_ctx* c, int32_t nsteps) {
+  return guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_step before canard_setup");
+    if (nsteps < 0) throw ApiError(CANARD_ERR_ARG, "negative step count");
+    for (int i = 0; i < nsteps; ++i) one_step(c);
+    sync_check(c);
+  });
+}
+
+int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
+  return guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_phase before canard_setup");
+    if ((phase == CANARD_PH_MOVEF_A || phase == CANARD_PH_TIMESTEP || phase == CANARD_PH_VISCOUS ||
+         phase == CANARD_PH_FLUXES || phase == CANARD_PH_GCBC || phase == CANARD_PH_RKUPDATE) &&
+        (nk < 1 || nk > 4))
+      throw ApiError(CANARD_ERR_ARG, "stage index nk must be 1..4");
+    // parameters of stage nk for the current dt / timo
+    auto params = [&]() {
+      StageParams* hp = host_slot(c, 4);
+      for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], nk, hp[i]);
+      CK(cudaMemcpyAsync(dev_slot(c, 4), hp, c->cases.size() * sizeof(StageParams), cudaMemcpyHostToDevice,
+                         c->st));
+      return dev_slot(c, 4);
+    };
+    switch (phase) {
+      case CANARD_PH_FILTER: ph_filter(c); break;
+      case CANARD_PH_COPYQO: ph_copyqo(c); break;
+      case CANARD_PH_PRIM: ph_prim(c); break;
+      case CANARD_PH_MOVEF_A: break;
+      case CANARD_PH_TIMESTEP: if (nk == 1) timestep(c); break;
+      case CANARD_PH_VISCOUS: ph_viscous(c); break;
+      case CANARD_PH_FLUXES: ph_fluxes(c, params()); break;
+      case CANARD_PH_GCBC: ph_gcbc(c, params()); break;
+      case CANARD_PH_SPONGE: ph_sponge(c); break;
+      case CANARD_PH_RKUPDATE: ph_rk(c, params()); break;
+      case CANARD_PH_WALL: break;
+      case CANARD_PH_AVERAGE: ph_average(c); break;
+      case CANARD_PH_ADVANCE:
+        for (auto& cs : c->cases) { cs.n = cs.n + 1; cs.timo = cs.timo + cs.dt; }
+        break;
+      default: throw ApiError(CANARD_ERR_ARG, "unknown phase");
+    }
+    sync_check(c);
+  });
+}
+
+int canard_get_time(canard_ctx* c, int32_t icase, double* t) {
+  return guarded(c, [&] {
+    if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
+    const CaseState& cs = c->cases[icase];
+    t[0] = cs.n; t[1] = cs.ndt; t[2] = cs.dt; t[3] = cs.dts; t[4] = cs.dte; t[5] = cs.timo;
+  });
+}
+
+int canard_set_time(canard_ctx* c, int32_t icase, const double* t) {
+  return guarded(c, [&] {
+    if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
+    CaseState& cs = c->cases[icase];
+    cs.n = (int)t[0]; cs.ndt = (int)t[1]; cs.dt = t[2]; cs.dts = t[3]; cs.dte = t[4]; cs.timo = t[5];
+  });
+}
+
+// ---- unit operations (case 0) ------------------------------------------------------
+int canard_mpigo(canard_ctx* c, const double* const* fields, int32_t ncols, int32_t nt, int32_t nrt, int32_t n45,
+                 int32_t itag, int32_t m) {
+  (void)itag;
+  return guarded(c, [&] {
+    if (!fields || ncols < 1 || ncols > 3 || nt < 0 || nt > 1 || nrt < 0 || nrt > 1 || n45 < 0 || n45 > 1 || m < 1 ||
+        m > 5)
+      throw ApiError(CANARD_ERR_ARG, "bad mpigo argument");
+    if (nrt == 0 && ncols != 3) throw ApiError(CANARD_ERR_ARG, "nrall needs three columns");
+    const CaseState& cs = c->cases[0];
+    // stage the fields in the scratch columns 12..14 of every block
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) {
+      if (!fields[b - cs.b0]) throw ApiError(CANARD_ERR_ARG, "null field");
+      h2d_field(c, c->blocks[b], fptr(c->blocks[b], F_SCR + 12), fields[b - cs.b0], ncols);
+    }
+    auto col = [&](int b, int d) { return fptr(c->blocks[b], F_SCR + 12 + (nrt == 0 ? d : 0)); };
+    launch_mpigo(c, make_face_table(c, face_tasks(c, nt, n45, m, -1, col, 0), true));
+    sync_check(c);
+    free_transient(c);
+  });
+}
+
+static void unit_line(canard_ctx* c, int iblock, const double* in, double* out, int dir, int nt, int m) {
+  const int b = block_index(c, 0, iblock);
+  BlockState& B = c->blocks[b];
+  double* f = fptr(B, F_SCR + 11);
+  h2d_field(c, B, f, in, 1);
+  LineTask t;
+  fill_line_task(c, B, dir, nt, f, f, m, nt == 0, t);
+  launch_line(c, make_line_table(c, {t}, dir, true), dir, nt);
+  d2h_field(c, B, out, f, 1);
+  sync_check(c);
+  free_transient(c);
+}
+
+int canard_deriv(canard_ctx* c, int32_t iblock, const double* in, double* out, int32_t nn, int32_t m) {
+  return guarded(c, [&] {
+    if (!in || !out || nn < 1 || nn > 3 || m < 1 || m > 5) throw ApiError(CANARD_ERR_ARG, "bad deriv argument");
+    unit_line(c, iblock, in, out, nn - 1, 0, m);
+  });
+}
+
+int canard_filte(canard_ctx* c, int32_t iblock, double* f, int32_t inn, int32_t m) {
+  return guarded(c, [&] {
+    if (!f || inn < 1 || inn > 3 || m < 1 || m > 5) throw ApiError(CANARD_ERR_ARG, "bad filte argument");
+    unit_line(c, iblock, f, f, kNnf[inn - 1] - 1, 1, m);
+  });
+}
+
+int canard_set_timers(canard_ctx* c, int32_t on) {
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    collect_timers(c);
+    c->timers = on != 0;
+    for (int i = 0; i < T_NFAM; ++i) c->t_ms[i] = c->t_n[i] = c->t_bytes[i] = 0;
+  });
+}
+
+int canard_get_timers(canard_ctx* c, double* ms, double* launches, double* bytes, int32_t nmax) {
+  if (!c) return -CANARD_ERR_ARG;
+  int rc = guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    collect_timers(c);
+    for (int i = 0; i < T_NFAM && i < nmax; ++i) {
+      if (ms) ms[i] = c->t_ms[i];
+      if (launches) launches[i] = c->t_n[i];
+      if (bytes) bytes[i] = c->t_bytes[i];
+    }
+  });
+  return rc == CANARD_OK ? (int)T_NFAM : -rc;
+}
+
+const char* canard_timer_name(int32_t f) { return (f >= 0 && f < T_NFAM) ? kTimerNames[f] : ""; }
+
+int canard_launch_count(canard_ctx* c, int64_t* count) {
+  if (!c || !count) return CANARD_ERR_ARG;
+  *count = c->launches;
+  return CANARD_OK;
+}
+
+}  // extern "C"

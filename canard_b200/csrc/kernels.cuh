@@ -1,0 +1,969 @@
+// Device kernels of the Canard hot path for sm_100a.
+//
+// FP64 kernels are compiled without FMA contraction (-fmad=false) and evaluate
+// every expression in the reference's order, so on identical inputs they
+// reproduce the CPU restatement bit for bit (the Sutherland power is the only
+// library function, see pow15).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace canard {
+
+constexpr int kLanes = 32;          // lines per tile (one warp, one line per lane)
+constexpr int kErrTimeout = 4;
+constexpr long long kSpinLimit = 1LL << 28;  // bounded mbarrier waits
+
+struct DevScheme {
+  double pbci[2][2][12];  // [nt][side][i]
+  double pbco[2][2][12];
+  double pbcot[2][2];
+  double fa, fb, fc;
+  double fbc[3][5];       // [row][k]
+};
+
+// Per-case scalars of one RK stage (written by the host before each step).
+struct StageParams {
+  double umf[3], dudtmf[3];   // moving frame for fluxes / GCBC (movef before the update)
+  double umfb[3];             // moving frame after the update (wall condition)
+  double dtk, dt;
+};
+
+struct CaseConst {
+  double srefoo, srefp1dre;
+  int viscous;
+};
+
+struct BlockDev {
+  int X, Y, Z, Xp;
+  long long npad;
+  int case_id;
+  double *qa, *qo, *de, *p, *mu, *xim, *etm, *zem, *yaco, *tau, *scr, *xyz;
+};
+
+// ---------------------------------------------------------------------------
+// A family of lines of one block, direction and field, solved by one launch
+// together with other families (tile prefix sums select the family).
+struct LineTask {
+  const double* in;
+  double* out;
+  const double* lu;     // xl1, xl2, xu1, xu2, xu3 (each L entries)
+  const double* recv;   // [side][comp][jk], comp stride nbs, side stride ncomp*nbs
+  double* drva;         // drva(jk, m, side) of this block and direction, or null
+  const DevScheme* sc;
+  int X, Y, Z, Xp;
+  int L, nbs, m, ndf0, ndf1;
+  int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
+};
+
+// Interface contraction of one face (t_numerics%mpigo): the sender's face
+// lines are contracted with pbco and written into the receiver's buffers.
+struct FaceTask {
+  const double* src;    // sender field column for this direction
+  const double* dstf;   // receiver field column (coordinate-jump correction)
+  double* recv;         // receiver buffer [comp][jk] for (direction, side, m)
+  double* chain;        // sender's persistent send(:,nt+1,side) of the filter
+  const DevScheme* sc;
+  int nn, sb, nt, exch, corr, iik;
+  double ra0k;
+  int X, Y, Z, Xp, N;       // sender geometry
+  int XA, YA, ZA, XpA, NA;  // receiver geometry
+  int nbs, nj, line0;
+};
+
+struct GcbcTask {  // one GCBC face of one block
+  int b, nn, side, bc;
+  const double* cm;       // cm(jk,3,side) base of this face side: [d][jk]
+  double* drva;           // drva(jk,5,side): [c][jk]
+  const double* drvb;
+  const long long* pts;   // 5 device indices per line
+  const double* w;        // 5 weights per line
+  int nbs, nj, line0;
+  int X, Y, Z, Xp, N;
+};
+
+// ---------------------------------------------------------------------------
+// small PTX helpers: mbarrier + bulk asynchronous copies (sm_90+)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// Bounded wait for phase `parity`; returns false if the limit expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Correctly rounded x^1.5 for x > 0 (up to rare ties): x*sqrt(x) carried in
+// double-double arithmetic (Dekker's exact product, Newton remainder of sqrt).
+__device__ __forceinline__ double pow15(double x) {
+  const double s = sqrt(x);
+  const double r = fma(-s, s, x);          // exact: x - s^2
+  const double e = r / (2.0 * s);          // sqrt(x) = s + e + O(ulp^2)
+  const double p = x * s;
+  const double pe = fma(x, s, -p);         // exact: x*s - p
+  return p + (pe + x * e);
+}
+
+// ---------------------------------------------------------------------------
+// scheme constants (src/mo_parameters.f90:61-79)
+#define CA_ALPHA (4 / 9.0)
+#define CA_BETA (1 / 36.0)
+#define CA_AA (20 / 27.0)
+#define CA_AB (25 / 216.0)
+#define CA_A10 (-0.3506944444280639)
+#define CA_A12 (0.8249999999974599)
+#define CA_A13 (0.7444444444773477)
+#define CA_A14 (0.014583333334139971)
+#define CA_A01 (-6.666666667794732)
+#define CA_A02 (9.000000000052879)
+#define CA_A03 (1.333333333178555)
+#define CA_A04 (-0.0833333333455545)
+
+// Compact first derivative of one line held in shared memory with element
+// stride ST (src/mo_numerics.f90:742-792). On return the line holds the
+// derivative; *d0 / *dN receive the end values.
+template <int ST>
+__device__ __forceinline__ void sweep_deriv(double* __restrict__ s, int L, const double* __restrict__ lu,
+                                            int ndf0, int ndf1, const DevScheme* __restrict__ sc, double r00,
+                                            double r10, double r01, double r11) {
+#define S(i) s[(i)*ST]
+  const int N = L - 1;
+  const double* l1 = lu;
+  const double* l2 = lu + L;
+  const double* u1 = lu + 2 * L;
+  const double* u2 = lu + 3 * L;
+  const double* u3 = lu + 4 * L;
+  double b0, b1, bn1, bn;
+  if (ndf0 == 0) {
+    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4);
+    b0 = ((CA_A01 * (s1 - s0) + CA_A02 * (s2 - s0)) + CA_A03 * (s3 - s0)) + CA_A04 * (s4 - s0);
+    b1 = ((CA_A10 * (s0 - s1) + CA_A12 * (s2 - s1)) + CA_A13 * (s3 - s1)) + CA_A14 * (s4 - s1);
+  } else {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const double v = S(i);
+      t0 = t0 + sc->pbci[0][0][i] * v;
+      t1 = t1 + sc->pbci[0][1][i] * v;
+    }
+    b0 = t0 + r00;
+    b1 = t1 + r10;
+  }
+  if (ndf1 == 0) {
+    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4);
+    bn = ((CA_A01 * (e0 - e1) + CA_A02 * (e0 - e2)) + CA_A03 * (e0 - e3)) + CA_A04 * (e0 - e4);
+    bn1 = ((CA_A10 * (e1 - e0) + CA_A12 * (e1 - e2)) + CA_A13 * (e1 - e3)) + CA_A14 * (e1 - e4);
+  } else {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const double v = S(N - i);
+      t0 = t0 + sc->pbci[0][0][i] * v;
+      t1 = t1 + sc->pbci[0][1][i] * v;
+    }
+    bn = -t0 - r01;
+    bn1 = -t1 - r11;
+  }
+  // forward elimination, in place, originals kept in a register window
+  double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3);
+  double am2 = b0;
+  double am1 = b1 - __ldg(l2 + 1) * am2;
+  S(0) = am2;
+  S(1) = am1;
+  for (int i = 2; i <= N - 2; ++i) {
+    const double w4 = S(i + 2);
+    const double rhs = CA_AA * (w3 - w1) + CA_AB * (w4 - w0);
+    const double a = (rhs - __ldg(l1 + i) * am2) - __ldg(l2 + i) * am1;
+    S(i) = a;
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+    am2 = am1; am1 = a;
+  }
+  {
+    const double a = (bn1 - __ldg(l1 + N - 1) * am2) - __ldg(l2 + N - 1) * am1;
+    S(N - 1) = a;
+    am2 = am1; am1 = a;
+    const double an = (bn - __ldg(l1 + N) * am2) - __ldg(l2 + N) * am1;
+    S(N) = an;
+  }
+  // back substitution
+  double cp1 = __ldg(u1 + N) * S(N);
+  S(N) = cp1;
+  double c = __ldg(u1 + N - 1) * S(N - 1) - __ldg(u2 + N - 1) * cp1;
+  S(N - 1) = c;
+  double cp2 = cp1;
+  cp1 = c;
+  for (int i = N - 2; i >= 0; --i) {
+    c = (__ldg(u1 + i) * S(i) - __ldg(u2 + i) * cp1) - __ldg(u3 + i) * cp2;
+    S(i) = c;
+    cp2 = cp1;
+    cp1 = c;
+  }
+#undef S
+}
+
+// Compact filter increment of one line (src/mo_numerics.f90:922-977). On
+// return the line holds the increment (the caller adds the original field).
+template <int ST>
+__device__ __forceinline__ void sweep_filter(double* __restrict__ s, int L, const double* __restrict__ lu,
+                                             int ndf0, int ndf1, const DevScheme* __restrict__ sc, double r00,
+                                             double r10, double r20, double r01, double r11, double r21) {
+#define S(i) s[(i)*ST]
+  const int N = L - 1;
+  const double* l1 = lu;
+  const double* l2 = lu + L;
+  const double* u1 = lu + 2 * L;
+  const double* u2 = lu + 3 * L;
+  const double* u3 = lu + 4 * L;
+  const double fa = sc->fa, fb = sc->fb, fc = sc->fc;
+  double b0, b1, b2, bn2, bn1, bn;
+  if (ndf0 == 0) {
+    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
+    const double* f0 = sc->fbc[0];
+    const double* f1 = sc->fbc[1];
+    const double* f2 = sc->fbc[2];
+    b0 = (((f0[0] * (s1 - s0) + f0[1] * (s2 - s0)) + f0[2] * (s3 - s0)) + f0[3] * (s4 - s0)) + f0[4] * (s5 - s0);
+    b1 = (((f1[0] * (s0 - s1) + f1[1] * (s2 - s1)) + f1[2] * (s3 - s1)) + f1[3] * (s4 - s1)) + f1[4] * (s5 - s1);
+    b2 = (((f2[0] * (s0 - s2) + f2[1] * (s1 - s2)) + f2[2] * (s3 - s2)) + f2[3] * (s4 - s2)) + f2[4] * (s5 - s2);
+  } else {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const double v = S(i);
+      t0 = t0 + sc->pbci[1][0][i] * v;
+      t1 = t1 + sc->pbci[1][1][i] * v;
+    }
+    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
+    const double ra2 = s2 + s2;
+    b0 = t0 + r00;
+    b1 = t1 + r10;
+    b2 = (fa * ((s1 + s3) - ra2) + fb * ((s0 + s4) - ra2)) + fc * ((r20 + s5) - ra2);
+  }
+  if (ndf1 == 0) {
+    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
+    const double* f0 = sc->fbc[0];
+    const double* f1 = sc->fbc[1];
+    const double* f2 = sc->fbc[2];
+    bn = (((f0[0] * (e1 - e0) + f0[1] * (e2 - e0)) + f0[2] * (e3 - e0)) + f0[3] * (e4 - e0)) + f0[4] * (e5 - e0);
+    bn1 = (((f1[0] * (e0 - e1) + f1[1] * (e2 - e1)) + f1[2] * (e3 - e1)) + f1[3] * (e4 - e1)) + f1[4] * (e5 - e1);
+    bn2 = (((f2[0] * (e0 - e2) + f2[1] * (e1 - e2)) + f2[2] * (e3 - e2)) + f2[3] * (e4 - e2)) + f2[4] * (e5 - e2);
+  } else {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const double v = S(N - i);
+      t0 = t0 + sc->pbci[1][0][i] * v;
+      t1 = t1 + sc->pbci[1][1][i] * v;
+    }
+    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
+    const double ra2 = e2 + e2;
+    bn = t0 + r01;
+    bn1 = t1 + r11;
+    bn2 = (fa * ((e3 + e1) - ra2) + fb * ((e4 + e0) - ra2)) + fc * ((e5 + r21) - ra2);
+  }
+  // forward elimination: rows 0..2 from the closures, 3..N-3 interior
+  double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3), w4 = S(4), w5 = S(5);  // s[i-3..i+2] at i = 3
+  double am2 = b0;
+  double am1 = b1 - __ldg(l2 + 1) * am2;
+  double a2 = (b2 - __ldg(l1 + 2) * am2) - __ldg(l2 + 2) * am1;
+  S(0) = am2;
+  S(1) = am1;
+  S(2) = a2;
+  am2 = am1;
+  am1 = a2;
+  for (int i = 3; i <= N - 3; ++i) {
+    const double w6 = S(i + 3);
+    const double rk = w3 + w3;
+    const double rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+    const double a = (rhs - __ldg(l1 + i) * am2) - __ldg(l2 + i) * am1;
+    S(i) = a;
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    am2 = am1; am1 = a;
+  }
+  {
+    double a = (bn2 - __ldg(l1 + N - 2) * am2) - __ldg(l2 + N - 2) * am1;
+    S(N - 2) = a;
+    am2 = am1; am1 = a;
+    a = (bn1 - __ldg(l1 + N - 1) * am2) - __ldg(l2 + N - 1) * am1;
+    S(N - 1) = a;
+    am2 = am1; am1 = a;
+    a = (bn - __ldg(l1 + N) * am2) - __ldg(l2 + N) * am1;
+    S(N) = a;
+  }
+  double cp1 = __ldg(u1 + N) * S(N);
+  S(N) = cp1;
+  double c = __ldg(u1 + N - 1) * S(N - 1) - __ldg(u2 + N - 1) * cp1;
+  S(N - 1) = c;
+  double cp2 = cp1;
+  cp1 = c;
+  for (int i = N - 2; i >= 0; --i) {
+    c = (__ldg(u1 + i) * S(i) - __ldg(u2 + i) * cp1) - __ldg(u3 + i) * cp2;
+    S(i) = c;
+    cp2 = cp1;
+    cp1 = c;
+  }
+#undef S
+}
+
+__device__ __forceinline__ int find_task(const int* __restrict__ tile0, int ntasks, int tile) {
+  int lo = 0, hi = ntasks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(tile0 + mid) <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Line pitch (doubles) of the dir-1 shared-memory tile: >= round_up(L, 2) and
+// = 2 (mod 4), so rows start 16-byte aligned and 64-bit column walks see at
+// most 2-way bank conflicts.
+__host__ __device__ __forceinline__ int dir1_pitch(int L) {
+  int p = (L + 1) / 2 * 2;
+  if (p % 4 == 0) p += 2;
+  return p;
+}
+
+// One CTA = one warp = 32 lines. DIR: 1 xi, 2 eta, 3 zeta. OP: 0 derivative,
+// 1 filter (in place, f += increment).
+template <int DIR, int OP>
+__global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
+                                             int ntasks, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+  double* s = reinterpret_cast<double*>(smem_raw + 128);
+  const int lane = threadIdx.x;
+  const int ti = find_task(tile0s, ntasks, blockIdx.x);
+  const LineTask& T = tasks[ti];
+  const int lt = blockIdx.x - T.tile0;
+  const int L = T.L;
+  const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
+  // tile geometry
+  int nval, x0 = 0, r0 = 0, fix = 0;  // fix: z for dir 2, y for dir 3
+  if (DIR == 1) {
+    r0 = lt * kLanes;
+    nval = min(kLanes, Y * Z - r0);
+  } else {
+    fix = lt / T.ntx;
+    x0 = (lt % T.ntx) * kLanes;
+    nval = min(kLanes, X - x0);
+  }
+  const int P = dir1_pitch(L);
+  const uint32_t rowbytes = (DIR == 1) ? (uint32_t)((L + 1) / 2 * 2 * 8) : (uint32_t)((nval + 1) / 2 * 2 * 8);
+  const long long pstride = (DIR == 2) ? (long long)Xp : (long long)Xp * Y;  // dir 2/3 position stride
+  const long long base = (DIR == 1) ? (long long)r0 * Xp
+                                    : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
+  if (lane == 0) mbar_init(bar, 1);
+  __syncwarp();
+  if (lane == 0) mbar_expect_tx(bar, (DIR == 1) ? rowbytes * nval : rowbytes * L);
+  __syncwarp();
+  if (DIR == 1) {
+    if (lane < nval) bulk_g2s(s + lane * P, T.in + base + (long long)lane * Xp, rowbytes, bar);
+  } else {
+    for (int i = lane; i < L; i += kLanes) bulk_g2s(s + i * kLanes, T.in + base + i * pstride, rowbytes, bar);
+  }
+  if (!mbar_wait(bar, 0)) {
+    if (lane == 0) atomicExch(err, kErrTimeout);
+    return;
+  }
+  if (lane < nval) {
+    int jk;
+    if (DIR == 1) jk = r0 + lane;
+    else if (DIR == 2) jk = (x0 + lane) * Z + fix;
+    else jk = fix * X + x0 + lane;
+    const int nbs = T.nbs;
+    constexpr int ST = (DIR == 1) ? 1 : kLanes;
+    double* sl = (DIR == 1) ? s + lane * P : s + lane;
+    if (OP == 0) {
+      double r00 = 0, r10 = 0, r01 = 0, r11 = 0;
+      if (T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; }
+      if (T.ndf1) { r01 = T.recv[2 * nbs + jk]; r11 = T.recv[3 * nbs + jk]; }
+      sweep_deriv<ST>(sl, L, T.lu, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11);
+      if (T.drva) {
+        T.drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+        T.drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
+      }
+    } else {
+      double r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
+      if (T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; r20 = T.recv[2 * nbs + jk]; }
+      if (T.ndf1) { r01 = T.recv[3 * nbs + jk]; r11 = T.recv[4 * nbs + jk]; r21 = T.recv[5 * nbs + jk]; }
+      sweep_filter<ST>(sl, L, T.lu, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21);
+      if (DIR != 1) {
+        // f = f + increment; the original re-read is coalesced across lanes
+        for (int i = 0; i < L; ++i) sl[i * ST] = T.in[base + i * pstride + lane] + sl[i * ST];
+      }
+    }
+  }
+  if (OP == 1 && DIR == 1) {
+    __syncwarp();
+    for (int r = 0; r < nval; ++r) {
+      const double* g = T.in + base + (long long)r * Xp;
+      double* row = s + r * P;
+      for (int i = lane; i < L; i += kLanes) row[i] = g[i] + row[i];
+    }
+  }
+  fence_proxy_async();
+  __syncwarp();
+  if (DIR == 1) {
+    if (lane < nval) {
+      bulk_s2g(T.out + base + (long long)lane * Xp, s + lane * P, rowbytes);
+      bulk_commit();
+      bulk_wait_read0();
+    }
+  } else {
+    bool any = false;
+    for (int i = lane; i < L; i += kLanes) {
+      bulk_s2g(T.out + base + i * pstride, s + i * kLanes, rowbytes);
+      any = true;
+    }
+    if (any) {
+      bulk_commit();
+      bulk_wait_read0();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void line_xyz(int nn, int pos, int j, int k, int& x, int& y, int& z) {
+  if (nn == 1) { x = pos; y = j; z = k; }
+  else if (nn == 2) { x = k; y = pos; z = j; }
+  else { x = j; y = k; z = pos; }
+}
+
+// t_numerics%mpigo for a list of faces (src/mo_numerics.f90:429-565).
+__global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restrict__ line0s, int ntasks,
+                        int nlines) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
+    const int ti = find_task(line0s, ntasks, g);
+    const FaceTask& T = tasks[ti];
+    const int jk = g - T.line0;
+    const int j = jk % T.nj, k = jk / T.nj;
+    const int istart = T.sb * T.N, step = 1 - 2 * T.sb;
+    int x, y, z;
+    line_xyz(T.nn, istart, j, k, x, y, z);
+    const double resk = T.ra0k * T.src[((long long)z * T.Y + y) * T.Xp + x];
+    const DevScheme* sc = T.sc;
+    const int nt = T.nt;
+    double t0 = 0.0, t1 = 0.0, sap0 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      line_xyz(T.nn, istart + step * (i + T.iik), j, k, x, y, z);
+      const double v = T.src[((long long)z * T.Y + y) * T.Xp + x];
+      if (i == 0) sap0 = v;
+      t0 = t0 + sc->pbco[nt][0][i] * v;
+      t1 = t1 + sc->pbco[nt][1][i] * v;
+    }
+    double snd0 = t0 - resk * sc->pbcot[nt][0];
+    double snd1 = t1 - resk * sc->pbcot[nt][1];
+    double snd2 = 0.0;
+    if (nt == 1) {
+      const double old = T.chain[jk];
+      snd2 = old + ((sap0 - resk) - old);
+      T.chain[jk] = snd2;
+    }
+    if (T.exch) {
+      if (T.corr) {  // receiver side is periodic and n45 = n45go
+        line_xyz(T.nn, (1 - T.sb) * T.NA, j, k, x, y, z);
+        const double f = T.dstf[((long long)z * T.YA + y) * T.XpA + x];
+        snd0 = snd0 + f * sc->pbcot[nt][0];
+        snd1 = snd1 + f * sc->pbcot[nt][1];
+        if (nt == 1) snd2 = snd2 + f; else snd1 = snd1 + 0.0 * f;
+      }
+      T.recv[jk] = snd0;
+      T.recv[T.nbs + jk] = snd1;
+      if (nt == 1) T.recv[2 * T.nbs + jk] = snd2;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// element-wise kernels: blockIdx.y = block
+#define FOR_POINTS(BD)                                                              \
+  const BlockDev& B = BD;                                                           \
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < B.npad; \
+       l += (long long)gridDim.x * blockDim.x)                                      \
+    if ((int)(l % B.Xp) < B.X)
+
+constexpr double kGam = 1.4;
+#define KGAMM1 (kGam - 1.0)
+
+// primitives, pressure, Sutherland viscosity (src/mo_canard_driver.f90:267-275)
+__global__ void k_prim(const BlockDev* __restrict__ bd, const CaseConst* __restrict__ cc) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const CaseConst C = cc[B.case_id];
+    const double* q = B.qa;
+    double* de = B.de;
+    const double q0 = q[l], q1 = q[l + n], q2 = q[l + 2 * n], q3 = q[l + 3 * n], q4 = q[l + 4 * n];
+    const double d1 = 1.0 / q0;
+    const double d2 = q1 * d1, d3 = q2 * d1, d4 = q3 * d1;
+    const double p = KGAMM1 * (q4 - 0.5 * ((q1 * d2 + q2 * d3) + q3 * d4));
+    const double d5 = (kGam * p) * d1;
+    de[l] = d1; de[l + n] = d2; de[l + 2 * n] = d3; de[l + 3 * n] = d4; de[l + 4 * n] = d5;
+    B.p[l] = p;
+    B.mu[l] = (C.srefp1dre * pow15(d5)) / (d5 + C.srefoo);
+  }
+}
+
+// time-step maxima (src/mo_physics.f90:185-207); values are >= 0, so their
+// bit patterns order like the values and atomicMax on them is exact.
+__global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                        const CaseConst* __restrict__ cc, unsigned long long* __restrict__ out) {
+  const BlockDev& B0 = bd[blockIdx.y];
+  const StageParams S = sp[B0.case_id];
+  const int visc = cc[B0.case_id].viscous;
+  double m1 = 0.0, m2 = 0.0;
+  FOR_POINTS(B0) {
+    const long long n = B.npad;
+    const double *xi = B.xim, *et = B.etm, *ze = B.zem, *de = B.de;
+    double r1 = xi[l] * xi[l];
+    r1 = r1 + xi[l + n] * xi[l + n];
+    r1 = r1 + xi[l + 2 * n] * xi[l + 2 * n];
+    r1 = r1 + et[l] * et[l];
+    r1 = r1 + et[l + n] * et[l + n];
+    r1 = r1 + et[l + 2 * n] * et[l + 2 * n];
+    r1 = r1 + ze[l] * ze[l];
+    r1 = r1 + ze[l + n] * ze[l + n];
+    r1 = r1 + ze[l + 2 * n] * ze[l + 2 * n];
+    const double u = de[l + n] + S.umf[0], v = de[l + 2 * n] + S.umf[1], w = de[l + 3 * n] + S.umf[2];
+    double r2 = fabs((xi[l] * u + xi[l + n] * v) + xi[l + 2 * n] * w) +
+                fabs((et[l] * u + et[l + n] * v) + et[l + 2 * n] * w);
+    r2 = r2 + fabs((ze[l] * u + ze[l + n] * v) + ze[l + 2 * n] * w);
+    const double ssi = fabs(B.yaco[l]);
+    m1 = fmax(m1, (sqrt(de[l + 4 * n] * r1) + r2) * ssi);
+    if (visc) m2 = fmax(m2, (((de[l] * B.mu[l]) * r1) * ssi) * ssi);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out + 2 * B0.case_id, (unsigned long long)__double_as_longlong(m1));
+    atomicMax(out + 2 * B0.case_id + 1, (unsigned long long)__double_as_longlong(m2));
+  }
+}
+
+// viscous stresses and heat flux from the 12 gradients in scr
+// (src/mo_physics.f90:245-299); scr field g*3+d = d/d(xi_d) of u, v, w, T.
+__global__ void k_viscous_assemble(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double *xi = B.xim, *et = B.etm, *ze = B.zem, *g = B.scr;
+    auto comb = [&](int f, int c) {
+      return (xi[l + c * n] * g[l + (3 * f) * n] + et[l + c * n] * g[l + (3 * f + 1) * n]) +
+             ze[l + c * n] * g[l + (3 * f + 2) * n];
+    };
+    double txx = comb(0, 0), hzz = comb(0, 1), tzx = comb(0, 2);
+    double txy = comb(1, 0), tyy = comb(1, 1), hxx = comb(1, 2);
+    double hyy = comb(2, 0), tyz = comb(2, 1), tzz = comb(2, 2);
+    const double s1 = comb(3, 0), s2 = comb(3, 1), s3 = comb(3, 2);
+    double* de = B.de;
+    const double rr1 = de[l] * B.yaco[l];
+    const double rr2 = (1.0 / (KGAMM1 * 0.71)) * rr1;
+    const double d5 = (2.0 / 3.0) * ((txx + tyy) + tzz);
+    de[l + 4 * n] = d5;
+    txx = rr1 * ((txx + txx) - d5);
+    tyy = rr1 * ((tyy + tyy) - d5);
+    tzz = rr1 * ((tzz + tzz) - d5);
+    txy = rr1 * (txy + hzz);
+    tyz = rr1 * (tyz + hxx);
+    tzx = rr1 * (tzx + hyy);
+    const double u = de[l + n], v = de[l + 2 * n], w = de[l + 3 * n];
+    hxx = ((rr2 * s1 + u * txx) + v * txy) + w * tzx;
+    hyy = ((rr2 * s2 + u * txy) + v * tyy) + w * tyz;
+    hzz = ((rr2 * s3 + u * tzx) + v * tyz) + w * tzz;
+    double* t = B.tau;
+    t[l] = txx; t[l + n] = tyy; t[l + 2 * n] = tzz; t[l + 3 * n] = txy; t[l + 4 * n] = tyz;
+    t[l + 5 * n] = tzx; t[l + 6 * n] = hxx; t[l + 7 * n] = hyy; t[l + 8 * n] = hzz;
+  }
+}
+
+// de(:,1) = ss(:,1) before the viscous gradients (src/mo_physics.f90:228)
+__global__ void k_copy_mu(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) { B.de[l] = B.mu[l]; }
+}
+
+// flux components rr(:,d,m) into scr field (m-1)*3 + d (src/mo_physics.f90:319-382)
+__global__ void k_flux(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                       const CaseConst* __restrict__ cc) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const StageParams S = sp[B.case_id];
+    const int visc = cc[B.case_id].viscous;
+    const double* q = B.qa;
+    double* de = B.de;
+    const double p = B.p[l];
+    const double* mt[3] = {B.xim, B.etm, B.zem};
+    const double u = de[l + n] + S.umf[0], v = de[l + 2 * n] + S.umf[1], w = de[l + 3 * n] + S.umf[2];
+    double ssd[3], m[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
+      ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
+    }
+    double* r = B.scr;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[l + d * n] = q[l] * ssd[d];
+    double tau[3][3];
+    double hx = 0, hy = 0, hz = 0;
+    if (visc) {
+      const double* t = B.tau;
+      tau[0][0] = t[l]; tau[0][1] = t[l + 3 * n]; tau[0][2] = t[l + 5 * n];
+      tau[1][0] = t[l + 3 * n]; tau[1][1] = t[l + n]; tau[1][2] = t[l + 4 * n];
+      tau[2][0] = t[l + 5 * n]; tau[2][1] = t[l + 4 * n]; tau[2][2] = t[l + 2 * n];
+      hx = t[l + 6 * n]; hy = t[l + 7 * n]; hz = t[l + 8 * n];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double qc = q[l + (c + 1) * n];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double v1 = qc * ssd[d] + m[d][c] * p;
+        if (visc) {
+          v1 = v1 - m[d][0] * tau[c][0];
+          v1 = v1 - m[d][1] * tau[c][1];
+          v1 = v1 - m[d][2] * tau[c][2];
+        }
+        r[l + (3 * (c + 1) + d) * n] = v1;
+      }
+    }
+    const double d5 = q[l + 4 * n] + p;
+    de[l + 4 * n] = d5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double v1 = d5 * ssd[d] - p * ((S.umf[0] * m[d][0] + S.umf[1] * m[d][1]) + S.umf[2] * m[d][2]);
+      if (visc) {
+        v1 = v1 - m[d][0] * hx;
+        v1 = v1 - m[d][1] * hy;
+        v1 = v1 - m[d][2] * hz;
+      }
+      r[l + (12 + d) * n] = v1;
+    }
+  }
+}
+
+// de(:,m) = sum of the three flux derivatives (src/mo_physics.f90:399)
+__global__ void k_flux_sum(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double* r = B.scr;
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+      B.de[l + m * n] = (r[l + (3 * m) * n] + r[l + (3 * m + 1) * n]) + r[l + (3 * m + 2) * n];
+  }
+}
+
+// RK stage update (src/mo_canard_driver.f90:329-334)
+__global__ void k_rk(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double r1 = sp[B.case_id].dtk * B.yaco[l];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) B.qa[l + c * n] = B.qo[l + c * n] - r1 * B.de[l + c * n];
+  }
+}
+
+__global__ void k_copy5(const BlockDev* __restrict__ bd) {  // qo = qa
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) B.qo[l + c * n] = B.qa[l + c * n];
+  }
+}
+
+// cofactor metrics from the 9 coordinate derivatives in scr (src/mo_grid.f90:107-115);
+// scr field 3*(m-1)+(d-1) = d(coordinate m)/d(xi_d)
+__global__ void k_cofactors(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double* g = B.scr;
+    const double q1 = g[l], q2 = g[l + n], q3 = g[l + 2 * n];
+    const double a1 = g[l + 3 * n], a2 = g[l + 4 * n], a3 = g[l + 5 * n];
+    const double d1 = g[l + 6 * n], d2 = g[l + 7 * n], d3 = g[l + 8 * n];
+    B.xim[l] = a2 * d3 - d2 * a3;
+    B.xim[l + n] = d2 * q3 - q2 * d3;
+    B.xim[l + 2 * n] = q2 * a3 - a2 * q3;
+    B.etm[l] = a3 * d1 - d3 * a1;
+    B.etm[l + n] = d3 * q1 - q3 * d1;
+    B.etm[l + 2 * n] = q3 * a1 - a3 * q1;
+    B.zem[l] = a1 * d2 - d1 * a2;
+    B.zem[l + n] = d1 * q2 - q1 * d2;
+    B.zem[l + 2 * n] = q1 * a2 - a1 * q2;
+  }
+}
+
+// Jacobian (src/mo_grid.f90:157-159)
+__global__ void k_jacobian(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double* g = B.scr;
+    const double *xi = B.xim, *et = B.etm, *ze = B.zem;
+    double s = g[l] * xi[l];
+    s = s + g[l + n] * et[l];
+    s = s + g[l + 2 * n] * ze[l];
+    s = s + g[l + 3 * n] * xi[l + n];
+    s = s + g[l + 4 * n] * et[l + n];
+    s = s + g[l + 5 * n] * ze[l + n];
+    s = s + g[l + 6 * n] * xi[l + 2 * n];
+    s = s + g[l + 7 * n] * et[l + 2 * n];
+    s = s + g[l + 8 * n] * ze[l + 2 * n];
+    B.yaco[l] = 3.0 / s;
+  }
+}
+
+// unit face normals cm{1,2,3} (src/mo_grid.f90:161-186); one thread per face line.
+struct CmTask { int b, nn, side, nbs, nj, N, line0; double* cm; };
+__global__ void k_face_normals(const BlockDev* __restrict__ bd, const CmTask* __restrict__ tasks,
+                               const int* __restrict__ line0s, int ntasks, int nlines) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
+    const CmTask& T = tasks[find_task(line0s, ntasks, g)];
+    const BlockDev& B = bd[T.b];
+    const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
+    int x, y, z;
+    line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
+    const long long l = ((long long)z * B.Y + y) * B.Xp + x;
+    const double* met = T.nn == 1 ? B.xim : T.nn == 2 ? B.etm : B.zem;
+    const double ya = B.yaco[l];
+    const double r0 = ya * met[l], r1 = ya * met[l + B.npad], r2 = ya * met[l + 2 * B.npad];
+    const double f = 1.0 / sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+    T.cm[jk] = f * r0;
+    T.cm[T.nbs + jk] = f * r1;
+    T.cm[2 * T.nbs + jk] = f * r2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// GCBC (src/mo_gcbc.f90:133-340, 506-611)
+struct Elem { double ao, aoi, ve[3], hv2, vn, vs; };
+
+__device__ __forceinline__ Elem eleme(const double cm[3], double q1, double q2, double q3, double q4, double pp,
+                                      const double umf[3]) {
+  Elem e;
+  const double rhoi = 1.0 / q1;
+  e.ao = sqrt((kGam * rhoi) * pp);
+  e.aoi = 1.0 / e.ao;
+  e.ve[0] = rhoi * q2; e.ve[1] = rhoi * q3; e.ve[2] = rhoi * q4;
+  e.hv2 = 0.5 * ((e.ve[0] * e.ve[0] + e.ve[1] * e.ve[1]) + e.ve[2] * e.ve[2]);
+  e.vn = (cm[0] * e.ve[0] + cm[1] * e.ve[1]) + cm[2] * e.ve[2];
+  e.vs = (cm[0] * umf[0] + cm[1] * umf[1]) + cm[2] * umf[2];
+  return e;
+}
+
+// r = X_{q->r} v (src/mo_gcbc.f90:506-548)
+__device__ __forceinline__ void q2r_apply(const Elem& e, const double cm[3], const double v[5], double r[5]) {
+  const double ho = (KGAMM1 * e.aoi) * e.aoi;
+  const double bo = 1 - ho * e.hv2;
+  const double co = e.aoi * e.vn;
+  double dm[3], rv[3];
+  for (int d = 0; d < 3; ++d) { dm[d] = e.aoi * cm[d]; rv[d] = ho * e.ve[d]; }
+  const double* ve = e.ve;
+  double xt[5][5];
+  xt[0][0] = (bo * cm[0] + dm[1] * ve[2]) - dm[2] * ve[1];
+  xt[0][1] = cm[0] * rv[0]; xt[0][2] = cm[0] * rv[1] + dm[2]; xt[0][3] = cm[0] * rv[2] - dm[1]; xt[0][4] = -ho * cm[0];
+  xt[1][0] = (bo * cm[1] + dm[2] * ve[0]) - dm[0] * ve[2];
+  xt[1][1] = cm[1] * rv[0] - dm[2]; xt[1][2] = cm[1] * rv[1]; xt[1][3] = cm[1] * rv[2] + dm[0]; xt[1][4] = -ho * cm[1];
+  xt[2][0] = (bo * cm[2] + dm[0] * ve[1]) - dm[1] * ve[0];
+  xt[2][1] = cm[2] * rv[0] + dm[1]; xt[2][2] = cm[2] * rv[1] - dm[0]; xt[2][3] = cm[2] * rv[2]; xt[2][4] = -ho * cm[2];
+  xt[3][0] = (1.0 - bo) - co; xt[3][1] = dm[0] - rv[0]; xt[3][2] = dm[1] - rv[1]; xt[3][3] = dm[2] - rv[2]; xt[3][4] = ho;
+  xt[4][0] = (1.0 - bo) + co; xt[4][1] = -dm[0] - rv[0]; xt[4][2] = -dm[1] - rv[1]; xt[4][3] = -dm[2] - rv[2]; xt[4][4] = ho;
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.0;
+    for (int c = 0; c < 5; ++c) s = s + xt[i][c] * v[c];
+    r[i] = s;
+  }
+}
+
+// r = X_{r->q} v (src/mo_gcbc.f90:552-591)
+__device__ __forceinline__ void r2q_apply(const Elem& e, const double cm[3], const double v[5], double r[5]) {
+  const double bo = e.hv2 + ((1.0 / KGAMM1) * e.ao) * e.ao;
+  const double co = e.ao * e.vn;
+  double dm[3];
+  for (int d = 0; d < 3; ++d) dm[d] = e.ao * cm[d];
+  const double* ve = e.ve;
+  double xt[5][5];
+  xt[0][0] = cm[0]; xt[0][1] = cm[1]; xt[0][2] = cm[2]; xt[0][3] = 0.5; xt[0][4] = 0.5;
+  xt[1][0] = cm[0] * ve[0]; xt[1][1] = cm[1] * ve[0] - dm[2]; xt[1][2] = cm[2] * ve[0] + dm[1];
+  xt[1][3] = 0.5 * (ve[0] + dm[0]); xt[1][4] = xt[1][3] - dm[0];
+  xt[2][0] = cm[0] * ve[1] + dm[2]; xt[2][1] = cm[1] * ve[1]; xt[2][2] = cm[2] * ve[1] - dm[0];
+  xt[2][3] = 0.5 * (ve[1] + dm[1]); xt[2][4] = xt[2][3] - dm[1];
+  xt[3][0] = cm[0] * ve[2] - dm[1]; xt[3][1] = cm[1] * ve[2] + dm[0]; xt[3][2] = cm[2] * ve[2];
+  xt[3][3] = 0.5 * (ve[2] + dm[2]); xt[3][4] = xt[3][3] - dm[2];
+  xt[4][0] = (e.hv2 * cm[0] + dm[2] * ve[1]) - dm[1] * ve[2];
+  xt[4][1] = (e.hv2 * cm[1] + dm[0] * ve[2]) - dm[2] * ve[0];
+  xt[4][2] = (e.hv2 * cm[2] + dm[1] * ve[0]) - dm[0] * ve[1];
+  xt[4][3] = 0.5 * (bo + co); xt[4][4] = xt[4][3] - co;
+  for (int i = 0; i < 5; ++i) {
+    double s = 0.0;
+    for (int c = 0; c < 5; ++c) s = s + xt[i][c] * v[c];
+    r[i] = s;
+  }
+}
+
+__global__ void k_gcbc_setup(const BlockDev* __restrict__ bd, const GcbcTask* __restrict__ tasks,
+                             const int* __restrict__ line0s, int ntasks, int nlines,
+                             const StageParams* __restrict__ sp) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
+    const GcbcTask& T = tasks[find_task(line0s, ntasks, g)];
+    const BlockDev& B = bd[T.b];
+    const StageParams S = sp[B.case_id];
+    const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
+    int x, y, z;
+    line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
+    const long long n = B.npad;
+    const long long l = ((long long)z * B.Y + y) * B.Xp + x;
+    const double cm[3] = {T.cm[jk], T.cm[T.nbs + jk], T.cm[2 * T.nbs + jk]};
+    const Elem e = eleme(cm, B.qa[l], B.qa[l + n], B.qa[l + 2 * n], B.qa[l + 3 * n], B.p[l], S.umf);
+    const double ra0 = (double)(((20 - T.bc) * (25 - T.bc) * (30 - T.bc)) / 3000);
+    const double ra1 = 1.0 - ra0;
+    double v[5], r[5];
+    for (int c = 0; c < 5; ++c) {
+      const double cha = ra0 * T.drva[(long long)c * T.nbs + jk] + ra1 * B.de[l + c * n];
+      v[c] = B.yaco[l] * cha;
+    }
+    q2r_apply(e, cm, v, r);
+    for (int c = 0; c < 5; ++c) T.drva[(long long)c * T.nbs + jk] = r[c];
+  }
+}
+
+__global__ void k_gcbc_update(const BlockDev* __restrict__ bd, const GcbcTask* __restrict__ tasks,
+                              const int* __restrict__ line0s, int ntasks, int nlines,
+                              const StageParams* __restrict__ sp) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
+    const GcbcTask& T = tasks[find_task(line0s, ntasks, g)];
+    const BlockDev& B = bd[T.b];
+    const StageParams S = sp[B.case_id];
+    const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
+    int x, y, z;
+    line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
+    const long long n = B.npad;
+    const long long l = ((long long)z * B.Y + y) * B.Xp + x;
+    const double cm[3] = {T.cm[jk], T.cm[T.nbs + jk], T.cm[2 * T.nbs + jk]};
+    const double q1 = B.qa[l];
+    const Elem e = eleme(cm, q1, B.qa[l + n], B.qa[l + 2 * n], B.qa[l + 3 * n], B.p[l], S.umf);
+    const double ra0 = 1 - 2 * T.side;
+    double cha[5], dha[5], drv[5];
+    for (int c = 0; c < 5; ++c) {
+      drv[c] = T.drva[(long long)c * T.nbs + jk];
+      cha[c] = drv[c];
+      dha[c] = T.drvb ? T.drvb[(long long)c * T.nbs + jk] : 0.0;
+    }
+    if (T.bc == 10) {
+      if (ra0 * ((e.vn + e.vs) + e.ao) > 0.0) cha[3] = 0.0;
+      if (ra0 * ((e.vn + e.vs) - e.ao) > 0.0) cha[4] = 0.0;
+    } else if (T.bc == 20 || T.bc == 25) {
+      const double dtwi = 1.0 / (4 * S.dt + 1.0e-8);
+      double sd = 0.0;
+      for (int d = 0; d < 3; ++d) sd = sd + cm[d] * S.dudtmf[d];
+      cha[3 + T.side] = cha[4 - T.side] + (((2.0 * ra0) * e.aoi) * q1) * (sd + dtwi * (e.vn + e.vs));
+    } else {
+      if (ra0 * (e.vn + e.vs) > 0.0) { cha[0] = dha[0]; cha[1] = dha[1]; cha[2] = dha[2]; }
+      if (ra0 * ((e.vn + e.vs) + e.ao) > 0.0) cha[3] = dha[3];
+      if (ra0 * ((e.vn + e.vs) - e.ao) > 0.0) cha[4] = dha[4];
+    }
+    double v[5];
+    for (int c = 0; c < 5; ++c) v[c] = cha[c] - drv[c];
+    r2q_apply(e, cm, v, dha);
+    for (int ii = 0; ii <= 4; ++ii) {
+      const long long pt = T.pts[(long long)jk * 5 + ii];
+      const double w = T.w[(long long)jk * 5 + ii];
+      for (int c = 0; c < 5; ++c) B.de[pt + c * n] = B.de[pt + c * n] + w * dha[c];
+    }
+  }
+}
+
+// sponge (src/mo_sponge.f90:265-278)
+struct SpongeTask { int b; const long long* pts; const double* asz; const double* bsz; int count, first; };
+__global__ void k_sponge(const BlockDev* __restrict__ bd, const SpongeTask* __restrict__ tasks,
+                         const int* __restrict__ first, int ntasks, int total) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const SpongeTask& T = tasks[find_task(first, ntasks, g)];
+    const BlockDev& B = bd[T.b];
+    const int e = g - T.first;
+    const long long l = T.pts[e], n = B.npad;
+    const double a = T.asz[e], bb = T.bsz[e];
+    B.de[l] = B.de[l] + a * (B.qa[l] - 1.0);
+    for (int d = 1; d <= 3; ++d) B.de[l + d * n] = B.de[l + d * n] + bb * (B.qa[l + d * n] - 0.0);
+    B.de[l + 4 * n] = B.de[l + 4 * n] + a * (B.qa[l + 4 * n] - (1.0 / kGam) * (1.0 / KGAMM1));
+  }
+}
+
+// junction / surface averaging: snapshot then ordered combination
+__global__ void k_avg_snapshot(const BlockDev* __restrict__ bd, const int* __restrict__ sb,
+                               const long long* __restrict__ sl, int nsrc, double* __restrict__ snap) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nsrc; e += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[sb[e]];
+    const long long l = sl[e];
+    for (int c = 0; c < 5; ++c) snap[(long long)e * 5 + c] = B.qa[l + c * B.npad];
+  }
+}
+// mode 0: sum and scale (average_point / average_line); mode 1: running
+// average of average_surface.
+__global__ void k_avg_combine(const BlockDev* __restrict__ bd, const int* __restrict__ tb,
+                              const long long* __restrict__ tl, const int* __restrict__ tfirst,
+                              const int* __restrict__ tcount, int ntg, const double* __restrict__ snap, int mode) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[tb[t]];
+    const long long l = tl[t];
+    const int f = tfirst[t], cnt = tcount[t];
+    for (int c = 0; c < 5; ++c) {
+      if (mode == 0) {
+        double acc = snap[(long long)f * 5 + c];
+        for (int j = 1; j < cnt; ++j) acc = acc + snap[(long long)(f + j) * 5 + c];
+        B.qa[l + c * B.npad] = (1.0 / (double)cnt) * acc;
+      } else {
+        double q = B.qa[l + c * B.npad];
+        double r1 = 1.0;
+        for (int j = 0; j < cnt; ++j) {
+          r1 = r1 + 1.0;
+          const double r2 = 1.0 / r1;
+          q = r2 * ((r1 - 1.0) * q + snap[(long long)(f + j) * 5 + c]) + 0.0 * q;
+        }
+        B.qa[l + c * B.npad] = q;
+      }
+    }
+  }
+}
+
+// drvb <- drva of the partner face (gcbc_comm, src/mo_gcbc.f90:186-220)
+__global__ void k_face_copy(const double* const* __restrict__ src, double* const* __restrict__ dst,
+                            const int* __restrict__ counts, int nfaces) {
+  const int f = blockIdx.y;
+  if (f >= nfaces) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < counts[f]; i += gridDim.x * blockDim.x)
+    dst[f][i] = src[f][i];
+}
+
+}  // namespace canard

@@ -1,0 +1,180 @@
+/*
+ * canard_gpu.h — C ABI of the B200 implementation of Canard's per-step hot path.
+ *
+ * The entry points replace the reference's Fortran type-bound procedures on the
+ * time-step path (EnricoDeg/Canard):
+ *   t_numerics%mpigo / deriv / filte        src/mo_numerics.f90:429-987
+ *   t_physics%calc_viscous_shear_stress     src/mo_physics.f90:216-301
+ *   t_physics%calc_fluxes                   src/mo_physics.f90:306-402
+ *   t_physics%calc_time_step                src/mo_physics.f90:171-211
+ *   gcbc_setup / gcbc_comm / gcbc_update     src/mo_gcbc.f90:133-340
+ *   average_surface                         src/mo_gcbc.f90:342-422
+ *   t_domdcomp%average_point / average_line src/mo_domdcomp.f90:439-559
+ *   spongego                                src/mo_sponge.f90:265-278
+ *   the time loop body (filter, RK stages)  src/mo_canard_driver.f90:226-431
+ * and the set-up they depend on (t_grid%grid_metrics src/mo_grid.f90:52-189,
+ * gcbc_init src/mo_gcbc.f90:40-131, spongeup src/mo_sponge.f90:224-261,
+ * search_point / search_line src/mo_domdcomp.f90:269-437, init_extra / init
+ * src/mo_numerics.f90:114-249).
+ *
+ * Conventions: all integers are int32_t (the reference's ni), all reals double
+ * (nr). Field arrays passed in or out are HOST pointers in the reference layout
+ * q(0:lmx, ncols), column-major, l = (k*(let+1)+j)*(lxi+1)+i. Every block is
+ * one sub-domain (the reference's nbpc = 1 per block). A context owns all device
+ * memory; it is single-stream and not thread-safe (one context per host
+ * thread), like the reference's t_numerics, which owns scratch lines.
+ *
+ * Every function returns CANARD_OK (0) or an error code; canard_last_error()
+ * gives the message. A failed call leaves the context usable unless the code is
+ * CANARD_ERR_CUDA.
+ */
+#ifndef CANARD_GPU_H
+#define CANARD_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CANARD_OK 0
+#define CANARD_ERR_ARG 1         /* bad argument (index, size, NULL) */
+#define CANARD_ERR_CUDA 2        /* CUDA runtime failure */
+#define CANARD_ERR_NAN 3         /* dt == 0 after step 2: the reference's "Canard: Overflow." */
+#define CANARD_ERR_TIMEOUT 4     /* a bounded device wait gave up */
+#define CANARD_ERR_UNSUPPORTED 5 /* configuration the path does not handle */
+#define CANARD_ERR_STATE 6       /* call order (e.g. step before setup) */
+
+#define CANARD_FP64 0            /* plain FP64 path */
+#define CANARD_FP32_MIXED 1      /* FP32 line solves/fluxes, FP64 state, RK, metrics, LU */
+
+typedef struct canard_ctx canard_ctx;
+
+/* One block: nml_domdcomp entries lximb/letmb/lzemb, nbbc, mbcd for block mb
+ * (src/mo_domdcomp.f90:232-267). nbc[d][s], mbcd[d][s]: direction d = xi, eta,
+ * zeta; side s = 0 (min), 1 (max). mbcd is the neighbour block within the same
+ * case, -1 for none. */
+typedef struct {
+  int32_t lxi, let, lze;
+  int32_t nbc[3][2];
+  int32_t mbcd[3][2];
+} canard_block_desc;
+
+/* One case: nml_numerics (fltk, fltrbc), nml_physics (reoo, tempoo, amach1..3,
+ * timf, nsmf), nml_canard (cfl), nml_sponge (szco) and the sponge geometry of
+ * nml_gridgen (szth0, szth1, doml0, doml1); viscous selects the reference's
+ * -DVISCOUS build. */
+typedef struct {
+  int32_t nblocks;
+  int32_t viscous;
+  double fltk, fltrbc;
+  double reoo, tempoo, amach1, amach2, amach3, timf;
+  int32_t nsmf;
+  double cfl;
+  double szco, szth0, szth1, doml0, doml1;
+} canard_case_desc;
+
+/* Field ids for canard_get_field / canard_set_field (ncols in brackets). */
+enum {
+  CANARD_F_QA = 0,    /* conserved state qa [5] */
+  CANARD_F_QO = 1,    /* RK stage start qo [5] */
+  CANARD_F_DE = 2,    /* de [5] */
+  CANARD_F_P = 3,     /* pressure [1] */
+  CANARD_F_SS1 = 4,   /* Sutherland viscosity ss(:,1) [1] */
+  CANARD_F_XIM = 5,   /* metrics [3] */
+  CANARD_F_ETM = 6,
+  CANARD_F_ZEM = 7,
+  CANARD_F_YACO = 8,  /* Jacobian [1] */
+  CANARD_F_TAU = 9,   /* txx tyy tzz txy tyz tzx hxx hyy hzz [9] */
+  CANARD_F_DRVA1 = 10, CANARD_F_DRVA2 = 11, CANARD_F_DRVA3 = 12, /* (nbsize,5,0:1) */
+  CANARD_F_CM1 = 13, CANARD_F_CM2 = 14, CANARD_F_CM3 = 15         /* (nbsize,3,0:1) */
+};
+
+/* Phase ids for canard_phase (one piece of src/mo_canard_driver.f90:234-371). */
+enum {
+  CANARD_PH_FILTER = 0,   /* mpigo + filte, 5 fields x 3 directions (:234-250) */
+  CANARD_PH_COPYQO = 1,   /* qo = qa (:252) */
+  CANARD_PH_PRIM = 2,     /* primitives, p, Sutherland (:267-275) */
+  CANARD_PH_TIMESTEP = 3, /* calc_time_step every 10th step + dt ramp (:278-294) */
+  CANARD_PH_VISCOUS = 4,  /* calc_viscous_shear_stress (:297) */
+  CANARD_PH_FLUXES = 5,   /* calc_fluxes (:301) */
+  CANARD_PH_GCBC = 6,     /* gcbc_setup + gcbc_comm + gcbc_update (:307-315) */
+  CANARD_PH_SPONGE = 7,   /* spongego (:321) */
+  CANARD_PH_RKUPDATE = 8, /* movef + RK update (:325-334) */
+  CANARD_PH_WALL = 9,     /* wall_condition_update (:342) */
+  CANARD_PH_AVERAGE = 10, /* average_point, average_line, average_surface (:347-355) */
+  CANARD_PH_ADVANCE = 11, /* n = n + 1, timo = timo + dt (:369-370) */
+  CANARD_PH_MOVEF_A = 12  /* movef before time advancing (:261-263) */
+};
+
+/* Context life cycle. blocks holds the blocks of all cases back to back
+ * (cases[0].nblocks entries first). Several cases make a batched context: the
+ * cases advance together, each with its own dt. */
+int canard_ctx_create(const canard_case_desc* cases, int32_t ncases,
+                      const canard_block_desc* blocks, int32_t precision,
+                      canard_ctx** out);
+void canard_ctx_destroy(canard_ctx* ctx);
+const char* canard_last_error(const canard_ctx* ctx);
+/* Run all device work of this context on the given cudaStream_t (NULL = the
+ * context's own stream). */
+int canard_set_stream(canard_ctx* ctx, void* cuda_stream);
+
+/* Grid, set-up, state. xyz is (0:lmx,3): x, y, z of every stored point
+ * (replaces read_grid_parallel, src/mo_io.f90:151-180). canard_setup runs
+ * grid_metrics on the device, then gcbc_init, the junction searches and
+ * spongeup; call it once after every block's grid is uploaded. */
+int canard_upload_grid(canard_ctx* ctx, int32_t icase, int32_t iblock, const double* xyz);
+int canard_setup(canard_ctx* ctx);
+int canard_set_state(canard_ctx* ctx, int32_t icase, int32_t iblock, const double* qa);
+int canard_get_state(canard_ctx* ctx, int32_t icase, int32_t iblock, double* qa);
+int canard_get_field(canard_ctx* ctx, int32_t icase, int32_t iblock, int32_t field,
+                     double* out, int64_t count);
+int canard_set_field(canard_ctx* ctx, int32_t icase, int32_t iblock, int32_t field,
+                     const double* in, int64_t count);
+
+/* Time loop. canard_step advances every case nsteps full steps (filter, 4 RK
+ * stages, junction averaging) with the reference's dt schedule; it returns
+ * CANARD_ERR_NAN where the reference's loop would stop with "Overflow."
+ * time6 = (n, ndt, dt, dts, dte, timo) of one case. */
+int canard_step(canard_ctx* ctx, int32_t nsteps);
+int canard_phase(canard_ctx* ctx, int32_t phase, int32_t nk);
+int canard_get_time(canard_ctx* ctx, int32_t icase, double* time6);
+int canard_set_time(canard_ctx* ctx, int32_t icase, const double* time6);
+
+/* Unit operations of t_numerics on host arrays, for case 0 (parity tests and
+ * drop-in calls). fields[b] = rfield(0:lmx, ncols) of block b. mpigo computes
+ * the interface contractions of every block face and exchanges them into the
+ * receive buffers of field m (src/mo_numerics.f90:429-705); deriv and filte
+ * then use them (src/mo_numerics.f90:709-987). deriv writes the line-end
+ * values into drva (read them with CANARD_F_DRVA*). in and out may alias. */
+int canard_mpigo(canard_ctx* ctx, const double* const* fields, int32_t ncols, int32_t nt,
+                 int32_t nrt, int32_t n45, int32_t itag, int32_t m);
+int canard_deriv(canard_ctx* ctx, int32_t iblock, const double* in, double* out,
+                 int32_t nn, int32_t m);
+int canard_filte(canard_ctx* ctx, int32_t iblock, double* f, int32_t inn, int32_t m);
+
+/* Host-only coefficient tables (no GPU needed), as used by the kernels:
+ * canard_coeffs writes pbci[nt][side][0:11], pbco[nt][side][0:11],
+ * pbcot[nt][side], alphf, betf, fa, fb, fc, albef[n][row][-2:2],
+ * fbc[row][0:4] (150 doubles; init_extracoeff_bounds, src/mo_numerics.f90:114-134).
+ * canard_penta writes the LU factors of one line of n points, xu (n,3) and
+ * xl (n,2) column-major (src/mo_numerics.f90:179-249). */
+int canard_coeffs(double fltk, double fltrbc, double* out150);
+int canard_penta(double fltk, double fltrbc, int32_t n, int32_t ns, int32_t ne, int32_t nt,
+                 double* xu, double* xl);
+int canard_version(void);
+
+/* Observability (the reference's mo_timer, src/mo_timer.f90:84-133, as CUDA
+ * events per kernel family). With timers on, every launch of the family is
+ * bracketed by events; canard_get_timers returns per family the accumulated
+ * device milliseconds, the number of launches and the algorithmic bytes moved
+ * (unique reads + writes of the launch's fields), and the number of families.
+ * canard_timer_name gives a family's name. canard_launch_count returns the
+ * number of kernel launches this context issued since it was created. */
+int canard_set_timers(canard_ctx* ctx, int32_t on);
+int canard_get_timers(canard_ctx* ctx, double* ms, double* launches, double* bytes, int32_t nmax);
+const char* canard_timer_name(int32_t family);
+int canard_launch_count(canard_ctx* ctx, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,195 @@
+"""GPU parity of the CUDA path against the CPU oracle, through the C ABI.
+
+FP64 kernels evaluate the reference's expressions in the reference's order
+without FMA contraction, so unit operations (mpigo, deriv, filte), the grid
+metrics and every phase are compared BIT FOR BIT. The only library power on
+the device, the Sutherland T^1.5, is correctly rounded on the GPU while the
+oracle calls glibc's pow; the two can differ by one ulp, so after the
+primitive phase the tests carry the oracle's viscosity over to stay bit exact,
+and whole-step runs use the tolerance of the specification: relative L2
+<= 1e-10 after 10 steps.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from canard_b200 import api, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def case_periodic():
+    return cases.tgv(nx=24, ny=20, nz=16)
+
+
+def case_nonperiodic():
+    # even and odd line lengths, non-reflecting xi/eta, periodic zeta
+    blk = cases.BlockSpec(23, 18, 16, [[10, 10], [10, 10], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
+    Z, Y, X = blk.shape
+    x = np.linspace(-1, 1, X)
+    y = np.linspace(-0.8, 0.9, Y)
+    z = np.linspace(0, 1, Z)
+    Zz, Yy, Xx = np.meshgrid(z, y, x, indexing="ij")
+    xyz = np.stack([Xx + 0.02 * np.sin(3 * Yy), Yy + 0.03 * np.sin(2 * Xx), Zz])
+    rho, u, v, w, p = cases.vortex_state(Xx, Yy, 0.3, 3.0, 0.3)
+    return cases.CaseSpec([blk], viscous=1, reoo=2000.0, xyz=[xyz], qa=[cases._conserved(rho, u, v, w, p)],
+                          name="np")
+
+
+def case_multiblock():
+    return cases.curvilinear_4block(24, 16, 14)
+
+
+CASES = {"periodic": case_periodic, "nonperiodic": case_nonperiodic, "multiblock": case_multiblock}
+
+
+def random_fields(cs, seed, ncols=1):
+    rng = np.random.default_rng(seed)
+    return [rng.standard_normal(ncols * b.npts) for b in cs.blocks]
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_unit_deriv_bit_exact(name):
+    cs = CASES[name]()
+    o = po.Oracle(cs, setup=False)
+    g = api.Context(cs, setup=False, upload_state=False)
+    for m in (1, 4):
+        f = random_fields(cs, 10 + m)
+        o.mpigo([x.copy() for x in f], 0, 1, 0, m, m)
+        g.mpigo([x.copy() for x in f], 0, 1, 0, m, m)
+        for b, blk in enumerate(cs.blocks):
+            for nn in (1, 2, 3):
+                a = np.zeros(blk.npts)
+                c = np.zeros(blk.npts)
+                o.deriv(b, f[b], a, nn, m)
+                g.deriv(b, f[b], c, nn, m)
+                np.testing.assert_array_equal(c, a, err_msg=f"{name} b={b} nn={nn} m={m}")
+                da = o.get(b, po.A_DRVA[nn - 1])
+                dg = g.field(api.F_DRVA[nn - 1], b)
+                np.testing.assert_array_equal(dg, da)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_unit_filter_chain_bit_exact(name):
+    cs = CASES[name]()
+    o = po.Oracle(cs, setup=False)
+    g = api.Context(cs, setup=False, upload_state=False)
+    fo = random_fields(cs, 7)
+    fg = [x.copy() for x in fo]
+    # the filter's third send component carries state from call to call
+    # (src/mo_numerics.f90:509), so run the reference's sequence of passes
+    for m in (1, 2, 3):
+        for inn in (1, 2, 3):
+            o.mpigo(fo, 1, 1, 0, 3 * (m - 1) + inn, m)
+            g.mpigo(fg, 1, 1, 0, 3 * (m - 1) + inn, m)
+            for b in range(len(cs.blocks)):
+                o.filte(b, fo[b], inn, m)
+                g.filte(b, fg[b], inn, m)
+                np.testing.assert_array_equal(fg[b], fo[b], err_msg=f"{name} m={m} inn={inn} b={b}")
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_grid_metrics_bit_exact(name):
+    cs = CASES[name]()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    for b, blk in enumerate(cs.blocks):
+        for fo, fg in ((po.A_XIM, api.F_XIM), (po.A_ETM, api.F_ETM), (po.A_ZEM, api.F_ZEM), (po.A_YACO, api.F_YACO)):
+            np.testing.assert_array_equal(g.field(fg, b).ravel(), o.get(b, fo), err_msg=f"{name} b={b} f={fg}")
+        for d in range(3):
+            np.testing.assert_array_equal(g.field(api.F_CM[d], b), o.get(b, po.A_CM[d]))
+
+
+PHASES = [
+    (api.PH_PRIM, "prim"), (api.PH_VISCOUS, "viscous"), (api.PH_FLUXES, "fluxes"), (api.PH_GCBC, "gcbc"),
+    (api.PH_SPONGE, "sponge"), (api.PH_RKUPDATE, "rk"), (api.PH_AVERAGE, "average"),
+]
+
+
+def compare_state(o, g, cs, what, exact=True, fields=(("qa", po.A_QA, api.F_QA), ("de", po.A_DE, api.F_DE))):
+    for b in range(len(cs.blocks)):
+        for label, fo, fg in fields:
+            a = o.get(b, fo)
+            c = g.field(fg, b).ravel()
+            if exact:
+                np.testing.assert_array_equal(c, a, err_msg=f"{what}: {label} block {b}")
+            else:
+                assert rel_l2(c, a) < 1e-13, (what, label, b, rel_l2(c, a))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_phases_bit_exact(name):
+    cs = CASES[name]()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    t6 = [5, 1, 2.0e-3, 1.5e-3, 2.5e-3, 0.31]
+    o.set_time(t6)
+    g.set_time(t6)
+    o.phase(po.PH_FILTER)
+    g.phase(api.PH_FILTER)
+    compare_state(o, g, cs, "filter", fields=(("qa", po.A_QA, api.F_QA),))
+    o.phase(po.PH_COPYQO)
+    g.phase(api.PH_COPYQO)
+    for nk in (1, 2):
+        o.phase(po.PH_MOVEF_A, nk)
+        for ph, label in PHASES:
+            o.phase(ph, nk)
+            g.phase(ph, nk)
+            if ph == api.PH_PRIM:
+                for b in range(len(cs.blocks)):
+                    np.testing.assert_array_equal(g.field(api.F_P, b).ravel(), o.get(b, po.A_P))
+                    mo, mg = o.get(b, po.A_SS1), g.field(api.F_SS1, b).ravel()
+                    assert np.max(np.abs(mg - mo) / np.abs(mo)) <= 2.3e-16, "Sutherland power beyond 1 ulp"
+                    g.set_field(api.F_SS1, mo.reshape(g.field(api.F_SS1, b).shape), b)
+            compare_state(o, g, cs, f"{label} nk={nk}")
+            if ph == api.PH_VISCOUS and cs.viscous:
+                for b in range(len(cs.blocks)):
+                    np.testing.assert_array_equal(g.field(api.F_TAU, b).ravel(), o.get(b, po.A_TAU))
+            if ph == api.PH_FLUXES:
+                for b in range(len(cs.blocks)):
+                    for d in range(3):
+                        np.testing.assert_array_equal(g.field(api.F_DRVA[d], b), o.get(b, po.A_DRVA[d]))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_steps_match_oracle(name):
+    cs = CASES[name]()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    o.step(12)
+    g.step(12)
+    np.testing.assert_array_equal(g.time()[:2], o.time()[:2])
+    assert abs(g.time()[2] - o.time()[2]) <= 1e-12 * abs(o.time()[2])
+    for b in range(len(cs.blocks)):
+        err = rel_l2(g.state(b), o.state(b))
+        assert err <= 1e-10, (name, b, err)
+
+
+def test_tgv64_ten_steps_within_1e_10():
+    """C1: 64^3 Taylor-Green vortex (65^3 stored points), Re 1600, Mach 0.1,
+    FP64, 10 steps: relative L2 <= 1e-10 per conserved variable."""
+    cs = cases.tgv(64)
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    o.step(10)
+    g.step(10)
+    qo, qg = o.state(0), g.state(0)
+    for v in range(5):
+        err = rel_l2(qg[v], qo[v])
+        assert err <= 1e-10, (v, err)
+
+
+def test_error_status_instead_of_fault():
+    cs = case_periodic()
+    g = api.Context(cs)
+    with pytest.raises(api.CanardError) as e:
+        g.phase(99, 1)
+    assert e.value.code == api.ERR_ARG
+    with pytest.raises(api.CanardError) as e:
+        g.deriv(5, np.zeros(10), np.zeros(10), 1, 1)
+    assert e.value.code == api.ERR_ARG
+    g.step(1)  # the context stays usable
