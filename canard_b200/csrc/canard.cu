@@ -36,18 +36,21 @@ struct ApiError : std::runtime_error {
       throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));                       \
   } while (0)
 
+// Allocation is set-up only. The zero fill is ordered on the context stream:
+// that stream is non-blocking, so a fill on the legacy default stream could
+// land after later uploads.
 template <class T>
-T* dalloc(size_t n) {
+T* dalloc(size_t n, cudaStream_t st) {
   void* p = nullptr;
   if (n == 0) n = 1;
   CK(cudaMalloc(&p, n * sizeof(T)));
-  CK(cudaMemset(p, 0, n * sizeof(T)));
+  CK(cudaMemsetAsync(p, 0, n * sizeof(T), st));
   return static_cast<T*>(p);
 }
 
 template <class T>
 T* dupload(const std::vector<T>& v, cudaStream_t st) {
-  T* p = dalloc<T>(v.size());
+  T* p = dalloc<T>(v.size(), st);
   if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return p;
 }
@@ -819,7 +822,7 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
     for (const auto& t : p.targets) { tb.push_back(t.b); tl.push_back(t.l); tf.push_back(t.first); tc.push_back(t.count); }
     A.tb = dupload(tb, c->st); A.tl = dupload(tl, c->st); A.tfirst = dupload(tf, c->st); A.tcount = dupload(tc, c->st);
     A.sb = dupload(p.src_b, c->st); A.sl = dupload(sl, c->st);
-    A.snap = dalloc<double>((size_t)A.nsrc * 5);
+    A.snap = dalloc<double>((size_t)A.nsrc * 5, c->st);
   };
   upload_avg(P, c->avg_pt);
   upload_avg(Lp, c->avg_ln);
@@ -1013,7 +1016,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
   std::vector<BlockDev> bdv;
   for (auto& B : c->blocks) {
     const BlockGeom& g = B.g;
-    B.arena = dalloc<double>((size_t)F_COUNT * g.npad);
+    B.arena = dalloc<double>((size_t)F_COUNT * g.npad, c->st);
     BlockDev& d = B.dev;
     d.X = g.X; d.Y = g.Y; d.Z = g.Z; d.Xp = g.Xp; d.npad = g.npad; d.case_id = g.case_id;
     d.qa = fptr(B, F_QA); d.qo = fptr(B, F_QO); d.de = fptr(B, F_DE); d.p = fptr(B, F_P); d.mu = fptr(B, F_MU);
@@ -1027,12 +1030,12 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         std::vector<double> lu((size_t)5 * L);
         sch.lu(L, n0, n1, nt, lu.data());
         B.lu[nt][dir] = dupload(lu, c->st);
-        B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs);
+        B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs, c->st);
       }
-      B.chain[dir] = dalloc<double>((size_t)2 * nbs);
-      B.drva[dir] = dalloc<double>((size_t)10 * nbs);
-      B.drvb[dir] = dalloc<double>((size_t)10 * nbs);
-      B.cm[dir] = dalloc<double>((size_t)6 * nbs);
+      B.chain[dir] = dalloc<double>((size_t)2 * nbs, c->st);
+      B.drva[dir] = dalloc<double>((size_t)10 * nbs, c->st);
+      B.drvb[dir] = dalloc<double>((size_t)10 * nbs, c->st);
+      B.cm[dir] = dalloc<double>((size_t)6 * nbs, c->st);
     }
     bdv.push_back(d);
   }
@@ -1051,12 +1054,12 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
   }
   c->dcc = dupload(ccv, c->st);
   const size_t nslots = 2 * 5 * c->cases.size();
-  c->dsp = dalloc<StageParams>(nslots);
+  c->dsp = dalloc<StageParams>(nslots, c->st);
   CK(cudaMallocHost(&c->hsp, nslots * sizeof(StageParams)));
   std::memset(c->hsp, 0, nslots * sizeof(StageParams));
-  c->ddt = dalloc<unsigned long long>(2 * c->cases.size());
+  c->ddt = dalloc<unsigned long long>(2 * c->cases.size(), c->st);
   CK(cudaMallocHost(&c->hdt, 2 * c->cases.size() * sizeof(unsigned long long)));
-  c->derr = dalloc<int>(1);
+  c->derr = dalloc<int>(1, c->st);
   for (auto& e : c->ring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (auto& e : c->ring_ev) CK(cudaEventRecord(e, c->st));
   set_line_smem_limits();

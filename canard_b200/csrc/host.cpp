@@ -513,6 +513,15 @@ std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan&
           Lp.targets.push_back(t);
         }
       }
+    // A block corner lies on three of its edges; the reference writes it once
+    // per edge in edge order, so the last edge's average is the one that stays.
+    // Keep only that target (the combine kernel then writes every point once).
+    std::map<std::pair<int, int64_t>, size_t> last;
+    for (size_t i = 0; i < Lp.targets.size(); ++i) last[{Lp.targets[i].b, Lp.targets[i].l}] = i;
+    std::vector<AvgTarget> kept;
+    for (size_t i = 0; i < Lp.targets.size(); ++i)
+      if (last[{Lp.targets[i].b, Lp.targets[i].l}] == i) kept.push_back(Lp.targets[i]);
+    Lp.targets.swap(kept);
   }
   return "";
 }
