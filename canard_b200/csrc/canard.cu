@@ -66,6 +66,7 @@ struct Table {
   int total = 0;  // tiles or lines
   size_t smem = 0;
   double bytes = 0;  // algorithmic bytes of one launch
+  CUtensorMap* maps = nullptr;  // line tables: TMA descriptors (in, out) per task
 };
 
 struct CaseState {
@@ -83,6 +84,8 @@ struct BlockState {
   double* arena = nullptr;
   BlockDev dev;  // host copy of the device descriptor
   double *lu[2][3] = {};       // [nt][dir]: 5 * L
+  double luc[2][3][5] = {};    // bitwise-constant interior factors
+  int luc0[2][3] = {};         // first row of the constant range [luc0, L-4]
   double *recv[2][3] = {};     // [nt][dir]: 5 fields x 2 sides x ncomp x nbs
   double* chain[3] = {};       // [dir]: 2 sides x nbs
   double* drva[3] = {};        // (nbs,5,0:1)
@@ -224,6 +227,30 @@ double valid_points(const canard_ctx* c) {
 
 double* fptr(const BlockState& b, int f) { return b.arena + (size_t)f * b.g.npad; }
 
+// A tile moves in nc chunks of cr positions: about 64 positions each (2..8
+// chunks), cr even (16-byte aligned bulk copies) and at most 256 (a TMA box),
+// and the last chunk keeps at least 12 positions so the end closures only
+// need the first and the last chunk.
+void chunking(int L, int& nc, int& cr) {
+  nc = std::max(1, std::min(kMaxChunks, L / 64));
+  for (;; --nc) {
+    cr = ((L + nc - 1) / nc + 1) / 2 * 2;
+    if (nc <= 2 || (L - (nc - 1) * cr >= 12 && cr >= 12)) break;
+  }
+  if (nc == 1) cr = (L + 1) / 2 * 2;
+}
+
+// xi lines (dir 0) move as one bulk copy per line: per-lane copy instructions
+// are costly enough that chunking them does not pay.
+void chunking_dir(int dir, int L, int& nc, int& cr) {
+  if (dir == 0) {
+    nc = 1;
+    cr = (L + 1) / 2 * 2;
+  } else {
+    chunking(L, nc, cr);
+  }
+}
+
 // ---- line task construction ----------------------------------------------------
 void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const double* in,
                     double* out, int m, bool with_drva, LineTask& t) {
@@ -231,6 +258,9 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.in = in;
   t.out = out;
   t.lu = B.lu[nt][dir];
+  t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
+  t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
+  t.c0 = B.luc0[nt][dir];
   t.recv = B.recv_ptr(nt, dir, m, 0);
   t.drva = with_drva ? B.drva[dir] : nullptr;
   t.sc = c->cases[g.case_id].dsch;
@@ -240,6 +270,7 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.m = m;
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
+  chunking_dir(dir, t.L, t.nbox, t.by);
   if (dir == 0) {
     t.ntx = 1;
     t.ntiles = (g.Y * g.Z + kLanes - 1) / kLanes;
@@ -251,7 +282,41 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
 
 size_t line_smem(int dir, int L) {
   if (dir == 0) return 128 + (size_t)kLanes * dir1_pitch(L) * sizeof(double);
-  return 128 + (size_t)L * kLanes * sizeof(double);
+  int nc, cr;
+  chunking(L, nc, cr);
+  return 128 + (size_t)nc * cr * kLanes * sizeof(double);
+}
+
+// cuTensorMapEncodeTiled from the driver, found at run time (the library does
+// not link libcuda, so it loads on machines without a GPU).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess) throw CudaError("cuTensorMapEncodeTiled not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 3-D map over a padded field (X, Y, Z) with box (32, by, 1) for eta lines or
+// (32, 1, by) for zeta lines.
+CUtensorMap field_map(const double* base, int X, int Y, int Z, int Xp, int dir, int by) {
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
+  cuuint64_t strides[2] = {(cuuint64_t)Xp * sizeof(double), (cuuint64_t)Xp * Y * sizeof(double)};
+  cuuint32_t box[3] = {(cuuint32_t)kLanes, (cuuint32_t)(dir == 1 ? by : 1), (cuuint32_t)(dir == 2 ? by : 1)};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
 }
 
 Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir, bool transient) {
@@ -271,9 +336,19 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
   T.smem = sm;
   T.tasks = dupload(v, c->st);
   T.first = dupload(first, c->st);
+  std::vector<CUtensorMap> maps(2 * v.size());
+  if (dir != 0)
+    for (size_t i = 0; i < v.size(); ++i) {
+      maps[2 * i] = field_map(v[i].in, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by);
+      maps[2 * i + 1] = field_map(v[i].out, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by);
+    }
+  else
+    std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  T.maps = dupload(maps, c->st);
   if (transient) {
     c->transient.push_back(T.tasks);
     c->transient.push_back(T.first);
+    c->transient.push_back(T.maps);
   }
   return T;
 }
@@ -304,7 +379,7 @@ template <int DIR, int OP>
 void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  k_line<DIR, OP><<<T.total, kLanes, T.smem, c->st>>>(T.tasks, T.first, T.ntasks, c->derr);
+  k_line<DIR, OP><<<T.total, kLanes, T.smem, c->st>>>(T.tasks, T.first, T.ntasks, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -946,6 +1021,9 @@ void destroy(canard_ctx* c) {
   for (auto& p : c->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   auto ft = [](auto& T) { cudaFree(T.tasks); cudaFree(T.first); };
+  auto fl = [](Table<LineTask>& T) { cudaFree(T.maps); };
+  for (int m = 0; m < 5; ++m) for (int i = 0; i < 3; ++i) fl(c->filt[m][i]);
+  for (int d = 0; d < 3; ++d) { fl(c->visc[d]); fl(c->flux[d]); }
   for (int m = 0; m < 5; ++m) for (int i = 0; i < 3; ++i) { ft(c->filt[m][i]); ft(c->mp_filt[m][i]); }
   for (int d = 0; d < 3; ++d) { ft(c->visc[d]); ft(c->flux[d]); }
   ft(c->mp_visc); ft(c->mp_flux); ft(c->gc_setup); ft(c->sponge);
@@ -1030,6 +1108,20 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         std::vector<double> lu((size_t)5 * L);
         sch.lu(L, n0, n1, nt, lu.data());
         B.lu[nt][dir] = dupload(lu, c->st);
+        // rows [i0, L-4] whose five factors are bit-identical to row L-4
+        const int e = L - 4;
+        int i0 = e + 1;
+        if (e >= 0) {
+          i0 = e;
+          auto same = [&](int r) {
+            for (int k = 0; k < 5; ++k)
+              if (std::memcmp(&lu[(size_t)k * L + r], &lu[(size_t)k * L + e], sizeof(double)) != 0) return false;
+            return true;
+          };
+          while (i0 - 1 >= 3 && same(i0 - 1)) --i0;
+          for (int k = 0; k < 5; ++k) B.luc[nt][dir][k] = lu[(size_t)k * L + e];
+        }
+        B.luc0[nt][dir] = i0;
         B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs, c->st);
       }
       B.chain[dir] = dalloc<double>((size_t)2 * nbs, c->st);

@@ -5,6 +5,7 @@
 // reproduce the CPU restatement bit for bit (the Sutherland power is the only
 // library function, see pow15).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -48,12 +49,15 @@ struct LineTask {
   const double* in;
   double* out;
   const double* lu;     // xl1, xl2, xu1, xu2, xu3 (each L entries)
+  double cl1, cl2, cu1, cu2, cu3;  // the factors of rows [c0, L-4], bitwise constant there
+  int c0;
   const double* recv;   // [side][comp][jk], comp stride nbs, side stride ncomp*nbs
   double* drva;         // drva(jk, m, side) of this block and direction, or null
   const DevScheme* sc;
   int X, Y, Z, Xp;
   int L, nbs, m, ndf0, ndf1;
   int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
+  int nbox, by;            // dir 2/3: TMA boxes per tile and rows per box
 };
 
 // Interface contraction of one face (t_numerics%mpigo): the sender's face
@@ -120,6 +124,19 @@ __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t by
                "r"(bytes)
                : "memory");
 }
+// TMA tile copies of a 3-D box (coordinates x, y, z in elements)
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -154,20 +171,217 @@ __device__ __forceinline__ double pow15(double x) {
 #define CA_A03 (1.333333333178555)
 #define CA_A04 (-0.0833333333455545)
 
+// The LU factors of the Toeplitz interior converge to a fixed point: rows
+// [c0, L-4] hold bitwise identical factors (found on the host), which the
+// sweeps keep in registers. Only the closure rows near the ends read the
+// factor tables, so the dependent chain carries no memory latency there.
+struct LuRows {
+  const double* __restrict__ l1;
+  const double* __restrict__ l2;
+  const double* __restrict__ u1;
+  const double* __restrict__ u2;
+  const double* __restrict__ u3;
+  double cl1, cl2, cu1, cu2, cu3;
+  int c0, c1;
+  __device__ __forceinline__ LuRows(const double* lu, int L, double a, double b, double c, double d, double e,
+                                    int c0_)
+      : l1(lu), l2(lu + L), u1(lu + 2 * L), u2(lu + 3 * L), u3(lu + 4 * L), cl1(a), cl2(b), cu1(c), cu2(d),
+        cu3(e), c0(c0_), c1(L - 4) {}
+};
+
+constexpr int kMaxChunks = 8;
+
+#ifdef CANARD_TRACE
+__device__ long long* g_trace;  // per CTA: start, loads issued, data ready, forward done, end, SM id
+#define TRACE(k) \
+  if (threadIdx.x == 0) g_trace[(long long)blockIdx.x * 8 + (k)] = clock64();
+#else
+#define TRACE(k)
+#endif
+
+// A tile arrives in NC chunks of CR positions (rows), chunk 0 and the last
+// chunk first (the closures read both ends), then 1, 2, ...; the forward
+// sweep waits for a chunk only when its look-ahead reaches it.
+struct ChunkIn {
+  uint64_t* bars;
+  int CR, NC, L;
+  int next;   // next middle chunk to wait for
+  int ready;  // rows [0, ready) and the last chunk have arrived
+  __device__ __forceinline__ bool wait_next(int* err) {
+    if (next >= NC - 1) { ready = L; return true; }
+    if (!mbar_wait(bars + next, 0)) { atomicExch(err, kErrTimeout); return false; }
+    ++next;
+    ready = (next >= NC - 1) ? L : next * CR;
+    return true;
+  }
+};
+
+// Factor providers: the interior constants or the per-row tables.
+struct CoefConst {
+  double l1, l2, u1, u2, u3;
+  __device__ __forceinline__ double L1(int) const { return l1; }
+  __device__ __forceinline__ double L2(int) const { return l2; }
+  __device__ __forceinline__ double U1(int) const { return u1; }
+  __device__ __forceinline__ double U2(int) const { return u2; }
+  __device__ __forceinline__ double U3(int) const { return u3; }
+};
+struct CoefTable {
+  const double* __restrict__ l1;
+  const double* __restrict__ l2;
+  const double* __restrict__ u1;
+  const double* __restrict__ u2;
+  const double* __restrict__ u3;
+  __device__ __forceinline__ double L1(int i) const { return __ldg(l1 + i); }
+  __device__ __forceinline__ double L2(int i) const { return __ldg(l2 + i); }
+  __device__ __forceinline__ double U1(int i) const { return __ldg(u1 + i); }
+  __device__ __forceinline__ double U2(int i) const { return __ldg(u2 + i); }
+  __device__ __forceinline__ double U3(int i) const { return __ldg(u3 + i); }
+};
+
+// Rows are processed in blocks of eight: the block's inputs, right-hand sides
+// and factors are all formed before its dependent chain, so their latency
+// overlaps the chain. Every row is still evaluated with the reference's
+// operations in the reference's order (bit-identical to one row at a time).
+
+// forward rows i..i+7 of the derivative; window w0..w3 = s[i-2..i+1]
+template <int ST, class CF>
+__device__ __forceinline__ void fwd8_deriv(double* __restrict__ s, int i, const CF& cf, double& w0, double& w1,
+                                           double& w2, double& w3, double& am2, double& am1) {
+  double win[12], l1[8], l2[8], r[8], a[8];
+  win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    win[4 + k] = s[(i + 2 + k) * ST];
+    l1[k] = cf.L1(i + k);
+    l2[k] = cf.L2(i + k);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = CA_AA * (win[k + 3] - win[k + 1]) + CA_AB * (win[k + 4] - win[k]);
+  a[0] = (r[0] - l1[0] * am2) - l2[0] * am1;
+  a[1] = (r[1] - l1[1] * am1) - l2[1] * a[0];
+#pragma unroll
+  for (int k = 2; k < 8; ++k) a[k] = (r[k] - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = a[k];
+  w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11];
+  am2 = a[6]; am1 = a[7];
+}
+
+// forward rows i..i+7 of the filter; window w0..w5 = s[i-3..i+2]
+template <int ST, class CF>
+__device__ __forceinline__ void fwd8_filter(double* __restrict__ s, int i, const CF& cf, double fa, double fb,
+                                            double fc, double& w0, double& w1, double& w2, double& w3,
+                                            double& w4, double& w5, double& am2, double& am1) {
+  double win[14], l1[8], l2[8], r[8], a[8];
+  win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3; win[4] = w4; win[5] = w5;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    win[6 + k] = s[(i + 3 + k) * ST];
+    l1[k] = cf.L1(i + k);
+    l2[k] = cf.L2(i + k);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double rk = win[k + 3] + win[k + 3];
+    r[k] = (fa * ((win[k + 2] + win[k + 4]) - rk) + fb * ((win[k + 1] + win[k + 5]) - rk)) +
+           fc * ((win[k] + win[k + 6]) - rk);
+  }
+  a[0] = (r[0] - l1[0] * am2) - l2[0] * am1;
+  a[1] = (r[1] - l1[1] * am1) - l2[1] * a[0];
+#pragma unroll
+  for (int k = 2; k < 8; ++k) a[k] = (r[k] - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = a[k];
+  w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11]; w4 = win[12]; w5 = win[13];
+  am2 = a[6]; am1 = a[7];
+}
+
+// back substitution rows i, i-1, ..., i-7
+template <int ST, class CF>
+__device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf, double& cp1, double& cp2) {
+  double p[8], u2[8], u3[8], c[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    p[k] = cf.U1(i - k) * s[(i - k) * ST];
+    u2[k] = cf.U2(i - k);
+    u3[k] = cf.U3(i - k);
+  }
+  c[0] = (p[0] - u2[0] * cp1) - u3[0] * cp2;
+  c[1] = (p[1] - u2[1] * c[0]) - u3[1] * cp1;
+#pragma unroll
+  for (int k = 2; k < 8; ++k) c[k] = (p[k] - u2[k] * c[k - 1]) - u3[k] * c[k - 2];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[(i - k) * ST] = c[k];
+  cp2 = c[6];
+  cp1 = c[7];
+}
+
+// Drives the forward rows [FIRST, LAST] with look-ahead LA: blocks of eight
+// where the look-ahead rows have arrived, single rows otherwise.
+#define FORWARD_ROWS(FIRST, LAST, LA, BLOCK8, STEP)                           \
+  {                                                                           \
+    const CoefConst CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                    \
+    const CoefTable CT{F.l1, F.l2, F.u1, F.u2, F.u3};                         \
+    int i = (FIRST);                                                          \
+    while (i <= (LAST)) {                                                     \
+      const int e = min((LAST), CI.ready - 1 - (LA));                         \
+      if (e < i) {                                                            \
+        if (!CI.wait_next(err)) return false;                                 \
+        continue;                                                             \
+      }                                                                       \
+      {                                                                       \
+        const int h = min(F.c0, e + 1);                                       \
+        for (; i + 7 < h; i += 8) BLOCK8(CT);                                 \
+        for (; i < h; ++i) STEP(CT.L1(i), CT.L2(i))                           \
+        const int ce = min(F.c1, e);                                          \
+        for (; i + 7 <= ce; i += 8) BLOCK8(CC);                               \
+        for (; i + 7 <= e; i += 8) BLOCK8(CT);                                \
+        for (; i <= e; ++i) STEP(CT.L1(i), CT.L2(i))                          \
+      }                                                                       \
+    }                                                                         \
+  }
+
+// Back substitution over rows N-2 .. 0; after the lowest row of chunk c the
+// chunk is final and DONE(c) runs (add the original, store it).
+#define BACKWARD_ROWS(DONE)                                                   \
+  {                                                                           \
+    const CoefConst CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                    \
+    const CoefTable CT{F.l1, F.l2, F.u1, F.u2, F.u3};                         \
+    double cp1 = CT.U1(N) * S(N);                                             \
+    S(N) = cp1;                                                               \
+    double c = CT.U1(N - 1) * S(N - 1) - CT.U2(N - 1) * cp1;                  \
+    S(N - 1) = c;                                                             \
+    double cp2 = cp1;                                                         \
+    cp1 = c;                                                                  \
+    int i = N - 2;                                                            \
+    for (int ch = CI.NC - 1; ch >= 0; --ch) {                                 \
+      const int lo = ch * CI.CR;                                              \
+      for (; i > F.c1 && i - 7 >= lo; i -= 8) bwd8<ST>(s, i, CT, cp1, cp2);   \
+      {                                                                       \
+        const int ce = max(F.c0, lo);                                         \
+        for (; i - 7 >= ce; i -= 8) bwd8<ST>(s, i, CC, cp1, cp2);             \
+      }                                                                       \
+      for (; i - 7 >= lo; i -= 8) bwd8<ST>(s, i, CT, cp1, cp2);               \
+      for (; i >= lo; --i) {                                                  \
+        c = (CT.U1(i) * S(i) - CT.U2(i) * cp1) - CT.U3(i) * cp2;              \
+        S(i) = c;                                                             \
+        cp2 = cp1;                                                            \
+        cp1 = c;                                                              \
+      }                                                                       \
+      DONE(ch);                                                               \
+    }                                                                         \
+  }
+
 // Compact first derivative of one line held in shared memory with element
 // stride ST (src/mo_numerics.f90:742-792). On return the line holds the
-// derivative; *d0 / *dN receive the end values.
-template <int ST>
-__device__ __forceinline__ void sweep_deriv(double* __restrict__ s, int L, const double* __restrict__ lu,
-                                            int ndf0, int ndf1, const DevScheme* __restrict__ sc, double r00,
-                                            double r10, double r01, double r11) {
+// derivative; Done(ch) is called as chunks become final. Returns false if a
+// bounded wait gave up.
+template <int ST, class Done>
+__device__ __forceinline__ bool sweep_deriv(double* __restrict__ s, int L, const LuRows& F, int ndf0, int ndf1,
+                                            const DevScheme* __restrict__ sc, double r00, double r10, double r01,
+                                            double r11, ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
   const int N = L - 1;
-  const double* l1 = lu;
-  const double* l2 = lu + L;
-  const double* u1 = lu + 2 * L;
-  const double* u2 = lu + 3 * L;
-  const double* u3 = lu + 4 * L;
   double b0, b1, bn1, bn;
   if (ndf0 == 0) {
     const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4);
@@ -199,56 +413,47 @@ __device__ __forceinline__ void sweep_deriv(double* __restrict__ s, int L, const
     bn = -t0 - r01;
     bn1 = -t1 - r11;
   }
-  // forward elimination, in place, originals kept in a register window
+  // forward elimination, in place; originals kept in a register window
   double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3);
   double am2 = b0;
-  double am1 = b1 - __ldg(l2 + 1) * am2;
+  double am1 = b1 - __ldg(F.l2 + 1) * am2;
   S(0) = am2;
   S(1) = am1;
-  for (int i = 2; i <= N - 2; ++i) {
-    const double w4 = S(i + 2);
-    const double rhs = CA_AA * (w3 - w1) + CA_AB * (w4 - w0);
-    const double a = (rhs - __ldg(l1 + i) * am2) - __ldg(l2 + i) * am1;
-    S(i) = a;
-    w0 = w1; w1 = w2; w2 = w3; w3 = w4;
-    am2 = am1; am1 = a;
+#define FWD(L1, L2)                                                 \
+  {                                                                 \
+    const double w4 = S(i + 2);                                     \
+    const double rhs = CA_AA * (w3 - w1) + CA_AB * (w4 - w0);       \
+    const double a = (rhs - (L1) * am2) - (L2) * am1;               \
+    S(i) = a;                                                       \
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4;                             \
+    am2 = am1; am1 = a;                                             \
   }
+#define BLOCK8(CF) fwd8_deriv<ST>(s, i, CF, w0, w1, w2, w3, am2, am1)
+  FORWARD_ROWS(2, N - 2, 2, BLOCK8, FWD)
+#undef BLOCK8
+#undef FWD
   {
-    const double a = (bn1 - __ldg(l1 + N - 1) * am2) - __ldg(l2 + N - 1) * am1;
+    const double a = (bn1 - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
     S(N - 1) = a;
     am2 = am1; am1 = a;
-    const double an = (bn - __ldg(l1 + N) * am2) - __ldg(l2 + N) * am1;
+    const double an = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
     S(N) = an;
   }
-  // back substitution
-  double cp1 = __ldg(u1 + N) * S(N);
-  S(N) = cp1;
-  double c = __ldg(u1 + N - 1) * S(N - 1) - __ldg(u2 + N - 1) * cp1;
-  S(N - 1) = c;
-  double cp2 = cp1;
-  cp1 = c;
-  for (int i = N - 2; i >= 0; --i) {
-    c = (__ldg(u1 + i) * S(i) - __ldg(u2 + i) * cp1) - __ldg(u3 + i) * cp2;
-    S(i) = c;
-    cp2 = cp1;
-    cp1 = c;
-  }
+  TRACE(3)
+  BACKWARD_ROWS(done)
 #undef S
+  return true;
 }
 
 // Compact filter increment of one line (src/mo_numerics.f90:922-977). On
-// return the line holds the increment (the caller adds the original field).
-template <int ST>
-__device__ __forceinline__ void sweep_filter(double* __restrict__ s, int L, const double* __restrict__ lu,
-                                             int ndf0, int ndf1, const DevScheme* __restrict__ sc, double r00,
-                                             double r10, double r20, double r01, double r11, double r21) {
+// return the line holds the increment; Done(ch) adds the original field.
+template <int ST, class Done>
+__device__ __forceinline__ bool sweep_filter(double* __restrict__ s, int L, const LuRows& F, int ndf0, int ndf1,
+                                             const DevScheme* __restrict__ sc, double r00, double r10, double r20,
+                                             double r01, double r11, double r21, ChunkIn& CI, int* err,
+                                             Done&& done) {
 #define S(i) s[(i)*ST]
   const int N = L - 1;
-  const double* l1 = lu;
-  const double* l2 = lu + L;
-  const double* u1 = lu + 2 * L;
-  const double* u2 = lu + 3 * L;
-  const double* u3 = lu + 4 * L;
   const double fa = sc->fa, fb = sc->fb, fc = sc->fc;
   double b0, b1, b2, bn2, bn1, bn;
   if (ndf0 == 0) {
@@ -298,46 +503,43 @@ __device__ __forceinline__ void sweep_filter(double* __restrict__ s, int L, cons
   // forward elimination: rows 0..2 from the closures, 3..N-3 interior
   double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3), w4 = S(4), w5 = S(5);  // s[i-3..i+2] at i = 3
   double am2 = b0;
-  double am1 = b1 - __ldg(l2 + 1) * am2;
-  double a2 = (b2 - __ldg(l1 + 2) * am2) - __ldg(l2 + 2) * am1;
+  double am1 = b1 - __ldg(F.l2 + 1) * am2;
+  double a2 = (b2 - __ldg(F.l1 + 2) * am2) - __ldg(F.l2 + 2) * am1;
   S(0) = am2;
   S(1) = am1;
   S(2) = a2;
   am2 = am1;
   am1 = a2;
-  for (int i = 3; i <= N - 3; ++i) {
-    const double w6 = S(i + 3);
-    const double rk = w3 + w3;
-    const double rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
-    const double a = (rhs - __ldg(l1 + i) * am2) - __ldg(l2 + i) * am1;
-    S(i) = a;
-    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
-    am2 = am1; am1 = a;
+#define FWD(L1, L2)                                                                                       \
+  {                                                                                                       \
+    const double w6 = S(i + 3);                                                                           \
+    const double rk = w3 + w3;                                                                            \
+    const double rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);           \
+    const double a = (rhs - (L1) * am2) - (L2) * am1;                                                     \
+    S(i) = a;                                                                                             \
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;                                                 \
+    am2 = am1; am1 = a;                                                                                   \
   }
+#define BLOCK8(CF) fwd8_filter<ST>(s, i, CF, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1)
+  FORWARD_ROWS(3, N - 3, 3, BLOCK8, FWD)
+#undef BLOCK8
+#undef FWD
   {
-    double a = (bn2 - __ldg(l1 + N - 2) * am2) - __ldg(l2 + N - 2) * am1;
+    double a = (bn2 - __ldg(F.l1 + N - 2) * am2) - __ldg(F.l2 + N - 2) * am1;
     S(N - 2) = a;
     am2 = am1; am1 = a;
-    a = (bn1 - __ldg(l1 + N - 1) * am2) - __ldg(l2 + N - 1) * am1;
+    a = (bn1 - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
     S(N - 1) = a;
     am2 = am1; am1 = a;
-    a = (bn - __ldg(l1 + N) * am2) - __ldg(l2 + N) * am1;
+    a = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
     S(N) = a;
   }
-  double cp1 = __ldg(u1 + N) * S(N);
-  S(N) = cp1;
-  double c = __ldg(u1 + N - 1) * S(N - 1) - __ldg(u2 + N - 1) * cp1;
-  S(N - 1) = c;
-  double cp2 = cp1;
-  cp1 = c;
-  for (int i = N - 2; i >= 0; --i) {
-    c = (__ldg(u1 + i) * S(i) - __ldg(u2 + i) * cp1) - __ldg(u3 + i) * cp2;
-    S(i) = c;
-    cp2 = cp1;
-    cp1 = c;
-  }
+  BACKWARD_ROWS(done)
 #undef S
+  return true;
 }
+#undef FORWARD_ROWS
+#undef BACKWARD_ROWS
 
 __device__ __forceinline__ int find_task(const int* __restrict__ tile0, int ntasks, int tile) {
   int lo = 0, hi = ntasks - 1;
@@ -358,20 +560,23 @@ __host__ __device__ __forceinline__ int dir1_pitch(int L) {
 }
 
 // One CTA = one warp = 32 lines. DIR: 1 xi, 2 eta, 3 zeta. OP: 0 derivative,
-// 1 filter (in place, f += increment).
+// 1 filter (in place, f += increment). The tile moves in chunks (see
+// ChunkIn): loads overlap the forward sweep, stores the back substitution.
 template <int DIR, int OP>
 __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
-                                             int ntasks, int* __restrict__ err) {
+                                             int ntasks, const CUtensorMap* __restrict__ maps,
+                                             int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
   double* s = reinterpret_cast<double*>(smem_raw + 128);
   const int lane = threadIdx.x;
+  TRACE(0)
   const int ti = find_task(tile0s, ntasks, blockIdx.x);
   const LineTask& T = tasks[ti];
   const int lt = blockIdx.x - T.tile0;
   const int L = T.L;
   const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
-  // tile geometry
+  const int NC = T.nbox, CR = T.by;
   int nval, x0 = 0, r0 = 0, fix = 0;  // fix: z for dir 2, y for dir 3
   if (DIR == 1) {
     r0 = lt * kLanes;
@@ -382,78 +587,143 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     nval = min(kLanes, X - x0);
   }
   const int P = dir1_pitch(L);
-  const uint32_t rowbytes = (DIR == 1) ? (uint32_t)((L + 1) / 2 * 2 * 8) : (uint32_t)((nval + 1) / 2 * 2 * 8);
   const long long pstride = (DIR == 2) ? (long long)Xp : (long long)Xp * Y;  // dir 2/3 position stride
   const long long base = (DIR == 1) ? (long long)r0 * Xp
                                     : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
-  if (lane == 0) mbar_init(bar, 1);
-  __syncwarp();
-  if (lane == 0) mbar_expect_tx(bar, (DIR == 1) ? rowbytes * nval : rowbytes * L);
-  __syncwarp();
-  if (DIR == 1) {
-    if (lane < nval) bulk_g2s(s + lane * P, T.in + base + (long long)lane * Xp, rowbytes, bar);
-  } else {
-    for (int i = lane; i < L; i += kLanes) bulk_g2s(s + i * kLanes, T.in + base + i * pstride, rowbytes, bar);
+  const CUtensorMap* map_in = maps + 2 * ti;
+  const CUtensorMap* map_out = maps + 2 * ti + 1;
+  auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
+  if (lane == 0) {
+    for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
   }
-  if (!mbar_wait(bar, 0)) {
+  __syncwarp();
+  // issue the loads: chunk 0, the last chunk, then the middle ones
+  for (int k = 0; k < NC; ++k) {
+    const int c = (k == 0) ? 0 : (k == 1 ? NC - 1 : k - 1);
+    if (DIR == 1) {
+      const uint32_t bytes = (uint32_t)((chunk_len(c) + 1) / 2 * 2 * sizeof(double));
+      if (lane == 0) mbar_expect_tx(bars + c, bytes * nval);
+      __syncwarp();
+      if (lane < nval)
+        bulk_g2s(s + lane * P + c * CR, T.in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
+    } else if (lane == 0) {
+      mbar_expect_tx(bars + c, (uint32_t)(CR * kLanes * sizeof(double)));
+      if (DIR == 2) tma_load_3d(s + c * CR * kLanes, map_in, x0, c * CR, fix, bars + c);
+      else tma_load_3d(s + c * CR * kLanes, map_in, x0, fix, c * CR, bars + c);
+    }
+  }
+  TRACE(1)
+  if (!mbar_wait(bars, 0) || !mbar_wait(bars + NC - 1, 0)) {
     if (lane == 0) atomicExch(err, kErrTimeout);
     return;
   }
-  if (lane < nval) {
-    int jk;
-    if (DIR == 1) jk = r0 + lane;
-    else if (DIR == 2) jk = (x0 + lane) * Z + fix;
-    else jk = fix * X + x0 + lane;
-    const int nbs = T.nbs;
-    constexpr int ST = (DIR == 1) ? 1 : kLanes;
-    double* sl = (DIR == 1) ? s + lane * P : s + lane;
-    if (OP == 0) {
-      double r00 = 0, r10 = 0, r01 = 0, r11 = 0;
-      if (T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; }
-      if (T.ndf1) { r01 = T.recv[2 * nbs + jk]; r11 = T.recv[3 * nbs + jk]; }
-      sweep_deriv<ST>(sl, L, T.lu, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11);
-      if (T.drva) {
-        T.drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
-        T.drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
-      }
-    } else {
-      double r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
-      if (T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; r20 = T.recv[2 * nbs + jk]; }
-      if (T.ndf1) { r01 = T.recv[3 * nbs + jk]; r11 = T.recv[4 * nbs + jk]; r21 = T.recv[5 * nbs + jk]; }
-      sweep_filter<ST>(sl, L, T.lu, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21);
+  TRACE(2)
+  ChunkIn CI{bars, CR, NC, L, 1, (NC > 1 ? CR : L)};
+  if (NC <= 2) CI.ready = L;
+#ifdef CANARD_TRACE_WAITALL
+  while (CI.ready < L) CI.wait_next(err);
+  TRACE(7)
+#endif
+  // chunk c is final: (filter) add the original, then store it
+  auto done = [&](int c) {
+    const int lo = c * CR, len = chunk_len(c);
+    if (OP == 1) {
       if (DIR != 1) {
-        // f = f + increment; the original re-read is coalesced across lanes
-        for (int i = 0; i < L; ++i) sl[i * ST] = T.in[base + i * pstride + lane] + sl[i * ST];
+        if (lane < nval) {
+          const double* g = T.in + base + lane;
+          double* col = s + lane;
+          int i = lo;
+          for (; i + 8 <= lo + len; i += 8) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
+          }
+          for (; i < lo + len; ++i) col[i * kLanes] = __ldg(g + (long long)i * pstride) + col[i * kLanes];
+        }
+      } else {
+        __syncwarp();
+        const int tot = nval * len;
+        int e = lane;
+        for (; e + 7 * kLanes < tot; e += 8 * kLanes) {
+          double v[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
+            v[k] = __ldg(T.in + base + (long long)r * Xp + i);
+          }
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
+            s[r * P + i] = v[k] + s[r * P + i];
+          }
+        }
+        for (; e < tot; e += kLanes) {
+          const int r = e / len, i = lo + e - r * len;
+          s[r * P + i] = __ldg(T.in + base + (long long)r * Xp + i) + s[r * P + i];
+        }
       }
     }
-  }
-  if (OP == 1 && DIR == 1) {
+    fence_proxy_async();
     __syncwarp();
-    for (int r = 0; r < nval; ++r) {
-      const double* g = T.in + base + (long long)r * Xp;
-      double* row = s + r * P;
-      for (int i = lane; i < L; i += kLanes) row[i] = g[i] + row[i];
-    }
-  }
-  fence_proxy_async();
-  __syncwarp();
-  if (DIR == 1) {
-    if (lane < nval) {
-      bulk_s2g(T.out + base + (long long)lane * Xp, s + lane * P, rowbytes);
+    if (DIR == 1) {
+      if (lane < nval) {
+        bulk_s2g(T.out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                 (uint32_t)((len + 1) / 2 * 2 * sizeof(double)));
+        bulk_commit();
+      }
+    } else if (lane == 0) {
+      // positions past the block edge (and x past X) are not written
+      if (DIR == 2) tma_store_3d(map_out, x0, lo, fix, s + lo * kLanes);
+      else tma_store_3d(map_out, x0, fix, lo, s + lo * kLanes);
       bulk_commit();
-      bulk_wait_read0();
+    }
+  };
+  bool ok = true;
+  // every lane runs the sweep (lanes past the tile edge on zero-filled or
+  // stale columns) so the chunk hand-offs stay warp-uniform; only lanes with a
+  // line read the receive buffers or write drva
+  const bool has = lane < nval;
+  int jk = 0;
+  if (DIR == 1) jk = r0 + lane;
+  else if (DIR == 2) jk = (x0 + lane) * Z + fix;
+  else jk = fix * X + x0 + lane;
+  const int nbs = T.nbs;
+  constexpr int ST = (DIR == 1) ? 1 : kLanes;
+  double* sl = (DIR == 1) ? s + lane * P : s + lane;
+  const LuRows F(T.lu, L, T.cl1, T.cl2, T.cu1, T.cu2, T.cu3, T.c0);
+  if (OP == 0) {
+    double r00 = 0, r10 = 0, r01 = 0, r11 = 0;
+    if (has && T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; }
+    if (has && T.ndf1) { r01 = T.recv[2 * nbs + jk]; r11 = T.recv[3 * nbs + jk]; }
+    ok = sweep_deriv<ST>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11, CI, err, done);
+    if (ok && has && T.drva) {
+      T.drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+      T.drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
     }
   } else {
-    bool any = false;
-    for (int i = lane; i < L; i += kLanes) {
-      bulk_s2g(T.out + base + i * pstride, s + i * kLanes, rowbytes);
-      any = true;
-    }
-    if (any) {
-      bulk_commit();
-      bulk_wait_read0();
-    }
+    double r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
+    if (has && T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; r20 = T.recv[2 * nbs + jk]; }
+    if (has && T.ndf1) { r01 = T.recv[3 * nbs + jk]; r11 = T.recv[4 * nbs + jk]; r21 = T.recv[5 * nbs + jk]; }
+    ok = sweep_filter<ST>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, CI, err, done);
   }
+  // every issued bulk store has to finish reading shared memory before exit;
+  // after a timeout, wait for the chunks still in flight (bounded) instead
+  if (!ok) {
+    for (int c = CI.next; c < NC - 1; ++c) mbar_wait(bars + c, 0);
+    return;
+  }
+  TRACE(4)
+  bulk_wait_read0();
+  TRACE(5)
+#ifdef CANARD_TRACE
+  if (threadIdx.x == 0) {
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    g_trace[(long long)blockIdx.x * 8 + 6] = smid;
+  }
+#endif
 }
 
 // ---------------------------------------------------------------------------
