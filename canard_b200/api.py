@@ -94,6 +94,8 @@ def lib():
         L.canard_timer_name.restype = ctypes.c_char_p
         L.canard_timer_name.argtypes = [i32]
         L.canard_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.canard_deriv_noalloc.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, ctypes.c_double,
+                                           ctypes.c_double, vp]
         L.canard_coeffs.argtypes = [ctypes.c_double, ctypes.c_double, _DP]
         L.canard_penta.argtypes = [ctypes.c_double, ctypes.c_double, i32, i32, i32, i32, _DP, _DP]
         _lib = L

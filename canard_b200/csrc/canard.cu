@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1459,3 +1460,197 @@ int canard_launch_count(canard_ctx* c, int64_t* count) {
 }
 
 }  // extern "C"
+
+// ==================================================================================
+// Compact derivative without device allocation.
+//
+// For callers that cannot allocate device memory on the step path: solvers that
+// own every device buffer themselves (a Fortran code whose arrays come from its
+// own OpenACC/CUDA-Fortran pool), code running under a memory budget that
+// forbids allocator calls between steps, or a host thread that must not block
+// in the allocator. The caller passes device input and output; the scratch the
+// derivative needs (task records, TMA descriptors, coefficients, LU factors and
+// the periodic contraction buffers) lives in one file-scope device array of
+// fixed size that every GPU loading this library holds until the process exits.
+namespace {
+constexpr int kNaMaxLines = 65536;   // lines of the direction (nbsize)
+constexpr int kNaMaxPoints = 1024;   // points per line
+constexpr size_t kNaTask = 0;        // LineTask
+constexpr size_t kNaFace = 512;      // up to 2 FaceTask
+constexpr size_t kNaIdx = 1536;      // tile0 (1 int), line0 (2 ints)
+constexpr size_t kNaErr = 1600;      // device error flag
+constexpr size_t kNaChain = 1608;    // unused third send component (2 doubles)
+constexpr size_t kNaMaps = 1664;     // 2 CUtensorMap, 64-byte aligned
+constexpr size_t kNaScheme = 2048;   // DevScheme
+constexpr size_t kNaLu = 4096;       // 5 x kNaMaxPoints doubles
+constexpr size_t kNaRecv = kNaLu + 5 * kNaMaxPoints * sizeof(double);  // 2 sides x 2 comps x lines
+constexpr size_t kNaBytes = kNaRecv + (size_t)4 * kNaMaxLines * sizeof(double);
+static_assert(sizeof(LineTask) <= kNaFace - kNaTask, "LineTask slot");
+static_assert(2 * sizeof(FaceTask) <= kNaIdx - kNaFace, "FaceTask slots");
+static_assert(sizeof(DevScheme) <= kNaLu - kNaScheme, "scheme slot");
+static_assert(kNaMaps % 64 == 0 && kNaLu % 256 == 0 && kNaRecv % 256 == 0, "alignment");
+}  // namespace
+
+// about 2.1 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+std::mutex g_na_mu;
+unsigned char* g_na_addr[256] = {};
+
+// Device address of the scratch array for the current device. The symbol's
+// host-side name is only a stand-in, so the address is looked up once per
+// device (with that device current) and cached.
+unsigned char* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  if (dev < 0 || dev >= 256) throw ApiError(CANARD_ERR_ARG, "device index out of range");
+  if (!g_na_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) throw CudaError(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    set_line_smem_limits();
+    g_na_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_na_addr[dev];
+}
+}  // namespace
+
+extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t lxi, int32_t let, int32_t lze,
+                                    int32_t pitch, int32_t nn, int32_t nbc0, int32_t nbc1, double fltk,
+                                    double fltrbc, void* stream) {
+  auto fail = [](int code, const char* msg) {
+    std::fprintf(stderr, "canard_deriv_noalloc: %s\n", msg);
+    return code;
+  };
+  if (!d_in || !d_out) return fail(CANARD_ERR_ARG, "null field pointer");
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15)
+    return fail(CANARD_ERR_ARG, "fields must be 16-byte aligned");
+  if (lxi < 12 || let < 12 || lze < 12) return fail(CANARD_ERR_ARG, "every direction needs at least 13 points");
+  if (pitch < lxi + 1 || pitch % 4 != 0) return fail(CANARD_ERR_ARG, "pitch must be >= lxi+1 and a multiple of 4");
+  if (nn < 1 || nn > 3) return fail(CANARD_ERR_ARG, "direction nn must be 1, 2 or 3");
+  auto closure_ok = [](int b) {
+    return b == BC_NR || b == BC_WALLI || b == BC_WALLV || b == BC_CURV || b == BC_PERIODIC;
+  };
+  if (!closure_ok(nbc0) || !closure_ok(nbc1))
+    return fail(CANARD_ERR_UNSUPPORTED, "end codes must be 10, 20, 25, 30 or 45 (periodic on the same line)");
+  if ((nbc0 == BC_PERIODIC) != (nbc1 == BC_PERIODIC))
+    return fail(CANARD_ERR_UNSUPPORTED, "a periodic line needs code 45 at both ends");
+  if (!(fltrbc > 0.0)) return fail(CANARD_ERR_ARG, "fltrbc must be positive");
+  const int dir = nn - 1;
+  canard_block_desc bd{};
+  bd.lxi = lxi; bd.let = let; bd.lze = lze;
+  for (int d = 0; d < 3; ++d)
+    for (int sd = 0; sd < 2; ++sd) { bd.nbc[d][sd] = BC_NR; bd.mbcd[d][sd] = -1; }
+  bd.nbc[dir][0] = nbc0; bd.nbc[dir][1] = nbc1;
+  if (nbc0 == BC_PERIODIC) { bd.mbcd[dir][0] = 0; bd.mbcd[dir][1] = 0; }
+  BlockGeom g;
+  make_geom(bd, 0, 0, g);
+  g.Xp = pitch;
+  g.npad = (int64_t)pitch * g.Y * g.Z;
+  const int L = g.ijk[0][dir] + 1, nbs = g.nbs[dir];
+  if (L > kNaMaxPoints) return fail(CANARD_ERR_ARG, "more than 1024 points per line");
+  if (nbs > kNaMaxLines) return fail(CANARD_ERR_ARG, "more than 65536 lines in this direction");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  try {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    unsigned char* base = noalloc_scratch(dev);
+    Scheme sch;
+    sch.build(fltk, fltrbc);
+    const int n0 = nbc0 == BC_PERIODIC ? 1 : 0, n1 = n0;
+    std::vector<double> lu((size_t)5 * L);
+    sch.lu(L, n0, n1, 0, lu.data());
+    LineTask t{};
+    t.in = d_in;
+    t.out = d_out;
+    t.lu = reinterpret_cast<const double*>(base + kNaLu);
+    {  // bitwise-constant interior rows, as for the context path
+      const int e = L - 4;
+      int i0 = e;
+      auto same = [&](int r) {
+        for (int k = 0; k < 5; ++k)
+          if (std::memcmp(&lu[(size_t)k * L + r], &lu[(size_t)k * L + e], sizeof(double)) != 0) return false;
+        return true;
+      };
+      while (i0 - 1 >= 3 && same(i0 - 1)) --i0;
+      t.cl1 = lu[e]; t.cl2 = lu[(size_t)L + e]; t.cu1 = lu[(size_t)2 * L + e];
+      t.cu2 = lu[(size_t)3 * L + e]; t.cu3 = lu[(size_t)4 * L + e];
+      t.c0 = i0;
+    }
+    t.recv = reinterpret_cast<const double*>(base + kNaRecv);
+    t.drva = nullptr;
+    t.sc = reinterpret_cast<const DevScheme*>(base + kNaScheme);
+    t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp;
+    t.L = L; t.nbs = nbs; t.m = 1; t.ndf0 = n0; t.ndf1 = n1;
+    chunking_dir(dir, L, t.nbox, t.by);
+    if (dir == 0) {
+      t.ntx = 1;
+      t.ntiles = (g.Y * g.Z + kLanes - 1) / kLanes;
+    } else {
+      t.ntx = (g.X + kLanes - 1) / kLanes;
+      t.ntiles = t.ntx * (dir == 1 ? g.Z : g.Y);
+    }
+    t.tile0 = 0;
+    // periodic on the line itself: each end's contraction feeds the other end
+    FaceTask f[2];
+    int nf = 0;
+    if (n0) {
+      for (int sb = 0; sb < 2; ++sb) {
+        FaceTask& q = f[nf];
+        q = FaceTask{};
+        q.src = d_in;
+        q.dstf = d_in;
+        q.recv = reinterpret_cast<double*>(base + kNaRecv) + (size_t)(1 - sb) * 2 * nbs;
+        q.chain = reinterpret_cast<double*>(base + kNaChain);
+        q.sc = t.sc;
+        q.nn = nn; q.sb = sb; q.nt = 0; q.exch = 1; q.corr = 0; q.iik = 1; q.ra0k = 0.0;
+        q.X = g.X; q.Y = g.Y; q.Z = g.Z; q.Xp = g.Xp; q.N = L - 1;
+        q.XA = g.X; q.YA = g.Y; q.ZA = g.Z; q.XpA = g.Xp; q.NA = L - 1;
+        q.nbs = nbs; q.nj = g.ijk[1][dir] + 1; q.line0 = nf * nbs;
+        ++nf;
+      }
+    }
+    DevScheme ds{};
+    std::memcpy(ds.pbci, sch.pbci, sizeof(ds.pbci));
+    std::memcpy(ds.pbco, sch.pbco, sizeof(ds.pbco));
+    std::memcpy(ds.pbcot, sch.pbcot, sizeof(ds.pbcot));
+    ds.fa = sch.fa; ds.fb = sch.fb; ds.fc = sch.fc;
+    std::memcpy(ds.fbc, sch.fbc, sizeof(ds.fbc));
+    CUtensorMap maps[2];
+    std::memset(maps, 0, sizeof(maps));
+    if (dir != 0) {
+      maps[0] = field_map(d_in, g.X, g.Y, g.Z, g.Xp, dir, t.by);
+      maps[1] = field_map(d_out, g.X, g.Y, g.Z, g.Xp, dir, t.by);
+    }
+    const int idx[3] = {0, 0, nbs};
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, &t, sizeof(t), kNaTask, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, f, sizeof(f), kNaFace, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, idx, sizeof(idx), kNaIdx, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, maps, sizeof(maps), kNaMaps, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, &ds, sizeof(ds), kNaScheme, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, lu.data(), lu.size() * sizeof(double), kNaLu,
+                               cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(base + kNaErr, 0, sizeof(int), st));
+    if (nf) {
+      const int tot = nf * nbs;
+      k_mpigo<<<std::max(1, std::min((tot + 127) / 128, 148 * 16)), 128, 0, st>>>(
+          reinterpret_cast<const FaceTask*>(base + kNaFace), reinterpret_cast<const int*>(base + kNaIdx) + 1, nf,
+          tot);
+      CK(cudaGetLastError());
+    }
+    const size_t smem = line_smem(dir, L);
+    const LineTask* dt = reinterpret_cast<const LineTask*>(base + kNaTask);
+    const int* d0 = reinterpret_cast<const int*>(base + kNaIdx);
+    const CUtensorMap* dm = reinterpret_cast<const CUtensorMap*>(base + kNaMaps);
+    int* de = reinterpret_cast<int*>(base + kNaErr);
+    if (dir == 0) k_line<1, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
+    else if (dir == 1) k_line<2, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
+    else k_line<3, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
+    CK(cudaGetLastError());
+  } catch (const ApiError& e) {
+    return fail(e.code, e.what());
+  } catch (const std::exception& e) {
+    return fail(CANARD_ERR_CUDA, e.what());
+  }
+  return CANARD_OK;
+}

@@ -174,6 +174,31 @@ int canard_get_timers(canard_ctx* ctx, double* ms, double* launches, double* byt
 const char* canard_timer_name(int32_t family);
 int canard_launch_count(canard_ctx* ctx, int64_t* count);
 
+/* Compact first derivative without device allocation. This entry point has no
+ * counterpart in the reference. It serves callers that cannot allocate device
+ * memory: solvers that own every device buffer themselves, code under a memory
+ * budget that forbids allocator calls between steps, and host threads that
+ * must not block in the allocator. It computes what canard_mpigo + canard_deriv
+ * compute for one block, on DEVICE arrays, enqueued on `stream`:
+ *   d_in, d_out   device fields, element (i,j,k) at (k*(let+1)+j)*pitch + i,
+ *                 16-byte aligned, pitch >= lxi+1 and a multiple of 4; in may
+ *                 equal out; pad columns of out may be overwritten
+ *   nn            direction (1 xi, 2 eta, 3 zeta)
+ *   nbc0, nbc1    end closures: 10/20/25/30 one-sided, 45 periodic on the line
+ *                 itself (both ends)
+ *   fltk, fltrbc  nml_numerics values (fix the interface coefficients)
+ * Limits: at most 1024 points per line and 65536 lines in the direction;
+ * larger sizes return CANARD_ERR_ARG. The scratch is one static device array
+ * of about 2.1 MiB that every GPU loading the library holds until the process
+ * exits. Every call reuses it and leaves its last contents there, so calls
+ * that overlap on the GPU (on different streams) race. The first call on a
+ * device looks up the array's device address with that device current and
+ * caches it; make that first call before any stream capture. No cudaMalloc,
+ * cudaFree or other allocating routine is called. */
+int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t lxi, int32_t let, int32_t lze,
+                         int32_t pitch, int32_t nn, int32_t nbc0, int32_t nbc1, double fltk,
+                         double fltrbc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
