@@ -44,6 +44,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=256, help="cells per direction of the TGV block")
+    p.add_argument("--config", default="tgv", choices=["tgv", "batched", "curv4", "vortex"],
+                   help="tgv: single TGV block (default); batched: 64 independent cases with sides "
+                        "in 32..96; curv4: 4-block curvilinear grid with GCBC and sponge; vortex: "
+                        "isentropic vortex through a GCBC outflow")
     p.add_argument("--cpu-n", type=int, default=128, help="cells per direction of the CPU sample")
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=3)
@@ -171,11 +175,32 @@ def main():
 
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
-    cs = cases.tgv(args.n)
-    ctx = api.Context(cs)
+    if args.config == "tgv":
+        case_list = [cases.tgv(args.n)]
+        workload = (f"tgv{args.n}: Taylor-Green vortex {args.n}^3 cells ({args.n + 1}^3 points), Re 1600, "
+                    "Mach 0.1, viscous, FP64 plain, full time step")
+    elif args.config == "batched":
+        from canard_b200 import shard
+        all_cases = cases.batched(64, seed=11)
+        mine = shard.my_cases([c.npts for c in all_cases], world, rank)
+        case_list = [all_cases[i] for i in mine]
+        workload = ("batched: 64 independent single-block cases (sides 32..96, TGV / periodic vortex, "
+                    "Mach 0.1-0.5, Re 400-3200), FP64, one launch per phase and direction for all cases"
+                    + (f", sharded over {world} ranks by point count" if world > 1 else ""))
+    elif args.config == "curv4":
+        case_list = [cases.curvilinear_4block()]
+        workload = "curv4: 4 blocks of 192x128x64 cells, curvilinear, GCBC in/outflow, sponge, Re 1e5, FP64"
+    else:
+        case_list = [cases.vortex()]
+        workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
+    ctx = api.Context(case_list)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    npts = cs.npts
+    npts = sum(c.npts for c in case_list)
+    if args.config == "batched":
+        job_points, scaling = sum(c.npts for c in all_cases), "strong"
+    else:
+        job_points, scaling = world * npts, "weak"
 
     def barrier():
         if dist is not None:
@@ -200,7 +225,7 @@ def main():
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * npts * args.steps / (ms / 1e3) / 1e6
+    value = job_points * args.steps / (ms / 1e3) / 1e6
 
     # per-family device time (the reference's timers as CUDA events), one step
     ctx.set_timers(True)
@@ -228,9 +253,12 @@ def main():
                 "all_line_solves_gbs": lb / (lms / 1e3) / 1e9}
 
     # end to end through the C ABI: pinned host state in and out every step
-    qh = torch.empty((5,) + cs.blocks[0].shape, dtype=torch.float64, pin_memory=True)
-    qh.copy_(torch.from_numpy(ctx.state(0)))
-    qn = qh.numpy()
+    hosts = []
+    for ci, c in enumerate(case_list):
+        for bi, b in enumerate(c.blocks):
+            qh = torch.empty((5,) + b.shape, dtype=torch.float64, pin_memory=True)
+            qh.copy_(torch.from_numpy(ctx.state(bi, ci)))
+            hosts.append((ci, bi, qh, qh.numpy()))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -238,9 +266,11 @@ def main():
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(args.e2e_steps):
-        ctx.set_state(0, qn)
+        for ci, bi, _, qn in hosts:
+            ctx.set_state(bi, qn, ci)
         ctx.step(1)
-        ctx.get_state_into(0, qn)
+        for ci, bi, _, qn in hosts:
+            ctx.get_state_into(bi, qn, ci)
     f1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -249,8 +279,9 @@ def main():
         t = torch.tensor([ems], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ems = float(t.item())
-    e2e = {"value": world * npts * args.e2e_steps / (ems / 1e3) / 1e6, "unit": "Mpoint-steps/s",
-           "h2d_bytes_per_step": int(qh.numel() * 8), "d2h_bytes_per_step": int(qh.numel() * 8),
+    e2e = {"value": job_points * args.e2e_steps / (ems / 1e3) / 1e6, "unit": "Mpoint-steps/s",
+           "h2d_bytes_per_step": int(sum(h[2].numel() for h in hosts) * 8),
+           "d2h_bytes_per_step": int(sum(h[2].numel() for h in hosts) * 8),
            "steps": args.e2e_steps}
 
     cpu = None
@@ -263,14 +294,13 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded Taylor-Green vortex initial condition)",
-                "config": {"workload": f"tgv{args.n}: Taylor-Green vortex {args.n}^3 cells ({args.n + 1}^3 points),"
-                                       " Re 1600, Mach 0.1, viscous, FP64 plain, full time step",
-                           "points": npts, "precision": "fp64",
+                "scaling": scaling, "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
+                "config": {"workload": workload, "cases": len(case_list), "points": job_points, "precision": "fp64",
                            "l2": "inputs larger than L2 (state, metrics and work fields ~"
                                  f"{54 * 8 * npts / 1e9:.1f} GB resident)",
-                           "parallelism": "replicas" if world > 1 else "single"},
+                           "parallelism": ("case shards" if args.config == "batched" else "replicas")
+                           if world > 1 else "single"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks,
                 "families": {k: {"ms_per_step": v["ms"], "share": v["ms"] / tot if tot else 0.0,

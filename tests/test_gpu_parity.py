@@ -193,3 +193,22 @@ def test_error_status_instead_of_fault():
         g.deriv(5, np.zeros(10), np.zeros(10), 1, 1)
     assert e.value.code == api.ERR_ARG
     g.step(1)  # the context stays usable
+
+
+def test_batched_context_equals_single_cases():
+    """Independent cases advanced together in one context (one launch per phase
+    and direction for all cases, per-case dt) give exactly the single-case
+    results."""
+    cs_list = cases.batched(3, seed=5, lo=20, hi=30)
+    g = api.Context(cs_list)
+    g.step(12)
+    for i, cs in enumerate(cs_list):
+        one = api.Context(cs)
+        one.step(12)
+        np.testing.assert_array_equal(g.state(0, case=i), one.state(0))
+        np.testing.assert_array_equal(g.time(case=i), one.time())
+        one.close()
+    # and the oracle agrees for one of them
+    o = po.Oracle(cs_list[1])
+    o.step(12)
+    assert rel_l2(g.state(0, case=1), o.state(0)) <= 1e-10
