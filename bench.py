@@ -48,6 +48,9 @@ def parse():
                    help="tgv: single TGV block (default); batched: 64 independent cases with sides "
                         "in 32..96; curv4: 4-block curvilinear grid with GCBC and sponge; vortex: "
                         "isentropic vortex through a GCBC outflow")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                   help="fp64: plain FP64 path (bit-exact with the oracle); fp32: FP32 line solves, fluxes, "
+                        "viscous stresses and GCBC with the FP64 state, RK update, metrics and LU factors")
     p.add_argument("--cpu-n", type=int, default=128, help="cells per direction of the CPU sample")
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=3)
@@ -193,7 +196,10 @@ def main():
     else:
         case_list = [cases.vortex()]
         workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
-    ctx = api.Context(case_list)
+    prec = api.FP32_MIXED if args.precision == "fp32" else api.FP64
+    ctx = api.Context(case_list, precision=prec)
+    if args.precision == "fp32":
+        workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     npts = sum(c.npts for c in case_list)
@@ -294,11 +300,12 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": scaling, "vs_baseline": None, "dtype": "f64",
+                "scaling": scaling, "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
-                "config": {"workload": workload, "cases": len(case_list), "points": job_points, "precision": "fp64",
+                "config": {"workload": workload, "cases": len(case_list), "points": job_points, "precision": args.precision,
                            "l2": "inputs larger than L2 (state, metrics and work fields ~"
-                                 f"{54 * 8 * npts / 1e9:.1f} GB resident)",
+                                 f"{(54 * 8 + (41 * 4 if args.precision == 'fp32' else 0)) * npts / 1e9:.1f} GB "
+                                 "resident)",
                            "parallelism": ("case shards" if args.config == "batched" else "replicas")
                            if world > 1 else "single"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),

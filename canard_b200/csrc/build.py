@@ -1,7 +1,9 @@
 """Builds libcanard_b200.so in-tree with nvcc for sm_100a.
 
-FP64 kernels are compiled with -fmad=false (no multiply-add contraction) so
-they keep the reference's rounding order; host code with -ffp-contract=off.
+Three objects: the FP64 unit (canard.cu) with -fmad=false, so its kernels keep
+the reference's rounding order; the FP32 mixed-precision kernels
+(kernels_f32.cu) with multiply-add contraction; host set-up code (host.cpp)
+with -ffp-contract=off. Objects go to csrc/_build.
 """
 import os
 import subprocess
@@ -11,8 +13,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libcanard_b200.so")
-SOURCES = ["canard.cu", "host.cpp"]
-DEPS = SOURCES + ["kernels.cuh", "host.h"]
+BUILD = os.path.join(HERE, "_build")
+# (source, FMA contraction allowed)
+UNITS = [("canard.cu", False), ("kernels_f32.cu", True), ("host.cpp", False)]
+DEPS = [u for u, _ in UNITS] + ["kernels.cuh", "kernels_f32.h", "kernels_setup.cuh", "host.h"]
 
 
 def nvcc():
@@ -29,19 +33,29 @@ def needs_build():
     return any(os.path.getmtime(p) > t for p in paths)
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, defines=()):
     if not force and not needs_build():
         return OUT
     hostcxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-    cmd = [nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
-           "-ccbin", hostcxx,
-           "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
-           "-I", os.path.join(ROOT, "include"), "-I", HERE,
-           "-o", OUT] + [os.path.join(HERE, f) for f in SOURCES] + ["-lcudart"]
+    os.makedirs(BUILD, exist_ok=True)
+    common = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-ccbin", hostcxx,
+              "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+              "-I", os.path.join(ROOT, "include"), "-I", HERE] + ["-D" + d for d in defines]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+    objs, procs = [], []
+    for src, fma in UNITS:
+        obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+        cmd = common + ["-fmad=true" if fma else "-fmad=false", "-c", os.path.join(HERE, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    link = [nvcc(), "-shared", "-ccbin", hostcxx, "-gencode", "arch=compute_100a,code=sm_100a", "-o", OUT] + objs + ["-lcudart"]
+    subprocess.run(link, check=True)
     return OUT
 
 

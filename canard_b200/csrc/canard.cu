@@ -17,6 +17,8 @@
 #include "canard_gpu.h"
 #include "host.h"
 #include "kernels.cuh"
+#include "kernels_f32.h"
+#include "kernels_setup.cuh"
 
 using namespace canard;
 
@@ -68,7 +70,12 @@ struct Table {
   size_t smem = 0;
   double bytes = 0;  // algorithmic bytes of one launch
   CUtensorMap* maps = nullptr;  // line tables: TMA descriptors (in, out) per task
+  int kind = 0;  // line tables: a LineKind; face tables: 0 FP64 fields, 1 FP32 fields
 };
+
+// Element types of a line launch: tile (field) type and elimination type.
+enum LineKind { LK_F64 = 0, LK_F32 = 1, LK_F64_TILE_F32_SOLVE = 2 };
+inline size_t tile_elem(int kind) { return kind == LK_F32 ? sizeof(float) : sizeof(double); }
 
 struct CaseState {
   canard_case_desc d;
@@ -99,15 +106,27 @@ struct BlockState {
   double *sp_a = nullptr, *sp_b = nullptr;
   int sp_n = 0;
   std::vector<double> xyz_host;  // reference layout, kept for the sponge set-up
+  // mixed precision: FP32 work fields, factors and line-end buffers
+  float* arena32 = nullptr;
+  float* lu32[2][3] = {};
+  float* recv32[3] = {};  // derivative receive buffers of the FP32 fields
+  float* drva32[3] = {};
+  float* drvb32[3] = {};
   double* recv_ptr(int nt, int dir, int m, int side) const {
     const int nc = nt == 0 ? 2 : 3;
     return recv[nt][dir] + ((size_t)(m - 1) * 2 + side) * nc * g.nbs[dir];
+  }
+  float* recv32_ptr(int dir, int m, int side) const {
+    return recv32[dir] + ((size_t)(m - 1) * 2 + side) * 2 * g.nbs[dir];
   }
 };
 
 // field offsets inside a block arena (in units of npad)
 enum { F_QA = 0, F_QO = 5, F_DE = 10, F_P = 15, F_MU = 16, F_XIM = 17, F_ETM = 20, F_ZEM = 23, F_YACO = 26,
        F_TAU = 27, F_SCR = 36, F_XYZ = 51, F_COUNT = 54 };
+// FP32 field offsets inside the mixed-precision arena (in units of npad)
+enum { G_DE = 0, G_P = 5, G_MU = 6, G_TAU = 7, G_SCR = 16, G_XIM = 31, G_ETM = 34, G_ZEM = 37, G_YACO = 40,
+       G_COUNT = 41 };
 
 enum TimerFamily {
   T_DERIV_XI = 0, T_DERIV_ETA, T_DERIV_ZETA, T_FILTER_XI, T_FILTER_ETA, T_FILTER_ZETA, T_MPIGO, T_PRIM,
@@ -129,6 +148,7 @@ struct AvgDev {
 struct canard_ctx {
   std::string err;
   int precision = CANARD_FP64;
+  bool f32() const { return precision == CANARD_FP32_MIXED; }
   cudaStream_t own = nullptr, st = nullptr;
   std::vector<CaseState> cases;
   std::vector<BlockState> blocks;
@@ -147,9 +167,8 @@ struct canard_ctx {
   Table<LineTask> filt[5][3], visc[3], flux[3];
   Table<FaceTask> mp_filt[5][3], mp_visc, mp_flux;
   Table<GcbcTask> gc_setup, gc_upd[3][2];
-  std::vector<const double*> fc_src_h;
-  double** fc_src = nullptr;
-  double** fc_dst = nullptr;
+  void** fc_src = nullptr;
+  void** fc_dst = nullptr;
   int* fc_cnt = nullptr;
   int fc_n = 0, fc_max = 0;
   Table<SpongeTask> sponge;
@@ -227,6 +246,7 @@ double valid_points(const canard_ctx* c) {
 }
 
 double* fptr(const BlockState& b, int f) { return b.arena + (size_t)f * b.g.npad; }
+float* gptr(const BlockState& b, int f) { return b.arena32 + (size_t)f * b.g.npad; }
 
 // A tile moves in nc chunks of cr positions: about 64 positions each (2..8
 // chunks), cr even (16-byte aligned bulk copies) and at most 256 (a TMA box),
@@ -253,17 +273,18 @@ void chunking_dir(int dir, int L, int& nc, int& cr) {
 }
 
 // ---- line task construction ----------------------------------------------------
-void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const double* in,
-                    double* out, int m, bool with_drva, LineTask& t) {
+void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const void* in,
+                    void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64) {
   const BlockGeom& g = B.g;
   t.in = in;
   t.out = out;
-  t.lu = B.lu[nt][dir];
+  t.lu = (kind == LK_F64) ? static_cast<const void*>(B.lu[nt][dir]) : static_cast<const void*>(B.lu32[nt][dir]);
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
   t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
   t.c0 = B.luc0[nt][dir];
-  t.recv = B.recv_ptr(nt, dir, m, 0);
-  t.drva = with_drva ? B.drva[dir] : nullptr;
+  t.recv = (kind == LK_F32) ? static_cast<const void*>(B.recv32_ptr(dir, m, 0))
+                            : static_cast<const void*>(B.recv_ptr(nt, dir, m, 0));
+  t.drva = !with_drva ? nullptr : (kind == LK_F32 ? static_cast<void*>(B.drva32[dir]) : static_cast<void*>(B.drva[dir]));
   t.sc = c->cases[g.case_id].dsch;
   t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp;
   t.L = g.ijk[0][dir] + 1;
@@ -281,11 +302,14 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   }
 }
 
-size_t line_smem(int dir, int L) {
-  if (dir == 0) return 128 + (size_t)kLanes * dir1_pitch(L) * sizeof(double);
+size_t line_smem(int dir, int L, int kind = LK_F64) {
+  const size_t es = tile_elem(kind);
+  if (dir == 0) {
+    return 128 + (size_t)kLanes * (kind == LK_F32 ? dir1_pitch<float>(L) : dir1_pitch<double>(L)) * es;
+  }
   int nc, cr;
   chunking(L, nc, cr);
-  return 128 + (size_t)nc * cr * kLanes * sizeof(double);
+  return 128 + (size_t)nc * cr * kLanes * es;
 }
 
 // cuTensorMapEncodeTiled from the driver, found at run time (the library does
@@ -307,21 +331,25 @@ EncodeTiledFn encode_fn() {
 
 // 3-D map over a padded field (X, Y, Z) with box (32, by, 1) for eta lines or
 // (32, 1, by) for zeta lines.
-CUtensorMap field_map(const double* base, int X, int Y, int Z, int Xp, int dir, int by) {
+CUtensorMap field_map(const void* base, int X, int Y, int Z, int Xp, int dir, int by, size_t es = sizeof(double)) {
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
-  cuuint64_t strides[2] = {(cuuint64_t)Xp * sizeof(double), (cuuint64_t)Xp * Y * sizeof(double)};
+  cuuint64_t strides[2] = {(cuuint64_t)Xp * es, (cuuint64_t)Xp * Y * es};
   cuuint32_t box[3] = {(cuuint32_t)kLanes, (cuuint32_t)(dir == 1 ? by : 1), (cuuint32_t)(dir == 2 ? by : 1)};
-  cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType ty = es == sizeof(float) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  CUresult r = encode_fn()(&m, ty, 3, const_cast<void*>(base), dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return m;
 }
 
-Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir, bool transient) {
+Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir, bool transient,
+                                int kind = LK_F64) {
   Table<LineTask> T;
+  T.kind = kind;
+  const size_t es = tile_elem(kind);
   std::vector<int> first;
   int tot = 0;
   size_t sm = 0;
@@ -329,8 +357,8 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
     t.tile0 = tot;
     first.push_back(tot);
     tot += t.ntiles;
-    sm = std::max(sm, line_smem(dir, t.L));
-    T.bytes += 2.0 * sizeof(double) * t.X * t.Y * t.Z;  // read the field, write the result
+    sm = std::max(sm, line_smem(dir, t.L, kind));
+    T.bytes += 2.0 * es * t.X * t.Y * t.Z;  // read the field, write the result
   }
   T.ntasks = (int)v.size();
   T.total = tot;
@@ -340,8 +368,8 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
   std::vector<CUtensorMap> maps(2 * v.size());
   if (dir != 0)
     for (size_t i = 0; i < v.size(); ++i) {
-      maps[2 * i] = field_map(v[i].in, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by);
-      maps[2 * i + 1] = field_map(v[i].out, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by);
+      maps[2 * i] = field_map(v[i].in, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es);
+      maps[2 * i + 1] = field_map(v[i].out, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es);
     }
   else
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
@@ -376,23 +404,31 @@ Table<T> make_lines_table(canard_ctx* c, std::vector<T> v, bool transient, int T
   return Tb;
 }
 
-template <int DIR, int OP>
+template <int DIR, int OP, class TT, class RS>
 void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  k_line<DIR, OP><<<T.total, kLanes, T.smem, c->st>>>(T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
   CK(cudaGetLastError());
+}
+
+template <int DIR, int OP>
+void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.kind == LK_F64) launch_line_dir<DIR, OP, double, double>(c, T);
+  else if (OP == 0 && T.kind == LK_F32) launch_line_dir<DIR, 0, float, float>(c, T);
+  else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line_dir<DIR, 1, double, float>(c, T);
+  else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
 void launch_line(canard_ctx* c, const Table<LineTask>& T, int dir, int op) {
   if (op == 0) {
-    if (dir == 0) launch_line_dir<1, 0>(c, T);
-    else if (dir == 1) launch_line_dir<2, 0>(c, T);
-    else launch_line_dir<3, 0>(c, T);
+    if (dir == 0) launch_line_kind<1, 0>(c, T);
+    else if (dir == 1) launch_line_kind<2, 0>(c, T);
+    else launch_line_kind<3, 0>(c, T);
   } else {
-    if (dir == 0) launch_line_dir<1, 1>(c, T);
-    else if (dir == 1) launch_line_dir<2, 1>(c, T);
-    else launch_line_dir<3, 1>(c, T);
+    if (dir == 0) launch_line_kind<1, 1>(c, T);
+    else if (dir == 1) launch_line_kind<2, 1>(c, T);
+    else launch_line_kind<3, 1>(c, T);
   }
 }
 
@@ -400,12 +436,18 @@ void set_line_smem_limits() {
   static bool done = false;
   if (done) return;
   const int lim = 227 * 1024;
-  CK(cudaFuncSetAttribute(k_line<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  CK(cudaFuncSetAttribute(k_line<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  CK(cudaFuncSetAttribute(k_line<3, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  CK(cudaFuncSetAttribute(k_line<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  CK(cudaFuncSetAttribute(k_line<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  CK(cudaFuncSetAttribute(k_line<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+  CK((line_smem_limit<1, 0, double, double>(lim)));
+  CK((line_smem_limit<2, 0, double, double>(lim)));
+  CK((line_smem_limit<3, 0, double, double>(lim)));
+  CK((line_smem_limit<1, 1, double, double>(lim)));
+  CK((line_smem_limit<2, 1, double, double>(lim)));
+  CK((line_smem_limit<3, 1, double, double>(lim)));
+  CK((line_smem_limit<1, 0, float, float>(lim)));
+  CK((line_smem_limit<2, 0, float, float>(lim)));
+  CK((line_smem_limit<3, 0, float, float>(lim)));
+  CK((line_smem_limit<1, 1, double, float>(lim)));
+  CK((line_smem_limit<2, 1, double, float>(lim)));
+  CK((line_smem_limit<3, 1, double, float>(lim)));
   done = true;
 }
 
@@ -414,7 +456,7 @@ void set_line_smem_limits() {
 // gives the field column the block uses for that direction.
 template <class ColFn>
 std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, int exch_dir, ColFn col,
-                                 int only_case = -1) {
+                                 int only_case = -1, bool f32 = false) {
   std::vector<FaceTask> out;
   int line0 = 0;
   for (const FaceLink& L : c->links) {
@@ -426,7 +468,8 @@ std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, in
     FaceTask t{};
     t.src = col(L.src_b, d);
     t.dstf = col(L.dst_b, d);
-    t.recv = R.recv_ptr(nt, d, m, L.dst_side);
+    t.recv = f32 ? static_cast<void*>(R.recv32_ptr(d, m, L.dst_side))
+                 : static_cast<void*>(R.recv_ptr(nt, d, m, L.dst_side));
     t.chain = S.chain[d] + (size_t)L.src_side * S.g.nbs[d];
     t.sc = c->cases[S.g.case_id].dsch;
     t.nn = d + 1;
@@ -448,14 +491,15 @@ std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, in
   return out;
 }
 
-Table<FaceTask> make_face_table(canard_ctx* c, std::vector<FaceTask> v, bool transient) {
+Table<FaceTask> make_face_table(canard_ctx* c, std::vector<FaceTask> v, bool transient, int kind = 0) {
   Table<FaceTask> T;
+  T.kind = kind;
   std::vector<int> first;
   int tot = 0;
   for (auto& t : v) { t.line0 = tot; first.push_back(tot); tot += t.nbs; }
   T.ntasks = (int)v.size();
   T.total = tot;
-  T.bytes = (double)tot * (12 + (v.empty() ? 0 : (v[0].nt ? 3 : 2))) * sizeof(double);
+  T.bytes = (double)tot * (12 + (v.empty() ? 0 : (v[0].nt ? 3 : 2))) * (kind ? sizeof(float) : sizeof(double));
   T.tasks = dupload(v, c->st);
   T.first = dupload(first, c->st);
   if (transient) { c->transient.push_back(T.tasks); c->transient.push_back(T.first); }
@@ -467,7 +511,8 @@ void launch_mpigo(canard_ctx* c, const Table<FaceTask>& T) {
   const int thr = 128;
   const int grid = std::min((T.total + thr - 1) / thr, 148 * 16);
   Timed tm(c, T_MPIGO, T.bytes);
-  k_mpigo<<<grid, thr, 0, c->st>>>(T.tasks, T.first, T.ntasks, T.total);
+  if (T.kind) launch_mpigo_t<float>(grid, c->st, T.tasks, T.first, T.ntasks, T.total);
+  else launch_mpigo_t<double>(grid, c->st, T.tasks, T.first, T.ntasks, T.total);
   CK(cudaGetLastError());
 }
 
@@ -560,43 +605,86 @@ void ph_copyqo(canard_ctx* c) {
   CK(cudaGetLastError());
 }
 
+// Algorithmic bytes per point of an element-wise kernel: n64 FP64 values and
+// nr values of the flux type.
+double ew_bytes(const canard_ctx* c, int n64, int nr) {
+  return (8.0 * n64 + (c->f32() ? 4.0 : 8.0) * nr) * valid_points(c);
+}
+
 void ph_prim(canard_ctx* c) {
-  Timed tm(c, T_PRIM, 96.0 * valid_points(c));
-  k_prim<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, c->dcc);
+  Timed tm(c, T_PRIM, ew_bytes(c, 5, 7));
+  if (c->f32()) launch_prim<float>(ew_grid(c), c->st, c->dbd, c->dcc);
+  else launch_prim<double>(ew_grid(c), c->st, c->dbd, c->dcc);
   CK(cudaGetLastError());
 }
 
-void ph_viscous(canard_ctx* c) {
-  bool any = false;
-  for (auto& cs : c->cases) any = any || cs.d.viscous;
-  if (!any) return;
-  {
-    Timed tm(c, T_COPY, 16.0 * valid_points(c));
-    k_copy_mu<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
-    CK(cudaGetLastError());
-  }
+bool any_viscous(const canard_ctx* c) {
+  for (auto& cs : c->cases)
+    if (cs.d.viscous) return true;
+  return false;
+}
+
+// interface contraction and the 12 derivative sweeps of u, v, w, T
+void viscous_gradients(canard_ctx* c) {
   launch_mpigo(c, c->mp_visc);
   launch_line(c, c->visc[2], 2, 0);
   launch_line(c, c->visc[1], 1, 0);
   launch_line(c, c->visc[0], 0, 0);
-  Timed tm(c, T_VISCASM, 8.0 * (12 + 9 + 1 + 4 + 9 + 1) * valid_points(c));
-  k_viscous_assemble<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
-  CK(cudaGetLastError());
 }
 
-void ph_fluxes(canard_ctx* c, const StageParams* sp) {
-  {
-    Timed tm(c, T_FLUXCOMP, 8.0 * (5 + 1 + 3 + 9 + 9 + 15 + 1) * valid_points(c));
-    k_flux<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, sp, c->dcc);
-    CK(cudaGetLastError());
-  }
+// flux interface contraction, the 15 derivative sweeps and their sum into de
+void flux_derivatives(canard_ctx* c) {
   launch_mpigo(c, c->mp_flux);
   launch_line(c, c->flux[0], 0, 0);
   launch_line(c, c->flux[1], 1, 0);
   launch_line(c, c->flux[2], 2, 0);
-  Timed tm(c, T_FLUXSUM, 8.0 * 20 * valid_points(c));
-  k_flux_sum<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+  Timed tm(c, T_FLUXSUM, ew_bytes(c, 0, 20));
+  if (c->f32()) launch_flux_sum<float>(ew_grid(c), c->st, c->dbd);
+  else launch_flux_sum<double>(ew_grid(c), c->st, c->dbd);
   CK(cudaGetLastError());
+}
+
+// calc_viscous_shear_stress as the phase of the C ABI (tau stored)
+void ph_viscous(canard_ctx* c) {
+  if (!any_viscous(c)) return;
+  {
+    Timed tm(c, T_COPY, ew_bytes(c, 0, 2));
+    if (c->f32()) launch_copy_mu<float>(ew_grid(c), c->st, c->dbd);
+    else launch_copy_mu<double>(ew_grid(c), c->st, c->dbd);
+    CK(cudaGetLastError());
+  }
+  viscous_gradients(c);
+  Timed tm(c, T_VISCASM, ew_bytes(c, 0, 12 + 9 + 1 + 4 + 9 + 1));
+  if (c->f32()) launch_viscous_assemble<float>(ew_grid(c), c->st, c->dbd);
+  else launch_viscous_assemble<double>(ew_grid(c), c->st, c->dbd);
+  CK(cudaGetLastError());
+}
+
+// calc_fluxes as the phase of the C ABI (reads the stored tau)
+void ph_fluxes(canard_ctx* c, const StageParams* sp) {
+  {
+    Timed tm(c, T_FLUXCOMP, ew_bytes(c, 5, 1 + 3 + 9 + 9 + 15 + 1));
+    if (c->f32()) launch_flux<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
+    else launch_flux<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
+    CK(cudaGetLastError());
+  }
+  flux_derivatives(c);
+}
+
+// The step path: viscous stresses formed inside the flux kernel (no tau
+// round trip, no ss copy into de(:,1)); bit-identical to ph_viscous + ph_fluxes.
+void ph_visc_fluxes(canard_ctx* c, const StageParams* sp) {
+  const bool visc = any_viscous(c);
+  if (visc) viscous_gradients(c);
+  {
+    // reads: qa 5 (FP64); p, u, v, w, metrics 9, and if viscous 12 gradients, ss, yaco;
+    // writes: 15 flux components, de(:,5)
+    Timed tm(c, T_FLUXCOMP, ew_bytes(c, 5, 1 + 3 + 9 + (visc ? 12 + 1 + 1 : 0) + 15 + 1));
+    if (c->f32()) launch_flux_visc<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
+    else launch_flux_visc<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
+    CK(cudaGetLastError());
+  }
+  flux_derivatives(c);
 }
 
 void ph_gcbc(canard_ctx* c, const StageParams* sp) {
@@ -604,22 +692,29 @@ void ph_gcbc(canard_ctx* c, const StageParams* sp) {
   const int thr = 128;
   auto grid = [](int n) { return std::max(1, std::min((n + 127) / 128, 148 * 8)); };
   Timed tm(c, T_GCBC, 0.0);
-  k_gcbc_setup<<<grid(c->gc_setup.total), thr, 0, c->st>>>(c->dbd, c->gc_setup.tasks, c->gc_setup.first,
-                                                           c->gc_setup.ntasks, c->gc_setup.total, sp);
+  (void)thr;
+  if (c->f32())
+    launch_gcbc_setup<float>(grid(c->gc_setup.total), c->st, c->dbd, c->gc_setup.tasks, c->gc_setup.first,
+                             c->gc_setup.ntasks, c->gc_setup.total, sp);
+  else
+    launch_gcbc_setup<double>(grid(c->gc_setup.total), c->st, c->dbd, c->gc_setup.tasks, c->gc_setup.first,
+                              c->gc_setup.ntasks, c->gc_setup.total, sp);
   CK(cudaGetLastError());
   for (int d = 0; d < 3; ++d)
     for (int s = 0; s < 2; ++s) c->launches += c->gc_upd[d][s].ntasks > 0 ? 1 : 0;
   if (c->fc_n > 0) {
     c->launches += 1;
-    k_face_copy<<<dim3(std::max(1, std::min((c->fc_max + 255) / 256, 1024)), c->fc_n), 256, 0, c->st>>>(
-        c->fc_src, c->fc_dst, c->fc_cnt, c->fc_n);
+    const dim3 g(std::max(1, std::min((c->fc_max + 255) / 256, 1024)), c->fc_n);
+    if (c->f32()) launch_face_copy<float>(g, c->st, c->fc_src, c->fc_dst, c->fc_cnt, c->fc_n);
+    else launch_face_copy<double>(g, c->st, c->fc_src, c->fc_dst, c->fc_cnt, c->fc_n);
     CK(cudaGetLastError());
   }
   for (int d = 0; d < 3; ++d)
     for (int s = 0; s < 2; ++s) {
       const auto& T = c->gc_upd[d][s];
       if (T.ntasks == 0) continue;
-      k_gcbc_update<<<grid(T.total), thr, 0, c->st>>>(c->dbd, T.tasks, T.first, T.ntasks, T.total, sp);
+      if (c->f32()) launch_gcbc_update<float>(grid(T.total), c->st, c->dbd, T.tasks, T.first, T.ntasks, T.total, sp);
+      else launch_gcbc_update<double>(grid(T.total), c->st, c->dbd, T.tasks, T.first, T.ntasks, T.total, sp);
       CK(cudaGetLastError());
     }
 }
@@ -628,13 +723,17 @@ void ph_sponge(canard_ctx* c) {
   if (c->sponge.ntasks == 0 || c->sponge.total == 0) return;
   const int grid = std::max(1, std::min((c->sponge.total + 255) / 256, 148 * 8));
   Timed tm(c, T_SPONGE, 8.0 * 22 * c->sponge.total);
-  k_sponge<<<grid, 256, 0, c->st>>>(c->dbd, c->sponge.tasks, c->sponge.first, c->sponge.ntasks, c->sponge.total);
+  if (c->f32())
+    launch_sponge<float>(grid, c->st, c->dbd, c->sponge.tasks, c->sponge.first, c->sponge.ntasks, c->sponge.total);
+  else
+    launch_sponge<double>(grid, c->st, c->dbd, c->sponge.tasks, c->sponge.first, c->sponge.ntasks, c->sponge.total);
   CK(cudaGetLastError());
 }
 
 void ph_rk(canard_ctx* c, const StageParams* sp) {
-  Timed tm(c, T_RK, 8.0 * 16 * valid_points(c));
-  k_rk<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, sp);
+  Timed tm(c, T_RK, ew_bytes(c, 11, 5));
+  if (c->f32()) launch_rk<float>(ew_grid(c), c->st, c->dbd, sp);
+  else launch_rk<double>(ew_grid(c), c->st, c->dbd, sp);
   CK(cudaGetLastError());
 }
 
@@ -667,8 +766,9 @@ void timestep(canard_ctx* c) {
     for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], 1, hp[i]);
     CK(cudaMemcpyAsync(dev_slot(c, 4), hp, c->cases.size() * sizeof(StageParams), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemsetAsync(c->ddt, 0, 2 * c->cases.size() * sizeof(unsigned long long), c->st));
-    Timed tm(c, T_TIMESTEP, 8.0 * 17 * valid_points(c));
-    k_dtmax<<<ew_grid(c), 256, 0, c->st>>>(c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
+    Timed tm(c, T_TIMESTEP, ew_bytes(c, 10, 7));
+    if (c->f32()) launch_dtmax<float>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
+    else launch_dtmax<double>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->hdt, c->ddt, 2 * c->cases.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        c->st));
@@ -710,8 +810,7 @@ void one_step(canard_ctx* c) {
   for (int nk = 1; nk <= 4; ++nk) {
     const StageParams* sp = dev_slot(c, nk - 1);
     if (nk > 1) ph_prim(c);
-    ph_viscous(c);
-    ph_fluxes(c, sp);
+    ph_visc_fluxes(c, sp);
     ph_gcbc(c, sp);
     ph_sponge(c);
     ph_rk(c, sp);
@@ -727,6 +826,13 @@ void one_step(canard_ctx* c) {
 // ---- set-up ------------------------------------------------------------------------
 void build_tables(canard_ctx* c) {
   const int nb = nblk(c);
+  const bool f32 = c->f32();
+  // work field f (of the flux type) of block b, as an untyped pointer
+  auto wf = [&](int b, int f64_field, int f32_field) -> void* {
+    return f32 ? static_cast<void*>(gptr(c->blocks[b], f32_field)) : static_cast<void*>(fptr(c->blocks[b], f64_field));
+  };
+  const int dkind = f32 ? LK_F32 : LK_F64;                  // derivatives of work fields
+  const int fkind = f32 ? LK_F64_TILE_F32_SOLVE : LK_F64;   // filter of the FP64 state
   // filter passes
   for (int m = 1; m <= 5; ++m)
     for (int inn = 1; inn <= 3; ++inn) {
@@ -735,10 +841,10 @@ void build_tables(canard_ctx* c) {
       for (int b = 0; b < nb; ++b) {
         LineTask t;
         double* f = fptr(c->blocks[b], F_QA + m - 1);
-        fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t);
+        fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t, fkind);
         v.push_back(t);
       }
-      c->filt[m - 1][inn - 1] = make_line_table(c, v, dir, false);
+      c->filt[m - 1][inn - 1] = make_line_table(c, v, dir, false, fkind);
       c->mp_filt[m - 1][inn - 1] = make_face_table(
           c, face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }), false);
     }
@@ -749,20 +855,20 @@ void build_tables(canard_ctx* c) {
       if (!c->cases[c->blocks[b].g.case_id].d.viscous) continue;
       for (int m = 2; m <= 5; ++m) {
         LineTask t;
-        fill_line_task(c, c->blocks[b], dir, 0, fptr(c->blocks[b], F_DE + m - 1),
-                       fptr(c->blocks[b], F_SCR + 3 * (m - 2) + dir), m, false, t);
+        fill_line_task(c, c->blocks[b], dir, 0, wf(b, F_DE + m - 1, G_DE + m - 1),
+                       wf(b, F_SCR + 3 * (m - 2) + dir, G_SCR + 3 * (m - 2) + dir), m, false, t, dkind);
         v.push_back(t);
       }
     }
-    c->visc[dir] = make_line_table(c, v, dir, false);
+    c->visc[dir] = make_line_table(c, v, dir, false, dkind);
   }
   {
     std::vector<FaceTask> all;
     for (int m = 2; m <= 5; ++m) {
-      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int) { return fptr(c->blocks[b], F_DE + m - 1); });
+      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int) { return wf(b, F_DE + m - 1, G_DE + m - 1); }, -1, f32);
       all.insert(all.end(), v.begin(), v.end());
     }
-    c->mp_visc = make_face_table(c, all, false);
+    c->mp_visc = make_face_table(c, all, false, f32 ? 1 : 0);
   }
   // fluxes: scr 3*(m-1) + dir, in place
   for (int dir = 0; dir < 3; ++dir) {
@@ -770,19 +876,21 @@ void build_tables(canard_ctx* c) {
     for (int b = 0; b < nb; ++b)
       for (int m = 1; m <= 5; ++m) {
         LineTask t;
-        double* f = fptr(c->blocks[b], F_SCR + 3 * (m - 1) + dir);
-        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t);
+        void* f = wf(b, F_SCR + 3 * (m - 1) + dir, G_SCR + 3 * (m - 1) + dir);
+        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t, dkind);
         v.push_back(t);
       }
-    c->flux[dir] = make_line_table(c, v, dir, false);
+    c->flux[dir] = make_line_table(c, v, dir, false, dkind);
   }
   {
     std::vector<FaceTask> all;
     for (int m = 1; m <= 5; ++m) {
-      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int d) { return fptr(c->blocks[b], F_SCR + 3 * (m - 1) + d); });
+      auto v = face_tasks(
+          c, 0, 0, m, -1, [&](int b, int d) { return wf(b, F_SCR + 3 * (m - 1) + d, G_SCR + 3 * (m - 1) + d); }, -1,
+          f32);
       all.insert(all.end(), v.begin(), v.end());
     }
-    c->mp_flux = make_face_table(c, all, false);
+    c->mp_flux = make_face_table(c, all, false, f32 ? 1 : 0);
   }
 }
 
@@ -791,8 +899,8 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
   // GCBC tables need yaco (reference layout) on the host
   std::vector<GcbcTask> setup_tasks;
   std::vector<GcbcTask> upd[3][2];
-  std::vector<const double*> fsrc;
-  std::vector<double*> fdst;
+  std::vector<void*> fsrc;
+  std::vector<void*> fdst;
   std::vector<int> fcnt;
   std::vector<SpongeTask> sp_tasks;
   for (int b = 0; b < nb; ++b) {
@@ -819,8 +927,14 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
       GcbcTask t{};
       t.b = b; t.nn = f.nn; t.side = f.side; t.bc = f.bc;
       t.cm = B.cm[d] + (size_t)3 * f.side * g.nbs[d];
-      t.drva = B.drva[d] + (size_t)5 * f.side * g.nbs[d];
-      t.drvb = (f.bc == BC_CURV) ? B.drvb[d] + (size_t)5 * f.side * g.nbs[d] : nullptr;
+      const size_t off = (size_t)5 * f.side * g.nbs[d];
+      if (c->f32()) {
+        t.drva = B.drva32[d] + off;
+        t.drvb = (f.bc == BC_CURV) ? B.drvb32[d] + off : nullptr;
+      } else {
+        t.drva = B.drva[d] + off;
+        t.drvb = (f.bc == BC_CURV) ? B.drvb[d] + off : nullptr;
+      }
       t.pts = B.gc_pts + f.first;
       t.w = B.gc_w + f.first;
       t.nbs = g.nbs[d];
@@ -850,8 +964,13 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
     const BlockState& S = c->blocks[L.src_b];
     const int d = L.nn;
     if (R.g.nbc[d][L.dst_side] != BC_CURV) continue;
-    fsrc.push_back(S.drva[d] + (size_t)5 * L.src_side * S.g.nbs[d]);
-    fdst.push_back(R.drvb[d] + (size_t)5 * L.dst_side * R.g.nbs[d]);
+    if (c->f32()) {
+      fsrc.push_back(S.drva32[d] + (size_t)5 * L.src_side * S.g.nbs[d]);
+      fdst.push_back(R.drvb32[d] + (size_t)5 * L.dst_side * R.g.nbs[d]);
+    } else {
+      fsrc.push_back(S.drva[d] + (size_t)5 * L.src_side * S.g.nbs[d]);
+      fdst.push_back(R.drvb[d] + (size_t)5 * L.dst_side * R.g.nbs[d]);
+    }
     fcnt.push_back(5 * R.g.nbs[d]);
   }
   c->gc_setup = make_lines_table(c, setup_tasks, false, &GcbcTask::nbs, &GcbcTask::line0);
@@ -860,9 +979,7 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
       c->gc_upd[d][s] = make_lines_table(c, upd[d][s], false, &GcbcTask::nbs, &GcbcTask::line0);
   c->fc_n = (int)fsrc.size();
   if (c->fc_n) {
-    std::vector<double*> s2;
-    for (auto p : fsrc) s2.push_back(const_cast<double*>(p));
-    c->fc_src = dupload(s2, c->st);
+    c->fc_src = dupload(fsrc, c->st);
     c->fc_dst = dupload(fdst, c->st);
     c->fc_cnt = dupload(fcnt, c->st);
     c->fc_max = *std::max_element(fcnt.begin(), fcnt.end());
@@ -964,6 +1081,10 @@ void grid_metrics(canard_ctx* c) {
   k_face_normals<<<std::max(1, std::min((tot + 127) / 128, 1184)), 128, 0, c->st>>>(c->dbd, dt, df,
                                                                                      (int)cmt.size(), tot);
   CK(cudaGetLastError());
+  if (c->f32()) {
+    k_metrics_to_f32<<<ew_grid(c), 256, 0, c->st>>>(c->dbd);
+    CK(cudaGetLastError());
+  }
   sync_check(c);
   free_transient(c);
 }
@@ -1012,6 +1133,10 @@ void destroy(canard_ctx* c) {
     for (int nt = 0; nt < 2; ++nt)
       for (int d = 0; d < 3; ++d) { cudaFree(b.lu[nt][d]); cudaFree(b.recv[nt][d]); }
     for (int d = 0; d < 3; ++d) { cudaFree(b.chain[d]); cudaFree(b.drva[d]); cudaFree(b.drvb[d]); cudaFree(b.cm[d]); }
+    cudaFree(b.arena32);
+    for (int nt = 0; nt < 2; ++nt)
+      for (int d = 0; d < 3; ++d) cudaFree(b.lu32[nt][d]);
+    for (int d = 0; d < 3; ++d) { cudaFree(b.recv32[d]); cudaFree(b.drva32[d]); cudaFree(b.drvb32[d]); }
     cudaFree(b.gc_pts); cudaFree(b.gc_w); cudaFree(b.sp_pts); cudaFree(b.sp_a); cudaFree(b.sp_b);
   }
   for (auto& cs : c->cases) cudaFree(cs.dsch);
@@ -1101,6 +1226,13 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
     d.qa = fptr(B, F_QA); d.qo = fptr(B, F_QO); d.de = fptr(B, F_DE); d.p = fptr(B, F_P); d.mu = fptr(B, F_MU);
     d.xim = fptr(B, F_XIM); d.etm = fptr(B, F_ETM); d.zem = fptr(B, F_ZEM); d.yaco = fptr(B, F_YACO);
     d.tau = fptr(B, F_TAU); d.scr = fptr(B, F_SCR); d.xyz = fptr(B, F_XYZ);
+    d.f = Work<float>{};
+    if (c->f32()) {
+      B.arena32 = dalloc<float>((size_t)G_COUNT * g.npad, c->st);
+      d.f.de = gptr(B, G_DE); d.f.p = gptr(B, G_P); d.f.mu = gptr(B, G_MU); d.f.tau = gptr(B, G_TAU);
+      d.f.scr = gptr(B, G_SCR); d.f.xim = gptr(B, G_XIM); d.f.etm = gptr(B, G_ETM); d.f.zem = gptr(B, G_ZEM);
+      d.f.yaco = gptr(B, G_YACO);
+    }
     const Scheme& sch = c->cases[g.case_id].sch;
     for (int dir = 0; dir < 3; ++dir) {
       const int L = g.ijk[0][dir] + 1, nbs = g.nbs[dir];
@@ -1109,6 +1241,10 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         std::vector<double> lu((size_t)5 * L);
         sch.lu(L, n0, n1, nt, lu.data());
         B.lu[nt][dir] = dupload(lu, c->st);
+        if (c->f32()) {  // the FP64 factorisation, rounded for the FP32 eliminations
+          std::vector<float> lu32(lu.begin(), lu.end());
+          B.lu32[nt][dir] = dupload(lu32, c->st);
+        }
         // rows [i0, L-4] whose five factors are bit-identical to row L-4
         const int e = L - 4;
         int i0 = e + 1;
@@ -1126,6 +1262,11 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs, c->st);
       }
       B.chain[dir] = dalloc<double>((size_t)2 * nbs, c->st);
+      if (c->f32()) {
+        B.recv32[dir] = dalloc<float>((size_t)5 * 2 * 2 * nbs, c->st);
+        B.drva32[dir] = dalloc<float>((size_t)10 * nbs, c->st);
+        B.drvb32[dir] = dalloc<float>((size_t)10 * nbs, c->st);
+      }
       B.drva[dir] = dalloc<double>((size_t)10 * nbs, c->st);
       B.drvb[dir] = dalloc<double>((size_t)10 * nbs, c->st);
       B.cm[dir] = dalloc<double>((size_t)6 * nbs, c->st);
@@ -1194,7 +1335,7 @@ int canard_ctx_create(const canard_case_desc* cases, int32_t ncases, const canar
                       int32_t precision, canard_ctx** out) {
   if (!out) return CANARD_ERR_ARG;
   *out = nullptr;
-  if (precision != CANARD_FP64) return CANARD_ERR_UNSUPPORTED;
+  if (precision != CANARD_FP64 && precision != CANARD_FP32_MIXED) return CANARD_ERR_UNSUPPORTED;
   canard_ctx* c = new canard_ctx();
   c->precision = precision;
   int rc = guarded(c, [&] { create(c, cases, ncases, blocks); });
@@ -1264,23 +1405,28 @@ int canard_get_state(canard_ctx* c, int32_t icase, int32_t iblock, double* qa) {
   });
 }
 
-static void field_info(const BlockState& B, int field, const double*& dptr, int& ncols, bool& face,
-                       size_t& count) {
+// Device location of a field. In a mixed-precision context the work fields
+// (de, p, ss1, tau, drva) are FP32 and f32ptr is set instead of dptr.
+static void field_info(const canard_ctx* c, const BlockState& B, int field, const double*& dptr, int& ncols,
+                       bool& face, size_t& count, const float*& f32ptr) {
   face = false;
+  f32ptr = nullptr;
+  const bool w32 = c->f32();
   switch (field) {
     case CANARD_F_QA: dptr = fptr(B, F_QA); ncols = 5; break;
     case CANARD_F_QO: dptr = fptr(B, F_QO); ncols = 5; break;
-    case CANARD_F_DE: dptr = fptr(B, F_DE); ncols = 5; break;
-    case CANARD_F_P: dptr = fptr(B, F_P); ncols = 1; break;
-    case CANARD_F_SS1: dptr = fptr(B, F_MU); ncols = 1; break;
+    case CANARD_F_DE: dptr = fptr(B, F_DE); ncols = 5; if (w32) f32ptr = gptr(B, G_DE); break;
+    case CANARD_F_P: dptr = fptr(B, F_P); ncols = 1; if (w32) f32ptr = gptr(B, G_P); break;
+    case CANARD_F_SS1: dptr = fptr(B, F_MU); ncols = 1; if (w32) f32ptr = gptr(B, G_MU); break;
     case CANARD_F_XIM: dptr = fptr(B, F_XIM); ncols = 3; break;
     case CANARD_F_ETM: dptr = fptr(B, F_ETM); ncols = 3; break;
     case CANARD_F_ZEM: dptr = fptr(B, F_ZEM); ncols = 3; break;
     case CANARD_F_YACO: dptr = fptr(B, F_YACO); ncols = 1; break;
-    case CANARD_F_TAU: dptr = fptr(B, F_TAU); ncols = 9; break;
+    case CANARD_F_TAU: dptr = fptr(B, F_TAU); ncols = 9; if (w32) f32ptr = gptr(B, G_TAU); break;
     case CANARD_F_DRVA1: case CANARD_F_DRVA2: case CANARD_F_DRVA3: {
       const int d = field - CANARD_F_DRVA1;
       dptr = B.drva[d]; face = true; count = (size_t)10 * B.g.nbs[d]; ncols = 0;
+      if (w32) f32ptr = B.drva32[d];
       return;
     }
     case CANARD_F_CM1: case CANARD_F_CM2: case CANARD_F_CM3: {
@@ -1293,12 +1439,26 @@ static void field_info(const BlockState& B, int field, const double*& dptr, int&
   count = (size_t)ncols * B.g.X * B.g.Y * B.g.Z;
 }
 
+// element conversions between an FP32 field and its FP64 image (unit calls and
+// field access of mixed-precision contexts; not on the step path)
+void to_f64(canard_ctx* c, const float* a, double* b, size_t n) {
+  k_f32_to_f64<<<std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 1184)), 256, 0, c->st>>>(a, b, (long long)n);
+  CK(cudaGetLastError());
+}
+void to_f32(canard_ctx* c, const double* a, float* b, size_t n) {
+  k_f64_to_f32<<<std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 1184)), 256, 0, c->st>>>(a, b, (long long)n);
+  CK(cudaGetLastError());
+}
+
 int canard_get_field(canard_ctx* c, int32_t icase, int32_t iblock, int32_t field, double* out, int64_t count) {
   return guarded(c, [&] {
     BlockState& B = c->blocks[block_index(c, icase, iblock)];
-    const double* dp; int nc; bool face; size_t n;
-    field_info(B, field, dp, nc, face, n);
+    const double* dp; int nc; bool face; size_t n; const float* fp;
+    field_info(c, B, field, dp, nc, face, n, fp);
     if (!out || count != (int64_t)n) throw ApiError(CANARD_ERR_ARG, "count does not match the field size");
+    if (fp) {  // FP32 work field: widen into the FP64 slot of the same field, then copy
+      to_f64(c, fp, const_cast<double*>(dp), face ? n : (size_t)nc * B.g.npad);
+    }
     if (face) CK(cudaMemcpyAsync(out, dp, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     else d2h_field(c, B, out, dp, nc);
     CK(cudaStreamSynchronize(c->st));
@@ -1308,11 +1468,12 @@ int canard_get_field(canard_ctx* c, int32_t icase, int32_t iblock, int32_t field
 int canard_set_field(canard_ctx* c, int32_t icase, int32_t iblock, int32_t field, const double* in, int64_t count) {
   return guarded(c, [&] {
     BlockState& B = c->blocks[block_index(c, icase, iblock)];
-    const double* dp; int nc; bool face; size_t n;
-    field_info(B, field, dp, nc, face, n);
+    const double* dp; int nc; bool face; size_t n; const float* fp;
+    field_info(c, B, field, dp, nc, face, n, fp);
     if (!in || count != (int64_t)n) throw ApiError(CANARD_ERR_ARG, "count does not match the field size");
     if (face) CK(cudaMemcpyAsync(const_cast<double*>(dp), in, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
     else h2d_field(c, B, const_cast<double*>(dp), in, nc);
+    if (fp) to_f32(c, dp, const_cast<float*>(fp), face ? n : (size_t)nc * B.g.npad);
     CK(cudaStreamSynchronize(c->st));
   });
 }
@@ -1389,26 +1550,44 @@ int canard_mpigo(canard_ctx* c, const double* const* fields, int32_t ncols, int3
       throw ApiError(CANARD_ERR_ARG, "bad mpigo argument");
     if (nrt == 0 && ncols != 3) throw ApiError(CANARD_ERR_ARG, "nrall needs three columns");
     const CaseState& cs = c->cases[0];
-    // stage the fields in the scratch columns 12..14 of every block
+    // stage the fields in the scratch columns 12..14 of every block; a
+    // mixed-precision context contracts derivative inputs (nt = 0) in FP32
+    const bool w32 = c->f32() && nt == 0;
     for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) {
       if (!fields[b - cs.b0]) throw ApiError(CANARD_ERR_ARG, "null field");
-      h2d_field(c, c->blocks[b], fptr(c->blocks[b], F_SCR + 12), fields[b - cs.b0], ncols);
+      BlockState& B = c->blocks[b];
+      h2d_field(c, B, fptr(B, F_SCR + 12), fields[b - cs.b0], ncols);
+      if (w32) to_f32(c, fptr(B, F_SCR + 12), gptr(B, G_SCR + 12), (size_t)ncols * B.g.npad);
     }
-    auto col = [&](int b, int d) { return fptr(c->blocks[b], F_SCR + 12 + (nrt == 0 ? d : 0)); };
-    launch_mpigo(c, make_face_table(c, face_tasks(c, nt, n45, m, -1, col, 0), true));
+    auto col = [&](int b, int d) -> const void* {
+      const int k = 12 + (nrt == 0 ? d : 0);
+      return w32 ? static_cast<const void*>(gptr(c->blocks[b], G_SCR + k))
+                 : static_cast<const void*>(fptr(c->blocks[b], F_SCR + k));
+    };
+    launch_mpigo(c, make_face_table(c, face_tasks(c, nt, n45, m, -1, col, 0, w32), true, w32 ? 1 : 0));
     sync_check(c);
     free_transient(c);
   });
 }
 
+// One field through one line solve; in a mixed-precision context the
+// derivative runs on an FP32 copy and the filter on the FP64 field with an
+// FP32 elimination, as on the step path.
 static void unit_line(canard_ctx* c, int iblock, const double* in, double* out, int dir, int nt, int m) {
   const int b = block_index(c, 0, iblock);
   BlockState& B = c->blocks[b];
   double* f = fptr(B, F_SCR + 11);
   h2d_field(c, B, f, in, 1);
+  const int kind = !c->f32() ? LK_F64 : (nt == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
+  void* fd = f;
+  if (kind == LK_F32) {
+    fd = gptr(B, G_SCR + 11);
+    to_f32(c, f, gptr(B, G_SCR + 11), (size_t)B.g.npad);
+  }
   LineTask t;
-  fill_line_task(c, B, dir, nt, f, f, m, nt == 0, t);
-  launch_line(c, make_line_table(c, {t}, dir, true), dir, nt);
+  fill_line_task(c, B, dir, nt, fd, fd, m, nt == 0, t, kind);
+  launch_line(c, make_line_table(c, {t}, dir, true, kind), dir, nt);
+  if (kind == LK_F32) to_f64(c, gptr(B, G_SCR + 11), f, (size_t)B.g.npad);
   d2h_field(c, B, out, f, 1);
   sync_check(c);
   free_transient(c);
@@ -1563,7 +1742,7 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     LineTask t{};
     t.in = d_in;
     t.out = d_out;
-    t.lu = reinterpret_cast<const double*>(base + kNaLu);
+    t.lu = base + kNaLu;
     {  // bitwise-constant interior rows, as for the context path
       const int e = L - 4;
       int i0 = e;
@@ -1577,7 +1756,7 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
       t.cu2 = lu[(size_t)3 * L + e]; t.cu3 = lu[(size_t)4 * L + e];
       t.c0 = i0;
     }
-    t.recv = reinterpret_cast<const double*>(base + kNaRecv);
+    t.recv = base + kNaRecv;
     t.drva = nullptr;
     t.sc = reinterpret_cast<const DevScheme*>(base + kNaScheme);
     t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp;
@@ -1633,9 +1812,9 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     CK(cudaMemsetAsync(base + kNaErr, 0, sizeof(int), st));
     if (nf) {
       const int tot = nf * nbs;
-      k_mpigo<<<std::max(1, std::min((tot + 127) / 128, 148 * 16)), 128, 0, st>>>(
-          reinterpret_cast<const FaceTask*>(base + kNaFace), reinterpret_cast<const int*>(base + kNaIdx) + 1, nf,
-          tot);
+      launch_mpigo_t<double>(std::max(1, std::min((tot + 127) / 128, 148 * 16)), st,
+                             reinterpret_cast<const FaceTask*>(base + kNaFace),
+                             reinterpret_cast<const int*>(base + kNaIdx) + 1, nf, tot);
       CK(cudaGetLastError());
     }
     const size_t smem = line_smem(dir, L);
@@ -1643,9 +1822,9 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     const int* d0 = reinterpret_cast<const int*>(base + kNaIdx);
     const CUtensorMap* dm = reinterpret_cast<const CUtensorMap*>(base + kNaMaps);
     int* de = reinterpret_cast<int*>(base + kNaErr);
-    if (dir == 0) k_line<1, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
-    else if (dir == 1) k_line<2, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
-    else k_line<3, 0><<<t.ntiles, kLanes, smem, st>>>(dt, d0, 1, dm, de);
+    if (dir == 0) launch_line_t<1, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
+    else if (dir == 1) launch_line_t<2, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
+    else launch_line_t<3, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
     CK(cudaGetLastError());
   } catch (const ApiError& e) {
     return fail(e.code, e.what());

@@ -1,9 +1,15 @@
 // Device kernels of the Canard hot path for sm_100a.
 //
-// FP64 kernels are compiled without FMA contraction (-fmad=false) and evaluate
-// every expression in the reference's order, so on identical inputs they
-// reproduce the CPU restatement bit for bit (the Sutherland power is the only
-// library function, see pow15).
+// Every kernel is a template over its arithmetic types and is instantiated
+// twice:
+//  * FP64 plain: all types double, compiled without FMA contraction
+//    (-fmad=false) and evaluating every expression in the reference's order,
+//    so on identical inputs it reproduces the CPU restatement bit for bit (the
+//    Sutherland power is the only library function, see pow15);
+//  * FP32 mixed: line solves, fluxes, viscous stresses and GCBC in float with
+//    FMA contraction (a separate translation unit), while the conserved state,
+//    the RK update, the metric and Jacobian masters, the primitive
+//    computation and the LU factorisation stay FP64.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -11,7 +17,7 @@
 
 namespace canard {
 
-constexpr int kLanes = 32;          // lines per tile (one warp, one line per lane)
+constexpr int kLanes = 32;            // lines per tile (one warp, one line per lane)
 constexpr int kErrTimeout = 4;
 constexpr long long kSpinLimit = 1LL << 28;  // bounded mbarrier waits
 
@@ -35,37 +41,58 @@ struct CaseConst {
   int viscous;
 };
 
+// Work fields of one block in the arithmetic type R of the flux path.
+template <class R>
+struct Work {
+  R *de, *p, *mu, *tau, *scr;
+  const R *xim, *etm, *zem, *yaco;
+};
+
 struct BlockDev {
   int X, Y, Z, Xp;
   long long npad;
   int case_id;
+  // FP64: state, metric and Jacobian masters, and the FP64 work fields
   double *qa, *qo, *de, *p, *mu, *xim, *etm, *zem, *yaco, *tau, *scr, *xyz;
+  Work<float> f;  // FP32 work fields and metric copies (mixed precision only)
 };
+
+template <class R>
+__device__ __forceinline__ Work<R> work(const BlockDev& B);
+template <>
+__device__ __forceinline__ Work<double> work<double>(const BlockDev& B) {
+  return {B.de, B.p, B.mu, B.tau, B.scr, B.xim, B.etm, B.zem, B.yaco};
+}
+template <>
+__device__ __forceinline__ Work<float> work<float>(const BlockDev& B) {
+  return B.f;
+}
 
 // ---------------------------------------------------------------------------
 // A family of lines of one block, direction and field, solved by one launch
-// together with other families (tile prefix sums select the family).
+// together with other families (tile prefix sums select the family). Field
+// pointers have the tile type TT of the launch, factor tables the solve type.
 struct LineTask {
-  const double* in;
-  double* out;
-  const double* lu;     // xl1, xl2, xu1, xu2, xu3 (each L entries)
+  const void* in;
+  void* out;
+  const void* lu;       // xl1, xl2, xu1, xu2, xu3 (each L entries)
   double cl1, cl2, cu1, cu2, cu3;  // the factors of rows [c0, L-4], bitwise constant there
   int c0;
-  const double* recv;   // [side][comp][jk], comp stride nbs, side stride ncomp*nbs
-  double* drva;         // drva(jk, m, side) of this block and direction, or null
+  const void* recv;     // [side][comp][jk], comp stride nbs, side stride ncomp*nbs
+  void* drva;           // drva(jk, m, side) of this block and direction, or null
   const DevScheme* sc;
   int X, Y, Z, Xp;
   int L, nbs, m, ndf0, ndf1;
   int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
-  int nbox, by;            // dir 2/3: TMA boxes per tile and rows per box
+  int nbox, by;            // chunks per tile and positions per chunk
 };
 
 // Interface contraction of one face (t_numerics%mpigo): the sender's face
 // lines are contracted with pbco and written into the receiver's buffers.
 struct FaceTask {
-  const double* src;    // sender field column for this direction
-  const double* dstf;   // receiver field column (coordinate-jump correction)
-  double* recv;         // receiver buffer [comp][jk] for (direction, side, m)
+  const void* src;      // sender field column for this direction
+  const void* dstf;     // receiver field column (coordinate-jump correction)
+  void* recv;           // receiver buffer [comp][jk] for (direction, side, m)
   double* chain;        // sender's persistent send(:,nt+1,side) of the filter
   const DevScheme* sc;
   int nn, sb, nt, exch, corr, iik;
@@ -78,16 +105,18 @@ struct FaceTask {
 struct GcbcTask {  // one GCBC face of one block
   int b, nn, side, bc;
   const double* cm;       // cm(jk,3,side) base of this face side: [d][jk]
-  double* drva;           // drva(jk,5,side): [c][jk]
-  const double* drvb;
+  void* drva;             // drva(jk,5,side): [c][jk], in the flux type
+  const void* drvb;
   const long long* pts;   // 5 device indices per line
   const double* w;        // 5 weights per line
   int nbs, nj, line0;
   int X, Y, Z, Xp, N;
 };
 
+struct SpongeTask { int b; const long long* pts; const double* asz; const double* bsz; int count, first; };
+
 // ---------------------------------------------------------------------------
-// small PTX helpers: mbarrier + bulk asynchronous copies (sm_90+)
+// small PTX helpers: mbarrier + bulk and element asynchronous copies
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -175,16 +204,16 @@ __device__ __forceinline__ double pow15(double x) {
 // [c0, L-4] hold bitwise identical factors (found on the host), which the
 // sweeps keep in registers. Only the closure rows near the ends read the
 // factor tables, so the dependent chain carries no memory latency there.
+template <class RS>
 struct LuRows {
-  const double* __restrict__ l1;
-  const double* __restrict__ l2;
-  const double* __restrict__ u1;
-  const double* __restrict__ u2;
-  const double* __restrict__ u3;
-  double cl1, cl2, cu1, cu2, cu3;
+  const RS* __restrict__ l1;
+  const RS* __restrict__ l2;
+  const RS* __restrict__ u1;
+  const RS* __restrict__ u2;
+  const RS* __restrict__ u3;
+  RS cl1, cl2, cu1, cu2, cu3;
   int c0, c1;
-  __device__ __forceinline__ LuRows(const double* lu, int L, double a, double b, double c, double d, double e,
-                                    int c0_)
+  __device__ __forceinline__ LuRows(const RS* lu, int L, RS a, RS b, RS c, RS d, RS e, int c0_)
       : l1(lu), l2(lu + L), u1(lu + 2 * L), u2(lu + 3 * L), u3(lu + 4 * L), cl1(a), cl2(b), cu1(c), cu2(d),
         cu3(e), c0(c0_), c1(L - 4) {}
 };
@@ -217,37 +246,42 @@ struct ChunkIn {
 };
 
 // Factor providers: the interior constants or the per-row tables.
+template <class RS>
 struct CoefConst {
-  double l1, l2, u1, u2, u3;
-  __device__ __forceinline__ double L1(int) const { return l1; }
-  __device__ __forceinline__ double L2(int) const { return l2; }
-  __device__ __forceinline__ double U1(int) const { return u1; }
-  __device__ __forceinline__ double U2(int) const { return u2; }
-  __device__ __forceinline__ double U3(int) const { return u3; }
+  RS l1, l2, u1, u2, u3;
+  __device__ __forceinline__ RS L1(int) const { return l1; }
+  __device__ __forceinline__ RS L2(int) const { return l2; }
+  __device__ __forceinline__ RS U1(int) const { return u1; }
+  __device__ __forceinline__ RS U2(int) const { return u2; }
+  __device__ __forceinline__ RS U3(int) const { return u3; }
 };
+template <class RS>
 struct CoefTable {
-  const double* __restrict__ l1;
-  const double* __restrict__ l2;
-  const double* __restrict__ u1;
-  const double* __restrict__ u2;
-  const double* __restrict__ u3;
-  __device__ __forceinline__ double L1(int i) const { return __ldg(l1 + i); }
-  __device__ __forceinline__ double L2(int i) const { return __ldg(l2 + i); }
-  __device__ __forceinline__ double U1(int i) const { return __ldg(u1 + i); }
-  __device__ __forceinline__ double U2(int i) const { return __ldg(u2 + i); }
-  __device__ __forceinline__ double U3(int i) const { return __ldg(u3 + i); }
+  const RS* __restrict__ l1;
+  const RS* __restrict__ l2;
+  const RS* __restrict__ u1;
+  const RS* __restrict__ u2;
+  const RS* __restrict__ u3;
+  __device__ __forceinline__ RS L1(int i) const { return __ldg(l1 + i); }
+  __device__ __forceinline__ RS L2(int i) const { return __ldg(l2 + i); }
+  __device__ __forceinline__ RS U1(int i) const { return __ldg(u1 + i); }
+  __device__ __forceinline__ RS U2(int i) const { return __ldg(u2 + i); }
+  __device__ __forceinline__ RS U3(int i) const { return __ldg(u3 + i); }
 };
 
 // Rows are processed in blocks of eight: the block's inputs, right-hand sides
 // and factors are all formed before its dependent chain, so their latency
 // overlaps the chain. Every row is still evaluated with the reference's
 // operations in the reference's order (bit-identical to one row at a time).
+// Right-hand sides are formed in the tile type TT, the elimination runs in the
+// solve type RS.
 
 // forward rows i..i+7 of the derivative; window w0..w3 = s[i-2..i+1]
-template <int ST, class CF>
-__device__ __forceinline__ void fwd8_deriv(double* __restrict__ s, int i, const CF& cf, double& w0, double& w1,
-                                           double& w2, double& w3, double& am2, double& am1) {
-  double win[12], l1[8], l2[8], r[8], a[8];
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void fwd8_deriv(TT* __restrict__ s, int i, const CF& cf, TT& w0, TT& w1, TT& w2, TT& w3,
+                                           RS& am2, RS& am1) {
+  TT win[12], r[8];
+  RS l1[8], l2[8], a[8];
   win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -256,23 +290,23 @@ __device__ __forceinline__ void fwd8_deriv(double* __restrict__ s, int i, const 
     l2[k] = cf.L2(i + k);
   }
 #pragma unroll
-  for (int k = 0; k < 8; ++k) r[k] = CA_AA * (win[k + 3] - win[k + 1]) + CA_AB * (win[k + 4] - win[k]);
-  a[0] = (r[0] - l1[0] * am2) - l2[0] * am1;
-  a[1] = (r[1] - l1[1] * am1) - l2[1] * a[0];
+  for (int k = 0; k < 8; ++k) r[k] = TT(CA_AA) * (win[k + 3] - win[k + 1]) + TT(CA_AB) * (win[k + 4] - win[k]);
+  a[0] = (RS(r[0]) - l1[0] * am2) - l2[0] * am1;
+  a[1] = (RS(r[1]) - l1[1] * am1) - l2[1] * a[0];
 #pragma unroll
-  for (int k = 2; k < 8; ++k) a[k] = (r[k] - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
+  for (int k = 2; k < 8; ++k) a[k] = (RS(r[k]) - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = a[k];
+  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = TT(a[k]);
   w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11];
   am2 = a[6]; am1 = a[7];
 }
 
 // forward rows i..i+7 of the filter; window w0..w5 = s[i-3..i+2]
-template <int ST, class CF>
-__device__ __forceinline__ void fwd8_filter(double* __restrict__ s, int i, const CF& cf, double fa, double fb,
-                                            double fc, double& w0, double& w1, double& w2, double& w3,
-                                            double& w4, double& w5, double& am2, double& am1) {
-  double win[14], l1[8], l2[8], r[8], a[8];
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void fwd8_filter(TT* __restrict__ s, int i, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
+                                            TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+  TT win[14], r[8];
+  RS l1[8], l2[8], a[8];
   win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3; win[4] = w4; win[5] = w5;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -282,27 +316,27 @@ __device__ __forceinline__ void fwd8_filter(double* __restrict__ s, int i, const
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const double rk = win[k + 3] + win[k + 3];
+    const TT rk = win[k + 3] + win[k + 3];
     r[k] = (fa * ((win[k + 2] + win[k + 4]) - rk) + fb * ((win[k + 1] + win[k + 5]) - rk)) +
            fc * ((win[k] + win[k + 6]) - rk);
   }
-  a[0] = (r[0] - l1[0] * am2) - l2[0] * am1;
-  a[1] = (r[1] - l1[1] * am1) - l2[1] * a[0];
+  a[0] = (RS(r[0]) - l1[0] * am2) - l2[0] * am1;
+  a[1] = (RS(r[1]) - l1[1] * am1) - l2[1] * a[0];
 #pragma unroll
-  for (int k = 2; k < 8; ++k) a[k] = (r[k] - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
+  for (int k = 2; k < 8; ++k) a[k] = (RS(r[k]) - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = a[k];
+  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = TT(a[k]);
   w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11]; w4 = win[12]; w5 = win[13];
   am2 = a[6]; am1 = a[7];
 }
 
 // back substitution rows i, i-1, ..., i-7
-template <int ST, class CF>
-__device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf, double& cp1, double& cp2) {
-  double p[8], u2[8], u3[8], c[8];
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void bwd8(TT* __restrict__ s, int i, const CF& cf, RS& cp1, RS& cp2) {
+  RS p[8], u2[8], u3[8], c[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    p[k] = cf.U1(i - k) * s[(i - k) * ST];
+    p[k] = cf.U1(i - k) * RS(s[(i - k) * ST]);
     u2[k] = cf.U2(i - k);
     u3[k] = cf.U3(i - k);
   }
@@ -311,7 +345,7 @@ __device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf
 #pragma unroll
   for (int k = 2; k < 8; ++k) c[k] = (p[k] - u2[k] * c[k - 1]) - u3[k] * c[k - 2];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) s[(i - k) * ST] = c[k];
+  for (int k = 0; k < 8; ++k) s[(i - k) * ST] = TT(c[k]);
   cp2 = c[6];
   cp1 = c[7];
 }
@@ -320,13 +354,14 @@ __device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf
 // where the look-ahead rows have arrived, single rows otherwise.
 #define FORWARD_ROWS(FIRST, LAST, LA, BLOCK8, STEP)                           \
   {                                                                           \
-    const CoefConst CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                    \
-    const CoefTable CT{F.l1, F.l2, F.u1, F.u2, F.u3};                         \
+    const CoefConst<RS> CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                \
+    const CoefTable<RS> CT{F.l1, F.l2, F.u1, F.u2, F.u3};                     \
     int i = (FIRST);                                                          \
     while (i <= (LAST)) {                                                     \
       const int e = min((LAST), CI.ready - 1 - (LA));                         \
       if (e < i) {                                                            \
         if (!CI.wait_next(err)) return false;                                 \
+        __syncwarp();                                                         \
         continue;                                                             \
       }                                                                       \
       {                                                                       \
@@ -345,26 +380,26 @@ __device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf
 // chunk is final and DONE(c) runs (add the original, store it).
 #define BACKWARD_ROWS(DONE)                                                   \
   {                                                                           \
-    const CoefConst CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                    \
-    const CoefTable CT{F.l1, F.l2, F.u1, F.u2, F.u3};                         \
-    double cp1 = CT.U1(N) * S(N);                                             \
-    S(N) = cp1;                                                               \
-    double c = CT.U1(N - 1) * S(N - 1) - CT.U2(N - 1) * cp1;                  \
-    S(N - 1) = c;                                                             \
-    double cp2 = cp1;                                                         \
+    const CoefConst<RS> CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                \
+    const CoefTable<RS> CT{F.l1, F.l2, F.u1, F.u2, F.u3};                     \
+    RS cp1 = CT.U1(N) * RS(S(N));                                             \
+    S(N) = TT(cp1);                                                           \
+    RS c = CT.U1(N - 1) * RS(S(N - 1)) - CT.U2(N - 1) * cp1;                  \
+    S(N - 1) = TT(c);                                                         \
+    RS cp2 = cp1;                                                             \
     cp1 = c;                                                                  \
     int i = N - 2;                                                            \
     for (int ch = CI.NC - 1; ch >= 0; --ch) {                                 \
       const int lo = ch * CI.CR;                                              \
-      for (; i > F.c1 && i - 7 >= lo; i -= 8) bwd8<ST>(s, i, CT, cp1, cp2);   \
+      for (; i > F.c1 && i - 7 >= lo; i -= 8) bwd8<ST, TT, RS>(s, i, CT, cp1, cp2); \
       {                                                                       \
         const int ce = max(F.c0, lo);                                         \
-        for (; i - 7 >= ce; i -= 8) bwd8<ST>(s, i, CC, cp1, cp2);             \
+        for (; i - 7 >= ce; i -= 8) bwd8<ST, TT, RS>(s, i, CC, cp1, cp2);     \
       }                                                                       \
-      for (; i - 7 >= lo; i -= 8) bwd8<ST>(s, i, CT, cp1, cp2);               \
+      for (; i - 7 >= lo; i -= 8) bwd8<ST, TT, RS>(s, i, CT, cp1, cp2);       \
       for (; i >= lo; --i) {                                                  \
-        c = (CT.U1(i) * S(i) - CT.U2(i) * cp1) - CT.U3(i) * cp2;              \
-        S(i) = c;                                                             \
+        c = (CT.U1(i) * RS(S(i)) - CT.U2(i) * cp1) - CT.U3(i) * cp2;          \
+        S(i) = TT(c);                                                         \
         cp2 = cp1;                                                            \
         cp1 = c;                                                              \
       }                                                                       \
@@ -376,68 +411,68 @@ __device__ __forceinline__ void bwd8(double* __restrict__ s, int i, const CF& cf
 // stride ST (src/mo_numerics.f90:742-792). On return the line holds the
 // derivative; Done(ch) is called as chunks become final. Returns false if a
 // bounded wait gave up.
-template <int ST, class Done>
-__device__ __forceinline__ bool sweep_deriv(double* __restrict__ s, int L, const LuRows& F, int ndf0, int ndf1,
-                                            const DevScheme* __restrict__ sc, double r00, double r10, double r01,
-                                            double r11, ChunkIn& CI, int* err, Done&& done) {
+template <int ST, class TT, class RS, class Done>
+__device__ __forceinline__ bool sweep_deriv(TT* __restrict__ s, int L, const LuRows<RS>& F, int ndf0, int ndf1,
+                                            const DevScheme* __restrict__ sc, TT r00, TT r10, TT r01, TT r11,
+                                            ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
   const int N = L - 1;
-  double b0, b1, bn1, bn;
+  TT b0, b1, bn1, bn;
   if (ndf0 == 0) {
-    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4);
-    b0 = ((CA_A01 * (s1 - s0) + CA_A02 * (s2 - s0)) + CA_A03 * (s3 - s0)) + CA_A04 * (s4 - s0);
-    b1 = ((CA_A10 * (s0 - s1) + CA_A12 * (s2 - s1)) + CA_A13 * (s3 - s1)) + CA_A14 * (s4 - s1);
+    const TT s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4);
+    b0 = ((TT(CA_A01) * (s1 - s0) + TT(CA_A02) * (s2 - s0)) + TT(CA_A03) * (s3 - s0)) + TT(CA_A04) * (s4 - s0);
+    b1 = ((TT(CA_A10) * (s0 - s1) + TT(CA_A12) * (s2 - s1)) + TT(CA_A13) * (s3 - s1)) + TT(CA_A14) * (s4 - s1);
   } else {
-    double t0 = 0.0, t1 = 0.0;
+    TT t0 = 0, t1 = 0;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      const double v = S(i);
-      t0 = t0 + sc->pbci[0][0][i] * v;
-      t1 = t1 + sc->pbci[0][1][i] * v;
+      const TT v = S(i);
+      t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+      t1 = t1 + TT(sc->pbci[0][1][i]) * v;
     }
     b0 = t0 + r00;
     b1 = t1 + r10;
   }
   if (ndf1 == 0) {
-    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4);
-    bn = ((CA_A01 * (e0 - e1) + CA_A02 * (e0 - e2)) + CA_A03 * (e0 - e3)) + CA_A04 * (e0 - e4);
-    bn1 = ((CA_A10 * (e1 - e0) + CA_A12 * (e1 - e2)) + CA_A13 * (e1 - e3)) + CA_A14 * (e1 - e4);
+    const TT e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4);
+    bn = ((TT(CA_A01) * (e0 - e1) + TT(CA_A02) * (e0 - e2)) + TT(CA_A03) * (e0 - e3)) + TT(CA_A04) * (e0 - e4);
+    bn1 = ((TT(CA_A10) * (e1 - e0) + TT(CA_A12) * (e1 - e2)) + TT(CA_A13) * (e1 - e3)) + TT(CA_A14) * (e1 - e4);
   } else {
-    double t0 = 0.0, t1 = 0.0;
+    TT t0 = 0, t1 = 0;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      const double v = S(N - i);
-      t0 = t0 + sc->pbci[0][0][i] * v;
-      t1 = t1 + sc->pbci[0][1][i] * v;
+      const TT v = S(N - i);
+      t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+      t1 = t1 + TT(sc->pbci[0][1][i]) * v;
     }
     bn = -t0 - r01;
     bn1 = -t1 - r11;
   }
   // forward elimination, in place; originals kept in a register window
-  double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3);
-  double am2 = b0;
-  double am1 = b1 - __ldg(F.l2 + 1) * am2;
-  S(0) = am2;
-  S(1) = am1;
+  TT w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3);
+  RS am2 = RS(b0);
+  RS am1 = RS(b1) - __ldg(F.l2 + 1) * am2;
+  S(0) = TT(am2);
+  S(1) = TT(am1);
 #define FWD(L1, L2)                                                 \
   {                                                                 \
-    const double w4 = S(i + 2);                                     \
-    const double rhs = CA_AA * (w3 - w1) + CA_AB * (w4 - w0);       \
-    const double a = (rhs - (L1) * am2) - (L2) * am1;               \
-    S(i) = a;                                                       \
+    const TT w4 = S(i + 2);                                         \
+    const TT rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4 - w0);   \
+    const RS a = (RS(rhs) - (L1) * am2) - (L2) * am1;               \
+    S(i) = TT(a);                                                   \
     w0 = w1; w1 = w2; w2 = w3; w3 = w4;                             \
     am2 = am1; am1 = a;                                             \
   }
-#define BLOCK8(CF) fwd8_deriv<ST>(s, i, CF, w0, w1, w2, w3, am2, am1)
+#define BLOCK8(CF) fwd8_deriv<ST, TT, RS>(s, i, CF, w0, w1, w2, w3, am2, am1)
   FORWARD_ROWS(2, N - 2, 2, BLOCK8, FWD)
 #undef BLOCK8
 #undef FWD
   {
-    const double a = (bn1 - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
-    S(N - 1) = a;
+    const RS a = (RS(bn1) - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
+    S(N - 1) = TT(a);
     am2 = am1; am1 = a;
-    const double an = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
-    S(N) = an;
+    const RS an = (RS(bn) - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
+    S(N) = TT(an);
   }
   TRACE(3)
   BACKWARD_ROWS(done)
@@ -447,92 +482,92 @@ __device__ __forceinline__ bool sweep_deriv(double* __restrict__ s, int L, const
 
 // Compact filter increment of one line (src/mo_numerics.f90:922-977). On
 // return the line holds the increment; Done(ch) adds the original field.
-template <int ST, class Done>
-__device__ __forceinline__ bool sweep_filter(double* __restrict__ s, int L, const LuRows& F, int ndf0, int ndf1,
-                                             const DevScheme* __restrict__ sc, double r00, double r10, double r20,
-                                             double r01, double r11, double r21, ChunkIn& CI, int* err,
-                                             Done&& done) {
+template <int ST, class TT, class RS, class Done>
+__device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const LuRows<RS>& F, int ndf0, int ndf1,
+                                             const DevScheme* __restrict__ sc, TT r00, TT r10, TT r20, TT r01,
+                                             TT r11, TT r21, ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
   const int N = L - 1;
-  const double fa = sc->fa, fb = sc->fb, fc = sc->fc;
-  double b0, b1, b2, bn2, bn1, bn;
+  const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
+  auto fbc = [&](int r, int k) { return TT(sc->fbc[r][k]); };
+  TT b0, b1, b2, bn2, bn1, bn;
   if (ndf0 == 0) {
-    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
-    const double* f0 = sc->fbc[0];
-    const double* f1 = sc->fbc[1];
-    const double* f2 = sc->fbc[2];
-    b0 = (((f0[0] * (s1 - s0) + f0[1] * (s2 - s0)) + f0[2] * (s3 - s0)) + f0[3] * (s4 - s0)) + f0[4] * (s5 - s0);
-    b1 = (((f1[0] * (s0 - s1) + f1[1] * (s2 - s1)) + f1[2] * (s3 - s1)) + f1[3] * (s4 - s1)) + f1[4] * (s5 - s1);
-    b2 = (((f2[0] * (s0 - s2) + f2[1] * (s1 - s2)) + f2[2] * (s3 - s2)) + f2[3] * (s4 - s2)) + f2[4] * (s5 - s2);
+    const TT s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
+    b0 = (((fbc(0, 0) * (s1 - s0) + fbc(0, 1) * (s2 - s0)) + fbc(0, 2) * (s3 - s0)) + fbc(0, 3) * (s4 - s0)) +
+         fbc(0, 4) * (s5 - s0);
+    b1 = (((fbc(1, 0) * (s0 - s1) + fbc(1, 1) * (s2 - s1)) + fbc(1, 2) * (s3 - s1)) + fbc(1, 3) * (s4 - s1)) +
+         fbc(1, 4) * (s5 - s1);
+    b2 = (((fbc(2, 0) * (s0 - s2) + fbc(2, 1) * (s1 - s2)) + fbc(2, 2) * (s3 - s2)) + fbc(2, 3) * (s4 - s2)) +
+         fbc(2, 4) * (s5 - s2);
   } else {
-    double t0 = 0.0, t1 = 0.0;
+    TT t0 = 0, t1 = 0;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      const double v = S(i);
-      t0 = t0 + sc->pbci[1][0][i] * v;
-      t1 = t1 + sc->pbci[1][1][i] * v;
+      const TT v = S(i);
+      t0 = t0 + TT(sc->pbci[1][0][i]) * v;
+      t1 = t1 + TT(sc->pbci[1][1][i]) * v;
     }
-    const double s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
-    const double ra2 = s2 + s2;
+    const TT s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5);
+    const TT ra2 = s2 + s2;
     b0 = t0 + r00;
     b1 = t1 + r10;
     b2 = (fa * ((s1 + s3) - ra2) + fb * ((s0 + s4) - ra2)) + fc * ((r20 + s5) - ra2);
   }
   if (ndf1 == 0) {
-    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
-    const double* f0 = sc->fbc[0];
-    const double* f1 = sc->fbc[1];
-    const double* f2 = sc->fbc[2];
-    bn = (((f0[0] * (e1 - e0) + f0[1] * (e2 - e0)) + f0[2] * (e3 - e0)) + f0[3] * (e4 - e0)) + f0[4] * (e5 - e0);
-    bn1 = (((f1[0] * (e0 - e1) + f1[1] * (e2 - e1)) + f1[2] * (e3 - e1)) + f1[3] * (e4 - e1)) + f1[4] * (e5 - e1);
-    bn2 = (((f2[0] * (e0 - e2) + f2[1] * (e1 - e2)) + f2[2] * (e3 - e2)) + f2[3] * (e4 - e2)) + f2[4] * (e5 - e2);
+    const TT e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
+    bn = (((fbc(0, 0) * (e1 - e0) + fbc(0, 1) * (e2 - e0)) + fbc(0, 2) * (e3 - e0)) + fbc(0, 3) * (e4 - e0)) +
+         fbc(0, 4) * (e5 - e0);
+    bn1 = (((fbc(1, 0) * (e0 - e1) + fbc(1, 1) * (e2 - e1)) + fbc(1, 2) * (e3 - e1)) + fbc(1, 3) * (e4 - e1)) +
+          fbc(1, 4) * (e5 - e1);
+    bn2 = (((fbc(2, 0) * (e0 - e2) + fbc(2, 1) * (e1 - e2)) + fbc(2, 2) * (e3 - e2)) + fbc(2, 3) * (e4 - e2)) +
+          fbc(2, 4) * (e5 - e2);
   } else {
-    double t0 = 0.0, t1 = 0.0;
+    TT t0 = 0, t1 = 0;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      const double v = S(N - i);
-      t0 = t0 + sc->pbci[1][0][i] * v;
-      t1 = t1 + sc->pbci[1][1][i] * v;
+      const TT v = S(N - i);
+      t0 = t0 + TT(sc->pbci[1][0][i]) * v;
+      t1 = t1 + TT(sc->pbci[1][1][i]) * v;
     }
-    const double e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
-    const double ra2 = e2 + e2;
+    const TT e0 = S(N), e1 = S(N - 1), e2 = S(N - 2), e3 = S(N - 3), e4 = S(N - 4), e5 = S(N - 5);
+    const TT ra2 = e2 + e2;
     bn = t0 + r01;
     bn1 = t1 + r11;
     bn2 = (fa * ((e3 + e1) - ra2) + fb * ((e4 + e0) - ra2)) + fc * ((e5 + r21) - ra2);
   }
   // forward elimination: rows 0..2 from the closures, 3..N-3 interior
-  double w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3), w4 = S(4), w5 = S(5);  // s[i-3..i+2] at i = 3
-  double am2 = b0;
-  double am1 = b1 - __ldg(F.l2 + 1) * am2;
-  double a2 = (b2 - __ldg(F.l1 + 2) * am2) - __ldg(F.l2 + 2) * am1;
-  S(0) = am2;
-  S(1) = am1;
-  S(2) = a2;
+  TT w0 = S(0), w1 = S(1), w2 = S(2), w3 = S(3), w4 = S(4), w5 = S(5);  // s[i-3..i+2] at i = 3
+  RS am2 = RS(b0);
+  RS am1 = RS(b1) - __ldg(F.l2 + 1) * am2;
+  const RS a2 = (RS(b2) - __ldg(F.l1 + 2) * am2) - __ldg(F.l2 + 2) * am1;
+  S(0) = TT(am2);
+  S(1) = TT(am1);
+  S(2) = TT(a2);
   am2 = am1;
   am1 = a2;
 #define FWD(L1, L2)                                                                                       \
   {                                                                                                       \
-    const double w6 = S(i + 3);                                                                           \
-    const double rk = w3 + w3;                                                                            \
-    const double rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);           \
-    const double a = (rhs - (L1) * am2) - (L2) * am1;                                                     \
-    S(i) = a;                                                                                             \
+    const TT w6 = S(i + 3);                                                                               \
+    const TT rk = w3 + w3;                                                                                \
+    const TT rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);               \
+    const RS a = (RS(rhs) - (L1) * am2) - (L2) * am1;                                                     \
+    S(i) = TT(a);                                                                                         \
     w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;                                                 \
     am2 = am1; am1 = a;                                                                                   \
   }
-#define BLOCK8(CF) fwd8_filter<ST>(s, i, CF, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1)
+#define BLOCK8(CF) fwd8_filter<ST, TT, RS>(s, i, CF, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1)
   FORWARD_ROWS(3, N - 3, 3, BLOCK8, FWD)
 #undef BLOCK8
 #undef FWD
   {
-    double a = (bn2 - __ldg(F.l1 + N - 2) * am2) - __ldg(F.l2 + N - 2) * am1;
-    S(N - 2) = a;
+    RS a = (RS(bn2) - __ldg(F.l1 + N - 2) * am2) - __ldg(F.l2 + N - 2) * am1;
+    S(N - 2) = TT(a);
     am2 = am1; am1 = a;
-    a = (bn1 - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
-    S(N - 1) = a;
+    a = (RS(bn1) - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
+    S(N - 1) = TT(a);
     am2 = am1; am1 = a;
-    a = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
-    S(N) = a;
+    a = (RS(bn) - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
+    S(N) = TT(a);
   }
   BACKWARD_ROWS(done)
 #undef S
@@ -550,29 +585,41 @@ __device__ __forceinline__ int find_task(const int* __restrict__ tile0, int ntas
   return lo;
 }
 
-// Line pitch (doubles) of the dir-1 shared-memory tile: >= round_up(L, 2) and
-// = 2 (mod 4), so rows start 16-byte aligned and 64-bit column walks see at
-// most 2-way bank conflicts.
+// Line pitch (elements) of the row-major xi tile, whose rows arrive by one
+// bulk copy per line: rows start 16-byte aligned; FP64: = 2 (mod 4) doubles,
+// so 64-bit column walks see at most 2-way bank conflicts; FP32: an odd number
+// of 16-byte units (4-way for 32-bit walks, which measured faster than
+// element-wise copies into a conflict-free transposed tile).
+template <class TT>
 __host__ __device__ __forceinline__ int dir1_pitch(int L) {
-  int p = (L + 1) / 2 * 2;
-  if (p % 4 == 0) p += 2;
+  if (sizeof(TT) == 8) {
+    int p = (L + 1) / 2 * 2;
+    if (p % 4 == 0) p += 2;
+    return p;
+  }
+  int p = (L + 3) / 4 * 4;
+  if ((p / 4) % 2 == 0) p += 4;
   return p;
 }
 
 // One CTA = one warp = 32 lines. DIR: 1 xi, 2 eta, 3 zeta. OP: 0 derivative,
-// 1 filter (in place, f += increment). The tile moves in chunks (see
-// ChunkIn): loads overlap the forward sweep, stores the back substitution.
-template <int DIR, int OP>
+// 1 filter (in place, f += increment). TT: field and tile type, RS: type of
+// the elimination. The tile moves in chunks (see ChunkIn): loads overlap the
+// forward sweep, stores the back substitution.
+template <int DIR, int OP, class TT, class RS>
 __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
                                              int ntasks, const CUtensorMap* __restrict__ maps,
                                              int* __restrict__ err) {
+  constexpr int kVec = 16 / (int)sizeof(TT);  // elements per 16 bytes
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
-  double* s = reinterpret_cast<double*>(smem_raw + 128);
+  TT* s = reinterpret_cast<TT*>(smem_raw + 128);
   const int lane = threadIdx.x;
   TRACE(0)
   const int ti = find_task(tile0s, ntasks, blockIdx.x);
   const LineTask& T = tasks[ti];
+  const TT* in = static_cast<const TT*>(T.in);
+  TT* out = static_cast<TT*>(T.out);
   const int lt = blockIdx.x - T.tile0;
   const int L = T.L;
   const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
@@ -586,7 +633,7 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     x0 = (lt % T.ntx) * kLanes;
     nval = min(kLanes, X - x0);
   }
-  const int P = dir1_pitch(L);
+  const int P = dir1_pitch<TT>(L);
   const long long pstride = (DIR == 2) ? (long long)Xp : (long long)Xp * Y;  // dir 2/3 position stride
   const long long base = (DIR == 1) ? (long long)r0 * Xp
                                     : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
@@ -601,13 +648,13 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   for (int k = 0; k < NC; ++k) {
     const int c = (k == 0) ? 0 : (k == 1 ? NC - 1 : k - 1);
     if (DIR == 1) {
-      const uint32_t bytes = (uint32_t)((chunk_len(c) + 1) / 2 * 2 * sizeof(double));
+      const uint32_t bytes = (uint32_t)((chunk_len(c) + kVec - 1) / kVec * kVec * sizeof(TT));
       if (lane == 0) mbar_expect_tx(bars + c, bytes * nval);
       __syncwarp();
       if (lane < nval)
-        bulk_g2s(s + lane * P + c * CR, T.in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
+        bulk_g2s(s + lane * P + c * CR, in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
     } else if (lane == 0) {
-      mbar_expect_tx(bars + c, (uint32_t)(CR * kLanes * sizeof(double)));
+      mbar_expect_tx(bars + c, (uint32_t)(CR * kLanes * sizeof(TT)));
       if (DIR == 2) tma_load_3d(s + c * CR * kLanes, map_in, x0, c * CR, fix, bars + c);
       else tma_load_3d(s + c * CR * kLanes, map_in, x0, fix, c * CR, bars + c);
     }
@@ -615,8 +662,11 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   TRACE(1)
   if (!mbar_wait(bars, 0) || !mbar_wait(bars + NC - 1, 0)) {
     if (lane == 0) atomicExch(err, kErrTimeout);
+    // copies may still be landing: wait for the other chunks (bounded) before exit
+    for (int c = 1; c < NC - 1; ++c) mbar_wait(bars + c, 0);
     return;
   }
+  __syncwarp();
   TRACE(2)
   ChunkIn CI{bars, CR, NC, L, 1, (NC > 1 ? CR : L)};
   if (NC <= 2) CI.ready = L;
@@ -630,11 +680,20 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     if (OP == 1) {
       if (DIR != 1) {
         if (lane < nval) {
-          const double* g = T.in + base + lane;
-          double* col = s + lane;
+          const TT* g = in + base + lane;
+          TT* col = s + lane;
           int i = lo;
+          // 32 loads in flight per lane: the originals come back from L2, and
+          // fewer outstanding loads leave this step latency-bound
+          for (; i + 32 <= lo + len; i += 32) {
+            TT v[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+#pragma unroll
+            for (int k = 0; k < 32; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
+          }
           for (; i + 8 <= lo + len; i += 8) {
-            double v[8];
+            TT v[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
 #pragma unroll
@@ -646,12 +705,25 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
         __syncwarp();
         const int tot = nval * len;
         int e = lane;
+        for (; e + 31 * kLanes < tot; e += 32 * kLanes) {
+          TT v[32];
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
+            v[k] = __ldg(in + base + (long long)r * Xp + i);
+          }
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
+            s[r * P + i] = v[k] + s[r * P + i];
+          }
+        }
         for (; e + 7 * kLanes < tot; e += 8 * kLanes) {
-          double v[8];
+          TT v[8];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
             const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
-            v[k] = __ldg(T.in + base + (long long)r * Xp + i);
+            v[k] = __ldg(in + base + (long long)r * Xp + i);
           }
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
@@ -661,7 +733,7 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
         }
         for (; e < tot; e += kLanes) {
           const int r = e / len, i = lo + e - r * len;
-          s[r * P + i] = __ldg(T.in + base + (long long)r * Xp + i) + s[r * P + i];
+          s[r * P + i] = __ldg(in + base + (long long)r * Xp + i) + s[r * P + i];
         }
       }
     }
@@ -669,8 +741,8 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     __syncwarp();
     if (DIR == 1) {
       if (lane < nval) {
-        bulk_s2g(T.out + base + (long long)lane * Xp + lo, s + lane * P + lo,
-                 (uint32_t)((len + 1) / 2 * 2 * sizeof(double)));
+        bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                 (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
         bulk_commit();
       }
     } else if (lane == 0) {
@@ -691,22 +763,24 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   else jk = fix * X + x0 + lane;
   const int nbs = T.nbs;
   constexpr int ST = (DIR == 1) ? 1 : kLanes;
-  double* sl = (DIR == 1) ? s + lane * P : s + lane;
-  const LuRows F(T.lu, L, T.cl1, T.cl2, T.cu1, T.cu2, T.cu3, T.c0);
+  TT* sl = (DIR == 1) ? s + lane * P : s + lane;
+  const LuRows<RS> F(static_cast<const RS*>(T.lu), L, RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3), T.c0);
+  const TT* recv = static_cast<const TT*>(T.recv);
   if (OP == 0) {
-    double r00 = 0, r10 = 0, r01 = 0, r11 = 0;
-    if (has && T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; }
-    if (has && T.ndf1) { r01 = T.recv[2 * nbs + jk]; r11 = T.recv[3 * nbs + jk]; }
-    ok = sweep_deriv<ST>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11, CI, err, done);
+    TT r00 = 0, r10 = 0, r01 = 0, r11 = 0;
+    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; }
+    if (has && T.ndf1) { r01 = recv[2 * nbs + jk]; r11 = recv[3 * nbs + jk]; }
+    ok = sweep_deriv<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11, CI, err, done);
     if (ok && has && T.drva) {
-      T.drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
-      T.drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
+      TT* drva = static_cast<TT*>(T.drva);
+      drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+      drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
     }
   } else {
-    double r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
-    if (has && T.ndf0) { r00 = T.recv[jk]; r10 = T.recv[nbs + jk]; r20 = T.recv[2 * nbs + jk]; }
-    if (has && T.ndf1) { r01 = T.recv[3 * nbs + jk]; r11 = T.recv[4 * nbs + jk]; r21 = T.recv[5 * nbs + jk]; }
-    ok = sweep_filter<ST>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, CI, err, done);
+    TT r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
+    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; r20 = recv[2 * nbs + jk]; }
+    if (has && T.ndf1) { r01 = recv[3 * nbs + jk]; r11 = recv[4 * nbs + jk]; r21 = recv[5 * nbs + jk]; }
+    ok = sweep_filter<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, CI, err, done);
   }
   // every issued bulk store has to finish reading shared memory before exit;
   // after a timeout, wait for the chunks still in flight (bounded) instead
@@ -733,48 +807,63 @@ __device__ __forceinline__ void line_xyz(int nn, int pos, int j, int k, int& x, 
   else { x = j; y = k; z = pos; }
 }
 
-// t_numerics%mpigo for a list of faces (src/mo_numerics.f90:429-565).
+// t_numerics%mpigo for a list of faces (src/mo_numerics.f90:429-565), in the
+// field type T.
+template <class T>
 __global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restrict__ line0s, int ntasks,
                         int nlines) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
     const int ti = find_task(line0s, ntasks, g);
-    const FaceTask& T = tasks[ti];
-    const int jk = g - T.line0;
-    const int j = jk % T.nj, k = jk / T.nj;
-    const int istart = T.sb * T.N, step = 1 - 2 * T.sb;
+    const FaceTask& F = tasks[ti];
+    const T* src = static_cast<const T*>(F.src);
+    // eta faces run x fastest across threads so their reads coalesce; the
+    // other faces already do (zeta) or read 12 contiguous values (xi)
+    const int gl = g - F.line0;
+    int j, k, jk;
+    if (F.nn == 2) {
+      k = gl % F.X;
+      j = gl / F.X;
+      jk = j + F.nj * k;
+    } else {
+      jk = gl;
+      j = jk % F.nj;
+      k = jk / F.nj;
+    }
+    const int istart = F.sb * F.N, step = 1 - 2 * F.sb;
     int x, y, z;
-    line_xyz(T.nn, istart, j, k, x, y, z);
-    const double resk = T.ra0k * T.src[((long long)z * T.Y + y) * T.Xp + x];
-    const DevScheme* sc = T.sc;
-    const int nt = T.nt;
-    double t0 = 0.0, t1 = 0.0, sap0 = 0.0;
+    line_xyz(F.nn, istart, j, k, x, y, z);
+    const T resk = T(F.ra0k) * src[((long long)z * F.Y + y) * F.Xp + x];
+    const DevScheme* sc = F.sc;
+    const int nt = F.nt;
+    T t0 = 0, t1 = 0, sap0 = 0;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      line_xyz(T.nn, istart + step * (i + T.iik), j, k, x, y, z);
-      const double v = T.src[((long long)z * T.Y + y) * T.Xp + x];
+      line_xyz(F.nn, istart + step * (i + F.iik), j, k, x, y, z);
+      const T v = src[((long long)z * F.Y + y) * F.Xp + x];
       if (i == 0) sap0 = v;
-      t0 = t0 + sc->pbco[nt][0][i] * v;
-      t1 = t1 + sc->pbco[nt][1][i] * v;
+      t0 = t0 + T(sc->pbco[nt][0][i]) * v;
+      t1 = t1 + T(sc->pbco[nt][1][i]) * v;
     }
-    double snd0 = t0 - resk * sc->pbcot[nt][0];
-    double snd1 = t1 - resk * sc->pbcot[nt][1];
-    double snd2 = 0.0;
+    T snd0 = t0 - resk * T(sc->pbcot[nt][0]);
+    T snd1 = t1 - resk * T(sc->pbcot[nt][1]);
+    T snd2 = 0;
     if (nt == 1) {
-      const double old = T.chain[jk];
+      const T old = T(F.chain[jk]);
       snd2 = old + ((sap0 - resk) - old);
-      T.chain[jk] = snd2;
+      F.chain[jk] = double(snd2);
     }
-    if (T.exch) {
-      if (T.corr) {  // receiver side is periodic and n45 = n45go
-        line_xyz(T.nn, (1 - T.sb) * T.NA, j, k, x, y, z);
-        const double f = T.dstf[((long long)z * T.YA + y) * T.XpA + x];
-        snd0 = snd0 + f * sc->pbcot[nt][0];
-        snd1 = snd1 + f * sc->pbcot[nt][1];
-        if (nt == 1) snd2 = snd2 + f; else snd1 = snd1 + 0.0 * f;
+    if (F.exch) {
+      T* recv = static_cast<T*>(F.recv);
+      if (F.corr) {  // receiver side is periodic and n45 = n45go
+        line_xyz(F.nn, (1 - F.sb) * F.NA, j, k, x, y, z);
+        const T f = static_cast<const T*>(F.dstf)[((long long)z * F.YA + y) * F.XpA + x];
+        snd0 = snd0 + f * T(sc->pbcot[nt][0]);
+        snd1 = snd1 + f * T(sc->pbcot[nt][1]);
+        if (nt == 1) snd2 = snd2 + f; else snd1 = snd1 + T(0) * f;
       }
-      T.recv[jk] = snd0;
-      T.recv[T.nbs + jk] = snd1;
-      if (nt == 1) T.recv[2 * T.nbs + jk] = snd2;
+      recv[jk] = snd0;
+      recv[F.nbs + jk] = snd1;
+      if (nt == 1) recv[2 * F.nbs + jk] = snd2;
     }
   }
 }
@@ -790,26 +879,31 @@ __global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restric
 constexpr double kGam = 1.4;
 #define KGAMM1 (kGam - 1.0)
 
-// primitives, pressure, Sutherland viscosity (src/mo_canard_driver.f90:267-275)
+// primitives, pressure, Sutherland viscosity (src/mo_canard_driver.f90:267-275),
+// evaluated in FP64 and stored in the flux type R
+template <class R>
 __global__ void k_prim(const BlockDev* __restrict__ bd, const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const CaseConst C = cc[B.case_id];
     const double* q = B.qa;
-    double* de = B.de;
+    R* de = W.de;
     const double q0 = q[l], q1 = q[l + n], q2 = q[l + 2 * n], q3 = q[l + 3 * n], q4 = q[l + 4 * n];
     const double d1 = 1.0 / q0;
     const double d2 = q1 * d1, d3 = q2 * d1, d4 = q3 * d1;
     const double p = KGAMM1 * (q4 - 0.5 * ((q1 * d2 + q2 * d3) + q3 * d4));
     const double d5 = (kGam * p) * d1;
-    de[l] = d1; de[l + n] = d2; de[l + 2 * n] = d3; de[l + 3 * n] = d4; de[l + 4 * n] = d5;
-    B.p[l] = p;
-    B.mu[l] = (C.srefp1dre * pow15(d5)) / (d5 + C.srefoo);
+    de[l] = R(d1); de[l + n] = R(d2); de[l + 2 * n] = R(d3); de[l + 3 * n] = R(d4); de[l + 4 * n] = R(d5);
+    W.p[l] = R(p);
+    W.mu[l] = R((C.srefp1dre * pow15(d5)) / (d5 + C.srefoo));
   }
 }
 
-// time-step maxima (src/mo_physics.f90:185-207); values are >= 0, so their
-// bit patterns order like the values and atomicMax on them is exact.
+// time-step maxima (src/mo_physics.f90:185-207) in FP64 from the FP64 metrics;
+// values are >= 0, so their bit patterns order like the values and atomicMax
+// on them is exact.
+template <class R>
 __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
                         const CaseConst* __restrict__ cc, unsigned long long* __restrict__ out) {
   const BlockDev& B0 = bd[blockIdx.y];
@@ -817,8 +911,10 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
   const int visc = cc[B0.case_id].viscous;
   double m1 = 0.0, m2 = 0.0;
   FOR_POINTS(B0) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
-    const double *xi = B.xim, *et = B.etm, *ze = B.zem, *de = B.de;
+    const double *xi = B.xim, *et = B.etm, *ze = B.zem;
+    const R* de = W.de;
     double r1 = xi[l] * xi[l];
     r1 = r1 + xi[l + n] * xi[l + n];
     r1 = r1 + xi[l + 2 * n] * xi[l + 2 * n];
@@ -828,13 +924,14 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
     r1 = r1 + ze[l] * ze[l];
     r1 = r1 + ze[l + n] * ze[l + n];
     r1 = r1 + ze[l + 2 * n] * ze[l + 2 * n];
-    const double u = de[l + n] + S.umf[0], v = de[l + 2 * n] + S.umf[1], w = de[l + 3 * n] + S.umf[2];
+    const double u = double(de[l + n]) + S.umf[0], v = double(de[l + 2 * n]) + S.umf[1],
+                 w = double(de[l + 3 * n]) + S.umf[2];
     double r2 = fabs((xi[l] * u + xi[l + n] * v) + xi[l + 2 * n] * w) +
                 fabs((et[l] * u + et[l + n] * v) + et[l + 2 * n] * w);
     r2 = r2 + fabs((ze[l] * u + ze[l + n] * v) + ze[l + 2 * n] * w);
     const double ssi = fabs(B.yaco[l]);
-    m1 = fmax(m1, (sqrt(de[l + 4 * n] * r1) + r2) * ssi);
-    if (visc) m2 = fmax(m2, (((de[l] * B.mu[l]) * r1) * ssi) * ssi);
+    m1 = fmax(m1, (sqrt(double(de[l + 4 * n]) * r1) + r2) * ssi);
+    if (visc) m2 = fmax(m2, (((double(de[l]) * double(W.mu[l])) * r1) * ssi) * ssi);
   }
   for (int o = 16; o > 0; o >>= 1) {
     m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
@@ -846,394 +943,428 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
   }
 }
 
-// viscous stresses and heat flux from the 12 gradients in scr
+// viscous stresses and heat flux of one point from the 12 gradients in scr
 // (src/mo_physics.f90:245-299); scr field g*3+d = d/d(xi_d) of u, v, w, T.
+// t = txx tyy tzz txy tyz tzx hxx hyy hzz; d5 = (2/3) div u.
+template <class R>
+__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5) {
+  const R *xi = W.xim, *et = W.etm, *ze = W.zem, *g = W.scr;
+  auto comb = [&](int f, int c) {
+    return (xi[l + c * n] * g[l + (3 * f) * n] + et[l + c * n] * g[l + (3 * f + 1) * n]) +
+           ze[l + c * n] * g[l + (3 * f + 2) * n];
+  };
+  R txx = comb(0, 0), hzz = comb(0, 1), tzx = comb(0, 2);
+  R txy = comb(1, 0), tyy = comb(1, 1), hxx = comb(1, 2);
+  R hyy = comb(2, 0), tyz = comb(2, 1), tzz = comb(2, 2);
+  const R s1 = comb(3, 0), s2 = comb(3, 1), s3 = comb(3, 2);
+  const R rr1 = mu * W.yaco[l];
+  const R rr2 = R(1.0 / (KGAMM1 * 0.71)) * rr1;
+  d5 = R(2.0 / 3.0) * ((txx + tyy) + tzz);
+  txx = rr1 * ((txx + txx) - d5);
+  tyy = rr1 * ((tyy + tyy) - d5);
+  tzz = rr1 * ((tzz + tzz) - d5);
+  txy = rr1 * (txy + hzz);
+  tyz = rr1 * (tyz + hxx);
+  tzx = rr1 * (tzx + hyy);
+  const R u = W.de[l + n], v = W.de[l + 2 * n], w = W.de[l + 3 * n];
+  hxx = ((rr2 * s1 + u * txx) + v * txy) + w * tzx;
+  hyy = ((rr2 * s2 + u * txy) + v * tyy) + w * tyz;
+  hzz = ((rr2 * s3 + u * tzx) + v * tyz) + w * tzz;
+  t[0] = txx; t[1] = tyy; t[2] = tzz; t[3] = txy; t[4] = tyz; t[5] = tzx; t[6] = hxx; t[7] = hyy; t[8] = hzz;
+}
+
+// flux components rr(:,d,m) of one point into scr field (m-1)*3 + d and
+// de(:,5) = qa(:,5) + p (src/mo_physics.f90:319-382); t as from visc_point
+template <class R>
+__device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
+                                           long long l, long long n, const R t[9]) {
+  const double* q = B.qa;
+  R* de = W.de;
+  const R p = W.p[l];
+  const R* mt[3] = {W.xim, W.etm, W.zem};
+  const R um0 = R(S.umf[0]), um1 = R(S.umf[1]), um2 = R(S.umf[2]);
+  const R u = de[l + n] + um0, v = de[l + 2 * n] + um1, w = de[l + 3 * n] + um2;
+  R ssd[3], m[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
+    ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
+  }
+  R* r = W.scr;
+  const R q0 = R(q[l]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r[l + d * n] = q0 * ssd[d];
+  R tau[3][3];
+  R hx = 0, hy = 0, hz = 0;
+  if (visc) {
+    tau[0][0] = t[0]; tau[0][1] = t[3]; tau[0][2] = t[5];
+    tau[1][0] = t[3]; tau[1][1] = t[1]; tau[1][2] = t[4];
+    tau[2][0] = t[5]; tau[2][1] = t[4]; tau[2][2] = t[2];
+    hx = t[6]; hy = t[7]; hz = t[8];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const R qc = R(q[l + (c + 1) * n]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      R v1 = qc * ssd[d] + m[d][c] * p;
+      if (visc) {
+        v1 = v1 - m[d][0] * tau[c][0];
+        v1 = v1 - m[d][1] * tau[c][1];
+        v1 = v1 - m[d][2] * tau[c][2];
+      }
+      r[l + (3 * (c + 1) + d) * n] = v1;
+    }
+  }
+  const R d5 = R(q[l + 4 * n]) + p;
+  de[l + 4 * n] = d5;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    R v1 = d5 * ssd[d] - p * ((um0 * m[d][0] + um1 * m[d][1]) + um2 * m[d][2]);
+    if (visc) {
+      v1 = v1 - m[d][0] * hx;
+      v1 = v1 - m[d][1] * hy;
+      v1 = v1 - m[d][2] * hz;
+    }
+    r[l + (12 + d) * n] = v1;
+  }
+}
+
+// calc_viscous_shear_stress on its own (the phase of the C ABI): tau and
+// de(:,5); de(:,1) holds ss(:,1)
+template <class R>
 __global__ void k_viscous_assemble(const BlockDev* __restrict__ bd) {
   FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
-    const double *xi = B.xim, *et = B.etm, *ze = B.zem, *g = B.scr;
-    auto comb = [&](int f, int c) {
-      return (xi[l + c * n] * g[l + (3 * f) * n] + et[l + c * n] * g[l + (3 * f + 1) * n]) +
-             ze[l + c * n] * g[l + (3 * f + 2) * n];
-    };
-    double txx = comb(0, 0), hzz = comb(0, 1), tzx = comb(0, 2);
-    double txy = comb(1, 0), tyy = comb(1, 1), hxx = comb(1, 2);
-    double hyy = comb(2, 0), tyz = comb(2, 1), tzz = comb(2, 2);
-    const double s1 = comb(3, 0), s2 = comb(3, 1), s3 = comb(3, 2);
-    double* de = B.de;
-    const double rr1 = de[l] * B.yaco[l];
-    const double rr2 = (1.0 / (KGAMM1 * 0.71)) * rr1;
-    const double d5 = (2.0 / 3.0) * ((txx + tyy) + tzz);
-    de[l + 4 * n] = d5;
-    txx = rr1 * ((txx + txx) - d5);
-    tyy = rr1 * ((tyy + tyy) - d5);
-    tzz = rr1 * ((tzz + tzz) - d5);
-    txy = rr1 * (txy + hzz);
-    tyz = rr1 * (tyz + hxx);
-    tzx = rr1 * (tzx + hyy);
-    const double u = de[l + n], v = de[l + 2 * n], w = de[l + 3 * n];
-    hxx = ((rr2 * s1 + u * txx) + v * txy) + w * tzx;
-    hyy = ((rr2 * s2 + u * txy) + v * tyy) + w * tyz;
-    hzz = ((rr2 * s3 + u * tzx) + v * tyz) + w * tzz;
-    double* t = B.tau;
-    t[l] = txx; t[l + n] = tyy; t[l + 2 * n] = tzz; t[l + 3 * n] = txy; t[l + 4 * n] = tyz;
-    t[l + 5 * n] = tzx; t[l + 6 * n] = hxx; t[l + 7 * n] = hyy; t[l + 8 * n] = hzz;
+    R t[9], d5;
+    visc_point<R>(W, l, n, W.de[l], t, d5);
+    W.de[l + 4 * n] = d5;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) W.tau[l + k * n] = t[k];
   }
 }
 
 // de(:,1) = ss(:,1) before the viscous gradients (src/mo_physics.f90:228)
+template <class R>
 __global__ void k_copy_mu(const BlockDev* __restrict__ bd) {
-  FOR_POINTS(bd[blockIdx.y]) { B.de[l] = B.mu[l]; }
+  FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
+    W.de[l] = W.mu[l];
+  }
 }
 
-// flux components rr(:,d,m) into scr field (m-1)*3 + d (src/mo_physics.f90:319-382)
+// calc_fluxes on its own (the phase of the C ABI), from the stored tau
+template <class R>
 __global__ void k_flux(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
                        const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
-    const StageParams S = sp[B.case_id];
-    const int visc = cc[B.case_id].viscous;
-    const double* q = B.qa;
-    double* de = B.de;
-    const double p = B.p[l];
-    const double* mt[3] = {B.xim, B.etm, B.zem};
-    const double u = de[l + n] + S.umf[0], v = de[l + 2 * n] + S.umf[1], w = de[l + 3 * n] + S.umf[2];
-    double ssd[3], m[3][3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
-      ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
-    }
-    double* r = B.scr;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) r[l + d * n] = q[l] * ssd[d];
-    double tau[3][3];
-    double hx = 0, hy = 0, hz = 0;
+    const bool visc = cc[B.case_id].viscous != 0;
+    R t[9] = {};
     if (visc) {
-      const double* t = B.tau;
-      tau[0][0] = t[l]; tau[0][1] = t[l + 3 * n]; tau[0][2] = t[l + 5 * n];
-      tau[1][0] = t[l + 3 * n]; tau[1][1] = t[l + n]; tau[1][2] = t[l + 4 * n];
-      tau[2][0] = t[l + 5 * n]; tau[2][1] = t[l + 4 * n]; tau[2][2] = t[l + 2 * n];
-      hx = t[l + 6 * n]; hy = t[l + 7 * n]; hz = t[l + 8 * n];
-    }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double qc = q[l + (c + 1) * n];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double v1 = qc * ssd[d] + m[d][c] * p;
-        if (visc) {
-          v1 = v1 - m[d][0] * tau[c][0];
-          v1 = v1 - m[d][1] * tau[c][1];
-          v1 = v1 - m[d][2] * tau[c][2];
-        }
-        r[l + (3 * (c + 1) + d) * n] = v1;
-      }
+      for (int k = 0; k < 9; ++k) t[k] = W.tau[l + k * n];
     }
-    const double d5 = q[l + 4 * n] + p;
-    de[l + 4 * n] = d5;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      double v1 = d5 * ssd[d] - p * ((S.umf[0] * m[d][0] + S.umf[1] * m[d][1]) + S.umf[2] * m[d][2]);
-      if (visc) {
-        v1 = v1 - m[d][0] * hx;
-        v1 = v1 - m[d][1] * hy;
-        v1 = v1 - m[d][2] * hz;
-      }
-      r[l + (12 + d) * n] = v1;
+    flux_point<R>(W, B, sp[B.case_id], visc, l, n, t);
+  }
+}
+
+// The step path's fusion of the two: stresses stay in registers instead of a
+// 9-field round trip through memory. Same operations in the same order, so
+// the results are bit-identical to k_viscous_assemble followed by k_flux
+// (de(:,1) = ss(:,1) is read from ss directly).
+template <class R>
+__global__ void k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                            const CaseConst* __restrict__ cc) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
+    const long long n = B.npad;
+    const bool visc = cc[B.case_id].viscous != 0;
+    R t[9] = {};
+    if (visc) {
+      R d5;
+      visc_point<R>(W, l, n, W.mu[l], t, d5);
     }
+    flux_point<R>(W, B, sp[B.case_id], visc, l, n, t);
   }
 }
 
 // de(:,m) = sum of the three flux derivatives (src/mo_physics.f90:399)
+template <class R>
 __global__ void k_flux_sum(const BlockDev* __restrict__ bd) {
   FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
-    const double* r = B.scr;
+    const R* r = W.scr;
 #pragma unroll
     for (int m = 0; m < 5; ++m)
-      B.de[l + m * n] = (r[l + (3 * m) * n] + r[l + (3 * m + 1) * n]) + r[l + (3 * m + 2) * n];
+      W.de[l + m * n] = (r[l + (3 * m) * n] + r[l + (3 * m + 1) * n]) + r[l + (3 * m + 2) * n];
   }
 }
 
-// RK stage update (src/mo_canard_driver.f90:329-334)
+// RK stage update in FP64 (src/mo_canard_driver.f90:329-334)
+template <class R>
 __global__ void k_rk(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp) {
   FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const double r1 = sp[B.case_id].dtk * B.yaco[l];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) B.qa[l + c * n] = B.qo[l + c * n] - r1 * B.de[l + c * n];
-  }
-}
-
-__global__ void k_copy5(const BlockDev* __restrict__ bd) {  // qo = qa
-  FOR_POINTS(bd[blockIdx.y]) {
-    const long long n = B.npad;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) B.qo[l + c * n] = B.qa[l + c * n];
-  }
-}
-
-// cofactor metrics from the 9 coordinate derivatives in scr (src/mo_grid.f90:107-115);
-// scr field 3*(m-1)+(d-1) = d(coordinate m)/d(xi_d)
-__global__ void k_cofactors(const BlockDev* __restrict__ bd) {
-  FOR_POINTS(bd[blockIdx.y]) {
-    const long long n = B.npad;
-    const double* g = B.scr;
-    const double q1 = g[l], q2 = g[l + n], q3 = g[l + 2 * n];
-    const double a1 = g[l + 3 * n], a2 = g[l + 4 * n], a3 = g[l + 5 * n];
-    const double d1 = g[l + 6 * n], d2 = g[l + 7 * n], d3 = g[l + 8 * n];
-    B.xim[l] = a2 * d3 - d2 * a3;
-    B.xim[l + n] = d2 * q3 - q2 * d3;
-    B.xim[l + 2 * n] = q2 * a3 - a2 * q3;
-    B.etm[l] = a3 * d1 - d3 * a1;
-    B.etm[l + n] = d3 * q1 - q3 * d1;
-    B.etm[l + 2 * n] = q3 * a1 - a3 * q1;
-    B.zem[l] = a1 * d2 - d1 * a2;
-    B.zem[l + n] = d1 * q2 - q1 * d2;
-    B.zem[l + 2 * n] = q1 * a2 - a1 * q2;
-  }
-}
-
-// Jacobian (src/mo_grid.f90:157-159)
-__global__ void k_jacobian(const BlockDev* __restrict__ bd) {
-  FOR_POINTS(bd[blockIdx.y]) {
-    const long long n = B.npad;
-    const double* g = B.scr;
-    const double *xi = B.xim, *et = B.etm, *ze = B.zem;
-    double s = g[l] * xi[l];
-    s = s + g[l + n] * et[l];
-    s = s + g[l + 2 * n] * ze[l];
-    s = s + g[l + 3 * n] * xi[l + n];
-    s = s + g[l + 4 * n] * et[l + n];
-    s = s + g[l + 5 * n] * ze[l + n];
-    s = s + g[l + 6 * n] * xi[l + 2 * n];
-    s = s + g[l + 7 * n] * et[l + 2 * n];
-    s = s + g[l + 8 * n] * ze[l + 2 * n];
-    B.yaco[l] = 3.0 / s;
-  }
-}
-
-// unit face normals cm{1,2,3} (src/mo_grid.f90:161-186); one thread per face line.
-struct CmTask { int b, nn, side, nbs, nj, N, line0; double* cm; };
-__global__ void k_face_normals(const BlockDev* __restrict__ bd, const CmTask* __restrict__ tasks,
-                               const int* __restrict__ line0s, int ntasks, int nlines) {
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
-    const CmTask& T = tasks[find_task(line0s, ntasks, g)];
-    const BlockDev& B = bd[T.b];
-    const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
-    int x, y, z;
-    line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
-    const long long l = ((long long)z * B.Y + y) * B.Xp + x;
-    const double* met = T.nn == 1 ? B.xim : T.nn == 2 ? B.etm : B.zem;
-    const double ya = B.yaco[l];
-    const double r0 = ya * met[l], r1 = ya * met[l + B.npad], r2 = ya * met[l + 2 * B.npad];
-    const double f = 1.0 / sqrt((r0 * r0 + r1 * r1) + r2 * r2);
-    T.cm[jk] = f * r0;
-    T.cm[T.nbs + jk] = f * r1;
-    T.cm[2 * T.nbs + jk] = f * r2;
+    for (int c = 0; c < 5; ++c) B.qa[l + c * n] = B.qo[l + c * n] - r1 * double(W.de[l + c * n]);
   }
 }
 
 // ---------------------------------------------------------------------------
-// GCBC (src/mo_gcbc.f90:133-340, 506-611)
-struct Elem { double ao, aoi, ve[3], hv2, vn, vs; };
+// GCBC (src/mo_gcbc.f90:133-340, 506-611) in the flux type R
+template <class R>
+struct Elem { R ao, aoi, ve[3], hv2, vn, vs; };
 
-__device__ __forceinline__ Elem eleme(const double cm[3], double q1, double q2, double q3, double q4, double pp,
-                                      const double umf[3]) {
-  Elem e;
-  const double rhoi = 1.0 / q1;
-  e.ao = sqrt((kGam * rhoi) * pp);
-  e.aoi = 1.0 / e.ao;
+template <class R>
+__device__ __forceinline__ Elem<R> eleme(const R cm[3], R q1, R q2, R q3, R q4, R pp, const double umf[3]) {
+  Elem<R> e;
+  const R rhoi = R(1) / q1;
+  e.ao = sqrt((R(kGam) * rhoi) * pp);
+  e.aoi = R(1) / e.ao;
   e.ve[0] = rhoi * q2; e.ve[1] = rhoi * q3; e.ve[2] = rhoi * q4;
-  e.hv2 = 0.5 * ((e.ve[0] * e.ve[0] + e.ve[1] * e.ve[1]) + e.ve[2] * e.ve[2]);
+  e.hv2 = R(0.5) * ((e.ve[0] * e.ve[0] + e.ve[1] * e.ve[1]) + e.ve[2] * e.ve[2]);
   e.vn = (cm[0] * e.ve[0] + cm[1] * e.ve[1]) + cm[2] * e.ve[2];
-  e.vs = (cm[0] * umf[0] + cm[1] * umf[1]) + cm[2] * umf[2];
+  e.vs = (cm[0] * R(umf[0]) + cm[1] * R(umf[1])) + cm[2] * R(umf[2]);
   return e;
 }
 
 // r = X_{q->r} v (src/mo_gcbc.f90:506-548)
-__device__ __forceinline__ void q2r_apply(const Elem& e, const double cm[3], const double v[5], double r[5]) {
-  const double ho = (KGAMM1 * e.aoi) * e.aoi;
-  const double bo = 1 - ho * e.hv2;
-  const double co = e.aoi * e.vn;
-  double dm[3], rv[3];
+template <class R>
+__device__ __forceinline__ void q2r_apply(const Elem<R>& e, const R cm[3], const R v[5], R r[5]) {
+  const R ho = (R(KGAMM1) * e.aoi) * e.aoi;
+  const R bo = R(1) - ho * e.hv2;
+  const R co = e.aoi * e.vn;
+  R dm[3], rv[3];
   for (int d = 0; d < 3; ++d) { dm[d] = e.aoi * cm[d]; rv[d] = ho * e.ve[d]; }
-  const double* ve = e.ve;
-  double xt[5][5];
+  const R* ve = e.ve;
+  R xt[5][5];
   xt[0][0] = (bo * cm[0] + dm[1] * ve[2]) - dm[2] * ve[1];
   xt[0][1] = cm[0] * rv[0]; xt[0][2] = cm[0] * rv[1] + dm[2]; xt[0][3] = cm[0] * rv[2] - dm[1]; xt[0][4] = -ho * cm[0];
   xt[1][0] = (bo * cm[1] + dm[2] * ve[0]) - dm[0] * ve[2];
   xt[1][1] = cm[1] * rv[0] - dm[2]; xt[1][2] = cm[1] * rv[1]; xt[1][3] = cm[1] * rv[2] + dm[0]; xt[1][4] = -ho * cm[1];
   xt[2][0] = (bo * cm[2] + dm[0] * ve[1]) - dm[1] * ve[0];
   xt[2][1] = cm[2] * rv[0] + dm[1]; xt[2][2] = cm[2] * rv[1] - dm[0]; xt[2][3] = cm[2] * rv[2]; xt[2][4] = -ho * cm[2];
-  xt[3][0] = (1.0 - bo) - co; xt[3][1] = dm[0] - rv[0]; xt[3][2] = dm[1] - rv[1]; xt[3][3] = dm[2] - rv[2]; xt[3][4] = ho;
-  xt[4][0] = (1.0 - bo) + co; xt[4][1] = -dm[0] - rv[0]; xt[4][2] = -dm[1] - rv[1]; xt[4][3] = -dm[2] - rv[2]; xt[4][4] = ho;
+  xt[3][0] = (R(1) - bo) - co; xt[3][1] = dm[0] - rv[0]; xt[3][2] = dm[1] - rv[1]; xt[3][3] = dm[2] - rv[2];
+  xt[3][4] = ho;
+  xt[4][0] = (R(1) - bo) + co; xt[4][1] = -dm[0] - rv[0]; xt[4][2] = -dm[1] - rv[1]; xt[4][3] = -dm[2] - rv[2];
+  xt[4][4] = ho;
   for (int i = 0; i < 5; ++i) {
-    double s = 0.0;
+    R s = 0;
     for (int c = 0; c < 5; ++c) s = s + xt[i][c] * v[c];
     r[i] = s;
   }
 }
 
 // r = X_{r->q} v (src/mo_gcbc.f90:552-591)
-__device__ __forceinline__ void r2q_apply(const Elem& e, const double cm[3], const double v[5], double r[5]) {
-  const double bo = e.hv2 + ((1.0 / KGAMM1) * e.ao) * e.ao;
-  const double co = e.ao * e.vn;
-  double dm[3];
+template <class R>
+__device__ __forceinline__ void r2q_apply(const Elem<R>& e, const R cm[3], const R v[5], R r[5]) {
+  const R bo = e.hv2 + (R(1.0 / KGAMM1) * e.ao) * e.ao;
+  const R co = e.ao * e.vn;
+  R dm[3];
   for (int d = 0; d < 3; ++d) dm[d] = e.ao * cm[d];
-  const double* ve = e.ve;
-  double xt[5][5];
-  xt[0][0] = cm[0]; xt[0][1] = cm[1]; xt[0][2] = cm[2]; xt[0][3] = 0.5; xt[0][4] = 0.5;
+  const R* ve = e.ve;
+  R xt[5][5];
+  xt[0][0] = cm[0]; xt[0][1] = cm[1]; xt[0][2] = cm[2]; xt[0][3] = R(0.5); xt[0][4] = R(0.5);
   xt[1][0] = cm[0] * ve[0]; xt[1][1] = cm[1] * ve[0] - dm[2]; xt[1][2] = cm[2] * ve[0] + dm[1];
-  xt[1][3] = 0.5 * (ve[0] + dm[0]); xt[1][4] = xt[1][3] - dm[0];
+  xt[1][3] = R(0.5) * (ve[0] + dm[0]); xt[1][4] = xt[1][3] - dm[0];
   xt[2][0] = cm[0] * ve[1] + dm[2]; xt[2][1] = cm[1] * ve[1]; xt[2][2] = cm[2] * ve[1] - dm[0];
-  xt[2][3] = 0.5 * (ve[1] + dm[1]); xt[2][4] = xt[2][3] - dm[1];
+  xt[2][3] = R(0.5) * (ve[1] + dm[1]); xt[2][4] = xt[2][3] - dm[1];
   xt[3][0] = cm[0] * ve[2] - dm[1]; xt[3][1] = cm[1] * ve[2] + dm[0]; xt[3][2] = cm[2] * ve[2];
-  xt[3][3] = 0.5 * (ve[2] + dm[2]); xt[3][4] = xt[3][3] - dm[2];
+  xt[3][3] = R(0.5) * (ve[2] + dm[2]); xt[3][4] = xt[3][3] - dm[2];
   xt[4][0] = (e.hv2 * cm[0] + dm[2] * ve[1]) - dm[1] * ve[2];
   xt[4][1] = (e.hv2 * cm[1] + dm[0] * ve[2]) - dm[2] * ve[0];
   xt[4][2] = (e.hv2 * cm[2] + dm[1] * ve[0]) - dm[0] * ve[1];
-  xt[4][3] = 0.5 * (bo + co); xt[4][4] = xt[4][3] - co;
+  xt[4][3] = R(0.5) * (bo + co); xt[4][4] = xt[4][3] - co;
   for (int i = 0; i < 5; ++i) {
-    double s = 0.0;
+    R s = 0;
     for (int c = 0; c < 5; ++c) s = s + xt[i][c] * v[c];
     r[i] = s;
   }
 }
 
+template <class R>
 __global__ void k_gcbc_setup(const BlockDev* __restrict__ bd, const GcbcTask* __restrict__ tasks,
                              const int* __restrict__ line0s, int ntasks, int nlines,
                              const StageParams* __restrict__ sp) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
     const GcbcTask& T = tasks[find_task(line0s, ntasks, g)];
     const BlockDev& B = bd[T.b];
+    const Work<R> W = work<R>(B);
     const StageParams S = sp[B.case_id];
     const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
     int x, y, z;
     line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
     const long long n = B.npad;
     const long long l = ((long long)z * B.Y + y) * B.Xp + x;
-    const double cm[3] = {T.cm[jk], T.cm[T.nbs + jk], T.cm[2 * T.nbs + jk]};
-    const Elem e = eleme(cm, B.qa[l], B.qa[l + n], B.qa[l + 2 * n], B.qa[l + 3 * n], B.p[l], S.umf);
-    const double ra0 = (double)(((20 - T.bc) * (25 - T.bc) * (30 - T.bc)) / 3000);
-    const double ra1 = 1.0 - ra0;
-    double v[5], r[5];
+    const R cm[3] = {R(T.cm[jk]), R(T.cm[T.nbs + jk]), R(T.cm[2 * T.nbs + jk])};
+    const Elem<R> e =
+        eleme<R>(cm, R(B.qa[l]), R(B.qa[l + n]), R(B.qa[l + 2 * n]), R(B.qa[l + 3 * n]), W.p[l], S.umf);
+    const R ra0 = R(((20 - T.bc) * (25 - T.bc) * (30 - T.bc)) / 3000);
+    const R ra1 = R(1) - ra0;
+    R* drva = static_cast<R*>(T.drva);
+    R v[5], r[5];
     for (int c = 0; c < 5; ++c) {
-      const double cha = ra0 * T.drva[(long long)c * T.nbs + jk] + ra1 * B.de[l + c * n];
-      v[c] = B.yaco[l] * cha;
+      const R cha = ra0 * drva[(long long)c * T.nbs + jk] + ra1 * W.de[l + c * n];
+      v[c] = W.yaco[l] * cha;
     }
-    q2r_apply(e, cm, v, r);
-    for (int c = 0; c < 5; ++c) T.drva[(long long)c * T.nbs + jk] = r[c];
+    q2r_apply<R>(e, cm, v, r);
+    for (int c = 0; c < 5; ++c) drva[(long long)c * T.nbs + jk] = r[c];
   }
 }
 
+template <class R>
 __global__ void k_gcbc_update(const BlockDev* __restrict__ bd, const GcbcTask* __restrict__ tasks,
                               const int* __restrict__ line0s, int ntasks, int nlines,
                               const StageParams* __restrict__ sp) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
     const GcbcTask& T = tasks[find_task(line0s, ntasks, g)];
     const BlockDev& B = bd[T.b];
+    const Work<R> W = work<R>(B);
     const StageParams S = sp[B.case_id];
     const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
     int x, y, z;
     line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
     const long long n = B.npad;
     const long long l = ((long long)z * B.Y + y) * B.Xp + x;
-    const double cm[3] = {T.cm[jk], T.cm[T.nbs + jk], T.cm[2 * T.nbs + jk]};
-    const double q1 = B.qa[l];
-    const Elem e = eleme(cm, q1, B.qa[l + n], B.qa[l + 2 * n], B.qa[l + 3 * n], B.p[l], S.umf);
-    const double ra0 = 1 - 2 * T.side;
-    double cha[5], dha[5], drv[5];
+    const R cm[3] = {R(T.cm[jk]), R(T.cm[T.nbs + jk]), R(T.cm[2 * T.nbs + jk])};
+    const R q1 = R(B.qa[l]);
+    const Elem<R> e = eleme<R>(cm, q1, R(B.qa[l + n]), R(B.qa[l + 2 * n]), R(B.qa[l + 3 * n]), W.p[l], S.umf);
+    const R ra0 = R(1 - 2 * T.side);
+    const R* drva = static_cast<const R*>(T.drva);
+    const R* drvb = static_cast<const R*>(T.drvb);
+    R cha[5], dha[5], drv[5];
     for (int c = 0; c < 5; ++c) {
-      drv[c] = T.drva[(long long)c * T.nbs + jk];
+      drv[c] = drva[(long long)c * T.nbs + jk];
       cha[c] = drv[c];
-      dha[c] = T.drvb ? T.drvb[(long long)c * T.nbs + jk] : 0.0;
+      dha[c] = drvb ? drvb[(long long)c * T.nbs + jk] : R(0);
     }
     if (T.bc == 10) {
-      if (ra0 * ((e.vn + e.vs) + e.ao) > 0.0) cha[3] = 0.0;
-      if (ra0 * ((e.vn + e.vs) - e.ao) > 0.0) cha[4] = 0.0;
+      if (ra0 * ((e.vn + e.vs) + e.ao) > R(0)) cha[3] = 0;
+      if (ra0 * ((e.vn + e.vs) - e.ao) > R(0)) cha[4] = 0;
     } else if (T.bc == 20 || T.bc == 25) {
-      const double dtwi = 1.0 / (4 * S.dt + 1.0e-8);
-      double sd = 0.0;
-      for (int d = 0; d < 3; ++d) sd = sd + cm[d] * S.dudtmf[d];
-      cha[3 + T.side] = cha[4 - T.side] + (((2.0 * ra0) * e.aoi) * q1) * (sd + dtwi * (e.vn + e.vs));
+      const R dtwi = R(1.0 / (4 * S.dt + 1.0e-8));
+      R sd = 0;
+      for (int d = 0; d < 3; ++d) sd = sd + cm[d] * R(S.dudtmf[d]);
+      cha[3 + T.side] = cha[4 - T.side] + (((R(2) * ra0) * e.aoi) * q1) * (sd + dtwi * (e.vn + e.vs));
     } else {
-      if (ra0 * (e.vn + e.vs) > 0.0) { cha[0] = dha[0]; cha[1] = dha[1]; cha[2] = dha[2]; }
-      if (ra0 * ((e.vn + e.vs) + e.ao) > 0.0) cha[3] = dha[3];
-      if (ra0 * ((e.vn + e.vs) - e.ao) > 0.0) cha[4] = dha[4];
+      if (ra0 * (e.vn + e.vs) > R(0)) { cha[0] = dha[0]; cha[1] = dha[1]; cha[2] = dha[2]; }
+      if (ra0 * ((e.vn + e.vs) + e.ao) > R(0)) cha[3] = dha[3];
+      if (ra0 * ((e.vn + e.vs) - e.ao) > R(0)) cha[4] = dha[4];
     }
-    double v[5];
+    R v[5];
     for (int c = 0; c < 5; ++c) v[c] = cha[c] - drv[c];
-    r2q_apply(e, cm, v, dha);
+    r2q_apply<R>(e, cm, v, dha);
     for (int ii = 0; ii <= 4; ++ii) {
       const long long pt = T.pts[(long long)jk * 5 + ii];
-      const double w = T.w[(long long)jk * 5 + ii];
-      for (int c = 0; c < 5; ++c) B.de[pt + c * n] = B.de[pt + c * n] + w * dha[c];
+      const R w = R(T.w[(long long)jk * 5 + ii]);
+      for (int c = 0; c < 5; ++c) W.de[pt + c * n] = W.de[pt + c * n] + w * dha[c];
     }
   }
 }
 
-// sponge (src/mo_sponge.f90:265-278)
-struct SpongeTask { int b; const long long* pts; const double* asz; const double* bsz; int count, first; };
+// sponge (src/mo_sponge.f90:265-278): the forcing is formed in FP64 from the
+// FP64 state and added to de in the flux type
+template <class R>
 __global__ void k_sponge(const BlockDev* __restrict__ bd, const SpongeTask* __restrict__ tasks,
                          const int* __restrict__ first, int ntasks, int total) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const SpongeTask& T = tasks[find_task(first, ntasks, g)];
     const BlockDev& B = bd[T.b];
+    R* de = work<R>(B).de;
     const int e = g - T.first;
     const long long l = T.pts[e], n = B.npad;
     const double a = T.asz[e], bb = T.bsz[e];
-    B.de[l] = B.de[l] + a * (B.qa[l] - 1.0);
-    for (int d = 1; d <= 3; ++d) B.de[l + d * n] = B.de[l + d * n] + bb * (B.qa[l + d * n] - 0.0);
-    B.de[l + 4 * n] = B.de[l + 4 * n] + a * (B.qa[l + 4 * n] - (1.0 / kGam) * (1.0 / KGAMM1));
-  }
-}
-
-// junction / surface averaging: snapshot then ordered combination
-__global__ void k_avg_snapshot(const BlockDev* __restrict__ bd, const int* __restrict__ sb,
-                               const long long* __restrict__ sl, int nsrc, double* __restrict__ snap) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nsrc; e += gridDim.x * blockDim.x) {
-    const BlockDev& B = bd[sb[e]];
-    const long long l = sl[e];
-    for (int c = 0; c < 5; ++c) snap[(long long)e * 5 + c] = B.qa[l + c * B.npad];
-  }
-}
-// mode 0: sum and scale (average_point / average_line); mode 1: running
-// average of average_surface.
-__global__ void k_avg_combine(const BlockDev* __restrict__ bd, const int* __restrict__ tb,
-                              const long long* __restrict__ tl, const int* __restrict__ tfirst,
-                              const int* __restrict__ tcount, int ntg, const double* __restrict__ snap, int mode) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
-    const BlockDev& B = bd[tb[t]];
-    const long long l = tl[t];
-    const int f = tfirst[t], cnt = tcount[t];
-    for (int c = 0; c < 5; ++c) {
-      if (mode == 0) {
-        double acc = snap[(long long)f * 5 + c];
-        for (int j = 1; j < cnt; ++j) acc = acc + snap[(long long)(f + j) * 5 + c];
-        B.qa[l + c * B.npad] = (1.0 / (double)cnt) * acc;
-      } else {
-        double q = B.qa[l + c * B.npad];
-        double r1 = 1.0;
-        for (int j = 0; j < cnt; ++j) {
-          r1 = r1 + 1.0;
-          const double r2 = 1.0 / r1;
-          q = r2 * ((r1 - 1.0) * q + snap[(long long)(f + j) * 5 + c]) + 0.0 * q;
-        }
-        B.qa[l + c * B.npad] = q;
-      }
-    }
+    de[l] = R(double(de[l]) + a * (B.qa[l] - 1.0));
+    for (int d = 1; d <= 3; ++d) de[l + d * n] = R(double(de[l + d * n]) + bb * (B.qa[l + d * n] - 0.0));
+    de[l + 4 * n] = R(double(de[l + 4 * n]) + a * (B.qa[l + 4 * n] - (1.0 / kGam) * (1.0 / KGAMM1)));
   }
 }
 
 // drvb <- drva of the partner face (gcbc_comm, src/mo_gcbc.f90:186-220)
-__global__ void k_face_copy(const double* const* __restrict__ src, double* const* __restrict__ dst,
+template <class R>
+__global__ void k_face_copy(const void* const* __restrict__ src, void* const* __restrict__ dst,
                             const int* __restrict__ counts, int nfaces) {
   const int f = blockIdx.y;
   if (f >= nfaces) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < counts[f]; i += gridDim.x * blockDim.x)
-    dst[f][i] = src[f][i];
+  const R* s = static_cast<const R*>(src[f]);
+  R* d = static_cast<R*>(dst[f]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < counts[f]; i += gridDim.x * blockDim.x) d[i] = s[i];
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers. The FP64 translation unit instantiates them for double; the
+// float instantiations are made once, by the FMA-enabled FP32 translation
+// unit, and declared extern everywhere else (kernels_f32.h).
+template <class R>
+void launch_prim(dim3 g, cudaStream_t st, const BlockDev* bd, const CaseConst* cc) {
+  k_prim<R><<<g, 256, 0, st>>>(bd, cc);
+}
+template <class R>
+void launch_dtmax(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc,
+                  unsigned long long* out) {
+  k_dtmax<R><<<g, 256, 0, st>>>(bd, sp, cc, out);
+}
+template <class R>
+void launch_copy_mu(dim3 g, cudaStream_t st, const BlockDev* bd) {
+  k_copy_mu<R><<<g, 256, 0, st>>>(bd);
+}
+template <class R>
+void launch_viscous_assemble(dim3 g, cudaStream_t st, const BlockDev* bd) {
+  k_viscous_assemble<R><<<g, 256, 0, st>>>(bd);
+}
+template <class R>
+void launch_flux(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc) {
+  k_flux<R><<<g, 256, 0, st>>>(bd, sp, cc);
+}
+template <class R>
+void launch_flux_visc(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc) {
+  k_flux_visc<R><<<g, 256, 0, st>>>(bd, sp, cc);
+}
+template <class R>
+void launch_flux_sum(dim3 g, cudaStream_t st, const BlockDev* bd) {
+  k_flux_sum<R><<<g, 256, 0, st>>>(bd);
+}
+template <class R>
+void launch_rk(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp) {
+  k_rk<R><<<g, 256, 0, st>>>(bd, sp);
+}
+template <class R>
+void launch_gcbc_setup(int grid, cudaStream_t st, const BlockDev* bd, const GcbcTask* t, const int* f, int nt,
+                       int total, const StageParams* sp) {
+  k_gcbc_setup<R><<<grid, 128, 0, st>>>(bd, t, f, nt, total, sp);
+}
+template <class R>
+void launch_gcbc_update(int grid, cudaStream_t st, const BlockDev* bd, const GcbcTask* t, const int* f, int nt,
+                        int total, const StageParams* sp) {
+  k_gcbc_update<R><<<grid, 128, 0, st>>>(bd, t, f, nt, total, sp);
+}
+template <class R>
+void launch_sponge(int grid, cudaStream_t st, const BlockDev* bd, const SpongeTask* t, const int* f, int nt,
+                   int total) {
+  k_sponge<R><<<grid, 256, 0, st>>>(bd, t, f, nt, total);
+}
+template <class R>
+void launch_face_copy(dim3 g, cudaStream_t st, const void* const* src, void* const* dst, const int* cnt, int n) {
+  k_face_copy<R><<<g, 256, 0, st>>>(src, dst, cnt, n);
+}
+template <class T>
+void launch_mpigo_t(int grid, cudaStream_t st, const FaceTask* t, const int* f, int nt, int total) {
+  k_mpigo<T><<<grid, 128, 0, st>>>(t, f, nt, total);
+}
+template <int DIR, int OP, class TT, class RS>
+void launch_line_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
+                   const CUtensorMap* maps, int* err) {
+  k_line<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, int OP, class TT, class RS>
+cudaError_t line_smem_limit(int bytes) {
+  return cudaFuncSetAttribute(k_line<DIR, OP, TT, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace canard

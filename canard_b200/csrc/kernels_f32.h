@@ -1,0 +1,48 @@
+// The float instantiations of the kernel launchers. kernels_f32.cu defines
+// them (CANARD_F32_EXTERN empty) in a translation unit compiled with FMA
+// contraction; every other unit declares them extern, so it neither
+// instantiates nor compiles the FP32 kernels itself.
+#pragma once
+#include "kernels.cuh"
+
+#ifndef CANARD_F32_EXTERN
+#define CANARD_F32_EXTERN extern
+#endif
+
+namespace canard {
+
+CANARD_F32_EXTERN template void launch_prim<float>(dim3, cudaStream_t, const BlockDev*, const CaseConst*);
+CANARD_F32_EXTERN template void launch_dtmax<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*,
+                                                    const CaseConst*, unsigned long long*);
+CANARD_F32_EXTERN template void launch_copy_mu<float>(dim3, cudaStream_t, const BlockDev*);
+CANARD_F32_EXTERN template void launch_viscous_assemble<float>(dim3, cudaStream_t, const BlockDev*);
+CANARD_F32_EXTERN template void launch_flux<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*,
+                                                   const CaseConst*);
+CANARD_F32_EXTERN template void launch_flux_visc<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*,
+                                                        const CaseConst*);
+CANARD_F32_EXTERN template void launch_flux_sum<float>(dim3, cudaStream_t, const BlockDev*);
+CANARD_F32_EXTERN template void launch_rk<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*);
+CANARD_F32_EXTERN template void launch_gcbc_setup<float>(int, cudaStream_t, const BlockDev*, const GcbcTask*,
+                                                         const int*, int, int, const StageParams*);
+CANARD_F32_EXTERN template void launch_gcbc_update<float>(int, cudaStream_t, const BlockDev*, const GcbcTask*,
+                                                          const int*, int, int, const StageParams*);
+CANARD_F32_EXTERN template void launch_sponge<float>(int, cudaStream_t, const BlockDev*, const SpongeTask*,
+                                                     const int*, int, int);
+CANARD_F32_EXTERN template void launch_face_copy<float>(dim3, cudaStream_t, const void* const*, void* const*,
+                                                        const int*, int);
+CANARD_F32_EXTERN template void launch_mpigo_t<float>(int, cudaStream_t, const FaceTask*, const int*, int, int);
+
+#define CANARD_F32_LINE(DIR, OP, TT)                                                                          \
+  CANARD_F32_EXTERN template void launch_line_t<DIR, OP, TT, float>(int, size_t, cudaStream_t, const LineTask*, \
+                                                                    const int*, int, const CUtensorMap*, int*); \
+  CANARD_F32_EXTERN template cudaError_t line_smem_limit<DIR, OP, TT, float>(int);
+// derivatives on FP32 fields; filter of the FP64 state with an FP32 elimination
+CANARD_F32_LINE(1, 0, float)
+CANARD_F32_LINE(2, 0, float)
+CANARD_F32_LINE(3, 0, float)
+CANARD_F32_LINE(1, 1, double)
+CANARD_F32_LINE(2, 1, double)
+CANARD_F32_LINE(3, 1, double)
+#undef CANARD_F32_LINE
+
+}  // namespace canard

@@ -1,0 +1,141 @@
+// FP64-only device kernels of set-up and of the state bookkeeping: grid
+// metrics, Jacobian, face normals, the qo copy, junction averaging and the
+// FP32 copies of the metrics. Included by the FP64 translation unit only.
+#pragma once
+#include "kernels.cuh"
+
+namespace canard {
+
+__global__ void k_copy5(const BlockDev* __restrict__ bd) {  // qo = qa
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) B.qo[l + c * n] = B.qa[l + c * n];
+  }
+}
+
+// cofactor metrics from the 9 coordinate derivatives in scr (src/mo_grid.f90:107-115);
+// scr field 3*(m-1)+(d-1) = d(coordinate m)/d(xi_d)
+__global__ void k_cofactors(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double* g = B.scr;
+    const double q1 = g[l], q2 = g[l + n], q3 = g[l + 2 * n];
+    const double a1 = g[l + 3 * n], a2 = g[l + 4 * n], a3 = g[l + 5 * n];
+    const double d1 = g[l + 6 * n], d2 = g[l + 7 * n], d3 = g[l + 8 * n];
+    B.xim[l] = a2 * d3 - d2 * a3;
+    B.xim[l + n] = d2 * q3 - q2 * d3;
+    B.xim[l + 2 * n] = q2 * a3 - a2 * q3;
+    B.etm[l] = a3 * d1 - d3 * a1;
+    B.etm[l + n] = d3 * q1 - q3 * d1;
+    B.etm[l + 2 * n] = q3 * a1 - a3 * q1;
+    B.zem[l] = a1 * d2 - d1 * a2;
+    B.zem[l + n] = d1 * q2 - q1 * d2;
+    B.zem[l + 2 * n] = q1 * a2 - a1 * q2;
+  }
+}
+
+// Jacobian (src/mo_grid.f90:157-159)
+__global__ void k_jacobian(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    const double* g = B.scr;
+    const double *xi = B.xim, *et = B.etm, *ze = B.zem;
+    double s = g[l] * xi[l];
+    s = s + g[l + n] * et[l];
+    s = s + g[l + 2 * n] * ze[l];
+    s = s + g[l + 3 * n] * xi[l + n];
+    s = s + g[l + 4 * n] * et[l + n];
+    s = s + g[l + 5 * n] * ze[l + n];
+    s = s + g[l + 6 * n] * xi[l + 2 * n];
+    s = s + g[l + 7 * n] * et[l + 2 * n];
+    s = s + g[l + 8 * n] * ze[l + 2 * n];
+    B.yaco[l] = 3.0 / s;
+  }
+}
+
+// unit face normals cm{1,2,3} (src/mo_grid.f90:161-186); one thread per face line.
+struct CmTask { int b, nn, side, nbs, nj, N, line0; double* cm; };
+__global__ void k_face_normals(const BlockDev* __restrict__ bd, const CmTask* __restrict__ tasks,
+                               const int* __restrict__ line0s, int ntasks, int nlines) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nlines; g += gridDim.x * blockDim.x) {
+    const CmTask& T = tasks[find_task(line0s, ntasks, g)];
+    const BlockDev& B = bd[T.b];
+    const int jk = g - T.line0, j = jk % T.nj, k = jk / T.nj;
+    int x, y, z;
+    line_xyz(T.nn, T.side * T.N, j, k, x, y, z);
+    const long long l = ((long long)z * B.Y + y) * B.Xp + x;
+    const double* met = T.nn == 1 ? B.xim : T.nn == 2 ? B.etm : B.zem;
+    const double ya = B.yaco[l];
+    const double r0 = ya * met[l], r1 = ya * met[l + B.npad], r2 = ya * met[l + 2 * B.npad];
+    const double f = 1.0 / sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+    T.cm[jk] = f * r0;
+    T.cm[T.nbs + jk] = f * r1;
+    T.cm[2 * T.nbs + jk] = f * r2;
+  }
+}
+
+// junction / surface averaging: snapshot then ordered combination
+__global__ void k_avg_snapshot(const BlockDev* __restrict__ bd, const int* __restrict__ sb,
+                               const long long* __restrict__ sl, int nsrc, double* __restrict__ snap) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nsrc; e += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[sb[e]];
+    const long long l = sl[e];
+    for (int c = 0; c < 5; ++c) snap[(long long)e * 5 + c] = B.qa[l + c * B.npad];
+  }
+}
+// mode 0: sum and scale (average_point / average_line); mode 1: running
+// average of average_surface.
+__global__ void k_avg_combine(const BlockDev* __restrict__ bd, const int* __restrict__ tb,
+                              const long long* __restrict__ tl, const int* __restrict__ tfirst,
+                              const int* __restrict__ tcount, int ntg, const double* __restrict__ snap, int mode) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[tb[t]];
+    const long long l = tl[t];
+    const int f = tfirst[t], cnt = tcount[t];
+    for (int c = 0; c < 5; ++c) {
+      if (mode == 0) {
+        double acc = snap[(long long)f * 5 + c];
+        for (int j = 1; j < cnt; ++j) acc = acc + snap[(long long)(f + j) * 5 + c];
+        B.qa[l + c * B.npad] = (1.0 / (double)cnt) * acc;
+      } else {
+        double q = B.qa[l + c * B.npad];
+        double r1 = 1.0;
+        for (int j = 0; j < cnt; ++j) {
+          r1 = r1 + 1.0;
+          const double r2 = 1.0 / r1;
+          q = r2 * ((r1 - 1.0) * q + snap[(long long)(f + j) * 5 + c]) + 0.0 * q;
+        }
+        B.qa[l + c * B.npad] = q;
+      }
+    }
+  }
+}
+
+// FP32 copies of the metrics and the Jacobian for the mixed-precision flux path
+__global__ void k_metrics_to_f32(const BlockDev* __restrict__ bd) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const long long n = B.npad;
+    float* xi = const_cast<float*>(B.f.xim);
+    float* et = const_cast<float*>(B.f.etm);
+    float* ze = const_cast<float*>(B.f.zem);
+    for (int c = 0; c < 3; ++c) {
+      xi[l + c * n] = float(B.xim[l + c * n]);
+      et[l + c * n] = float(B.etm[l + c * n]);
+      ze[l + c * n] = float(B.zem[l + c * n]);
+    }
+    const_cast<float*>(B.f.yaco)[l] = float(B.yaco[l]);
+  }
+}
+
+// conversions between an FP64 and an FP32 field of n elements (unit calls)
+__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = float(a[i]);
+}
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = double(a[i]);
+}
+
+}  // namespace canard

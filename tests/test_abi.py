@@ -67,11 +67,14 @@ def test_context_without_gpu_reports_an_error():
 
 
 def test_unsupported_configurations_are_rejected_before_device_work():
-    # mixed precision is declared but a context must be FP64 on this build's
-    # plain path; walls are not on this path
+    # walls are not on this path; precisions other than FP64 and FP32-mixed
+    # do not exist
     blk = cases.BlockSpec(16, 16, 16, [[20, 10], [10, 10], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
     cs = cases.CaseSpec([blk])
     h = ctypes.c_void_p()
     c, b = api._structs([cs])
-    rc = api.lib().canard_ctx_create(c, 1, b, 0, ctypes.byref(h))
-    assert rc in (api.ERR_UNSUPPORTED, api.ERR_CUDA)
+    for prec in (api.FP64, api.FP32_MIXED):
+        rc = api.lib().canard_ctx_create(c, 1, b, prec, ctypes.byref(h))
+        assert rc in (api.ERR_UNSUPPORTED, api.ERR_CUDA)
+    c, b = api._structs([cases.tgv(16)])
+    assert api.lib().canard_ctx_create(c, 1, b, 7, ctypes.byref(h)) == api.ERR_UNSUPPORTED
