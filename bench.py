@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the FP32-mixed and batched comparison lines added to the default run")
     return p.parse_args()
 
 
@@ -84,6 +86,104 @@ def cpu_arm(n, steps, warmup=0):
     sample = (f"TGV {n}^3 cells ({n + 1}^3 points), viscous FP64, {steps} full steps after set-up"
               f"{' and ' + str(warmup) + ' warm-up steps' if warmup else ''}, OpenMP over lines")
     return v, threads, sample, dt
+
+
+def state_errors(qg, qr, uref):
+    """Relative L2 error per conserved variable of qg against qr; momentum
+    components against the momentum scale ||rho|| * uref where that exceeds
+    their own norm (a component that is zero by symmetry has no relative error)."""
+    rho = np.linalg.norm(qr[0].ravel())
+    out = []
+    for v in range(5):
+        den = np.linalg.norm(qr[v].ravel())
+        if 1 <= v <= 3:
+            den = max(den, rho * uref)
+        out.append(float(np.linalg.norm((qg[v] - qr[v]).ravel()) / den))
+    return out
+
+
+def time_steps(ctx, steps, stream, torch):
+    """Device milliseconds of `steps` steps (CUDA events on the launching stream)."""
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ctx.step(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def fp32_extra(args, api, cases, torch, stream, value64):
+    """FP32-mixed on the same workload: throughput, and the error after 10 steps
+    from the initial condition against the FP64 path."""
+    cs = cases.tgv(args.n)
+    c32 = api.Context(cs, precision=api.FP32_MIXED)
+    c32.set_stream(stream.cuda_stream)
+    c32.step(args.warmup)
+    ms = time_steps(c32, args.steps, stream, torch)
+    c32.close()
+    v32 = cs.npts * args.steps / (ms / 1e3) / 1e6
+    a = api.Context(cs)
+    b = api.Context(cs, precision=api.FP32_MIXED)
+    a.step(10)
+    b.step(10)
+    errs = state_errors(b.state(0), a.state(0), 0.1)
+    a.close()
+    b.close()
+    return {"value": v32, "unit": "Mpoint-steps/s", "ms_per_step": ms / args.steps, "steps": args.steps,
+            "speedup_vs_fp64": v32 / value64,
+            "rel_l2_vs_fp64_after_10_steps": errs,
+            "note": "per variable (rho, rho u, rho v, rho w, rho E); momenta against ||rho|| * 0.1 (TGV V0) where "
+                    "that exceeds their own norm"}
+
+
+def batched_extra(args, api, cases, torch, stream):
+    """64 independent cases (sides 32..96): one context, one launch per phase
+    and direction for all cases, each step one CUDA graph, FP32-mixed and
+    FP64; against the per-case FP64 plain path (one context per case, kernels
+    launched one by one, case after case)."""
+    allc = cases.batched(64, seed=11)
+    npts = sum(c.npts for c in allc)
+    out = {"workload": "64 cases, sides 32..96 (seed 11), TGV / periodic vortex, Mach 0.1-0.5, Re 400-3200",
+           "points": npts, "steps": args.steps}
+    states = {}
+    for key, prec in (("fp32_mixed_graph", api.FP32_MIXED), ("fp64_graph", api.FP64)):
+        g = api.Context(allc, precision=prec)
+        g.set_stream(stream.cuda_stream)
+        g.step(args.warmup)
+        ms = time_steps(g, args.steps, stream, torch)
+        out[key] = npts * args.steps / (ms / 1e3) / 1e6
+        states[key] = [g.state(0, i) for i in range(len(allc))]
+        g.close()
+    ctxs = []
+    for c in allc:
+        x = api.Context(c)
+        x.set_graphs(False)
+        x.set_stream(stream.cuda_stream)
+        x.step(args.warmup)
+        ctxs.append(x)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    a.record(stream)
+    for x in ctxs:
+        x.step(args.steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = max(a.elapsed_time(b), (time.perf_counter() - t0) * 1e3)
+    out["fp64_per_case_plain"] = npts * args.steps / (ms / 1e3) / 1e6
+    ref = [x.state(0) for x in ctxs]
+    for x in ctxs:
+        x.close()
+    out["speedup_fp32_graph_vs_fp64_per_case"] = out["fp32_mixed_graph"] / out["fp64_per_case_plain"]
+    out["speedup_fp64_graph_vs_fp64_per_case"] = out["fp64_graph"] / out["fp64_per_case_plain"]
+    out["fp64_graph_bit_identical_to_per_case"] = bool(all(np.array_equal(s, r)
+                                                            for s, r in zip(states["fp64_graph"], ref)))
+    errs = [state_errors(s, r, 0.5) for s, r in zip(states["fp32_mixed_graph"], ref)]
+    out["fp32_max_rel_l2_vs_fp64"] = float(max(max(e) for e in errs))
+    return out
 
 
 class Clocks:
@@ -290,6 +390,14 @@ def main():
            "d2h_bytes_per_step": int(sum(h[2].numel() for h in hosts) * 8),
            "steps": args.e2e_steps}
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras and args.config == "tgv" and args.precision == "fp64":
+        ctx.close()
+        torch.cuda.empty_cache()
+        extras["fp32_mixed"] = fp32_extra(args, api, cases, torch, stream, value)
+        extras["batched"] = batched_extra(args, api, cases, torch, stream)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ctx.close()
@@ -312,6 +420,7 @@ def main():
                 "clocks": clocks,
                 "families": {k: {"ms_per_step": v["ms"], "share": v["ms"] / tot if tot else 0.0,
                                  "launches": v["launches"]} for k, v in fam.items() if v["launches"]}}
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

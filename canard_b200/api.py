@@ -90,6 +90,7 @@ def lib():
         L.canard_deriv.argtypes = [vp, i32, _DP, _DP, i32, i32]
         L.canard_filte.argtypes = [vp, i32, _DP, i32, i32]
         L.canard_set_timers.argtypes = [vp, i32]
+        L.canard_set_graphs.argtypes = [vp, i32]
         L.canard_get_timers.argtypes = [vp, _DP, _DP, _DP, i32]
         L.canard_timer_name.restype = ctypes.c_char_p
         L.canard_timer_name.argtypes = [i32]
@@ -202,6 +203,9 @@ class Context:
 
     def set_timers(self, on):
         self._check(lib().canard_set_timers(self.h, 1 if on else 0))
+
+    def set_graphs(self, on):
+        self._check(lib().canard_set_graphs(self.h, 1 if on else 0))
 
     def timers(self):
         """Per kernel family: device ms, launches, algorithmic bytes since set_timers(True)."""

@@ -83,8 +83,7 @@ struct CaseState {
   DevScheme* dsch = nullptr;
   int b0 = 0, nb = 0;
   double reoo, srefoo, srefp1dre, uoo[3];
-  int n = 0, ndt = 0;
-  double dt = 0, dts = 0, dte = 0, timo = 0;
+  long long n = 0;  // host mirror of the device step counter (decides the dt-reduction launch)
 };
 
 struct BlockState {
@@ -155,12 +154,14 @@ struct canard_ctx {
   std::vector<FaceLink> links;  // global block indices
   BlockDev* dbd = nullptr;
   CaseConst* dcc = nullptr;
-  StageParams* dsp = nullptr;       // [2 ring][5 slots][ncases]
-  StageParams* hsp = nullptr;       // pinned, same shape
-  cudaEvent_t ring_ev[2] = {nullptr, nullptr};
-  int ring = 0;
+  StageParams* dsp = nullptr;       // [5 slots][ncases]: stages 1..4, then the dt reduction / phase calls
+  TimeDev* dtime = nullptr;         // [ncases] time-loop state
+  double* dsn2 = nullptr;           // ramp factors sin(0.05 pi k)^2, k < kRampTable
   unsigned long long* ddt = nullptr;  // [ncases][2]
-  unsigned long long* hdt = nullptr;  // pinned
+  // one step as a CUDA graph, without [0] and with [1] the dt reduction
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};
+  bool use_graphs = true;
   int* derr = nullptr;
   bool setup_done = false;
   // hot-path tables
@@ -536,58 +537,27 @@ void sync_check(canard_ctx* c) {
   CK(cudaMemcpy(&e, c->derr, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
     CK(cudaMemset(c->derr, 0, sizeof(int)));
+    if (e == kErrOverflow) throw ApiError(CANARD_ERR_NAN, "Canard: Overflow. (dt == 0 after step 2)");
     throw ApiError(CANARD_ERR_TIMEOUT, "a bounded device wait gave up (error flag set by a kernel)");
   }
 }
 
-// ---- moving frame, src/mo_physics.f90:144-169 (host arithmetic) ----------------
-void movef(const CaseState& cs, double dtko, double dtk, double umf[3], double dudtmf[3]) {
-  const double pi = std::acos(-1.0);
-  if (cs.d.nsmf == 0) {
-    const double ra0 = pi / cs.d.timf;
-    const double ra1 = ra0 * std::min(cs.timo, cs.d.timf);
-    const double ra2 = ra0 * std::min(cs.timo + dtko, cs.d.timf);
-    double fctr = 1.0 - std::cos(ra1);
-    double dfdt = ra0 * std::sin(ra2);
-    double progmf = 0.5 * (fctr + dtk * dfdt);
-    for (int d = 0; d < 3; ++d) umf[d] = progmf * cs.uoo[d];
-    fctr = std::sin(ra1);
-    dfdt = ra0 * std::cos(ra2);
-    progmf = (0.5 * ra0) * (fctr + dtk * dfdt);
-    for (int d = 0; d < 3; ++d) dudtmf[d] = progmf * cs.uoo[d];
-  } else {
-    for (int d = 0; d < 3; ++d) { umf[d] = cs.uoo[d]; dudtmf[d] = 0.0; }
-  }
+constexpr int kRampTable = 64;
+
+StageParams* dev_slot(canard_ctx* c, int slot) {  // slot 0..3 = stages, 4 = dt reduction / phase calls
+  return c->dsp + (size_t)slot * c->cases.size();
 }
 
-// stage parameters of stage nk (1..4) for the case's current dt, timo
-void stage_params(const CaseState& cs, int nk, StageParams& p) {
-  const int nkrk = 4;
-  double dtko = (cs.dt * std::min(std::max(nk - 2, 0), 1)) / (nkrk - nk + 3);
-  double dtk = (cs.dt * std::min(nk - 1, 1)) / (nkrk - nk + 2);
-  movef(cs, dtko, dtk, p.umf, p.dudtmf);
-  dtko = (cs.dt * std::min(nk - 1, 1)) / (nkrk - nk + 2);
-  dtk = cs.dt / (nkrk - nk + 1);
-  double dud[3];
-  movef(cs, dtko, dtk, p.umfb, dud);
-  p.dtk = dtk;
-  p.dt = cs.dt;
-}
+int ncase(const canard_ctx* c) { return (int)c->cases.size(); }
 
-StageParams* dev_slot(canard_ctx* c, int slot) {  // slot 0..3 = stages, 4 = time step
-  return c->dsp + ((size_t)c->ring * 5 + slot) * c->cases.size();
-}
-StageParams* host_slot(canard_ctx* c, int slot) {
-  return c->hsp + ((size_t)c->ring * 5 + slot) * c->cases.size();
-}
-
-// writes the stage parameters of all cases for all 4 stages into the ring
-// slot and uploads them
-void upload_stage_params(canard_ctx* c) {
-  for (int nk = 1; nk <= 4; ++nk)
-    for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], nk, host_slot(c, nk - 1)[i]);
-  CK(cudaMemcpyAsync(dev_slot(c, 0), host_slot(c, 0), 4 * c->cases.size() * sizeof(StageParams),
-                     cudaMemcpyHostToDevice, c->st));
+// stage scalars of stages nk0..nk1 into slots nk0-1..nk1-1 (or, with
+// to_slot >= 0, of one stage into that slot), from the device time state
+void stage_params(canard_ctx* c, int nk0, int nk1, int to_slot = -1) {
+  const int n = (nk1 - nk0 + 1) * ncase(c);
+  StageParams* out = to_slot >= 0 ? dev_slot(c, to_slot) : dev_slot(c, nk0 - 1);
+  c->launches += 1;
+  k_stage_params<<<(n + 127) / 128, 128, 0, c->st>>>(c->dtime, c->dcc, out, nk0, nk1, ncase(c));
+  CK(cudaGetLastError());
 }
 
 // ---- phases --------------------------------------------------------------------
@@ -755,58 +725,44 @@ void ph_average(canard_ctx* c) {
   run_avg(c, c->avg_sf, 1);
 }
 
-// time step reduction (src/mo_physics.f90:171-211) + dt ramp
-// (src/mo_canard_driver.f90:278-294) for the cases that need it this step.
+bool needs_dt_reduction(const canard_ctx* c) {
+  for (auto& cs : c->cases)
+    if (cs.n % 10 == 1) return true;
+  return false;
+}
+
+// time step reduction (src/mo_physics.f90:171-211) every tenth step and the dt
+// ramp (src/mo_canard_driver.f90:278-294), all on the device
 void timestep(canard_ctx* c) {
-  bool need = false;
-  for (auto& cs : c->cases) need = need || (cs.n % 10 == 1);
-  if (need) {
-    // stage-1 moving-frame velocity (dtko = dtk = 0 at nk = 1)
-    StageParams* hp = host_slot(c, 4);
-    for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], 1, hp[i]);
-    CK(cudaMemcpyAsync(dev_slot(c, 4), hp, c->cases.size() * sizeof(StageParams), cudaMemcpyHostToDevice, c->st));
+  if (needs_dt_reduction(c)) {
+    stage_params(c, 1, 1, 4);  // stage-1 moving frame (dtko = dtk = 0)
     CK(cudaMemsetAsync(c->ddt, 0, 2 * c->cases.size() * sizeof(unsigned long long), c->st));
     Timed tm(c, T_TIMESTEP, ew_bytes(c, 10, 7));
     if (c->f32()) launch_dtmax<float>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
     else launch_dtmax<double>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(c->hdt, c->ddt, 2 * c->cases.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                       c->st));
-    CK(cudaStreamSynchronize(c->st));
   }
-  for (size_t i = 0; i < c->cases.size(); ++i) {
-    CaseState& cs = c->cases[i];
-    if (cs.n % 10 == 1) {
-      cs.ndt = cs.n;
-      cs.dts = cs.dte;
-      double r1, r2;
-      std::memcpy(&r1, &c->hdt[2 * i], 8);
-      std::memcpy(&r2, &c->hdt[2 * i + 1], 8);
-      const double ra0 = cs.d.cfl / r1;
-      double ra1 = ra0;
-      if (cs.d.viscous) ra1 = 0.5 / r2;
-      cs.dte = std::min(ra0, ra1);
-    }
-    const double pi = std::acos(-1.0);
-    const double sn = std::sin((0.05 * pi) * (cs.n - cs.ndt));
-    cs.dt = cs.dts + (cs.dte - cs.dts) * (sn * sn);
-  }
+  c->launches += 1;
+  k_time_dt<<<(ncase(c) + 127) / 128, 128, 0, c->st>>>(c->dtime, c->ddt, c->dcc, c->dsn2, kRampTable, ncase(c),
+                                                       c->derr);
+  CK(cudaGetLastError());
 }
 
-void wait_ring(canard_ctx* c) {
-  c->ring ^= 1;
-  CK(cudaEventSynchronize(c->ring_ev[c->ring]));
+void time_advance(canard_ctx* c) {
+  c->launches += 1;
+  k_time_advance<<<(ncase(c) + 127) / 128, 128, 0, c->st>>>(c->dtime, ncase(c));
+  CK(cudaGetLastError());
+  for (auto& cs : c->cases) cs.n = cs.n + 1;
 }
 
-void one_step(canard_ctx* c) {
-  for (auto& cs : c->cases)
-    if (cs.dt == 0.0 && cs.n > 2) throw ApiError(CANARD_ERR_NAN, "Canard: Overflow. (dt == 0 after step 2)");
-  wait_ring(c);
+// The time-loop body (src/mo_canard_driver.f90:226-370): every launch on c->st,
+// no host synchronisation, so it can be captured as a graph.
+void step_body(canard_ctx* c) {
   ph_filter(c);
   ph_copyqo(c);
   ph_prim(c);
   timestep(c);
-  upload_stage_params(c);
+  stage_params(c, 1, 4);
   for (int nk = 1; nk <= 4; ++nk) {
     const StageParams* sp = dev_slot(c, nk - 1);
     if (nk > 1) ph_prim(c);
@@ -816,11 +772,51 @@ void one_step(canard_ctx* c) {
     ph_rk(c, sp);
     ph_average(c);
   }
-  CK(cudaEventRecord(c->ring_ev[c->ring], c->st));
-  for (auto& cs : c->cases) {
-    cs.n = cs.n + 1;
-    cs.timo = cs.timo + cs.dt;
+  time_advance(c);
+}
+
+// One step: replays the captured graph of the step (captured on first use,
+// per variant with and without the dt reduction), or launches the kernels
+// directly while per-family timers are on.
+void one_step(canard_ctx* c) {
+  if (!c->use_graphs || c->timers) {
+    step_body(c);
+    return;
   }
+  const int v = needs_dt_reduction(c) ? 1 : 0;
+  if (!c->graph[v]) {
+    // capture on the context's own stream (a legacy default stream cannot
+    // capture); the graph then runs on whatever stream the context uses
+    cudaStream_t user = c->st;
+    CK(cudaStreamSynchronize(user));
+    c->st = c->own;
+    const long long l0 = c->launches;
+    const long long n0 = c->cases.empty() ? 0 : c->cases[0].n;
+    std::vector<long long> nsave;
+    for (auto& cs : c->cases) nsave.push_back(cs.n);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    try {
+      step_body(c);
+    } catch (...) {
+      cudaStreamEndCapture(c->st, &g);
+      if (g) cudaGraphDestroy(g);
+      c->st = user;
+      throw;
+    }
+    CK(cudaStreamEndCapture(c->st, &g));
+    c->st = user;
+    (void)n0;
+    for (size_t i = 0; i < c->cases.size(); ++i) c->cases[i].n = nsave[i];
+    c->graph_launches[v] = c->launches - l0;
+    c->launches = l0;
+    cudaError_t e = cudaGraphInstantiate(&c->graph[v], g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+  CK(cudaGraphLaunch(c->graph[v], c->st));
+  c->launches += c->graph_launches[v];
+  for (auto& cs : c->cases) cs.n = cs.n + 1;
 }
 
 // ---- set-up ------------------------------------------------------------------------
@@ -1141,9 +1137,8 @@ void destroy(canard_ctx* c) {
   }
   for (auto& cs : c->cases) cudaFree(cs.dsch);
   cudaFree(c->dbd); cudaFree(c->dcc); cudaFree(c->dsp); cudaFree(c->ddt); cudaFree(c->derr);
-  if (c->hsp) cudaFreeHost(c->hsp);
-  if (c->hdt) cudaFreeHost(c->hdt);
-  for (auto e : c->ring_ev) if (e) cudaEventDestroy(e);
+  cudaFree(c->dtime); cudaFree(c->dsn2);
+  for (auto g : c->graph) if (g) cudaGraphExecDestroy(g);
   for (auto& p : c->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   auto ft = [](auto& T) { cudaFree(T.tasks); cudaFree(T.first); };
@@ -1276,7 +1271,10 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
   c->dbd = dupload(bdv, c->st);
   std::vector<CaseConst> ccv;
   for (auto& cs : c->cases) {
-    CaseConst k{cs.srefoo, cs.srefp1dre, cs.d.viscous};
+    CaseConst k{};
+    k.srefoo = cs.srefoo; k.srefp1dre = cs.srefp1dre; k.viscous = cs.d.viscous; k.nsmf = cs.d.nsmf;
+    k.cfl = cs.d.cfl; k.timf = cs.d.timf;
+    for (int d = 0; d < 3; ++d) k.uoo[d] = cs.uoo[d];
     ccv.push_back(k);
     DevScheme ds{};
     std::memcpy(ds.pbci, cs.sch.pbci, sizeof(ds.pbci));
@@ -1287,15 +1285,20 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
     cs.dsch = dupload(std::vector<DevScheme>{ds}, c->st);
   }
   c->dcc = dupload(ccv, c->st);
-  const size_t nslots = 2 * 5 * c->cases.size();
-  c->dsp = dalloc<StageParams>(nslots, c->st);
-  CK(cudaMallocHost(&c->hsp, nslots * sizeof(StageParams)));
-  std::memset(c->hsp, 0, nslots * sizeof(StageParams));
+  c->dsp = dalloc<StageParams>(5 * c->cases.size(), c->st);
+  c->dtime = dalloc<TimeDev>(c->cases.size(), c->st);  // n = ndt = 0, dt = dts = dte = timo = 0
+  {
+    // ramp factors with the host's libm, as the CPU code evaluates them
+    const double pi = std::acos(-1.0);
+    std::vector<double> sn2(kRampTable);
+    for (int k = 0; k < kRampTable; ++k) {
+      const double sn = std::sin((0.05 * pi) * k);
+      sn2[k] = sn * sn;
+    }
+    c->dsn2 = dupload(sn2, c->st);
+  }
   c->ddt = dalloc<unsigned long long>(2 * c->cases.size(), c->st);
-  CK(cudaMallocHost(&c->hdt, 2 * c->cases.size() * sizeof(unsigned long long)));
   c->derr = dalloc<int>(1, c->st);
-  for (auto& e : c->ring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  for (auto& e : c->ring_ev) CK(cudaEventRecord(e, c->st));
   set_line_smem_limits();
   build_tables(c);
   CK(cudaStreamSynchronize(c->st));
@@ -1496,10 +1499,7 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
       throw ApiError(CANARD_ERR_ARG, "stage index nk must be 1..4");
     // parameters of stage nk for the current dt / timo
     auto params = [&]() {
-      StageParams* hp = host_slot(c, 4);
-      for (size_t i = 0; i < c->cases.size(); ++i) stage_params(c->cases[i], nk, hp[i]);
-      CK(cudaMemcpyAsync(dev_slot(c, 4), hp, c->cases.size() * sizeof(StageParams), cudaMemcpyHostToDevice,
-                         c->st));
+      stage_params(c, nk, nk, 4);
       return dev_slot(c, 4);
     };
     switch (phase) {
@@ -1515,9 +1515,7 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
       case CANARD_PH_RKUPDATE: ph_rk(c, params()); break;
       case CANARD_PH_WALL: break;
       case CANARD_PH_AVERAGE: ph_average(c); break;
-      case CANARD_PH_ADVANCE:
-        for (auto& cs : c->cases) { cs.n = cs.n + 1; cs.timo = cs.timo + cs.dt; }
-        break;
+      case CANARD_PH_ADVANCE: time_advance(c); break;
       default: throw ApiError(CANARD_ERR_ARG, "unknown phase");
     }
     sync_check(c);
@@ -1527,16 +1525,21 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
 int canard_get_time(canard_ctx* c, int32_t icase, double* t) {
   return guarded(c, [&] {
     if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
-    const CaseState& cs = c->cases[icase];
-    t[0] = cs.n; t[1] = cs.ndt; t[2] = cs.dt; t[3] = cs.dts; t[4] = cs.dte; t[5] = cs.timo;
+    TimeDev d;
+    CK(cudaMemcpyAsync(&d, c->dtime + icase, sizeof(d), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    t[0] = (double)d.n; t[1] = (double)d.ndt; t[2] = d.dt; t[3] = d.dts; t[4] = d.dte; t[5] = d.timo;
   });
 }
 
 int canard_set_time(canard_ctx* c, int32_t icase, const double* t) {
   return guarded(c, [&] {
     if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
-    CaseState& cs = c->cases[icase];
-    cs.n = (int)t[0]; cs.ndt = (int)t[1]; cs.dt = t[2]; cs.dts = t[3]; cs.dte = t[4]; cs.timo = t[5];
+    TimeDev d;
+    d.n = (long long)t[0]; d.ndt = (long long)t[1]; d.dt = t[2]; d.dts = t[3]; d.dte = t[4]; d.timo = t[5];
+    CK(cudaMemcpyAsync(c->dtime + icase, &d, sizeof(d), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->cases[icase].n = d.n;
   });
 }
 
@@ -1631,6 +1634,13 @@ int canard_get_timers(canard_ctx* c, double* ms, double* launches, double* bytes
 }
 
 const char* canard_timer_name(int32_t f) { return (f >= 0 && f < T_NFAM) ? kTimerNames[f] : ""; }
+
+int canard_set_graphs(canard_ctx* c, int32_t on) {
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    c->use_graphs = on != 0;
+  });
+}
 
 int canard_launch_count(canard_ctx* c, int64_t* count) {
   if (!c || !count) return CANARD_ERR_ARG;

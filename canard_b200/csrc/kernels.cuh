@@ -19,6 +19,7 @@ namespace canard {
 
 constexpr int kLanes = 32;            // lines per tile (one warp, one line per lane)
 constexpr int kErrTimeout = 4;
+constexpr int kErrOverflow = 8;  // dt == 0 after step 2 ("Canard: Overflow.")
 constexpr long long kSpinLimit = 1LL << 28;  // bounded mbarrier waits
 
 struct DevScheme {
@@ -39,6 +40,15 @@ struct StageParams {
 struct CaseConst {
   double srefoo, srefp1dre;
   int viscous;
+  int nsmf;                // 1: constant moving frame; 0: frame ramped over timf
+  double cfl, timf, uoo[3];
+};
+
+// Time-loop state of one case (src/mo_canard_driver.f90:226-370), kept on the
+// device so that a whole step needs no host round trip.
+struct TimeDev {
+  long long n, ndt;
+  double dt, dts, dte, timo;
 };
 
 // Work fields of one block in the arithmetic type R of the flux path.

@@ -138,4 +138,97 @@ __global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b
     b[i] = double(a[i]);
 }
 
+// ---------------------------------------------------------------------------
+// Time-step control on the device.
+
+// dt of the step (src/mo_canard_driver.f90:278-294): a new dte from the maxima
+// of k_dtmax every tenth step, then the sin^2 ramp from dts to dte. The ramp
+// factors sin(0.05 pi k)^2 come from a host table (the same libm values the
+// CPU code uses); k past the table falls back to the device sine. Also flags
+// the reference's overflow stop (dt == 0 after step 2) seen at step start.
+__global__ void k_time_dt(TimeDev* __restrict__ td, const unsigned long long* __restrict__ dtm,
+                          const CaseConst* __restrict__ cc, const double* __restrict__ sn2, int nsn2, int ncases,
+                          int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncases) return;
+  TimeDev t = td[i];
+  if (t.dt == 0.0 && t.n > 2) atomicExch(err, kErrOverflow);
+  if (t.n % 10 == 1) {
+    t.ndt = t.n;
+    t.dts = t.dte;
+    const double r1 = __longlong_as_double((long long)dtm[2 * i]);
+    const double r2 = __longlong_as_double((long long)dtm[2 * i + 1]);
+    const double ra0 = cc[i].cfl / r1;
+    double ra1 = ra0;
+    if (cc[i].viscous) ra1 = 0.5 / r2;
+    t.dte = (ra1 < ra0) ? ra1 : ra0;
+  }
+  const long long k = t.n - t.ndt;
+  double s2;
+  if (k >= 0 && k < nsn2) {
+    s2 = sn2[k];
+  } else {
+    const double sn = sin((0.05 * 3.141592653589793) * (double)k);
+    s2 = sn * sn;
+  }
+  t.dt = t.dts + (t.dte - t.dts) * s2;
+  td[i] = t;
+}
+
+// moving frame (src/mo_physics.f90:144-169); with nsmf = 1 (or a frame at
+// rest) it is exact, with the timf ramp it uses the device sine and cosine
+__device__ __forceinline__ void movef_dev(const CaseConst& C, double timo, double dtko, double dtk, double umf[3],
+                                          double dudtmf[3]) {
+  if (C.nsmf == 0) {
+    const double pi = 3.141592653589793;
+    const double ra0 = pi / C.timf;
+    const double ra1 = ra0 * (C.timf < timo ? C.timf : timo);
+    const double t2 = timo + dtko;
+    const double ra2 = ra0 * (C.timf < t2 ? C.timf : t2);
+    double fctr = 1.0 - cos(ra1);
+    double dfdt = ra0 * sin(ra2);
+    double progmf = 0.5 * (fctr + dtk * dfdt);
+    for (int d = 0; d < 3; ++d) umf[d] = progmf * C.uoo[d];
+    fctr = sin(ra1);
+    dfdt = ra0 * cos(ra2);
+    progmf = (0.5 * ra0) * (fctr + dtk * dfdt);
+    for (int d = 0; d < 3; ++d) dudtmf[d] = progmf * C.uoo[d];
+  } else {
+    for (int d = 0; d < 3; ++d) { umf[d] = C.uoo[d]; dudtmf[d] = 0.0; }
+  }
+}
+
+// stage scalars of stages nk0..nk1 of every case into out[(nk - nk0) * ncases
+// + case] (src/mo_canard_driver.f90:261-263, 323-328)
+__global__ void k_stage_params(const TimeDev* __restrict__ td, const CaseConst* __restrict__ cc,
+                               StageParams* __restrict__ out, int nk0, int nk1, int ncases) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nst = nk1 - nk0 + 1;
+  if (g >= nst * ncases) return;
+  const int i = g % ncases, nk = nk0 + g / ncases;
+  const TimeDev t = td[i];
+  const CaseConst C = cc[i];
+  const int nkrk = 4;
+  StageParams p;
+  const int c1 = min(max(nk - 2, 0), 1), c2 = min(nk - 1, 1);
+  double dtko = (t.dt * c1) / (nkrk - nk + 3);
+  double dtk = (t.dt * c2) / (nkrk - nk + 2);
+  movef_dev(C, t.timo, dtko, dtk, p.umf, p.dudtmf);
+  dtko = (t.dt * c2) / (nkrk - nk + 2);
+  dtk = t.dt / (nkrk - nk + 1);
+  double dud[3];
+  movef_dev(C, t.timo, dtko, dtk, p.umfb, dud);
+  p.dtk = dtk;
+  p.dt = t.dt;
+  out[g] = p;
+}
+
+// n = n + 1, timo = timo + dt (src/mo_canard_driver.f90:369-370)
+__global__ void k_time_advance(TimeDev* __restrict__ td, int ncases) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncases) return;
+  td[i].n = td[i].n + 1;
+  td[i].timo = td[i].timo + td[i].dt;
+}
+
 }  // namespace canard

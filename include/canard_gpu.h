@@ -174,6 +174,14 @@ int canard_get_timers(canard_ctx* ctx, double* ms, double* launches, double* byt
 const char* canard_timer_name(int32_t family);
 int canard_launch_count(canard_ctx* ctx, int64_t* count);
 
+/* Step execution. canard_step runs each time step as one CUDA graph (captured
+ * on the first step of each kind: with and without the every-tenth-step dt
+ * reduction) whose kernels read the device-resident time state, so a step
+ * costs one host call and no host synchronisation. With graphs off (or the
+ * timers on) the same kernels are launched one by one. The reference has no
+ * counterpart; the results are identical either way. Default: on. */
+int canard_set_graphs(canard_ctx* ctx, int32_t on);
+
 /* Compact first derivative without device allocation. This entry point has no
  * counterpart in the reference. It serves callers that cannot allocate device
  * memory: solvers that own every device buffer themselves, code under a memory

@@ -212,3 +212,30 @@ def test_batched_context_equals_single_cases():
     o = po.Oracle(cs_list[1])
     o.step(12)
     assert rel_l2(g.state(0, case=1), o.state(0)) <= 1e-10
+
+
+def test_graph_replay_equals_direct_launches():
+    """canard_step replays a captured CUDA graph of the step; with the
+    per-family timers on it launches the kernels one by one. Both give the
+    same state bit for bit, across the dt-reduction steps (n % 10 == 1)."""
+    cs = case_multiblock()
+    a = api.Context(cs)
+    b = api.Context(cs)
+    b.set_timers(True)
+    a.step(13)
+    b.step(13)
+    for blk in range(len(cs.blocks)):
+        np.testing.assert_array_equal(a.state(blk), b.state(blk))
+    np.testing.assert_array_equal(a.time(), b.time())
+    assert a.launch_count() == b.launch_count()
+
+
+def test_overflow_is_reported():
+    """dt == 0 after step 2 is the reference's 'Canard: Overflow.' stop; made
+    on the host by setting the time state, then reported by the step."""
+    cs = case_periodic()
+    g = api.Context(cs)
+    g.set_time([5, 1, 0.0, 0.0, 0.0, 0.1])
+    with pytest.raises(api.CanardError) as e:
+        g.step(1)
+    assert e.value.code == api.ERR_NAN
