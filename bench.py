@@ -300,7 +300,10 @@ def main():
     ctx = api.Context(case_list, precision=prec)
     if args.precision == "fp32":
         workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
-    stream = torch.cuda.current_stream()
+    # a non-default stream: the library launches on it and the CUDA events
+    # below are recorded on it (handle 0 would mean the context's own stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     npts = sum(c.npts for c in case_list)
     if args.config == "batched":

@@ -76,6 +76,82 @@ struct Table {
 // Element types of a line launch: tile (field) type and elimination type.
 enum LineKind { LK_F64 = 0, LK_F32 = 1, LK_F64_TILE_F32_SOLVE = 2 };
 inline size_t tile_elem(int kind) { return kind == LK_F32 ? sizeof(float) : sizeof(double); }
+// FP32 eliminations use the split solve (16 lines per tile), FP64 the one-lane sweeps (32)
+inline int tile_lanes(int kind) { return kind == LK_F64 ? kLanes : kHalf; }
+
+// First row of the second half of a split solve: balances the two halves'
+// register-constant rows (the first half's rows below c0 use the tables
+// alone), with a parity that puts their lock-step rows into different banks.
+int split_row(int L, int dir, int nt, int c0) {
+  const int first = nt == 0 ? 2 : 3;   // first interior row of the elimination
+  int h = (L - 3 + first + std::max(c0, first)) / 2;
+  auto good = [&](int x) {
+    if (dir == 0) return ((x - first) % 4 + 4) % 4 == 2;  // row-major tile, 16-byte units of 4 floats
+    return ((x - first) % 2 + 2) % 2 == 1;                // [row][16] tile
+  };
+  while (!good(h)) ++h;
+  const int lo = nt == 0 ? 4 : 6, hi = L - (nt == 0 ? 2 : 3);
+  return std::max(lo, std::min(h, hi));
+}
+
+// Correction tables of the split solve (see sweep2), from the FP64 factors:
+// H0, H1 = the second half's back substitution (rows L-1..h) of the
+// homogeneous forward solutions started at rows h-2, h-1 (index row - h);
+// E0, E1 = the homogeneous backward solutions started at rows h, h+1 (index
+// h-1-row); each L + 8 entries; returns the lengths beyond which every entry
+// stays below 1e-12 (set to zero).
+void split_tables(const std::vector<double>& lu, int L, int h, std::vector<float>& out, int& kg, int& ke) {
+  const double* l1 = lu.data();
+  const double* l2 = l1 + L;
+  const double* u1 = l1 + 2 * L;
+  const double* u2 = l1 + 3 * L;
+  const double* u3 = l1 + 4 * L;
+  const int N = L - 1;
+  std::vector<double> G0(L, 0.0), G1(L, 0.0), H0(L + 2, 0.0), H1(L + 2, 0.0), E0(L + 2, 0.0), E1(L + 2, 0.0);
+  // forward homogeneous: G[i] = -l1[i] G[i-2] - l2[i] G[i-1], started at rows h-2, h-1
+  double p2a = 1.0, p1a = 0.0, p2b = 0.0, p1b = 1.0;
+  for (int i = h; i < L; ++i) {
+    const double ga = -l1[i] * p2a - l2[i] * p1a, gb = -l1[i] * p2b - l2[i] * p1b;
+    G0[i] = ga; G1[i] = gb;
+    p2a = p1a; p1a = ga; p2b = p1b; p1b = gb;
+  }
+  // the second half's back substitution of G (rows N..h)
+  auto back = [&](const std::vector<double>& g, std::vector<double>& hh) {
+    double c1 = u1[N] * g[N];
+    hh[N - h] = c1;
+    double c = u1[N - 1] * g[N - 1] - u2[N - 1] * c1;
+    hh[N - 1 - h] = c;
+    double c2 = c1;
+    c1 = c;
+    for (int i = N - 2; i >= h; --i) {
+      c = u1[i] * g[i] - u2[i] * c1 - u3[i] * c2;
+      hh[i - h] = c;
+      c2 = c1;
+      c1 = c;
+    }
+  };
+  back(G0, H0);
+  back(G1, H1);
+  // backward homogeneous: E[i] = -u2[i] E[i+1] - u3[i] E[i+2], started at rows h, h+1
+  double n1a = 1.0, n2a = 0.0, n1b = 0.0, n2b = 1.0;
+  for (int i = h - 1; i >= 0; --i) {
+    const double ea = -u2[i] * n1a - u3[i] * n2a, eb = -u2[i] * n1b - u3[i] * n2b;
+    E0[h - 1 - i] = ea; E1[h - 1 - i] = eb;
+    n2a = n1a; n1a = ea; n2b = n1b; n1b = eb;
+  }
+  auto len = [&](const std::vector<double>& a, const std::vector<double>& b, int n) {
+    int k = 0;
+    for (int j = 0; j < n; ++j)
+      if (std::fabs(a[j]) > 1e-12 || std::fabs(b[j]) > 1e-12) k = j + 1;
+    return k;
+  };
+  kg = std::max(2, len(H0, H1, L - h));  // c(h), c(h+1) always read H at 0 and 1
+  ke = len(E0, E1, h);
+  const int LT = L + 8;  // padded: the kernel reads the tables in blocks of eight
+  out.assign((size_t)4 * LT, 0.0f);
+  for (int j = 0; j < kg; ++j) { out[j] = (float)H0[j]; out[LT + j] = (float)H1[j]; }
+  for (int j = 0; j < ke; ++j) { out[2 * LT + j] = (float)E0[j]; out[3 * LT + j] = (float)E1[j]; }
+}
 
 struct CaseState {
   canard_case_desc d;
@@ -107,7 +183,10 @@ struct BlockState {
   std::vector<double> xyz_host;  // reference layout, kept for the sponge set-up
   // mixed precision: FP32 work fields, factors and line-end buffers
   float* arena32 = nullptr;
-  float* lu32[2][3] = {};
+  float* lu32[2][3] = {};   // FP32 factors (5 L) followed by the split-solve tables (4 (L + 8))
+  int h32[2][3] = {}, kg32[2][3] = {}, ke32[2][3] = {};
+  float luc32[2][3][5] = {};  // bitwise-constant interior FP32 factors
+  int luc032[2][3] = {};      // first row of that range
   float* recv32[3] = {};  // derivative receive buffers of the FP32 fields
   float* drva32[3] = {};
   float* drvb32[3] = {};
@@ -251,13 +330,13 @@ float* gptr(const BlockState& b, int f) { return b.arena32 + (size_t)f * b.g.npa
 
 // A tile moves in nc chunks of cr positions: about 64 positions each (2..8
 // chunks), cr even (16-byte aligned bulk copies) and at most 256 (a TMA box),
-// and the last chunk keeps at least 12 positions so the end closures only
-// need the first and the last chunk.
+// and the first and the last chunk keep at least 13 positions, so the end
+// closures and the in-kernel periodic contraction only need those two.
 void chunking(int L, int& nc, int& cr) {
   nc = std::max(1, std::min(kMaxChunks, L / 64));
   for (;; --nc) {
     cr = ((L + nc - 1) / nc + 1) / 2 * 2;
-    if (nc <= 2 || (L - (nc - 1) * cr >= 12 && cr >= 12)) break;
+    if (nc <= 2 || (L - (nc - 1) * cr >= 13 && cr >= 13)) break;
   }
   if (nc == 1) cr = (L + 1) / 2 * 2;
 }
@@ -274,9 +353,17 @@ void chunking_dir(int dir, int L, int& nc, int& cr) {
 }
 
 // ---- line task construction ----------------------------------------------------
+// Both ends of direction dir periodic onto the block itself: the interface
+// contraction of a derivative pass can be formed inside the line kernel.
+bool self_periodic(const BlockGeom& g, int dir) {
+  return g.nbc[dir][0] == BC_PERIODIC && g.nbc[dir][1] == BC_PERIODIC && g.nbr[dir][0] == g.block_in_case &&
+         g.nbr[dir][1] == g.block_in_case;
+}
+
 void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const void* in,
-                    void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64) {
+                    void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64, bool allow_selfp = false) {
   const BlockGeom& g = B.g;
+  t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
   t.out = out;
   t.lu = (kind == LK_F64) ? static_cast<const void*>(B.lu[nt][dir]) : static_cast<const void*>(B.lu32[nt][dir]);
@@ -293,24 +380,35 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.m = m;
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
+  t.h = t.kg = t.ke = 0;
+  if (tile_lanes(kind) == kHalf) {
+    t.h = B.h32[nt][dir];
+    t.kg = B.kg32[nt][dir];
+    t.ke = B.ke32[nt][dir];
+    t.cl1 = B.luc32[nt][dir][0]; t.cl2 = B.luc32[nt][dir][1]; t.cu1 = B.luc32[nt][dir][2];
+    t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
+    t.c0 = B.luc032[nt][dir];
+  }
   chunking_dir(dir, t.L, t.nbox, t.by);
+  const int lanes = tile_lanes(kind);
   if (dir == 0) {
     t.ntx = 1;
-    t.ntiles = (g.Y * g.Z + kLanes - 1) / kLanes;
+    t.ntiles = (g.Y * g.Z + lanes - 1) / lanes;
   } else {
-    t.ntx = (g.X + kLanes - 1) / kLanes;
+    t.ntx = (g.X + lanes - 1) / lanes;
     t.ntiles = t.ntx * (dir == 1 ? g.Z : g.Y);
   }
 }
 
 size_t line_smem(int dir, int L, int kind = LK_F64) {
   const size_t es = tile_elem(kind);
+  const int lanes = tile_lanes(kind);
   if (dir == 0) {
-    return 128 + (size_t)kLanes * (kind == LK_F32 ? dir1_pitch<float>(L) : dir1_pitch<double>(L)) * es;
+    return 128 + (size_t)lanes * (kind == LK_F32 ? dir1_pitch<float>(L) : dir1_pitch<double>(L)) * es;
   }
   int nc, cr;
   chunking(L, nc, cr);
-  return 128 + (size_t)nc * cr * kLanes * es;
+  return 128 + (size_t)nc * cr * lanes * es;
 }
 
 // cuTensorMapEncodeTiled from the driver, found at run time (the library does
@@ -332,11 +430,12 @@ EncodeTiledFn encode_fn() {
 
 // 3-D map over a padded field (X, Y, Z) with box (32, by, 1) for eta lines or
 // (32, 1, by) for zeta lines.
-CUtensorMap field_map(const void* base, int X, int Y, int Z, int Xp, int dir, int by, size_t es = sizeof(double)) {
+CUtensorMap field_map(const void* base, int X, int Y, int Z, int Xp, int dir, int by, size_t es = sizeof(double),
+                      int lanes = kLanes) {
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
   cuuint64_t strides[2] = {(cuuint64_t)Xp * es, (cuuint64_t)Xp * Y * es};
-  cuuint32_t box[3] = {(cuuint32_t)kLanes, (cuuint32_t)(dir == 1 ? by : 1), (cuuint32_t)(dir == 2 ? by : 1)};
+  cuuint32_t box[3] = {(cuuint32_t)lanes, (cuuint32_t)(dir == 1 ? by : 1), (cuuint32_t)(dir == 2 ? by : 1)};
   cuuint32_t estr[3] = {1, 1, 1};
   const CUtensorMapDataType ty = es == sizeof(float) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   CUresult r = encode_fn()(&m, ty, 3, const_cast<void*>(base), dims, strides, box, estr,
@@ -369,8 +468,8 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
   std::vector<CUtensorMap> maps(2 * v.size());
   if (dir != 0)
     for (size_t i = 0; i < v.size(); ++i) {
-      maps[2 * i] = field_map(v[i].in, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es);
-      maps[2 * i + 1] = field_map(v[i].out, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es);
+      maps[2 * i] = field_map(v[i].in, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es, tile_lanes(kind));
+      maps[2 * i + 1] = field_map(v[i].out, v[i].X, v[i].Y, v[i].Z, v[i].Xp, dir, v[i].by, es, tile_lanes(kind));
     }
   else
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
@@ -413,11 +512,19 @@ void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
+template <int DIR, int OP, class TT>
+void launch_line2_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
+  launch_line2_t<DIR, OP, TT>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  CK(cudaGetLastError());
+}
+
 template <int DIR, int OP>
 void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   if (T.kind == LK_F64) launch_line_dir<DIR, OP, double, double>(c, T);
-  else if (OP == 0 && T.kind == LK_F32) launch_line_dir<DIR, 0, float, float>(c, T);
-  else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line_dir<DIR, 1, double, float>(c, T);
+  else if (OP == 0 && T.kind == LK_F32) launch_line2_dir<DIR, 0, float>(c, T);
+  else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line2_dir<DIR, 1, double>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -443,12 +550,12 @@ void set_line_smem_limits() {
   CK((line_smem_limit<1, 1, double, double>(lim)));
   CK((line_smem_limit<2, 1, double, double>(lim)));
   CK((line_smem_limit<3, 1, double, double>(lim)));
-  CK((line_smem_limit<1, 0, float, float>(lim)));
-  CK((line_smem_limit<2, 0, float, float>(lim)));
-  CK((line_smem_limit<3, 0, float, float>(lim)));
-  CK((line_smem_limit<1, 1, double, float>(lim)));
-  CK((line_smem_limit<2, 1, double, float>(lim)));
-  CK((line_smem_limit<3, 1, double, float>(lim)));
+  CK((line2_smem_limit<1, 0, float>(lim)));
+  CK((line2_smem_limit<2, 0, float>(lim)));
+  CK((line2_smem_limit<3, 0, float>(lim)));
+  CK((line2_smem_limit<1, 1, double>(lim)));
+  CK((line2_smem_limit<2, 1, double>(lim)));
+  CK((line2_smem_limit<3, 1, double>(lim)));
   done = true;
 }
 
@@ -457,7 +564,7 @@ void set_line_smem_limits() {
 // gives the field column the block uses for that direction.
 template <class ColFn>
 std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, int exch_dir, ColFn col,
-                                 int only_case = -1, bool f32 = false) {
+                                 int only_case = -1, bool f32 = false, bool skip_selfp = false) {
   std::vector<FaceTask> out;
   int line0 = 0;
   for (const FaceLink& L : c->links) {
@@ -466,6 +573,7 @@ std::vector<FaceTask> face_tasks(const canard_ctx* c, int nt, int n45, int m, in
     const BlockState& R = c->blocks[L.dst_b];
     const int d = L.nn;
     if (!bc_interface(S.g.nbc[d][L.src_side])) continue;
+    if (skip_selfp && L.src_b == L.dst_b && self_periodic(S.g, d)) continue;  // formed in the line kernel
     FaceTask t{};
     t.src = col(L.src_b, d);
     t.dstf = col(L.dst_b, d);
@@ -852,7 +960,7 @@ void build_tables(canard_ctx* c) {
       for (int m = 2; m <= 5; ++m) {
         LineTask t;
         fill_line_task(c, c->blocks[b], dir, 0, wf(b, F_DE + m - 1, G_DE + m - 1),
-                       wf(b, F_SCR + 3 * (m - 2) + dir, G_SCR + 3 * (m - 2) + dir), m, false, t, dkind);
+                       wf(b, F_SCR + 3 * (m - 2) + dir, G_SCR + 3 * (m - 2) + dir), m, false, t, dkind, true);
         v.push_back(t);
       }
     }
@@ -861,7 +969,8 @@ void build_tables(canard_ctx* c) {
   {
     std::vector<FaceTask> all;
     for (int m = 2; m <= 5; ++m) {
-      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int) { return wf(b, F_DE + m - 1, G_DE + m - 1); }, -1, f32);
+      auto v = face_tasks(c, 0, 0, m, -1, [&](int b, int) { return wf(b, F_DE + m - 1, G_DE + m - 1); }, -1, f32,
+                          true);
       all.insert(all.end(), v.begin(), v.end());
     }
     c->mp_visc = make_face_table(c, all, false, f32 ? 1 : 0);
@@ -873,7 +982,7 @@ void build_tables(canard_ctx* c) {
       for (int m = 1; m <= 5; ++m) {
         LineTask t;
         void* f = wf(b, F_SCR + 3 * (m - 1) + dir, G_SCR + 3 * (m - 1) + dir);
-        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t, dkind);
+        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t, dkind, true);
         v.push_back(t);
       }
     c->flux[dir] = make_line_table(c, v, dir, false, dkind);
@@ -883,7 +992,7 @@ void build_tables(canard_ctx* c) {
     for (int m = 1; m <= 5; ++m) {
       auto v = face_tasks(
           c, 0, 0, m, -1, [&](int b, int d) { return wf(b, F_SCR + 3 * (m - 1) + d, G_SCR + 3 * (m - 1) + d); }, -1,
-          f32);
+          f32, true);
       all.insert(all.end(), v.begin(), v.end());
     }
     c->mp_flux = make_face_table(c, all, false, f32 ? 1 : 0);
@@ -1237,7 +1346,22 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         sch.lu(L, n0, n1, nt, lu.data());
         B.lu[nt][dir] = dupload(lu, c->st);
         if (c->f32()) {  // the FP64 factorisation, rounded for the FP32 eliminations
-          std::vector<float> lu32(lu.begin(), lu.end());
+          std::vector<float> lu32(lu.begin(), lu.end()), hom;
+          // rows [c0, L-4] whose rounded factors are bit-identical to row L-4
+          const int e = L - 4;
+          int c0f = e;
+          auto same32 = [&](int r) {
+            for (int k = 0; k < 5; ++k)
+              if (std::memcmp(&lu32[(size_t)k * L + r], &lu32[(size_t)k * L + e], sizeof(float)) != 0) return false;
+            return true;
+          };
+          while (c0f - 1 >= 3 && same32(c0f - 1)) --c0f;
+          for (int k = 0; k < 5; ++k) B.luc32[nt][dir][k] = lu32[(size_t)k * L + e];
+          B.luc032[nt][dir] = c0f;
+          const int h = split_row(L, dir, nt, c0f);
+          split_tables(lu, L, h, hom, B.kg32[nt][dir], B.ke32[nt][dir]);
+          B.h32[nt][dir] = h;
+          lu32.insert(lu32.end(), hom.begin(), hom.end());
           B.lu32[nt][dir] = dupload(lu32, c->st);
         }
         // rows [i0, L-4] whose five factors are bit-identical to row L-4

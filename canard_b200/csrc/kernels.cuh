@@ -93,6 +93,8 @@ struct LineTask {
   const DevScheme* sc;
   int X, Y, Z, Xp;
   int L, nbs, m, ndf0, ndf1;
+  int selfp;               // derivative of a line periodic onto itself: contraction formed in the kernel
+  int h, kg, ke;           // split solves: first row of the second half; homogeneous table lengths
   int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
   int nbox, by;            // chunks per tile and positions per chunk
 };
@@ -778,8 +780,25 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   const TT* recv = static_cast<const TT*>(T.recv);
   if (OP == 0) {
     TT r00 = 0, r10 = 0, r01 = 0, r11 = 0;
-    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; }
-    if (has && T.ndf1) { r01 = recv[2 * nbs + jk]; r11 = recv[3 * nbs + jk]; }
+    if (T.selfp) {
+      // The line is periodic onto itself, so the interface contraction the
+      // other end would send (src/mo_numerics.f90:503-518 with n45 = 0) is
+      // formed here from the tile: side 0 receives the sums over positions
+      // N-1..N-12, side 1 over positions 1..12, accumulated in the same order.
+      const DevScheme* sc = T.sc;
+      const int N = L - 1;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const TT v = sl[(N - 1 - i) * ST], w = sl[(1 + i) * ST];
+        r00 = r00 + TT(sc->pbco[0][0][i]) * v;
+        r10 = r10 + TT(sc->pbco[0][1][i]) * v;
+        r01 = r01 + TT(sc->pbco[0][0][i]) * w;
+        r11 = r11 + TT(sc->pbco[0][1][i]) * w;
+      }
+    } else {
+      if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; }
+      if (has && T.ndf1) { r01 = recv[2 * nbs + jk]; r11 = recv[3 * nbs + jk]; }
+    }
     ok = sweep_deriv<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11, CI, err, done);
     if (ok && has && T.drva) {
       TT* drva = static_cast<TT*>(T.drva);
@@ -808,6 +827,471 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     g_trace[(long long)blockIdx.x * 8 + 6] = smid;
   }
 #endif
+}
+
+// ---------------------------------------------------------------------------
+// Split line solves of the FP32 path. One warp holds 16 lines; lane l owns
+// rows [0, h) of line l and lane l+16 rows [h, L) of the same line, and both
+// halves run the same instruction stream over their own rows, so each
+// dependent recurrence is about half as long as in k_line and a warp's tile
+// needs half the shared memory. The second half eliminates forward from a
+// zero start and substitutes backward from its true end; the first half
+// eliminates forward exactly and substitutes backward from a zero start.
+// By linearity the true solution is then
+//   rows >= h:  c = c_part + H0 a(h-2) + H1 a(h-1)
+//   rows <  h:  c = c_part + E0 c(h) + E1 c(h+1)
+// where H0, H1 are the second half's back substitution of the homogeneous
+// forward solutions started at rows h-2, h-1, and E0, E1 the homogeneous
+// backward solutions started at rows h, h+1. They depend only on the LU
+// factors and decay geometrically away from h; the host tabulates them in
+// FP64 (stored FP32) as far as they exceed 1e-12. Algebraically this is the
+// same elimination; the rounding differs from the one-lane order, which is
+// why only the FP32 path uses it.
+constexpr int kHalf = 16;
+
+// Correction tables of one (block, direction, system): H0, H1 indexed by
+// row - h, E0, E1 indexed by h-1-row, each L + 8 long (zero past kh / ke,
+// so blocks of eight read past the end without a bound).
+struct SplitTables {
+  const float* __restrict__ h0;
+  const float* __restrict__ h1;
+  const float* __restrict__ e0;
+  const float* __restrict__ e1;
+  int kh, ke;
+};
+
+// Forward elimination of rows [ib, ie) with per-lane bounds (window w0..w3 =
+// s[i-2..i+1] on entry), blocks of eight.
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void fwd_rows_deriv(TT* s, int ib, int ie, const CF& cf, TT& w0, TT& w1, TT& w2,
+                                               TT& w3, RS& am2, RS& am1) {
+  int i = ib;
+  for (; i + 7 < ie; i += 8) fwd8_deriv<ST, TT, RS>(s, i, cf, w0, w1, w2, w3, am2, am1);
+  for (; i < ie; ++i) {
+    const TT w4 = s[(i + 2) * ST];
+    const TT rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4 - w0);
+    const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
+    s[i * ST] = TT(a);
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+    am2 = am1; am1 = a;
+  }
+}
+
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void fwd_rows_filter(TT* s, int ib, int ie, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
+                                                TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+  int i = ib;
+  for (; i + 7 < ie; i += 8) fwd8_filter<ST, TT, RS>(s, i, cf, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  for (; i < ie; ++i) {
+    const TT w6 = s[(i + 3) * ST];
+    const TT rk = w3 + w3;
+    const TT rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+    const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
+    s[i * ST] = TT(a);
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    am2 = am1; am1 = a;
+  }
+}
+
+// back substitution of rows ihi down to ilo (inclusive), per-lane bounds
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void bwd_rows(TT* s, int ihi, int ilo, const CF& cf, RS& cp1, RS& cp2) {
+  int i = ihi;
+  for (; i - 7 >= ilo; i -= 8) bwd8<ST, TT, RS>(s, i, cf, cp1, cp2);
+  for (; i >= ilo; --i) {
+    const RS c = (cf.U1(i) * RS(s[i * ST]) - cf.U2(i) * cp1) - cf.U3(i) * cp2;
+    s[i * ST] = TT(c);
+    cp2 = cp1;
+    cp1 = c;
+  }
+}
+
+// Rows [ib, ie) in three per-lane segments: table factors below c0, the
+// register constants on [c0, c1], table factors above c1.
+template <int OP, int ST, class TT, class RS>
+__device__ __forceinline__ void fwd3(TT* s, int ib, int ie, int c0, int c1, const CoefTable<RS>& ct,
+                                     const CoefConst<RS>& cc, TT fa, TT fb, TT fc, TT& w0, TT& w1, TT& w2, TT& w3,
+                                     TT& w4, TT& w5, RS& am2, RS& am1) {
+  const int m0 = max(ib, c0), m1 = min(ie, c1 + 1);
+  if (OP == 0) {
+    fwd_rows_deriv<ST, TT, RS>(s, ib, min(ie, m0), ct, w0, w1, w2, w3, am2, am1);
+    fwd_rows_deriv<ST, TT, RS>(s, m0, m1, cc, w0, w1, w2, w3, am2, am1);
+    fwd_rows_deriv<ST, TT, RS>(s, max(ib, c1 + 1), ie, ct, w0, w1, w2, w3, am2, am1);
+  } else {
+    fwd_rows_filter<ST, TT, RS>(s, ib, min(ie, m0), ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS>(s, m0, m1, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS>(s, max(ib, c1 + 1), ie, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  }
+}
+
+// rows ihi down to ilo in the same three segments
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void bwd3(TT* s, int ihi, int ilo, int c0, int c1, const CoefTable<RS>& ct,
+                                     const CoefConst<RS>& cc, RS& cp1, RS& cp2) {
+  bwd_rows<ST, TT, RS>(s, ihi, max(ilo, c1 + 1), ct, cp1, cp2);
+  bwd_rows<ST, TT, RS>(s, min(ihi, c1), max(ilo, c0), cc, cp1, cp2);
+  bwd_rows<ST, TT, RS>(s, min(ihi, c0 - 1), ilo, ct, cp1, cp2);
+}
+
+// OP 0: derivative, OP 1: filter increment, of the lane's half of its line.
+// On return (after a warp-wide barrier) the tile holds the derivative or the
+// increment. q0, q1 (, q2): interface values received by the lane's own end
+// (side 0 for the first half, side 1 for the second).
+template <int OP, int ST, class TT>
+__device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int half, const CoefTable<float>& cf,
+                                       const CoefConst<float>& cc, int c0, const SplitTables& H, int ndf0,
+                                       int ndf1, const DevScheme* __restrict__ sc, TT q0, TT q1, TT q2) {
+  using RS = float;
+  constexpr int NE = OP == 0 ? 2 : 3;  // closure rows at each end
+  const int N = L - 1;
+  const unsigned full = 0xffffffffu;
+  const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
+  auto fbc = [&](int r, int k) { return TT(sc->fbc[r][k]); };
+  // ---- reads of the original line, before any row is overwritten
+  TT b[3] = {0, 0, 0};           // closure right-hand sides of the own end (second half: bn, bn1, bn2)
+  TT w0, w1, w2, w3, w4 = 0, w5 = 0;
+  TT x[3] = {0, 0, 0};           // first half: originals at h, h+1 (, h+2)
+  if (half == 0) {
+    if (OP == 0) {
+      if (ndf0 == 0) {
+        const TT s0 = s[0], s1 = s[ST], s2 = s[2 * ST], s3 = s[3 * ST], s4 = s[4 * ST];
+        b[0] = ((TT(CA_A01) * (s1 - s0) + TT(CA_A02) * (s2 - s0)) + TT(CA_A03) * (s3 - s0)) + TT(CA_A04) * (s4 - s0);
+        b[1] = ((TT(CA_A10) * (s0 - s1) + TT(CA_A12) * (s2 - s1)) + TT(CA_A13) * (s3 - s1)) + TT(CA_A14) * (s4 - s1);
+      } else {
+        TT t0 = 0, t1 = 0;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const TT v = s[i * ST];
+          t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+          t1 = t1 + TT(sc->pbci[0][1][i]) * v;
+        }
+        b[0] = t0 + q0;
+        b[1] = t1 + q1;
+      }
+      w0 = s[0]; w1 = s[ST]; w2 = s[2 * ST]; w3 = s[3 * ST];
+    } else {
+      const TT s0 = s[0], s1 = s[ST], s2 = s[2 * ST], s3 = s[3 * ST], s4 = s[4 * ST], s5 = s[5 * ST];
+      if (ndf0 == 0) {
+        b[0] = (((fbc(0, 0) * (s1 - s0) + fbc(0, 1) * (s2 - s0)) + fbc(0, 2) * (s3 - s0)) + fbc(0, 3) * (s4 - s0)) +
+               fbc(0, 4) * (s5 - s0);
+        b[1] = (((fbc(1, 0) * (s0 - s1) + fbc(1, 1) * (s2 - s1)) + fbc(1, 2) * (s3 - s1)) + fbc(1, 3) * (s4 - s1)) +
+               fbc(1, 4) * (s5 - s1);
+        b[2] = (((fbc(2, 0) * (s0 - s2) + fbc(2, 1) * (s1 - s2)) + fbc(2, 2) * (s3 - s2)) + fbc(2, 3) * (s4 - s2)) +
+               fbc(2, 4) * (s5 - s2);
+      } else {
+        TT t0 = 0, t1 = 0;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const TT v = s[i * ST];
+          t0 = t0 + TT(sc->pbci[1][0][i]) * v;
+          t1 = t1 + TT(sc->pbci[1][1][i]) * v;
+        }
+        const TT ra2 = s2 + s2;
+        b[0] = t0 + q0;
+        b[1] = t1 + q1;
+        b[2] = (fa * ((s1 + s3) - ra2) + fb * ((s0 + s4) - ra2)) + fc * ((q2 + s5) - ra2);
+      }
+      w0 = s0; w1 = s1; w2 = s2; w3 = s3; w4 = s4; w5 = s5;
+      x[2] = s[(h + 2) * ST];
+    }
+    x[0] = s[h * ST];
+    x[1] = s[(h + 1) * ST];
+  } else {
+    if (OP == 0) {
+      if (ndf1 == 0) {
+        const TT e0 = s[N * ST], e1 = s[(N - 1) * ST], e2 = s[(N - 2) * ST], e3 = s[(N - 3) * ST],
+                 e4 = s[(N - 4) * ST];
+        b[0] = ((TT(CA_A01) * (e0 - e1) + TT(CA_A02) * (e0 - e2)) + TT(CA_A03) * (e0 - e3)) + TT(CA_A04) * (e0 - e4);
+        b[1] = ((TT(CA_A10) * (e1 - e0) + TT(CA_A12) * (e1 - e2)) + TT(CA_A13) * (e1 - e3)) + TT(CA_A14) * (e1 - e4);
+      } else {
+        TT t0 = 0, t1 = 0;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const TT v = s[(N - i) * ST];
+          t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+          t1 = t1 + TT(sc->pbci[0][1][i]) * v;
+        }
+        b[0] = -t0 - q0;
+        b[1] = -t1 - q1;
+      }
+      w0 = s[(h - 2) * ST]; w1 = s[(h - 1) * ST]; w2 = s[h * ST]; w3 = s[(h + 1) * ST];
+    } else {
+      const TT e0 = s[N * ST], e1 = s[(N - 1) * ST], e2 = s[(N - 2) * ST], e3 = s[(N - 3) * ST],
+               e4 = s[(N - 4) * ST], e5 = s[(N - 5) * ST];
+      if (ndf1 == 0) {
+        b[0] = (((fbc(0, 0) * (e1 - e0) + fbc(0, 1) * (e2 - e0)) + fbc(0, 2) * (e3 - e0)) + fbc(0, 3) * (e4 - e0)) +
+               fbc(0, 4) * (e5 - e0);
+        b[1] = (((fbc(1, 0) * (e0 - e1) + fbc(1, 1) * (e2 - e1)) + fbc(1, 2) * (e3 - e1)) + fbc(1, 3) * (e4 - e1)) +
+               fbc(1, 4) * (e5 - e1);
+        b[2] = (((fbc(2, 0) * (e0 - e2) + fbc(2, 1) * (e1 - e2)) + fbc(2, 2) * (e3 - e2)) + fbc(2, 3) * (e4 - e2)) +
+               fbc(2, 4) * (e5 - e2);
+      } else {
+        TT t0 = 0, t1 = 0;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const TT v = s[(N - i) * ST];
+          t0 = t0 + TT(sc->pbci[1][0][i]) * v;
+          t1 = t1 + TT(sc->pbci[1][1][i]) * v;
+        }
+        const TT ra2 = e2 + e2;
+        b[0] = t0 + q0;
+        b[1] = t1 + q1;
+        b[2] = (fa * ((e3 + e1) - ra2) + fb * ((e4 + e0) - ra2)) + fc * ((e5 + q2) - ra2);
+      }
+      w0 = s[(h - 3) * ST]; w1 = s[(h - 2) * ST]; w2 = s[(h - 1) * ST];
+      w3 = s[h * ST]; w4 = s[(h + 1) * ST]; w5 = s[(h + 2) * ST];
+    }
+  }
+  __syncwarp();
+  // ---- forward elimination: closure rows (first half), the shared interior
+  // loop, then NE tail rows whose right-hand sides come from registers
+  RS am2 = 0, am1 = 0;
+  if (half == 0) {
+    am2 = RS(b[0]);
+    am1 = RS(b[1]) - cf.L2(1) * am2;
+    s[0] = TT(am2);
+    s[ST] = TT(am1);
+    if (OP == 1) {
+      const RS a2 = (RS(b[2]) - cf.L1(2) * am2) - cf.L2(2) * am1;
+      s[2 * ST] = TT(a2);
+      am2 = am1;
+      am1 = a2;
+    }
+  }
+  const int fb0 = half == 0 ? NE : h;          // interior rows [fb0, fe0)
+  const int fe0 = half == 0 ? h - NE : N + 1 - NE;
+  const int c1 = L - 4;
+  fwd3<OP, ST, TT, RS>(s, fb0, fe0, c0, c1, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const int i = fe0 + k;
+    TT rhs;
+    if (OP == 0) {
+      const TT w4n = x[k];
+      rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4n - w0);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4n;
+    } else {
+      const TT w6 = x[k];
+      const TT rk = w3 + w3;
+      rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    }
+    if (half == 1) rhs = b[NE - 1 - k];
+    const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
+    s[i * ST] = TT(a);
+    am2 = am1;
+    am1 = a;
+  }
+  // the first half's a(h-2), a(h-1), needed by the second half's correction
+  const int src = threadIdx.x & (kHalf - 1);
+  const RS A0 = __shfl_sync(full, am2, src), A1 = __shfl_sync(full, am1, src);
+  __syncwarp();
+  // ---- back substitution: two end rows (second half), then the shared loop
+  RS cp1 = 0, cp2 = 0;
+  if (half == 1) {
+    cp1 = cf.U1(N) * RS(s[N * ST]);
+    s[N * ST] = TT(cp1);
+    const RS c = cf.U1(N - 1) * RS(s[(N - 1) * ST]) - cf.U2(N - 1) * cp1;
+    s[(N - 1) * ST] = TT(c);
+    cp2 = cp1;
+    cp1 = c;
+  }
+  bwd3<ST, TT, RS>(s, half == 0 ? h - 1 : N - 2, half == 0 ? 0 : h, c0, c1, cf, cc, cp1, cp2);
+  // the second half's true c(h), c(h+1), needed by the first half's correction
+  RS ch0 = 0, ch1 = 0;
+  if (half == 1) {
+    ch0 = cp1 + (__ldg(H.h0) * A0 + __ldg(H.h1) * A1);
+    ch1 = cp2 + (__ldg(H.h0 + 1) * A0 + __ldg(H.h1 + 1) * A1);
+  }
+  const RS C0 = __shfl_sync(full, ch0, src + kHalf), C1 = __shfl_sync(full, ch1, src + kHalf);
+  __syncwarp();
+  // ---- both corrections in one loop: first half rows h-1, h-2, ... with
+  // (E0, E1; c(h), c(h+1)), second half rows h, h+1, ... with (H0, H1; a(h-2), a(h-1))
+  {
+    const float* t0 = half == 0 ? H.e0 : H.h0;
+    const float* t1 = half == 0 ? H.e1 : H.h1;
+    const RS s0 = half == 0 ? C0 : A0, s1 = half == 0 ? C1 : A1;
+    const int cnt = half == 0 ? min(H.ke, h) : min(H.kh, L - h);
+    const int i0 = half == 0 ? h - 1 : h, di = half == 0 ? -1 : 1;
+    const int kmax = max(min(H.ke, h), min(H.kh, L - h));
+    for (int j0 = 0; j0 < kmax; j0 += 8) {
+      float g0[8], g1[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        g0[k] = __ldg(t0 + j0 + k);
+        g1[k] = __ldg(t1 + j0 + k);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (j0 + k < cnt) {
+          const int i = i0 + di * (j0 + k);
+          s[i * ST] = TT(RS(s[i * ST]) + (g0[k] * s0 + g1[k] * s1));
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// One CTA = one warp = 16 lines, split solve (see above). DIR: 1 xi, 2 eta,
+// 3 zeta. OP: 0 derivative, 1 filter (in place). TT: field and tile type;
+// the elimination is FP32.
+template <int DIR, int OP, class TT>
+__global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
+                                              int ntasks, const CUtensorMap* __restrict__ maps,
+                                              int* __restrict__ err) {
+  constexpr int kVec = 16 / (int)sizeof(TT);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  TT* s = reinterpret_cast<TT*>(smem_raw + 128);
+  const int lane = threadIdx.x;
+  const int half = lane >> 4, li = lane & (kHalf - 1);
+  const int ti = find_task(tile0s, ntasks, blockIdx.x);
+  const LineTask& T = tasks[ti];
+  const TT* in = static_cast<const TT*>(T.in);
+  TT* out = static_cast<TT*>(T.out);
+  const int lt = blockIdx.x - T.tile0;
+  const int L = T.L, h = T.h;
+  const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
+  const int NC = T.nbox, CR = T.by;
+  int nval, x0 = 0, r0 = 0, fix = 0;
+  if (DIR == 1) {
+    r0 = lt * kHalf;
+    nval = min(kHalf, Y * Z - r0);
+  } else {
+    fix = lt / T.ntx;
+    x0 = (lt % T.ntx) * kHalf;
+    nval = min(kHalf, X - x0);
+  }
+  const int P = dir1_pitch<TT>(L);
+  const long long pstride = (DIR == 2) ? (long long)Xp : (long long)Xp * Y;
+  const long long base = (DIR == 1) ? (long long)r0 * Xp
+                                    : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
+  const CUtensorMap* map_in = maps + 2 * ti;
+  const CUtensorMap* map_out = maps + 2 * ti + 1;
+  auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
+  if (lane == 0)
+    for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+  __syncwarp();
+  for (int c = 0; c < NC; ++c) {
+    if (DIR == 1) {
+      const uint32_t bytes = (uint32_t)((chunk_len(c) + kVec - 1) / kVec * kVec * sizeof(TT));
+      if (lane == 0) mbar_expect_tx(bars + c, bytes * nval);
+      __syncwarp();
+      if (lane < nval) bulk_g2s(s + lane * P + c * CR, in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
+    } else if (lane == 0) {
+      mbar_expect_tx(bars + c, (uint32_t)(CR * kHalf * sizeof(TT)));
+      if (DIR == 2) tma_load_3d(s + c * CR * kHalf, map_in, x0, c * CR, fix, bars + c);
+      else tma_load_3d(s + c * CR * kHalf, map_in, x0, fix, c * CR, bars + c);
+    }
+  }
+  bool ok = true;
+  for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
+  if (!ok) {
+    if (lane == 0) atomicExch(err, kErrTimeout);
+    return;
+  }
+  __syncwarp();
+  constexpr int ST = (DIR == 1) ? 1 : kHalf;
+  TT* sl = (DIR == 1) ? s + li * P : s + li;
+  const bool has = li < nval;
+  int jk = 0;
+  if (DIR == 1) jk = r0 + li;
+  else if (DIR == 2) jk = (x0 + li) * Z + fix;
+  else jk = fix * X + x0 + li;
+  const int nbs = T.nbs, N = L - 1;
+  const float* lu = static_cast<const float*>(T.lu);
+  const CoefTable<float> cf{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
+  const float* hb = lu + 5 * L;  // correction tables follow the factors
+  const int LT = L + 8;
+  const SplitTables H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke};
+  const TT* recv = static_cast<const TT*>(T.recv);
+  // interface sums received by the own end
+  TT q0 = 0, q1 = 0, q2 = 0;
+  if (OP == 0 && T.selfp) {
+    // periodic onto itself: the contraction the other end would send (see k_line)
+    const DevScheme* sc = T.sc;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const TT v = half == 0 ? sl[(N - 1 - i) * ST] : sl[(1 + i) * ST];
+      q0 = q0 + TT(sc->pbco[0][0][i]) * v;
+      q1 = q1 + TT(sc->pbco[0][1][i]) * v;
+    }
+  } else if (has) {
+    const int nc = OP == 0 ? 2 : 3;
+    if (half == 0 && T.ndf0) {
+      q0 = recv[jk]; q1 = recv[nbs + jk];
+      if (OP == 1) q2 = recv[2 * nbs + jk];
+    }
+    if (half == 1 && T.ndf1) {
+      q0 = recv[nc * nbs + jk]; q1 = recv[(nc + 1) * nbs + jk];
+      if (OP == 1) q2 = recv[(nc + 2) * nbs + jk];
+    }
+  }
+  const CoefConst<float> cc{float(T.cl1), float(T.cl2), float(T.cu1), float(T.cu2), float(T.cu3)};
+  sweep2<OP, ST, TT>(sl, L, h, half, cf, cc, T.c0, H, T.ndf0, T.ndf1, T.sc, q0, q1, q2);
+  if (OP == 0 && has && T.drva) {
+    TT* drva = static_cast<TT*>(T.drva);
+    if (half == 0) drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+    else drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[N * ST];
+  }
+  // filter: add the originals; then store every chunk
+  if (OP == 1) {
+    if (DIR != 1) {
+      // lanes of both halves split the rows of the 16 columns
+      if (has) {
+        const TT* g = in + base + li;
+        TT* col = s + li;
+        const int lo = half == 0 ? 0 : h, hi = half == 0 ? h : L;
+        int i = lo;
+        for (; i + 16 <= hi; i += 16) {
+          TT v[16];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) col[(i + k) * kHalf] = v[k] + col[(i + k) * kHalf];
+        }
+        for (; i < hi; ++i) col[i * kHalf] = __ldg(g + (long long)i * pstride) + col[i * kHalf];
+      }
+    } else {
+      const int tot = nval * L;
+      int e = lane;
+      for (; e + 15 * kLanes < tot; e += 16 * kLanes) {
+        TT v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int q = e + k * kLanes, r = q / L, i = q - r * L;
+          v[k] = __ldg(in + base + (long long)r * Xp + i);
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int q = e + k * kLanes, r = q / L, i = q - r * L;
+          s[r * P + i] = v[k] + s[r * P + i];
+        }
+      }
+      for (; e < tot; e += kLanes) {
+        const int r = e / L, i = e - r * L;
+        s[r * P + i] = __ldg(in + base + (long long)r * Xp + i) + s[r * P + i];
+      }
+    }
+    __syncwarp();
+  }
+  fence_proxy_async();
+  __syncwarp();
+  for (int c = 0; c < NC; ++c) {
+    const int lo = c * CR, len = chunk_len(c);
+    if (DIR == 1) {
+      if (lane < nval) {
+        bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                 (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
+      }
+    } else if (lane == 0) {
+      if (DIR == 2) tma_store_3d(map_out, x0, lo, fix, s + lo * kHalf);
+      else tma_store_3d(map_out, x0, fix, lo, s + lo * kHalf);
+    }
+  }
+  bulk_commit();
+  bulk_wait_read0();
 }
 
 // ---------------------------------------------------------------------------
@@ -1371,6 +1855,15 @@ template <int DIR, int OP, class TT, class RS>
 void launch_line_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
                    const CUtensorMap* maps, int* err) {
   k_line<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, int OP, class TT>
+void launch_line2_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
+                    const CUtensorMap* maps, int* err) {
+  k_line2<DIR, OP, TT><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, int OP, class TT>
+cudaError_t line2_smem_limit(int bytes) {
+  return cudaFuncSetAttribute(k_line2<DIR, OP, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 template <int DIR, int OP, class TT, class RS>
 cudaError_t line_smem_limit(int bytes) {

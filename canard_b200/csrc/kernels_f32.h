@@ -32,11 +32,11 @@ CANARD_F32_EXTERN template void launch_face_copy<float>(dim3, cudaStream_t, cons
                                                         const int*, int);
 CANARD_F32_EXTERN template void launch_mpigo_t<float>(int, cudaStream_t, const FaceTask*, const int*, int, int);
 
-#define CANARD_F32_LINE(DIR, OP, TT)                                                                          \
-  CANARD_F32_EXTERN template void launch_line_t<DIR, OP, TT, float>(int, size_t, cudaStream_t, const LineTask*, \
-                                                                    const int*, int, const CUtensorMap*, int*); \
-  CANARD_F32_EXTERN template cudaError_t line_smem_limit<DIR, OP, TT, float>(int);
-// derivatives on FP32 fields; filter of the FP64 state with an FP32 elimination
+#define CANARD_F32_LINE(DIR, OP, TT)                                                                      \
+  CANARD_F32_EXTERN template void launch_line2_t<DIR, OP, TT>(int, size_t, cudaStream_t, const LineTask*,   \
+                                                              const int*, int, const CUtensorMap*, int*);   \
+  CANARD_F32_EXTERN template cudaError_t line2_smem_limit<DIR, OP, TT>(int);
+// split solves: derivatives on FP32 fields; filter of the FP64 state with an FP32 elimination
 CANARD_F32_LINE(1, 0, float)
 CANARD_F32_LINE(2, 0, float)
 CANARD_F32_LINE(3, 0, float)
