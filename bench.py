@@ -52,9 +52,16 @@ def parse():
                    help="fp64: plain FP64 path (bit-exact with the oracle); fp32: FP32 line solves, fluxes, "
                         "viscous stresses and GCBC with the FP64 state, RK update, metrics and LU factors")
     p.add_argument("--cpu-n", type=int, default=128, help="cells per direction of the CPU sample")
+    p.add_argument("--acc-nx", type=int, default=384)
+    p.add_argument("--acc-ny", type=int, default=256)
+    p.add_argument("--acc-nz", type=int, default=128)
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--mode", default="step", choices=["step", "kernels", "accuracy"],
+                   help="step: the time-step benchmark (default); kernels: isolated derivative and filter "
+                        "launches per direction on 5 noise fields, checked against the oracle; accuracy: "
+                        "FP32-mixed against FP64 on the vortex case after 50/200/1000 steps")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the FP32-mixed and batched comparison lines added to the default run")
     return p.parse_args()
@@ -183,6 +190,95 @@ def batched_extra(args, api, cases, torch, stream):
                                                             for s, r in zip(states["fp64_graph"], ref)))
     errs = [state_errors(s, r, 0.5) for s, r in zip(states["fp32_mixed_graph"], ref)]
     out["fp32_max_rel_l2_vs_fp64"] = float(max(max(e) for e in errs))
+    out["fp32_max_abs_vs_fp64"] = float(max(np.abs(s - r).max() for s, r in zip(states["fp32_mixed_graph"], ref)))
+    return out
+
+
+def kernels_mode(args, api, cases, torch):
+    """Isolated line solves (the reference's deriv / filte over one direction):
+    5 FP64 fields of seeded N(0,1) noise plus sin modes k = 1..32 on the TGV
+    block; per (precision, operation, direction) the average device time of
+    one launch over the 5 fields, its algorithmic GB/s (each field read and
+    written once) against the measured copy peak, and the error against the
+    oracle's line solve of the same fields."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    cs = cases.tgv(args.n)
+    blk = cs.blocks[0]
+    fields = cases.noise_fields(blk, 5)
+    o = po.Oracle(cs, setup=False, threads=os.cpu_count() or 1)
+    ref = {}
+    for op in (0, 1):
+        for nn in (1, 2, 3):
+            res = []
+            for k in range(5):
+                f = fields[k].ravel().copy()
+                if op == 0:
+                    o.mpigo([f.copy()], 0, 1, 0, k + 1, k + 1)
+                    r = np.zeros_like(f)
+                    o.deriv(0, f, r, nn, k + 1)
+                else:
+                    o.mpigo([f], 1, 1, 0, k + 1, k + 1)
+                    o.filte(0, f, {2: 1, 3: 2, 1: 3}[nn], k + 1)
+                    r = f
+                res.append(r.reshape(blk.shape))
+            ref[(op, nn)] = np.stack(res)
+        o = po.Oracle(cs, setup=False, threads=os.cpu_count() or 1)  # fresh filter send chain
+    peak, peak_kind = peaks()
+    rows = []
+    for prec, name in ((api.FP64, "fp64"), (api.FP32_MIXED, "fp32")):
+        ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
+        for op in (0, 1):
+            for nn in (1, 2, 3):
+                out, ms = ctx.line_bench(op, nn, fields, reps=args.steps)
+                es = 4 if (name == "fp32" and op == 0) else 8
+                gbs = 5 * blk.npts * 2 * es / (ms / 1e3) / 1e9
+                r = ref[(op, nn)]
+                err = float(np.linalg.norm((out - r).ravel()) / np.linalg.norm(r.ravel()))
+                rows.append({"precision": name, "op": "deriv" if op == 0 else "filter", "dir": "xi eta zeta".split()[nn - 1],
+                             "ms_per_launch": ms, "gbs": gbs, "frac_of_peak": gbs / peak,
+                             "rel_l2_vs_oracle": err, "bit_exact": bool(np.array_equal(out, r))})
+            # the filter chain of a context carries over calls: a fresh context per operation
+        ctx.close()
+    return {"mode": "kernels", "workload": f"tgv{args.n} block ({args.n + 1}^3 points), 5 fields of N(0,1) noise "
+            "+ sum of sin modes k=1..32 (seed 20261203)", "peak_gbs": peak, "peak_kind": peak_kind,
+            "launches_timed": args.steps, "kernels": rows}
+
+
+def accuracy_mode(args, api, cases, torch):
+    """FP32-mixed against FP64 on the isentropic vortex through a GCBC outflow:
+    the 384x256x128 case on the GPU after 50, 200 and 1000 steps (relative L2
+    per conserved variable, momenta against ||rho|| * 0.5), and a 96x64x32
+    copy against the oracle after 50 steps (both precisions)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    out = {"mode": "accuracy"}
+    big = cases.vortex(nx=args.acc_nx, ny=args.acc_ny, nz=args.acc_nz)
+    a = api.Context(big)
+    b = api.Context(big, precision=api.FP32_MIXED)
+    done, rows = 0, []
+    for n in (50, 200, 1000):
+        a.step(n - done)
+        b.step(n - done)
+        done = n
+        rows.append({"steps": n, "rel_l2_fp32_vs_fp64": state_errors(b.state(0), a.state(0), 0.5),
+                     "time": a.time()[5]})
+    a.close()
+    b.close()
+    out["vortex_gpu"] = {"case": big.name, "points": big.npts, "rows": rows}
+    small = cases.vortex(nx=96, ny=64, nz=32)
+    o = po.Oracle(small, threads=os.cpu_count() or 1)
+    o.step(50)
+    qo = o.state(0)
+    res = {}
+    for prec, name in ((api.FP64, "fp64"), (api.FP32_MIXED, "fp32")):
+        g = api.Context(small, precision=prec)
+        g.step(50)
+        res[name] = state_errors(g.state(0), qo, 0.5)
+        g.close()
+    out["vortex_vs_oracle_50_steps"] = {"case": small.name, "points": small.npts, "rel_l2": res}
+    out["note"] = ("per conserved variable (rho, rho u, rho v, rho w, rho E); momentum components against "
+                   "||rho|| * 0.5 where that exceeds their own norm (rho w is zero by symmetry)")
     return out
 
 
@@ -276,6 +372,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from canard_b200 import api, cases
 
+    if args.mode == "kernels":
+        print(json.dumps(kernels_mode(args, api, cases, torch)), flush=True)
+        return 0
+    if args.mode == "accuracy":
+        print(json.dumps(accuracy_mode(args, api, cases, torch)), flush=True)
+        return 0
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
     if args.config == "tgv":

@@ -91,6 +91,7 @@ def lib():
         L.canard_filte.argtypes = [vp, i32, _DP, i32, i32]
         L.canard_set_timers.argtypes = [vp, i32]
         L.canard_set_graphs.argtypes = [vp, i32]
+        L.canard_line_bench.argtypes = [vp, i32, i32, i32, _DP, _DP, i32, ctypes.POINTER(ctypes.c_double)]
         L.canard_get_timers.argtypes = [vp, _DP, _DP, _DP, i32]
         L.canard_timer_name.restype = ctypes.c_char_p
         L.canard_timer_name.argtypes = [i32]
@@ -206,6 +207,16 @@ class Context:
 
     def set_graphs(self, on):
         self._check(lib().canard_set_graphs(self.h, 1 if on else 0))
+
+    def line_bench(self, op, nn, fields, reps=10):
+        """One direction's derivative (op 0) or filter (op 1) over up to 5
+        fields of block 0 (array (nfields, ...) in the reference layout):
+        returns (result of one launch, average ms of `reps` timed launches)."""
+        f = np.ascontiguousarray(fields, np.float64)
+        out = np.zeros_like(f)
+        ms = ctypes.c_double()
+        self._check(lib().canard_line_bench(self.h, op, nn, f.shape[0], _dp(f), _dp(out), reps, ctypes.byref(ms)))
+        return out, ms.value
 
     def timers(self):
         """Per kernel family: device ms, launches, algorithmic bytes since set_timers(True)."""

@@ -134,12 +134,19 @@ def vortex_state(X, Y, mach, strength=5.0, radius=1.0, xc=0.0, yc=0.0):
     return rho, mach + du, dv, np.zeros_like(du), p
 
 
-def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, viscous=1) -> CaseSpec:
-    """Isentropic vortex advected through a non-reflecting (GCBC) outflow.
+def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, viscous=1,
+           sponge_cells=20) -> CaseSpec:
+    """Isentropic vortex carried by a Mach ``mach`` stream through a
+    non-reflecting (GCBC) outflow, in Canard's moving-frame form: the state
+    holds the vortex around fluid at rest, the frame moves at Mach ``mach``
+    along x (amach1 = mach, nsmf = 1), and sponges over ``sponge_cells`` cells
+    at both x ends hold the far field (src/mo_sponge.f90:34-88; the sponge
+    profile spans 2 szth, so szth = half the sponge width). Without them the
+    all-non-reflecting box drifts and the reference algorithm itself stops
+    being finite after a few hundred steps.
 
-    Domain [-8, 8] x [-16/3, 16/3] x [0, 4], xi faces BC 10, eta faces BC 10,
-    zeta periodic. The vortex is moved by the uniform stream in the lab frame
-    (amach = 0), so ``reoo = Re / M``."""
+    Domain [-8, 8] x [-16/3, 16/3] x [0, 4] at 384x256x128 cells, xi faces BC
+    10, eta faces BC 10, zeta periodic."""
     bc = [[BC_NON_REFLECTIVE, BC_NON_REFLECTIVE], [BC_NON_REFLECTIVE, BC_NON_REFLECTIVE],
           [BC_PERIODIC, BC_PERIODIC]]
     mb = [[-1, -1], [-1, -1], [0, 0]]
@@ -151,8 +158,11 @@ def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, v
     z = dx * np.arange(nz + 1)
     Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
     rho, u, v, w, p = vortex_state(X, Y, mach, strength, radius)
-    return CaseSpec([blk], viscous=viscous, reoo=re / mach, xyz=[np.stack([X, Y, Z])],
-                    qa=[_conserved(rho, u, v, w, p)], name=f"vortex{nx}x{ny}x{nz}")
+    szth = 0.5 * sponge_cells * dx
+    return CaseSpec([blk], viscous=viscous, reoo=re, amach=(mach, 0.0, 0.0), nsmf=1,
+                    szco=1.0, szth0=szth, szth1=szth, doml0=8.0, doml1=8.0,
+                    xyz=[np.stack([X, Y, Z])], qa=[_conserved(rho, u - mach, v, w, p)],
+                    name=f"vortex{nx}x{ny}x{nz}")
 
 
 def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, seed=7,

@@ -1734,6 +1734,62 @@ int canard_filte(canard_ctx* c, int32_t iblock, double* f, int32_t inn, int32_t 
   });
 }
 
+int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, const double* in, double* out,
+                      int32_t reps, double* ms_per_launch) {
+  return guarded(c, [&] {
+    if (!in || !out || !ms_per_launch || op < 0 || op > 1 || nn < 1 || nn > 3 || nfields < 1 || nfields > 5 ||
+        reps < 1)
+      throw ApiError(CANARD_ERR_ARG, "bad line bench argument");
+    BlockState& B = c->blocks[block_index(c, 0, 0)];
+    const int dir = nn - 1;
+    const int kind = !c->f32() ? LK_F64 : (op == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
+    const size_t L = (size_t)B.g.X * B.g.Y * B.g.Z;
+    std::vector<LineTask> tasks;
+    for (int k = 0; k < nfields; ++k) {
+      double* f = fptr(B, F_SCR + k);
+      h2d_field(c, B, f, in + k * L, 1);
+      void* src = f;
+      void* dst = op == 0 ? static_cast<void*>(fptr(B, F_SCR + 5 + k)) : static_cast<void*>(f);
+      if (kind == LK_F32) {
+        to_f32(c, f, gptr(B, G_SCR + k), (size_t)B.g.npad);
+        src = gptr(B, G_SCR + k);
+        dst = gptr(B, G_SCR + 5 + k);
+      }
+      LineTask t;
+      fill_line_task(c, B, dir, op, src, dst, k + 1, false, t, kind, true);
+      tasks.push_back(t);
+      // interface contraction of the faces not formed in the kernel
+      const bool w32 = kind == LK_F32;
+      auto col = [&](int b, int) -> const void* {
+        return w32 ? static_cast<const void*>(gptr(c->blocks[b], G_SCR + k))
+                   : static_cast<const void*>(fptr(c->blocks[b], F_SCR + k));
+      };
+      launch_mpigo(c, make_face_table(c, face_tasks(c, op, 0, k + 1, dir, col, 0, w32, op == 0), true, w32 ? 1 : 0));
+    }
+    const Table<LineTask> T = make_line_table(c, tasks, dir, true, kind);
+    launch_line(c, T, dir, op);
+    for (int k = 0; k < nfields; ++k) {
+      double* r = fptr(B, F_SCR + (op == 0 ? 5 : 0) + k);
+      if (kind == LK_F32) to_f64(c, gptr(B, G_SCR + 5 + k), r, (size_t)B.g.npad);
+      d2h_field(c, B, out + k * L, r, 1);
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->st));
+    for (int r = 0; r < reps; ++r) launch_line(c, T, dir, op);
+    CK(cudaEventRecord(e1, c->st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_per_launch = ms / reps;
+    sync_check(c);
+    free_transient(c);
+  });
+}
+
 int canard_set_timers(canard_ctx* c, int32_t on) {
   return guarded(c, [&] {
     CK(cudaStreamSynchronize(c->st));

@@ -162,6 +162,18 @@ int canard_penta(double fltk, double fltrbc, int32_t n, int32_t ns, int32_t ne, 
                  double* xu, double* xl);
 int canard_version(void);
 
+/* Isolated line-solve bench (no counterpart in the reference): nfields <= 5
+ * fields of block 0 of case 0 (host arrays in the reference layout, field k
+ * at in + k*(lxi+1)(let+1)(lze+1)) are copied to the device once; one launch
+ * of the direction's derivative (op 0) or filter (op 1, in place) over all of
+ * them runs after their interface contraction and its result is copied to
+ * out; then `reps` more launches are timed with CUDA events on the context
+ * stream and *ms_per_launch receives their average. In a mixed-precision
+ * context the derivative runs on FP32 copies, the filter on the FP64 fields
+ * with an FP32 elimination, as on the step path. */
+int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, const double* in, double* out,
+                      int32_t reps, double* ms_per_launch);
+
 /* Observability (the reference's mo_timer, src/mo_timer.f90:84-133, as CUDA
  * events per kernel family). With timers on, every launch of the family is
  * bracketed by events; canard_get_timers returns per family the accumulated

@@ -239,3 +239,29 @@ def test_overflow_is_reported():
     with pytest.raises(api.CanardError) as e:
         g.step(1)
     assert e.value.code == api.ERR_NAN
+
+
+@pytest.mark.parametrize("name", ["periodic", "nonperiodic"])
+def test_line_bench_matches_oracle(name):
+    """The isolated line-solve bench (5 fields, one launch per direction)
+    returns the oracle's derivative and filter bit for bit in FP64."""
+    cs = CASES[name]()
+    blk = cs.blocks[0]
+    fields = cases.noise_fields(blk, 5, kmax=4)
+    g = api.Context(cs, setup=False, upload_state=False)
+    for op in (0, 1):
+        o = po.Oracle(cs, setup=False)
+        for nn in (1, 2, 3):
+            out, ms = g.line_bench(op, nn, fields, reps=2)
+            assert ms > 0
+            for k in range(5):
+                f = fields[k].ravel().copy()
+                if op == 0:
+                    o.mpigo([f.copy()], 0, 1, 0, k + 1, k + 1)
+                    r = np.zeros_like(f)
+                    o.deriv(0, f, r, nn, k + 1)
+                else:
+                    o.mpigo([f], 1, 1, 0, k + 1, k + 1)
+                    o.filte(0, f, {2: 1, 3: 2, 1: 3}[nn], k + 1)
+                    r = f
+                np.testing.assert_array_equal(out[k].ravel(), r, err_msg=f"op {op} nn {nn} field {k}")
