@@ -247,9 +247,10 @@ def kernels_mode(args, api, cases, torch):
 
 def accuracy_mode(args, api, cases, torch):
     """FP32-mixed against FP64 on the isentropic vortex through a GCBC outflow:
-    the 384x256x128 case on the GPU after 50, 200 and 1000 steps (relative L2
-    per conserved variable, momenta against ||rho|| * 0.5), and a 96x64x32
-    copy against the oracle after 50 steps (both precisions)."""
+    the 384x256x128 case on the GPU after 50 ... 1000 steps (relative L2 per
+    conserved variable, momenta against ||rho|| * 0.5, and whether each state
+    is still finite), and a 96x64x32 copy against the oracle after 50 steps
+    (both precisions)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     out = {"mode": "accuracy"}
@@ -257,12 +258,14 @@ def accuracy_mode(args, api, cases, torch):
     a = api.Context(big)
     b = api.Context(big, precision=api.FP32_MIXED)
     done, rows = 0, []
-    for n in (50, 200, 1000):
+    for n in (50, 100, 200, 400, 1000):
         a.step(n - done)
         b.step(n - done)
         done = n
-        rows.append({"steps": n, "rel_l2_fp32_vs_fp64": state_errors(b.state(0), a.state(0), 0.5),
-                     "time": a.time()[5]})
+        qa, qb = a.state(0), b.state(0)
+        rows.append({"steps": n, "rel_l2_fp32_vs_fp64": state_errors(qb, qa, 0.5), "time": a.time()[5],
+                     "fp64_finite": bool(np.isfinite(qa).all()), "fp32_finite": bool(np.isfinite(qb).all()),
+                     "fp64_max_abs_q": float(np.nanmax(np.abs(qa)))})
     a.close()
     b.close()
     out["vortex_gpu"] = {"case": big.name, "points": big.npts, "rows": rows}
