@@ -62,6 +62,9 @@ def parse():
                    help="step: the time-step benchmark (default); kernels: isolated derivative and filter "
                         "launches per direction on 5 noise fields, checked against the oracle; accuracy: "
                         "FP32-mixed against FP64 on the vortex case after 50/200/1000 steps")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the line-tile autotuner (by default every timed context is tuned first; the "
+                        "per-case baseline of the batched comparison never is)")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the FP32-mixed and batched comparison lines added to the default run")
     return p.parse_args()
@@ -126,6 +129,8 @@ def fp32_extra(args, api, cases, torch, stream, value64):
     from the initial condition against the FP64 path."""
     cs = cases.tgv(args.n)
     c32 = api.Context(cs, precision=api.FP32_MIXED)
+    if not args.no_autotune:
+        c32.autotune(reps=3)
     c32.set_stream(stream.cuda_stream)
     c32.step(args.warmup)
     ms = time_steps(c32, args.steps, stream, torch)
@@ -157,6 +162,8 @@ def batched_extra(args, api, cases, torch, stream):
     states = {}
     for key, prec in (("fp32_mixed_graph", api.FP32_MIXED), ("fp64_graph", api.FP64)):
         g = api.Context(allc, precision=prec)
+        if not args.no_autotune:
+            g.autotune(reps=3)
         g.set_stream(stream.cuda_stream)
         g.step(args.warmup)
         ms = time_steps(g, args.steps, stream, torch)
@@ -403,6 +410,7 @@ def main():
         workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
     prec = api.FP32_MIXED if args.precision == "fp32" else api.FP64
     ctx = api.Context(case_list, precision=prec)
+    tuning = None if args.no_autotune else ctx.autotune(reps=3)
     if args.precision == "fp32":
         workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
     # a non-default stream: the library launches on it and the CUDA events
@@ -519,6 +527,7 @@ def main():
                 "scaling": scaling, "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
                 "config": {"workload": workload, "cases": len(case_list), "points": job_points, "precision": args.precision,
+                           "autotuned": not args.no_autotune,
                            "l2": "inputs larger than L2 (state, metrics and work fields ~"
                                  f"{(54 * 8 + (41 * 4 if args.precision == 'fp32' else 0)) * npts / 1e9:.1f} GB "
                                  "resident)",
@@ -528,6 +537,8 @@ def main():
                 "clocks": clocks,
                 "families": {k: {"ms_per_step": v["ms"], "share": v["ms"] / tot if tot else 0.0,
                                  "launches": v["launches"]} for k, v in fam.items() if v["launches"]}}
+        if tuning is not None:
+            line["autotune"] = tuning
         line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -91,6 +91,7 @@ def lib():
         L.canard_filte.argtypes = [vp, i32, _DP, i32, i32]
         L.canard_set_timers.argtypes = [vp, i32]
         L.canard_set_graphs.argtypes = [vp, i32]
+        L.canard_autotune.argtypes = [vp, i32, _DP, i32]
         L.canard_line_bench.argtypes = [vp, i32, i32, i32, _DP, _DP, i32, ctypes.POINTER(ctypes.c_double)]
         L.canard_get_timers.argtypes = [vp, _DP, _DP, _DP, i32]
         L.canard_timer_name.restype = ctypes.c_char_p
@@ -207,6 +208,23 @@ class Context:
 
     def set_graphs(self, on):
         self._check(lib().canard_set_graphs(self.h, 1 if on else 0))
+
+    def autotune(self, reps=5):
+        """Times the line-tile candidates of every (group, direction) and
+        installs the fastest; returns one dict per group and direction."""
+        rep = np.zeros(6 * 16)
+        k = lib().canard_autotune(self.h, reps, _dp(rep), 16)
+        if k < 0:
+            self._check(-k)
+        kinds = {0: "fp64", 1: "fp32-split", 2: "fp64-tile/fp32-split", 3: "fp32-one-lane",
+                 4: "fp64-tile/fp32-one-lane"}
+        out = []
+        for i in range(k):
+            g, d, kd, nc, best, dflt = rep[6 * i:6 * i + 6]
+            out.append({"group": ("filter", "viscous", "flux")[int(g)], "dir": "xi eta zeta".split()[int(d)],
+                        "kind": kinds.get(int(kd), str(int(kd))), "chunks": int(nc) or "default",
+                        "ms": best, "default_ms": dflt})
+        return out
 
     def line_bench(self, op, nn, fields, reps=10):
         """One direction's derivative (op 0) or filter (op 1) over up to 5

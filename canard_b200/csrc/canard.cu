@@ -74,10 +74,20 @@ struct Table {
 };
 
 // Element types of a line launch: tile (field) type and elimination type.
-enum LineKind { LK_F64 = 0, LK_F32 = 1, LK_F64_TILE_F32_SOLVE = 2 };
-inline size_t tile_elem(int kind) { return kind == LK_F32 ? sizeof(float) : sizeof(double); }
-// FP32 eliminations use the split solve (16 lines per tile), FP64 the one-lane sweeps (32)
-inline int tile_lanes(int kind) { return kind == LK_F64 ? kLanes : kHalf; }
+// Element types and solve form of a line launch: FP64 one-lane sweeps
+// (bit-exact); FP32 fields; FP64 fields with an FP32 elimination. The FP32
+// eliminations come as the split solve (16 lines per tile) or the one-lane
+// sweeps (32 lines); the autotuner picks per direction.
+enum LineKind {
+  LK_F64 = 0,
+  LK_F32 = 1,                  // split
+  LK_F64_TILE_F32_SOLVE = 2,   // split
+  LK_F32_1L = 3,
+  LK_F64_TILE_F32_SOLVE_1L = 4
+};
+inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L; }
+inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
+inline int tile_lanes(int kind) { return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE) ? kHalf : kLanes; }
 
 // First row of the second half of a split solve: balances the two halves'
 // register-constant rows (the first half's rows below c0 use the tables
@@ -245,6 +255,9 @@ struct canard_ctx {
   bool setup_done = false;
   // hot-path tables
   Table<LineTask> filt[5][3], visc[3], flux[3];
+  // line-tile choice per [group: 0 filter, 1 viscous gradients, 2 fluxes][direction]
+  // (kind < 0: the precision's default); set by canard_autotune
+  struct TuneChoice { int kind = -1; int nc = 0; } tune[3][3];
   Table<FaceTask> mp_filt[5][3], mp_visc, mp_flux;
   Table<GcbcTask> gc_setup, gc_upd[3][2];
   void** fc_src = nullptr;
@@ -332,8 +345,8 @@ float* gptr(const BlockState& b, int f) { return b.arena32 + (size_t)f * b.g.npa
 // chunks), cr even (16-byte aligned bulk copies) and at most 256 (a TMA box),
 // and the first and the last chunk keep at least 13 positions, so the end
 // closures and the in-kernel periodic contraction only need those two.
-void chunking(int L, int& nc, int& cr) {
-  nc = std::max(1, std::min(kMaxChunks, L / 64));
+void chunking(int L, int& nc, int& cr, int nc_req = 0) {
+  nc = std::max(1, std::min(kMaxChunks, nc_req > 0 ? nc_req : L / 64));
   for (;; --nc) {
     cr = ((L + nc - 1) / nc + 1) / 2 * 2;
     if (nc <= 2 || (L - (nc - 1) * cr >= 13 && cr >= 13)) break;
@@ -343,12 +356,12 @@ void chunking(int L, int& nc, int& cr) {
 
 // xi lines (dir 0) move as one bulk copy per line: per-lane copy instructions
 // are costly enough that chunking them does not pay.
-void chunking_dir(int dir, int L, int& nc, int& cr) {
+void chunking_dir(int dir, int L, int& nc, int& cr, int nc_req = 0) {
   if (dir == 0) {
     nc = 1;
     cr = (L + 1) / 2 * 2;
   } else {
-    chunking(L, nc, cr);
+    chunking(L, nc, cr, nc_req);
   }
 }
 
@@ -361,7 +374,8 @@ bool self_periodic(const BlockGeom& g, int dir) {
 }
 
 void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, int nt, const void* in,
-                    void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64, bool allow_selfp = false) {
+                    void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64, bool allow_selfp = false,
+                    int nc_req = 0) {
   const BlockGeom& g = B.g;
   t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
@@ -370,9 +384,10 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
   t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
   t.c0 = B.luc0[nt][dir];
-  t.recv = (kind == LK_F32) ? static_cast<const void*>(B.recv32_ptr(dir, m, 0))
-                            : static_cast<const void*>(B.recv_ptr(nt, dir, m, 0));
-  t.drva = !with_drva ? nullptr : (kind == LK_F32 ? static_cast<void*>(B.drva32[dir]) : static_cast<void*>(B.drva[dir]));
+  t.recv = kind_f32_fields(kind) ? static_cast<const void*>(B.recv32_ptr(dir, m, 0))
+                                 : static_cast<const void*>(B.recv_ptr(nt, dir, m, 0));
+  t.drva = !with_drva ? nullptr
+                      : (kind_f32_fields(kind) ? static_cast<void*>(B.drva32[dir]) : static_cast<void*>(B.drva[dir]));
   t.sc = c->cases[g.case_id].dsch;
   t.X = g.X; t.Y = g.Y; t.Z = g.Z; t.Xp = g.Xp;
   t.L = g.ijk[0][dir] + 1;
@@ -381,15 +396,17 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
   t.h = t.kg = t.ke = 0;
-  if (tile_lanes(kind) == kHalf) {
-    t.h = B.h32[nt][dir];
-    t.kg = B.kg32[nt][dir];
-    t.ke = B.ke32[nt][dir];
+  if (kind != LK_F64) {  // FP32 elimination: rounded factors and their constant range
     t.cl1 = B.luc32[nt][dir][0]; t.cl2 = B.luc32[nt][dir][1]; t.cu1 = B.luc32[nt][dir][2];
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
     t.c0 = B.luc032[nt][dir];
   }
-  chunking_dir(dir, t.L, t.nbox, t.by);
+  if (tile_lanes(kind) == kHalf) {
+    t.h = B.h32[nt][dir];
+    t.kg = B.kg32[nt][dir];
+    t.ke = B.ke32[nt][dir];
+  }
+  chunking_dir(dir, t.L, t.nbox, t.by, nc_req);
   const int lanes = tile_lanes(kind);
   if (dir == 0) {
     t.ntx = 1;
@@ -400,15 +417,13 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   }
 }
 
-size_t line_smem(int dir, int L, int kind = LK_F64) {
+// dynamic shared memory of one task's tile
+size_t line_smem(int dir, const LineTask& t, int kind) {
   const size_t es = tile_elem(kind);
   const int lanes = tile_lanes(kind);
-  if (dir == 0) {
-    return 128 + (size_t)lanes * (kind == LK_F32 ? dir1_pitch<float>(L) : dir1_pitch<double>(L)) * es;
-  }
-  int nc, cr;
-  chunking(L, nc, cr);
-  return 128 + (size_t)nc * cr * lanes * es;
+  if (dir == 0)
+    return 128 + (size_t)lanes * (kind_f32_fields(kind) ? dir1_pitch<float>(t.L) : dir1_pitch<double>(t.L)) * es;
+  return 128 + (size_t)t.nbox * t.by * lanes * es;
 }
 
 // cuTensorMapEncodeTiled from the driver, found at run time (the library does
@@ -457,7 +472,7 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
     t.tile0 = tot;
     first.push_back(tot);
     tot += t.ntiles;
-    sm = std::max(sm, line_smem(dir, t.L, kind));
+    sm = std::max(sm, line_smem(dir, t, kind));
     T.bytes += 2.0 * es * t.X * t.Y * t.Z;  // read the field, write the result
   }
   T.ntasks = (int)v.size();
@@ -525,6 +540,8 @@ void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   if (T.kind == LK_F64) launch_line_dir<DIR, OP, double, double>(c, T);
   else if (OP == 0 && T.kind == LK_F32) launch_line2_dir<DIR, 0, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line2_dir<DIR, 1, double>(c, T);
+  else if (OP == 0 && T.kind == LK_F32_1L) launch_line_dir<DIR, 0, float, float>(c, T);
+  else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE_1L) launch_line_dir<DIR, 1, double, float>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -556,6 +573,12 @@ void set_line_smem_limits() {
   CK((line2_smem_limit<1, 1, double>(lim)));
   CK((line2_smem_limit<2, 1, double>(lim)));
   CK((line2_smem_limit<3, 1, double>(lim)));
+  CK((line_smem_limit<1, 0, float, float>(lim)));
+  CK((line_smem_limit<2, 0, float, float>(lim)));
+  CK((line_smem_limit<3, 0, float, float>(lim)));
+  CK((line_smem_limit<1, 1, double, float>(lim)));
+  CK((line_smem_limit<2, 1, double, float>(lim)));
+  CK((line_smem_limit<3, 1, double, float>(lim)));
   done = true;
 }
 
@@ -928,44 +951,88 @@ void one_step(canard_ctx* c) {
 }
 
 // ---- set-up ------------------------------------------------------------------------
-void build_tables(canard_ctx* c) {
+// The line tasks of one group (0 filter of field m, 1 viscous gradients,
+// 2 fluxes) and direction, for line kind `kind` and chunk count `nc`
+// (0 = default). With `scratch`, filter tasks work on scratch fields instead
+// of the state (autotuning).
+std::vector<LineTask> group_tasks(canard_ctx* c, int grp, int dir, int m, int kind, int nc, bool scratch = false) {
   const int nb = nblk(c);
+  const bool w32 = kind_f32_fields(kind);
+  auto wf = [&](int b, int f64_field, int f32_field) -> void* {
+    return w32 ? static_cast<void*>(gptr(c->blocks[b], f32_field)) : static_cast<void*>(fptr(c->blocks[b], f64_field));
+  };
+  std::vector<LineTask> v;
+  for (int b = 0; b < nb; ++b) {
+    if (grp == 0) {
+      LineTask t;
+      double* f = fptr(c->blocks[b], scratch ? F_SCR + m - 1 : F_QA + m - 1);
+      fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t, kind, false, nc);
+      v.push_back(t);
+    } else if (grp == 1) {
+      // viscous gradients: de(:,m) m = 2..5 -> scr 3*(m-2) + dir
+      if (!c->cases[c->blocks[b].g.case_id].d.viscous) continue;
+      for (int mm = 2; mm <= 5; ++mm) {
+        LineTask t;
+        fill_line_task(c, c->blocks[b], dir, 0, wf(b, F_DE + mm - 1, G_DE + mm - 1),
+                       wf(b, F_SCR + 3 * (mm - 2) + dir, G_SCR + 3 * (mm - 2) + dir), mm, false, t, kind, true, nc);
+        v.push_back(t);
+      }
+    } else {
+      // fluxes: scr 3*(m-1) + dir, in place
+      for (int mm = 1; mm <= 5; ++mm) {
+        LineTask t;
+        void* f = wf(b, F_SCR + 3 * (mm - 1) + dir, G_SCR + 3 * (mm - 1) + dir);
+        fill_line_task(c, c->blocks[b], dir, 0, f, f, mm, true, t, kind, true, nc);
+        v.push_back(t);
+      }
+    }
+  }
+  return v;
+}
+
+int default_kind(const canard_ctx* c, int grp) {
+  if (!c->f32()) return LK_F64;
+  return grp == 0 ? LK_F64_TILE_F32_SOLVE : LK_F32;
+}
+
+int group_kind(const canard_ctx* c, int grp, int dir) {
+  const int k = c->tune[grp][dir].kind;
+  return k >= 0 ? k : default_kind(c, grp);
+}
+
+void free_line_table(Table<LineTask>& T) {
+  cudaFree(T.tasks);
+  cudaFree(T.first);
+  cudaFree(T.maps);
+  T = Table<LineTask>{};
+}
+
+void build_line_tables(canard_ctx* c) {
+  for (int m = 1; m <= 5; ++m)
+    for (int inn = 1; inn <= 3; ++inn) {
+      const int dir = kNnf[inn - 1] - 1, k = group_kind(c, 0, dir);
+      c->filt[m - 1][inn - 1] = make_line_table(c, group_tasks(c, 0, dir, m, k, c->tune[0][dir].nc), dir, false, k);
+    }
+  for (int dir = 0; dir < 3; ++dir) {
+    int k = group_kind(c, 1, dir);
+    c->visc[dir] = make_line_table(c, group_tasks(c, 1, dir, 0, k, c->tune[1][dir].nc), dir, false, k);
+    k = group_kind(c, 2, dir);
+    c->flux[dir] = make_line_table(c, group_tasks(c, 2, dir, 0, k, c->tune[2][dir].nc), dir, false, k);
+  }
+}
+
+void build_tables(canard_ctx* c) {
   const bool f32 = c->f32();
-  // work field f (of the flux type) of block b, as an untyped pointer
   auto wf = [&](int b, int f64_field, int f32_field) -> void* {
     return f32 ? static_cast<void*>(gptr(c->blocks[b], f32_field)) : static_cast<void*>(fptr(c->blocks[b], f64_field));
   };
-  const int dkind = f32 ? LK_F32 : LK_F64;                  // derivatives of work fields
-  const int fkind = f32 ? LK_F64_TILE_F32_SOLVE : LK_F64;   // filter of the FP64 state
-  // filter passes
+  build_line_tables(c);
   for (int m = 1; m <= 5; ++m)
     for (int inn = 1; inn <= 3; ++inn) {
       const int dir = kNnf[inn - 1] - 1;
-      std::vector<LineTask> v;
-      for (int b = 0; b < nb; ++b) {
-        LineTask t;
-        double* f = fptr(c->blocks[b], F_QA + m - 1);
-        fill_line_task(c, c->blocks[b], dir, 1, f, f, m, false, t, fkind);
-        v.push_back(t);
-      }
-      c->filt[m - 1][inn - 1] = make_line_table(c, v, dir, false, fkind);
       c->mp_filt[m - 1][inn - 1] = make_face_table(
           c, face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }), false);
     }
-  // viscous gradients: de(:,m) m = 2..5 -> scr 3*(m-2) + dir
-  for (int dir = 0; dir < 3; ++dir) {
-    std::vector<LineTask> v;
-    for (int b = 0; b < nb; ++b) {
-      if (!c->cases[c->blocks[b].g.case_id].d.viscous) continue;
-      for (int m = 2; m <= 5; ++m) {
-        LineTask t;
-        fill_line_task(c, c->blocks[b], dir, 0, wf(b, F_DE + m - 1, G_DE + m - 1),
-                       wf(b, F_SCR + 3 * (m - 2) + dir, G_SCR + 3 * (m - 2) + dir), m, false, t, dkind, true);
-        v.push_back(t);
-      }
-    }
-    c->visc[dir] = make_line_table(c, v, dir, false, dkind);
-  }
   {
     std::vector<FaceTask> all;
     for (int m = 2; m <= 5; ++m) {
@@ -974,18 +1041,6 @@ void build_tables(canard_ctx* c) {
       all.insert(all.end(), v.begin(), v.end());
     }
     c->mp_visc = make_face_table(c, all, false, f32 ? 1 : 0);
-  }
-  // fluxes: scr 3*(m-1) + dir, in place
-  for (int dir = 0; dir < 3; ++dir) {
-    std::vector<LineTask> v;
-    for (int b = 0; b < nb; ++b)
-      for (int m = 1; m <= 5; ++m) {
-        LineTask t;
-        void* f = wf(b, F_SCR + 3 * (m - 1) + dir, G_SCR + 3 * (m - 1) + dir);
-        fill_line_task(c, c->blocks[b], dir, 0, f, f, m, true, t, dkind, true);
-        v.push_back(t);
-      }
-    c->flux[dir] = make_line_table(c, v, dir, false, dkind);
   }
   {
     std::vector<FaceTask> all;
@@ -1707,14 +1762,14 @@ static void unit_line(canard_ctx* c, int iblock, const double* in, double* out, 
   h2d_field(c, B, f, in, 1);
   const int kind = !c->f32() ? LK_F64 : (nt == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
   void* fd = f;
-  if (kind == LK_F32) {
+  if (kind_f32_fields(kind)) {
     fd = gptr(B, G_SCR + 11);
     to_f32(c, f, gptr(B, G_SCR + 11), (size_t)B.g.npad);
   }
   LineTask t;
   fill_line_task(c, B, dir, nt, fd, fd, m, nt == 0, t, kind);
   launch_line(c, make_line_table(c, {t}, dir, true, kind), dir, nt);
-  if (kind == LK_F32) to_f64(c, gptr(B, G_SCR + 11), f, (size_t)B.g.npad);
+  if (kind_f32_fields(kind)) to_f64(c, gptr(B, G_SCR + 11), f, (size_t)B.g.npad);
   d2h_field(c, B, out, f, 1);
   sync_check(c);
   free_transient(c);
@@ -1742,7 +1797,8 @@ int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, co
       throw ApiError(CANARD_ERR_ARG, "bad line bench argument");
     BlockState& B = c->blocks[block_index(c, 0, 0)];
     const int dir = nn - 1;
-    const int kind = !c->f32() ? LK_F64 : (op == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
+    const canard_ctx::TuneChoice& tc = c->tune[op == 0 ? 2 : 0][dir];
+    const int kind = tc.kind >= 0 ? tc.kind : (!c->f32() ? LK_F64 : (op == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE));
     const size_t L = (size_t)B.g.X * B.g.Y * B.g.Z;
     std::vector<LineTask> tasks;
     for (int k = 0; k < nfields; ++k) {
@@ -1750,16 +1806,16 @@ int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, co
       h2d_field(c, B, f, in + k * L, 1);
       void* src = f;
       void* dst = op == 0 ? static_cast<void*>(fptr(B, F_SCR + 5 + k)) : static_cast<void*>(f);
-      if (kind == LK_F32) {
+      if (kind_f32_fields(kind)) {
         to_f32(c, f, gptr(B, G_SCR + k), (size_t)B.g.npad);
         src = gptr(B, G_SCR + k);
         dst = gptr(B, G_SCR + 5 + k);
       }
       LineTask t;
-      fill_line_task(c, B, dir, op, src, dst, k + 1, false, t, kind, true);
+      fill_line_task(c, B, dir, op, src, dst, k + 1, false, t, kind, true, tc.nc);
       tasks.push_back(t);
       // interface contraction of the faces not formed in the kernel
-      const bool w32 = kind == LK_F32;
+      const bool w32 = kind_f32_fields(kind);
       auto col = [&](int b, int) -> const void* {
         return w32 ? static_cast<const void*>(gptr(c->blocks[b], G_SCR + k))
                    : static_cast<const void*>(fptr(c->blocks[b], F_SCR + k));
@@ -1770,7 +1826,7 @@ int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, co
     launch_line(c, T, dir, op);
     for (int k = 0; k < nfields; ++k) {
       double* r = fptr(B, F_SCR + (op == 0 ? 5 : 0) + k);
-      if (kind == LK_F32) to_f64(c, gptr(B, G_SCR + 5 + k), r, (size_t)B.g.npad);
+      if (kind_f32_fields(kind)) to_f64(c, gptr(B, G_SCR + 5 + k), r, (size_t)B.g.npad);
       d2h_field(c, B, out + k * L, r, 1);
     }
     cudaEvent_t e0, e1;
@@ -1788,6 +1844,69 @@ int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, co
     sync_check(c);
     free_transient(c);
   });
+}
+
+int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
+  int rows = 0;
+  const int rc = guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_autotune before canard_setup");
+    if (reps < 1) throw ApiError(CANARD_ERR_ARG, "reps must be positive");
+    CK(cudaStreamSynchronize(c->st));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time_table = [&](const Table<LineTask>& T, int dir, int op) {
+      launch_line(c, T, dir, op);  // warm-up
+      CK(cudaEventRecord(e0, c->st));
+      for (int r = 0; r < reps; ++r) launch_line(c, T, dir, op);
+      CK(cudaEventRecord(e1, c->st));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return (double)ms / reps;
+    };
+    for (int grp = 0; grp < 3; ++grp)
+      for (int dir = 0; dir < 3; ++dir) {
+        const int op = grp == 0 ? 1 : 0;
+        std::vector<std::pair<int, int>> cand;  // (kind, nc)
+        std::vector<int> kinds{default_kind(c, grp)};
+        if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
+        for (int k : kinds) {
+          cand.push_back({k, 0});
+          if (dir != 0)
+            for (int nc : {2, 4, 8}) cand.push_back({k, nc});
+        }
+        double best = 1e300, def = 0;
+        canard_ctx::TuneChoice pick;
+        for (size_t i = 0; i < cand.size(); ++i) {
+          auto v = group_tasks(c, grp, dir, 1, cand[i].first, cand[i].second, true);
+          if (v.empty()) continue;
+          Table<LineTask> T = make_line_table(c, v, dir, true, cand[i].first);
+          if (T.smem > 227 * 1024) continue;
+          const double ms = time_table(T, dir, op);
+          if (i == 0) def = ms;
+          if (ms < best) { best = ms; pick.kind = cand[i].first; pick.nc = cand[i].second; }
+          free_transient(c);
+        }
+        if (best < 1e300) c->tune[grp][dir] = pick;
+        if (report && rows < nmax) {
+          double* r = report + 6 * rows;
+          r[0] = grp; r[1] = dir; r[2] = pick.kind; r[3] = pick.nc; r[4] = best < 1e300 ? best : 0; r[5] = def;
+        }
+        ++rows;
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // rebuild the step tables with the choices; the step graphs used the old ones
+    for (int m = 0; m < 5; ++m)
+      for (int i = 0; i < 3; ++i) free_line_table(c->filt[m][i]);
+    for (int d = 0; d < 3; ++d) { free_line_table(c->visc[d]); free_line_table(c->flux[d]); }
+    for (auto& g : c->graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    build_line_tables(c);
+    CK(cudaStreamSynchronize(c->st));
+  });
+  return rc == CANARD_OK ? rows : -rc;
 }
 
 int canard_set_timers(canard_ctx* c, int32_t on) {
@@ -2007,7 +2126,7 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
                              reinterpret_cast<const int*>(base + kNaIdx) + 1, nf, tot);
       CK(cudaGetLastError());
     }
-    const size_t smem = line_smem(dir, L);
+    const size_t smem = line_smem(dir, t, LK_F64);
     const LineTask* dt = reinterpret_cast<const LineTask*>(base + kNaTask);
     const int* d0 = reinterpret_cast<const int*>(base + kNaIdx);
     const CUtensorMap* dm = reinterpret_cast<const CUtensorMap*>(base + kNaMaps);

@@ -44,5 +44,17 @@ CANARD_F32_LINE(1, 1, double)
 CANARD_F32_LINE(2, 1, double)
 CANARD_F32_LINE(3, 1, double)
 #undef CANARD_F32_LINE
+// one-lane sweeps with an FP32 elimination (the autotuner's alternative)
+#define CANARD_F32_LINE1(DIR, OP, TT)                                                                         \
+  CANARD_F32_EXTERN template void launch_line_t<DIR, OP, TT, float>(int, size_t, cudaStream_t, const LineTask*, \
+                                                                    const int*, int, const CUtensorMap*, int*); \
+  CANARD_F32_EXTERN template cudaError_t line_smem_limit<DIR, OP, TT, float>(int);
+CANARD_F32_LINE1(1, 0, float)
+CANARD_F32_LINE1(2, 0, float)
+CANARD_F32_LINE1(3, 0, float)
+CANARD_F32_LINE1(1, 1, double)
+CANARD_F32_LINE1(2, 1, double)
+CANARD_F32_LINE1(3, 1, double)
+#undef CANARD_F32_LINE1
 
 }  // namespace canard

@@ -174,6 +174,19 @@ int canard_version(void);
 int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, const double* in, double* out,
                       int32_t reps, double* ms_per_launch);
 
+/* Line-tile autotuner (no counterpart in the reference). For each group of
+ * line solves (0: the filter passes, 1: the viscous gradients, 2: the flux
+ * derivatives) and direction, times the candidate tile shapes on the
+ * context's own blocks (filter candidates on scratch copies, the state is not
+ * touched): FP64 contexts try TMA staging depths (2, 4, 8 chunks per eta or
+ * zeta line); mixed-precision contexts also try the one-lane FP32 sweeps (32
+ * lines per tile) against the split solve (16 lines per tile). The fastest
+ * choice is installed in the step tables. Returns the number of groups
+ * (9) and fills up to nmax report rows of 6 doubles: group, direction
+ * (0..2), chosen kind, chosen chunk count (0 = default), its ms per launch
+ * and the default's. Call after canard_setup. */
+int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax);
+
 /* Observability (the reference's mo_timer, src/mo_timer.f90:84-133, as CUDA
  * events per kernel family). With timers on, every launch of the family is
  * bracketed by events; canard_get_timers returns per family the accumulated

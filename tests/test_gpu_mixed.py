@@ -146,3 +146,16 @@ def test_fp32_work_fields_are_readable():
         de_o = o.get(b, po.A_DE)
         assert rel_l2(de_g, de_o) <= 1e-3
         assert np.isfinite(g.field(api.F_DRVA[0], b)).all()
+
+
+def test_autotuned_fp32_within_1e_5():
+    cs = CASES["multiblock"]()
+    g = api.Context(cs, precision=api.FP32_MIXED)
+    rep = g.autotune(reps=2)
+    assert len(rep) == 9
+    o = po.Oracle(cs)
+    g.step(12)
+    o.step(12)
+    for b in range(len(cs.blocks)):
+        errs = state_errors(g.state(b), o.state(b), UREF["multiblock"])
+        assert max(errs) <= TOL_STEPS, (b, errs, rep)

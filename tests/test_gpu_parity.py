@@ -265,3 +265,17 @@ def test_line_bench_matches_oracle(name):
                     o.filte(0, f, {2: 1, 3: 2, 1: 3}[nn], k + 1)
                     r = f
                 np.testing.assert_array_equal(out[k].ravel(), r, err_msg=f"op {op} nn {nn} field {k}")
+
+
+def test_autotune_keeps_results():
+    """The line-tile autotuner changes only tile shapes and staging depths on
+    the FP64 path: a tuned context steps bit-identically to an untuned one."""
+    cs = case_multiblock()
+    a = api.Context(cs)
+    rep = a.autotune(reps=2)
+    assert len(rep) == 9 and all(r["ms"] > 0 for r in rep)
+    b = api.Context(cs)
+    a.step(12)
+    b.step(12)
+    for blk in range(len(cs.blocks)):
+        np.testing.assert_array_equal(a.state(blk), b.state(blk))
