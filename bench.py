@@ -462,11 +462,15 @@ def main():
     lms = sum(v["ms"] for v in line_fams.values())
     peak, peak_kind = peaks()
     achieved = dom["bytes"] / dom["launches"] / (dom["ms"] / dom["launches"] / 1e3) / 1e9
+    # DRAM bytes per launch from the ncu capture of a smaller case, scaled by the
+    # algorithmic bytes of this launch (the capture covers the FP64 kernels)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.precision == "fp64":
         try:
-            traffic = json.load(open(tpath)).get(dom_name)
+            r = json.load(open(tpath)).get(dom_name)
+            if r:
+                traffic = r["dram_bytes_per_algorithmic_byte"] * dom["bytes"] / dom["launches"]
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": f"k_line ({dom_name})", "achieved": achieved, "peak": peak,
