@@ -668,7 +668,8 @@ void sync_check(canard_ctx* c) {
   CK(cudaMemcpy(&e, c->derr, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
     CK(cudaMemset(c->derr, 0, sizeof(int)));
-    if (e == kErrOverflow) throw ApiError(CANARD_ERR_NAN, "Canard: Overflow. (dt == 0 after step 2)");
+    if (e == kErrOverflow)
+      throw ApiError(CANARD_ERR_NAN, "Canard: Overflow. (dt == 0 after step 2, or a non-finite state)");
     throw ApiError(CANARD_ERR_TIMEOUT, "a bounded device wait gave up (error flag set by a kernel)");
   }
 }
@@ -869,8 +870,8 @@ void timestep(canard_ctx* c) {
     stage_params(c, 1, 1, 4);  // stage-1 moving frame (dtko = dtk = 0)
     CK(cudaMemsetAsync(c->ddt, 0, 2 * c->cases.size() * sizeof(unsigned long long), c->st));
     Timed tm(c, T_TIMESTEP, ew_bytes(c, 10, 7));
-    if (c->f32()) launch_dtmax<float>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
-    else launch_dtmax<double>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt);
+    if (c->f32()) launch_dtmax<float>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt, c->derr);
+    else launch_dtmax<double>(ew_grid(c), c->st, c->dbd, dev_slot(c, 4), c->dcc, c->ddt, c->derr);
     CK(cudaGetLastError());
   }
   c->launches += 1;

@@ -1396,14 +1396,17 @@ __global__ void k_prim(const BlockDev* __restrict__ bd, const CaseConst* __restr
 
 // time-step maxima (src/mo_physics.f90:185-207) in FP64 from the FP64 metrics;
 // values are >= 0, so their bit patterns order like the values and atomicMax
-// on them is exact.
+// on them is exact. fmax drops NaN, so a non-finite state is flagged apart
+// (err = kErrOverflow): the reference's overflow stop only sees dt == 0.
 template <class R>
 __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
-                        const CaseConst* __restrict__ cc, unsigned long long* __restrict__ out) {
+                        const CaseConst* __restrict__ cc, unsigned long long* __restrict__ out,
+                        int* __restrict__ err) {
   const BlockDev& B0 = bd[blockIdx.y];
   const StageParams S = sp[B0.case_id];
   const int visc = cc[B0.case_id].viscous;
   double m1 = 0.0, m2 = 0.0;
+  bool bad = false;
   FOR_POINTS(B0) {
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
@@ -1424,9 +1427,12 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
                 fabs((et[l] * u + et[l + n] * v) + et[l + 2 * n] * w);
     r2 = r2 + fabs((ze[l] * u + ze[l + n] * v) + ze[l + 2 * n] * w);
     const double ssi = fabs(B.yaco[l]);
-    m1 = fmax(m1, (sqrt(double(de[l + 4 * n]) * r1) + r2) * ssi);
+    const double v1 = (sqrt(double(de[l + 4 * n]) * r1) + r2) * ssi;
+    bad = bad || !isfinite(v1);
+    m1 = fmax(m1, v1);
     if (visc) m2 = fmax(m2, (((double(de[l]) * double(W.mu[l])) * r1) * ssi) * ssi);
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(err, kErrOverflow);
   for (int o = 16; o > 0; o >>= 1) {
     m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
     m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
@@ -1801,8 +1807,8 @@ void launch_prim(dim3 g, cudaStream_t st, const BlockDev* bd, const CaseConst* c
 }
 template <class R>
 void launch_dtmax(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc,
-                  unsigned long long* out) {
-  k_dtmax<R><<<g, 256, 0, st>>>(bd, sp, cc, out);
+                  unsigned long long* out, int* err) {
+  k_dtmax<R><<<g, 256, 0, st>>>(bd, sp, cc, out, err);
 }
 template <class R>
 void launch_copy_mu(dim3 g, cudaStream_t st, const BlockDev* bd) {

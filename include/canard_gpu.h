@@ -38,7 +38,7 @@ extern "C" {
 #define CANARD_OK 0
 #define CANARD_ERR_ARG 1         /* bad argument (index, size, NULL) */
 #define CANARD_ERR_CUDA 2        /* CUDA runtime failure */
-#define CANARD_ERR_NAN 3         /* dt == 0 after step 2: the reference's "Canard: Overflow." */
+#define CANARD_ERR_NAN 3         /* dt == 0 after step 2 (the reference's "Canard: Overflow."), or a non-finite state */
 #define CANARD_ERR_TIMEOUT 4     /* a bounded device wait gave up */
 #define CANARD_ERR_UNSUPPORTED 5 /* configuration the path does not handle */
 #define CANARD_ERR_STATE 6       /* call order (e.g. step before setup) */

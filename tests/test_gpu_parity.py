@@ -279,3 +279,16 @@ def test_autotune_keeps_results():
     b.step(12)
     for blk in range(len(cs.blocks)):
         np.testing.assert_array_equal(a.state(blk), b.state(blk))
+
+
+def test_non_finite_state_is_reported():
+    """A NaN in the state (set from the host) is caught at the next dt
+    reduction (every tenth step) and reported as the overflow error."""
+    cs = case_periodic()
+    g = api.Context(cs)
+    q = g.state(0)
+    q[0, 3, 4, 5] = np.nan
+    g.set_state(0, q)
+    with pytest.raises(api.CanardError) as e:
+        g.step(2)  # the step with n % 10 == 1 reduces dt
+    assert e.value.code == api.ERR_NAN
