@@ -58,10 +58,13 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--mode", default="step", choices=["step", "kernels", "accuracy"],
+    p.add_argument("--mode", default="step", choices=["step", "kernels", "accuracy", "cpu"],
                    help="step: the time-step benchmark (default); kernels: isolated derivative and filter "
                         "launches per direction on 5 noise fields, checked against the oracle; accuracy: "
-                        "FP32-mixed against FP64 on the vortex case after 50/200/1000 steps")
+                        "FP32-mixed against FP64 on the vortex case after 50/200/1000 steps; cpu: the oracle "
+                        "(CPU restatement of the reference) on --config, --cpu-steps steps after one warm-up "
+                        "step, with --cpu-threads threads")
+    p.add_argument("--cpu-threads", type=int, default=0, help="oracle threads (0: all host threads)")
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the line-tile autotuner (by default every timed context is tuned first; the "
                         "per-case baseline of the batched comparison never is)")
@@ -201,6 +204,38 @@ def batched_extra(args, api, cases, torch, stream):
     return out
 
 
+def config_cases(args, cases):
+    if args.config == "tgv":
+        return [cases.tgv(args.n)], f"tgv{args.n}"
+    if args.config == "batched":
+        return cases.batched(64, seed=11), "batched64"
+    if args.config == "curv4":
+        return [cases.curvilinear_4block()], "curv4"
+    return [cases.vortex()], "vortex"
+
+
+def cpu_mode(args):
+    """The oracle on a whole config: Mpoint-steps/s over --cpu-steps steps
+    (after one untimed step); batched cases run one after the other."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from canard_b200 import cases
+    threads = args.cpu_threads or (os.cpu_count() or 1)
+    case_list, name = config_cases(args, cases)
+    npts, secs = 0, 0.0
+    for cs in case_list:
+        o = po.Oracle(cs, threads=threads)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(args.cpu_steps)
+        secs += time.perf_counter() - t0
+        npts += cs.npts
+        del o
+    v = npts * args.cpu_steps / secs / 1e6
+    return {"mode": "cpu", "config": name, "points": npts, "steps": args.cpu_steps, "threads": threads,
+            "seconds": secs, "value": v, "unit": "Mpoint-steps/s", "kind": "port (C++ restatement of the reference)"}
+
+
 def kernels_mode(args, api, cases, torch):
     """Isolated line solves (the reference's deriv / filte over one direction):
     5 FP64 fields of seeded N(0,1) noise plus sin modes k = 1..32 on the TGV
@@ -265,14 +300,28 @@ def accuracy_mode(args, api, cases, torch):
     a = api.Context(big)
     b = api.Context(big, precision=api.FP32_MIXED)
     done, rows = 0, []
+    stopped = {}
+
+    def advance(ctx, key, k):
+        # the dt reduction raises the overflow error once a state is non-finite
+        if key in stopped:
+            return
+        try:
+            ctx.step(k)
+        except api.CanardError as e:
+            stopped[key] = f"stopped between steps {done} and {done + k}: {e}"
+
     for n in (50, 100, 200, 400, 1000):
-        a.step(n - done)
-        b.step(n - done)
-        done = n
+        advance(a, "fp64", n - done)
+        advance(b, "fp32", n - done)
         qa, qb = a.state(0), b.state(0)
-        rows.append({"steps": n, "rel_l2_fp32_vs_fp64": state_errors(qb, qa, 0.5), "time": a.time()[5],
-                     "fp64_finite": bool(np.isfinite(qa).all()), "fp32_finite": bool(np.isfinite(qb).all()),
-                     "fp64_max_abs_q": float(np.nanmax(np.abs(qa)))})
+        done = n
+        row = {"steps": n, "time": a.time()[5], "fp64_finite": "fp64" not in stopped and bool(np.isfinite(qa).all()),
+               "fp32_finite": "fp32" not in stopped and bool(np.isfinite(qb).all())}
+        if row["fp64_finite"] and row["fp32_finite"]:
+            row["rel_l2_fp32_vs_fp64"] = state_errors(qb, qa, 0.5)
+        rows.append(row)
+    out["stopped"] = stopped
     a.close()
     b.close()
     out["vortex_gpu"] = {"case": big.name, "points": big.npts, "rows": rows}
@@ -342,6 +391,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.mode == "cpu":
+        if rank == 0:
+            print(json.dumps(cpu_mode(args)), flush=True)
+        return 0
 
     if args.impl == "reference":
         if rank != 0:

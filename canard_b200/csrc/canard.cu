@@ -251,6 +251,8 @@ struct canard_ctx {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   long long graph_launches[2] = {0, 0};
   bool use_graphs = true;
+  double* stage = nullptr;  // contiguous staging of host copies (reference layout)
+  size_t stage_n = 0;
   int* derr = nullptr;
   bool setup_done = false;
   // hot-path tables
@@ -1252,15 +1254,37 @@ void grid_metrics(canard_ctx* c) {
 
 // copy between a host array in the reference layout (ncols x X*Y*Z) and a
 // padded device field
+// Copies between a host array in the reference layout (ncols x X*Y*Z) and a
+// padded device field: one contiguous copy into the context's staging buffer
+// and a repacking kernel (a strided 2-D copy of rows of a few KB reaches
+// about half the link bandwidth).
 void h2d_field(canard_ctx* c, const BlockState& B, double* dst, const double* src, int ncols) {
   const BlockGeom& g = B.g;
-  CK(cudaMemcpy2DAsync(dst, g.Xp * sizeof(double), src, g.X * sizeof(double), g.X * sizeof(double),
-                       (size_t)g.Y * g.Z * ncols, cudaMemcpyHostToDevice, c->st));
+  const size_t n = (size_t)ncols * g.X * g.Y * g.Z;
+  if (n > c->stage_n) {
+    CK(cudaMemcpy2DAsync(dst, g.Xp * sizeof(double), src, g.X * sizeof(double), g.X * sizeof(double),
+                         (size_t)g.Y * g.Z * ncols, cudaMemcpyHostToDevice, c->st));
+    return;
+  }
+  CK(cudaMemcpyAsync(c->stage, src, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  const long long rows = (long long)g.Y * g.Z * ncols;
+  k_rows_repack<<<(unsigned)std::min<long long>((rows * g.X + 255) / 256, 148 * 16), 256, 0, c->st>>>(
+      c->stage, g.X, dst, g.Xp, g.X, rows);
+  CK(cudaGetLastError());
 }
 void d2h_field(canard_ctx* c, const BlockState& B, double* dst, const double* src, int ncols) {
   const BlockGeom& g = B.g;
-  CK(cudaMemcpy2DAsync(dst, g.X * sizeof(double), src, g.Xp * sizeof(double), g.X * sizeof(double),
-                       (size_t)g.Y * g.Z * ncols, cudaMemcpyDeviceToHost, c->st));
+  const size_t n = (size_t)ncols * g.X * g.Y * g.Z;
+  if (n > c->stage_n) {
+    CK(cudaMemcpy2DAsync(dst, g.X * sizeof(double), src, g.Xp * sizeof(double), g.X * sizeof(double),
+                         (size_t)g.Y * g.Z * ncols, cudaMemcpyDeviceToHost, c->st));
+    return;
+  }
+  const long long rows = (long long)g.Y * g.Z * ncols;
+  k_rows_repack<<<(unsigned)std::min<long long>((rows * g.X + 255) / 256, 148 * 16), 256, 0, c->st>>>(
+      src, g.Xp, c->stage, g.X, g.X, rows);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dst, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
 }
 
 int block_index(const canard_ctx* c, int icase, int iblock) {
@@ -1302,7 +1326,7 @@ void destroy(canard_ctx* c) {
   }
   for (auto& cs : c->cases) cudaFree(cs.dsch);
   cudaFree(c->dbd); cudaFree(c->dcc); cudaFree(c->dsp); cudaFree(c->ddt); cudaFree(c->derr);
-  cudaFree(c->dtime); cudaFree(c->dsn2);
+  cudaFree(c->dtime); cudaFree(c->dsn2); cudaFree(c->stage);
   for (auto g : c->graph) if (g) cudaGraphExecDestroy(g);
   for (auto& p : c->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
@@ -1479,6 +1503,9 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
   }
   c->ddt = dalloc<unsigned long long>(2 * c->cases.size(), c->st);
   c->derr = dalloc<int>(1, c->st);
+  // staging buffer of the host copies: the largest block's 5 state fields
+  for (auto& B : c->blocks) c->stage_n = std::max(c->stage_n, (size_t)5 * B.g.X * B.g.Y * B.g.Z);
+  c->stage = dalloc<double>(c->stage_n, c->st);
   set_line_smem_limits();
   build_tables(c);
   CK(cudaStreamSynchronize(c->st));

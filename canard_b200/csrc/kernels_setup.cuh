@@ -128,6 +128,17 @@ __global__ void k_metrics_to_f32(const BlockDev* __restrict__ bd) {
   }
 }
 
+// rows of `width` elements between two pitches (host-copy staging <-> padded fields)
+__global__ void k_rows_repack(const double* __restrict__ src, int spitch, double* __restrict__ dst, int dpitch,
+                              int width, long long rows) {
+  const long long n = rows * width;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / width;
+    const int x = (int)(e - r * width);
+    dst[r * dpitch + x] = src[r * spitch + x];
+  }
+}
+
 // conversions between an FP64 and an FP32 field of n elements (unit calls)
 __global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
