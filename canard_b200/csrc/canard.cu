@@ -256,6 +256,10 @@ struct canard_ctx {
   int* derr = nullptr;
   bool setup_done = false;
   // hot-path tables
+  // filt[m][inn]: the filter of conserved field m along direction kNnf[inn].
+  // Field-major as in the reference: every interface contraction advances the
+  // persistent send chains of all three directions, so field m+1's filter
+  // depends on field m's face values between its sweeps.
   Table<LineTask> filt[5][3], visc[3], flux[3];
   // line-tile choice per [group: 0 filter, 1 viscous gradients, 2 fluxes][direction]
   // (kind < 0: the precision's default); set by canard_autotune
@@ -268,6 +272,14 @@ struct canard_ctx {
   int fc_n = 0, fc_max = 0;
   Table<SpongeTask> sponge;
   AvgDev avg_pt, avg_ln, avg_sf;
+  // union of the three plans' target points: the primitives are recomputed
+  // there after averaging when the RK update already formed them
+  int prim_n = 0;
+  int* prim_tb = nullptr;
+  long long* prim_tl = nullptr;
+  // step-path fusions: flux sum inside the RK update (no GCBC, no sponge in
+  // the context), next stage's primitives inside the RK update
+  bool fuse_sum = false, fuse_prim = true;
   // timers (mo_timer equivalent) and launch counter
   bool timers = false;
   long long launches = 0;
@@ -695,6 +707,8 @@ void stage_params(canard_ctx* c, int nk0, int nk1, int to_slot = -1) {
 }
 
 // ---- phases --------------------------------------------------------------------
+// filtering (src/mo_canard_driver.f90:232-251): for each field, the
+// interface contraction and the filter sweep along each direction in turn
 void ph_filter(canard_ctx* c) {
   for (int m = 1; m <= 5; ++m)
     for (int inn = 1; inn <= 3; ++inn) {
@@ -736,12 +750,14 @@ void viscous_gradients(canard_ctx* c) {
   launch_line(c, c->visc[0], 0, 0);
 }
 
-// flux interface contraction, the 15 derivative sweeps and their sum into de
-void flux_derivatives(canard_ctx* c) {
+// flux interface contraction, the 15 derivative sweeps and (unless the RK
+// update forms it) their sum into de
+void flux_derivatives(canard_ctx* c, bool sum = true) {
   launch_mpigo(c, c->mp_flux);
   launch_line(c, c->flux[0], 0, 0);
   launch_line(c, c->flux[1], 1, 0);
   launch_line(c, c->flux[2], 2, 0);
+  if (!sum) return;
   Timed tm(c, T_FLUXSUM, ew_bytes(c, 0, 20));
   if (c->f32()) launch_flux_sum<float>(ew_grid(c), c->st, c->dbd);
   else launch_flux_sum<double>(ew_grid(c), c->st, c->dbd);
@@ -781,14 +797,16 @@ void ph_visc_fluxes(canard_ctx* c, const StageParams* sp) {
   const bool visc = any_viscous(c);
   if (visc) viscous_gradients(c);
   {
-    // reads: qa 5 (FP64); p, u, v, w, metrics 9, and if viscous 12 gradients, ss, yaco;
+    // reads: qa 5 (FP64; FP32 forms the state from 1/rho, u, v, w, p instead);
+    // p, u, v, w, metrics 9, and if viscous 12 gradients, ss, yaco;
     // writes: 15 flux components, de(:,5)
-    Timed tm(c, T_FLUXCOMP, ew_bytes(c, 5, 1 + 3 + 9 + (visc ? 12 + 1 + 1 : 0) + 15 + 1));
+    const int rd = 1 + 3 + 9 + (visc ? 12 + 1 + 1 : 0) + 15 + 1;
+    Timed tm(c, T_FLUXCOMP, c->f32() ? ew_bytes(c, 0, rd + 1) : ew_bytes(c, 5, rd));
     if (c->f32()) launch_flux_visc<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
     else launch_flux_visc<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc);
     CK(cudaGetLastError());
   }
-  flux_derivatives(c);
+  flux_derivatives(c, !c->fuse_sum);
 }
 
 void ph_gcbc(canard_ctx* c, const StageParams* sp) {
@@ -838,6 +856,27 @@ void ph_rk(canard_ctx* c, const StageParams* sp) {
   Timed tm(c, T_RK, ew_bytes(c, 11, 5));
   if (c->f32()) launch_rk<float>(ew_grid(c), c->st, c->dbd, sp);
   else launch_rk<double>(ew_grid(c), c->st, c->dbd, sp);
+  CK(cudaGetLastError());
+}
+
+// the step path's RK update: flux sum and next primitives fused as the
+// context allows (k_rk_next)
+void ph_rk_next(canard_ctx* c, const StageParams* sp, bool prim) {
+  // the last stage stores the summed right-hand side (readable after a step)
+  const int sum = c->fuse_sum ? (prim ? 1 : 2) : 0;
+  Timed tm(c, T_RK, ew_bytes(c, 11, (sum ? 15 : 5) + (sum == 2 ? 5 : 0) + (prim ? 7 : 0)));
+  if (c->f32()) launch_rk_next<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim);
+  else launch_rk_next<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim);
+  CK(cudaGetLastError());
+}
+
+// primitives at the averaged points (after ph_rk_next formed them everywhere)
+void ph_prim_points(canard_ctx* c) {
+  if (c->prim_n == 0) return;
+  Timed tm(c, T_PRIM, (8.0 * 5 + (c->f32() ? 4.0 : 8.0) * 7) * c->prim_n);
+  const int grid = std::max(1, std::min((c->prim_n + 255) / 256, 1184));
+  if (c->f32()) launch_prim_points<float>(grid, c->st, c->dbd, c->dcc, c->prim_tb, c->prim_tl, c->prim_n);
+  else launch_prim_points<double>(grid, c->st, c->dbd, c->dcc, c->prim_tb, c->prim_tl, c->prim_n);
   CK(cudaGetLastError());
 }
 
@@ -899,12 +938,14 @@ void step_body(canard_ctx* c) {
   stage_params(c, 1, 4);
   for (int nk = 1; nk <= 4; ++nk) {
     const StageParams* sp = dev_slot(c, nk - 1);
-    if (nk > 1) ph_prim(c);
+    if (nk > 1 && !c->fuse_prim) ph_prim(c);
     ph_visc_fluxes(c, sp);
     ph_gcbc(c, sp);
     ph_sponge(c);
-    ph_rk(c, sp);
+    const bool prim = c->fuse_prim && nk < 4;
+    ph_rk_next(c, sp, prim);
     ph_average(c);
+    if (prim) ph_prim_points(c);
   }
   time_advance(c);
 }
@@ -1183,6 +1224,20 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
   upload_avg(P, c->avg_pt);
   upload_avg(Lp, c->avg_ln);
   upload_avg(Sf, c->avg_sf);
+  std::vector<std::pair<int, long long>> pts;
+  for (const AvgPlan* p : {&P, &Lp, &Sf})
+    for (const auto& t : p->targets) pts.emplace_back(t.b, (long long)t.l);
+  std::sort(pts.begin(), pts.end());
+  pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
+  c->prim_n = (int)pts.size();
+  if (c->prim_n) {
+    std::vector<int> pb;
+    std::vector<long long> pl;
+    for (const auto& q : pts) { pb.push_back(q.first); pl.push_back(q.second); }
+    c->prim_tb = dupload(pb, c->st);
+    c->prim_tl = dupload(pl, c->st);
+  }
+  c->fuse_sum = c->gc_setup.ntasks == 0 && c->sponge.total == 0;
 }
 
 // t_grid%grid_metrics on the device (src/mo_grid.f90:52-189)
@@ -1339,6 +1394,7 @@ void destroy(canard_ctx* c) {
   ft(c->mp_visc); ft(c->mp_flux); ft(c->gc_setup); ft(c->sponge);
   for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) ft(c->gc_upd[d][s]);
   cudaFree(c->fc_src); cudaFree(c->fc_dst); cudaFree(c->fc_cnt);
+  cudaFree(c->prim_tb); cudaFree(c->prim_tl);
   for (AvgDev* A : {&c->avg_pt, &c->avg_ln, &c->avg_sf}) {
     cudaFree(A->tb); cudaFree(A->tl); cudaFree(A->tfirst); cudaFree(A->tcount); cudaFree(A->sb); cudaFree(A->sl);
     cudaFree(A->snap);

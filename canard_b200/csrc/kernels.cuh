@@ -288,83 +288,202 @@ struct CoefTable {
 // Right-hand sides are formed in the tile type TT, the elimination runs in the
 // solve type RS.
 
-// forward rows i..i+7 of the derivative; window w0..w3 = s[i-2..i+1]
-template <int ST, class TT, class RS, class CF>
-__device__ __forceinline__ void fwd8_deriv(TT* __restrict__ s, int i, const CF& cf, TT& w0, TT& w1, TT& w2, TT& w3,
-                                           RS& am2, RS& am1) {
-  TT win[12], r[8];
-  RS l1[8], l2[8], a[8];
+// Factors of one block of eight rows, loaded ahead of the block that uses
+// them (forward: l1, l2 of rows i..i+7; backward: u1, u2, u3 of rows i..i-7),
+// and the filter's originals of a backward block.
+template <class RS>
+struct F8 {
+  RS l1[8], l2[8];
+  template <class CF>
+  __device__ __forceinline__ void load(const CF& cf, int i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { l1[k] = cf.L1(i + k); l2[k] = cf.L2(i + k); }
+  }
+};
+template <class RS>
+struct B8 {
+  RS u1[8], u2[8], u3[8];
+  template <class CF>
+  __device__ __forceinline__ void load(const CF& cf, int i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { u1[k] = cf.U1(i - k); u2[k] = cf.U2(i - k); u3[k] = cf.U3(i - k); }
+  }
+};
+template <class TT>
+struct O8 {
+  TT o[8];
+  __device__ __forceinline__ void load(const TT* __restrict__ og, int ogs, int i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = __ldg(og + (long long)(i - k) * ogs);
+  }
+};
+
+// Right-hand sides of the derivative's rows i..i+7 (reads rows up to i+9);
+// window w0..w3 = s[i-2..i+1] on entry, s[i+6..i+9] on return
+template <int ST, class TT>
+__device__ __forceinline__ void rhs8_deriv(const TT* __restrict__ s, int i, TT& w0, TT& w1, TT& w2, TT& w3,
+                                           TT (&r)[8]) {
+  TT win[12];
   win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    win[4 + k] = s[(i + 2 + k) * ST];
-    l1[k] = cf.L1(i + k);
-    l2[k] = cf.L2(i + k);
-  }
+  for (int k = 0; k < 8; ++k) win[4 + k] = s[(i + 2 + k) * ST];
 #pragma unroll
   for (int k = 0; k < 8; ++k) r[k] = TT(CA_AA) * (win[k + 3] - win[k + 1]) + TT(CA_AB) * (win[k + 4] - win[k]);
-  a[0] = (RS(r[0]) - l1[0] * am2) - l2[0] * am1;
-  a[1] = (RS(r[1]) - l1[1] * am1) - l2[1] * a[0];
+  w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11];
+}
+
+// forward elimination of rows i..i+7 from their right-hand sides
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void chain8_fwd(TT* __restrict__ s, int i, const F8<RS>& f, const TT (&r)[8], RS& am2,
+                                           RS& am1) {
+  RS a[8];
+  a[0] = (RS(r[0]) - f.l1[0] * am2) - f.l2[0] * am1;
+  a[1] = (RS(r[1]) - f.l1[1] * am1) - f.l2[1] * a[0];
 #pragma unroll
-  for (int k = 2; k < 8; ++k) a[k] = (RS(r[k]) - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
+  for (int k = 2; k < 8; ++k) a[k] = (RS(r[k]) - f.l1[k] * a[k - 2]) - f.l2[k] * a[k - 1];
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[(i + k) * ST] = TT(a[k]);
-  w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11];
   am2 = a[6]; am1 = a[7];
 }
 
-// forward rows i..i+7 of the filter; window w0..w5 = s[i-3..i+2]
+// forward rows i..i+7 of the derivative; window w0..w3 = s[i-2..i+1]
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void fwd8_deriv_c(TT* __restrict__ s, int i, const F8<RS>& f, TT& w0, TT& w1, TT& w2,
+                                             TT& w3, RS& am2, RS& am1) {
+  TT r[8];
+  rhs8_deriv<ST, TT>(s, i, w0, w1, w2, w3, r);
+  chain8_fwd<ST, TT, RS>(s, i, f, r, am2, am1);
+}
 template <int ST, class TT, class RS, class CF>
-__device__ __forceinline__ void fwd8_filter(TT* __restrict__ s, int i, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
-                                            TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
-  TT win[14], r[8];
-  RS l1[8], l2[8], a[8];
+__device__ __forceinline__ void fwd8_deriv(TT* __restrict__ s, int i, const CF& cf, TT& w0, TT& w1, TT& w2, TT& w3,
+                                           RS& am2, RS& am1) {
+  F8<RS> f;
+  f.load(cf, i);
+  fwd8_deriv_c<ST, TT, RS>(s, i, f, w0, w1, w2, w3, am2, am1);
+}
+
+// Right-hand sides of the filter's rows i..i+7 (reads rows up to i+10);
+// window w0..w5 = s[i-3..i+2] on entry, s[i+5..i+10] on return
+template <int ST, class TT>
+__device__ __forceinline__ void rhs8_filter(const TT* __restrict__ s, int i, TT fa, TT fb, TT fc, TT& w0, TT& w1,
+                                            TT& w2, TT& w3, TT& w4, TT& w5, TT (&r)[8]) {
+  TT win[14];
   win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3; win[4] = w4; win[5] = w5;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    win[6 + k] = s[(i + 3 + k) * ST];
-    l1[k] = cf.L1(i + k);
-    l2[k] = cf.L2(i + k);
-  }
+  for (int k = 0; k < 8; ++k) win[6 + k] = s[(i + 3 + k) * ST];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const TT rk = win[k + 3] + win[k + 3];
     r[k] = (fa * ((win[k + 2] + win[k + 4]) - rk) + fb * ((win[k + 1] + win[k + 5]) - rk)) +
            fc * ((win[k] + win[k + 6]) - rk);
   }
-  a[0] = (RS(r[0]) - l1[0] * am2) - l2[0] * am1;
-  a[1] = (RS(r[1]) - l1[1] * am1) - l2[1] * a[0];
-#pragma unroll
-  for (int k = 2; k < 8; ++k) a[k] = (RS(r[k]) - l1[k] * a[k - 2]) - l2[k] * a[k - 1];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) s[(i + k) * ST] = TT(a[k]);
   w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11]; w4 = win[12]; w5 = win[13];
-  am2 = a[6]; am1 = a[7];
 }
 
-// back substitution rows i, i-1, ..., i-7
+// forward rows i..i+7 of the filter; window w0..w5 = s[i-3..i+2]
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void fwd8_filter_c(TT* __restrict__ s, int i, const F8<RS>& f, TT fa, TT fb, TT fc,
+                                              TT& w0, TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+  TT r[8];
+  rhs8_filter<ST, TT>(s, i, fa, fb, fc, w0, w1, w2, w3, w4, w5, r);
+  chain8_fwd<ST, TT, RS>(s, i, f, r, am2, am1);
+}
 template <int ST, class TT, class RS, class CF>
-__device__ __forceinline__ void bwd8(TT* __restrict__ s, int i, const CF& cf, RS& cp1, RS& cp2) {
-  RS p[8], u2[8], u3[8], c[8];
+__device__ __forceinline__ void fwd8_filter(TT* __restrict__ s, int i, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
+                                            TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+  F8<RS> f;
+  f.load(cf, i);
+  fwd8_filter_c<ST, TT, RS>(s, i, f, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+}
+
+// back substitution rows i, i-1, ..., i-7. ADD (filter): each row is stored
+// as original + increment, the originals in o.
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void bwd_p8(const TT* __restrict__ s, int i, const B8<RS>& b, RS (&p)[8]) {
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    p[k] = cf.U1(i - k) * RS(s[(i - k) * ST]);
-    u2[k] = cf.U2(i - k);
-    u3[k] = cf.U3(i - k);
-  }
-  c[0] = (p[0] - u2[0] * cp1) - u3[0] * cp2;
-  c[1] = (p[1] - u2[1] * c[0]) - u3[1] * cp1;
+  for (int k = 0; k < 8; ++k) p[k] = b.u1[k] * RS(s[(i - k) * ST]);
+}
+template <int ST, class TT, class RS, int ADD>
+__device__ __forceinline__ void bwd_chain8(TT* __restrict__ s, int i, const B8<RS>& b, const RS (&p)[8],
+                                           const O8<TT>& o, RS& cp1, RS& cp2) {
+  RS c[8];
+  c[0] = (p[0] - b.u2[0] * cp1) - b.u3[0] * cp2;
+  c[1] = (p[1] - b.u2[1] * c[0]) - b.u3[1] * cp1;
 #pragma unroll
-  for (int k = 2; k < 8; ++k) c[k] = (p[k] - u2[k] * c[k - 1]) - u3[k] * c[k - 2];
+  for (int k = 2; k < 8; ++k) c[k] = (p[k] - b.u2[k] * c[k - 1]) - b.u3[k] * c[k - 2];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) s[(i - k) * ST] = TT(c[k]);
+  for (int k = 0; k < 8; ++k) s[(i - k) * ST] = ADD ? o.o[k] + TT(c[k]) : TT(c[k]);
   cp2 = c[6];
   cp1 = c[7];
 }
+template <int ST, class TT, class RS, int ADD>
+__device__ __forceinline__ void bwd8_c(TT* __restrict__ s, int i, const B8<RS>& b, const O8<TT>& o, RS& cp1,
+                                       RS& cp2) {
+  RS p[8];
+  bwd_p8<ST, TT, RS>(s, i, b, p);
+  bwd_chain8<ST, TT, RS, ADD>(s, i, b, p, o, cp1, cp2);
+}
+template <int ST, class TT, class RS, class CF>
+__device__ __forceinline__ void bwd8(TT* __restrict__ s, int i, const CF& cf, RS& cp1, RS& cp2) {
+  B8<RS> b;
+  b.load(cf, i);
+  O8<TT> o;
+  bwd8_c<ST, TT, RS, 0>(s, i, b, o, cp1, cp2);
+}
+
+// A run of forward blocks of eight while COND(i) holds, software-pipelined:
+// one straight-line body forms the next block's right-hand sides (RHS8) and
+// loads its factors while the current block's dependent chain runs, so the
+// scheduler can fill the chain's latency. RHS8(i + 8) reads rows i+8.. that
+// the chain of rows i..i+7 does not write. CONST: register constants, no loads.
+#define FWD_RUN(COND, CF, CONST, RHS8)                                        \
+  if (COND(i)) {                                                              \
+    F8<RS> nx;                                                                \
+    nx.load(CF, i);                                                           \
+    TT rr[8];                                                                 \
+    RHS8(i, rr);                                                              \
+    while (COND(i + 8)) {                                                     \
+      const F8<RS> cu = nx;                                                   \
+      TT rc[8];                                                               \
+      _Pragma("unroll") for (int k = 0; k < 8; ++k) rc[k] = rr[k];            \
+      if (!(CONST)) nx.load(CF, i + 8);                                       \
+      RHS8(i + 8, rr);                                                        \
+      chain8_fwd<ST, TT, RS>(s, i, cu, rc, am2, am1);                         \
+      i += 8;                                                                 \
+    }                                                                         \
+    chain8_fwd<ST, TT, RS>(s, i, nx, rr, am2, am1);                           \
+    i += 8;                                                                   \
+  }
+
+// The same for back substitution blocks: the next block's u1 * (forward
+// result) products, factors and (ADD) originals are formed during the current
+// block's chain; they read rows below the ones the chain writes.
+#define BWD_RUN(COND, CF, CONST)                                              \
+  if (COND(i)) {                                                              \
+    B8<RS> bn;                                                                \
+    O8<TT> on;                                                                \
+    RS pn[8];                                                                 \
+    bn.load(CF, i);                                                           \
+    if (ADD) on.load(og, ogs, i);                                             \
+    bwd_p8<ST, TT, RS>(s, i, bn, pn);                                         \
+    while (COND(i - 8)) {                                                     \
+      const B8<RS> bu = bn;                                                   \
+      const O8<TT> ou = on;                                                   \
+      RS pu[8];                                                               \
+      _Pragma("unroll") for (int k = 0; k < 8; ++k) pu[k] = pn[k];            \
+      if (!(CONST)) bn.load(CF, i - 8);                                       \
+      if (ADD) on.load(og, ogs, i - 8);                                       \
+      bwd_p8<ST, TT, RS>(s, i - 8, bn, pn);                                   \
+      bwd_chain8<ST, TT, RS, ADD>(s, i, bu, pu, ou, cp1, cp2);                \
+      i -= 8;                                                                 \
+    }                                                                         \
+    bwd_chain8<ST, TT, RS, ADD>(s, i, bn, pn, on, cp1, cp2);                  \
+    i -= 8;                                                                   \
+  }
 
 // Drives the forward rows [FIRST, LAST] with look-ahead LA: blocks of eight
 // where the look-ahead rows have arrived, single rows otherwise.
-#define FORWARD_ROWS(FIRST, LAST, LA, BLOCK8, STEP)                           \
+#define FORWARD_ROWS(FIRST, LAST, LA, RHS8, STEP)                             \
   {                                                                           \
     const CoefConst<RS> CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                \
     const CoefTable<RS> CT{F.l1, F.l2, F.u1, F.u2, F.u3};                     \
@@ -378,40 +497,49 @@ __device__ __forceinline__ void bwd8(TT* __restrict__ s, int i, const CF& cf, RS
       }                                                                       \
       {                                                                       \
         const int h = min(F.c0, e + 1);                                       \
-        for (; i + 7 < h; i += 8) BLOCK8(CT);                                 \
+        FWD_RUN(FR_H, CT, false, RHS8)                                        \
         for (; i < h; ++i) STEP(CT.L1(i), CT.L2(i))                           \
         const int ce = min(F.c1, e);                                          \
-        for (; i + 7 <= ce; i += 8) BLOCK8(CC);                               \
-        for (; i + 7 <= e; i += 8) BLOCK8(CT);                                \
+        FWD_RUN(FR_CE, CC, true, RHS8)                                        \
+        FWD_RUN(FR_E, CT, false, RHS8)                                        \
         for (; i <= e; ++i) STEP(CT.L1(i), CT.L2(i))                          \
       }                                                                       \
     }                                                                         \
   }
 
+#define FR_H(x) ((x) + 7 < h)
+#define FR_CE(x) ((x) + 7 <= ce)
+#define FR_E(x) ((x) + 7 <= e)
+#define BR_TOP(x) ((x) > F.c1 && (x) - 7 >= lo)
+#define BR_CE(x) ((x) - 7 >= ce)
+#define BR_LO(x) ((x) - 7 >= lo)
+
 // Back substitution over rows N-2 .. 0; after the lowest row of chunk c the
-// chunk is final and DONE(c) runs (add the original, store it).
+// chunk is final and DONE(c) runs (stores it). With ADD (filter) every row is
+// stored as original + increment (OUT).
+#define OUT(i, v) (ADD ? __ldg(og + (long long)(i) * ogs) + TT(v) : TT(v))
 #define BACKWARD_ROWS(DONE)                                                   \
   {                                                                           \
     const CoefConst<RS> CC{F.cl1, F.cl2, F.cu1, F.cu2, F.cu3};                \
     const CoefTable<RS> CT{F.l1, F.l2, F.u1, F.u2, F.u3};                     \
     RS cp1 = CT.U1(N) * RS(S(N));                                             \
-    S(N) = TT(cp1);                                                           \
+    S(N) = OUT(N, cp1);                                                       \
     RS c = CT.U1(N - 1) * RS(S(N - 1)) - CT.U2(N - 1) * cp1;                  \
-    S(N - 1) = TT(c);                                                         \
+    S(N - 1) = OUT(N - 1, c);                                                 \
     RS cp2 = cp1;                                                             \
     cp1 = c;                                                                  \
     int i = N - 2;                                                            \
     for (int ch = CI.NC - 1; ch >= 0; --ch) {                                 \
       const int lo = ch * CI.CR;                                              \
-      for (; i > F.c1 && i - 7 >= lo; i -= 8) bwd8<ST, TT, RS>(s, i, CT, cp1, cp2); \
+      BWD_RUN(BR_TOP, CT, false)                                              \
       {                                                                       \
         const int ce = max(F.c0, lo);                                         \
-        for (; i - 7 >= ce; i -= 8) bwd8<ST, TT, RS>(s, i, CC, cp1, cp2);     \
+        BWD_RUN(BR_CE, CC, true)                                              \
       }                                                                       \
-      for (; i - 7 >= lo; i -= 8) bwd8<ST, TT, RS>(s, i, CT, cp1, cp2);       \
+      BWD_RUN(BR_LO, CT, false)                                               \
       for (; i >= lo; --i) {                                                  \
         c = (CT.U1(i) * RS(S(i)) - CT.U2(i) * cp1) - CT.U3(i) * cp2;          \
-        S(i) = TT(c);                                                         \
+        S(i) = OUT(i, c);                                                     \
         cp2 = cp1;                                                            \
         cp1 = c;                                                              \
       }                                                                       \
@@ -428,6 +556,9 @@ __device__ __forceinline__ bool sweep_deriv(TT* __restrict__ s, int L, const LuR
                                             const DevScheme* __restrict__ sc, TT r00, TT r10, TT r01, TT r11,
                                             ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
+  constexpr int ADD = 0;
+  const TT* og = nullptr;
+  const int ogs = 0;
   const int N = L - 1;
   TT b0, b1, bn1, bn;
   if (ndf0 == 0) {
@@ -475,9 +606,9 @@ __device__ __forceinline__ bool sweep_deriv(TT* __restrict__ s, int L, const LuR
     w0 = w1; w1 = w2; w2 = w3; w3 = w4;                             \
     am2 = am1; am1 = a;                                             \
   }
-#define BLOCK8(CF) fwd8_deriv<ST, TT, RS>(s, i, CF, w0, w1, w2, w3, am2, am1)
-  FORWARD_ROWS(2, N - 2, 2, BLOCK8, FWD)
-#undef BLOCK8
+#define RHS8(I, R) rhs8_deriv<ST, TT>(s, I, w0, w1, w2, w3, R)
+  FORWARD_ROWS(2, N - 2, 2, RHS8, FWD)
+#undef RHS8
 #undef FWD
   {
     const RS a = (RS(bn1) - __ldg(F.l1 + N - 1) * am2) - __ldg(F.l2 + N - 1) * am1;
@@ -492,13 +623,16 @@ __device__ __forceinline__ bool sweep_deriv(TT* __restrict__ s, int L, const LuR
   return true;
 }
 
-// Compact filter increment of one line (src/mo_numerics.f90:922-977). On
-// return the line holds the increment; Done(ch) adds the original field.
+// Compact filter of one line (src/mo_numerics.f90:922-977): the increment is
+// solved for and each row stored as original + increment, the original read
+// from og[row * ogs] (this lane's line in the unfiltered field).
 template <int ST, class TT, class RS, class Done>
 __device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const LuRows<RS>& F, int ndf0, int ndf1,
                                              const DevScheme* __restrict__ sc, TT r00, TT r10, TT r20, TT r01,
-                                             TT r11, TT r21, ChunkIn& CI, int* err, Done&& done) {
+                                             TT r11, TT r21, const TT* __restrict__ og, int ogs,
+                                             ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
+  constexpr int ADD = 1;
   const int N = L - 1;
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
   auto fbc = [&](int r, int k) { return TT(sc->fbc[r][k]); };
@@ -567,9 +701,9 @@ __device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const Lu
     w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;                                                 \
     am2 = am1; am1 = a;                                                                                   \
   }
-#define BLOCK8(CF) fwd8_filter<ST, TT, RS>(s, i, CF, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1)
-  FORWARD_ROWS(3, N - 3, 3, BLOCK8, FWD)
-#undef BLOCK8
+#define RHS8(I, R) rhs8_filter<ST, TT>(s, I, fa, fb, fc, w0, w1, w2, w3, w4, w5, R)
+  FORWARD_ROWS(3, N - 3, 3, RHS8, FWD)
+#undef RHS8
 #undef FWD
   {
     RS a = (RS(bn2) - __ldg(F.l1 + N - 2) * am2) - __ldg(F.l2 + N - 2) * am1;
@@ -581,12 +715,22 @@ __device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const Lu
     a = (RS(bn) - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
     S(N) = TT(a);
   }
+  TRACE(3)
   BACKWARD_ROWS(done)
 #undef S
   return true;
 }
 #undef FORWARD_ROWS
 #undef BACKWARD_ROWS
+#undef OUT
+#undef FWD_RUN
+#undef BWD_RUN
+#undef FR_H
+#undef FR_CE
+#undef FR_E
+#undef BR_TOP
+#undef BR_CE
+#undef BR_LO
 
 __device__ __forceinline__ int find_task(const int* __restrict__ tile0, int ntasks, int tile) {
   int lo = 0, hi = ntasks - 1;
@@ -686,69 +830,9 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   while (CI.ready < L) CI.wait_next(err);
   TRACE(7)
 #endif
-  // chunk c is final: (filter) add the original, then store it
+  // chunk c is final (the filter added the originals row by row): store it
   auto done = [&](int c) {
     const int lo = c * CR, len = chunk_len(c);
-    if (OP == 1) {
-      if (DIR != 1) {
-        if (lane < nval) {
-          const TT* g = in + base + lane;
-          TT* col = s + lane;
-          int i = lo;
-          // 32 loads in flight per lane: the originals come back from L2, and
-          // fewer outstanding loads leave this step latency-bound
-          for (; i + 32 <= lo + len; i += 32) {
-            TT v[32];
-#pragma unroll
-            for (int k = 0; k < 32; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
-#pragma unroll
-            for (int k = 0; k < 32; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
-          }
-          for (; i + 8 <= lo + len; i += 8) {
-            TT v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
-          }
-          for (; i < lo + len; ++i) col[i * kLanes] = __ldg(g + (long long)i * pstride) + col[i * kLanes];
-        }
-      } else {
-        __syncwarp();
-        const int tot = nval * len;
-        int e = lane;
-        for (; e + 31 * kLanes < tot; e += 32 * kLanes) {
-          TT v[32];
-#pragma unroll
-          for (int k = 0; k < 32; ++k) {
-            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
-            v[k] = __ldg(in + base + (long long)r * Xp + i);
-          }
-#pragma unroll
-          for (int k = 0; k < 32; ++k) {
-            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
-            s[r * P + i] = v[k] + s[r * P + i];
-          }
-        }
-        for (; e + 7 * kLanes < tot; e += 8 * kLanes) {
-          TT v[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
-            v[k] = __ldg(in + base + (long long)r * Xp + i);
-          }
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int q = e + k * kLanes, r = q / len, i = lo + q - r * len;
-            s[r * P + i] = v[k] + s[r * P + i];
-          }
-        }
-        for (; e < tot; e += kLanes) {
-          const int r = e / len, i = lo + e - r * len;
-          s[r * P + i] = __ldg(in + base + (long long)r * Xp + i) + s[r * P + i];
-        }
-      }
-    }
     fence_proxy_async();
     __syncwarp();
     if (DIR == 1) {
@@ -809,7 +893,12 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     TT r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
     if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; r20 = recv[2 * nbs + jk]; }
     if (has && T.ndf1) { r01 = recv[3 * nbs + jk]; r11 = recv[4 * nbs + jk]; r21 = recv[5 * nbs + jk]; }
-    ok = sweep_filter<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, CI, err, done);
+    // this lane's line of the unfiltered field (lanes without a line read
+    // lane 0's, whose results are not stored)
+    const TT* og = (DIR == 1) ? in + base + (long long)(has ? lane : 0) * Xp : in + base + (has ? lane : 0);
+    const int ogs = (DIR == 1) ? 1 : (int)pstride;
+    ok = sweep_filter<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, og, ogs, CI, err,
+                                  done);
   }
   // every issued bulk store has to finish reading shared memory before exit;
   // after a timeout, wait for the chunks still in flight (bounded) instead
@@ -1373,24 +1462,40 @@ __global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restric
 constexpr double kGam = 1.4;
 #define KGAMM1 (kGam - 1.0)
 
-// primitives, pressure, Sutherland viscosity (src/mo_canard_driver.f90:267-275),
-// evaluated in FP64 and stored in the flux type R
+// primitives, pressure, Sutherland viscosity of one point from its state
+// (src/mo_canard_driver.f90:267-275), evaluated in FP64, stored in the flux type R
+template <class R>
+__device__ __forceinline__ void prim_point(const Work<R>& W, const CaseConst& C, long long l, long long n, double q0,
+                                           double q1, double q2, double q3, double q4) {
+  R* de = W.de;
+  const double d1 = 1.0 / q0;
+  const double d2 = q1 * d1, d3 = q2 * d1, d4 = q3 * d1;
+  const double p = KGAMM1 * (q4 - 0.5 * ((q1 * d2 + q2 * d3) + q3 * d4));
+  const double d5 = (kGam * p) * d1;
+  de[l] = R(d1); de[l + n] = R(d2); de[l + 2 * n] = R(d3); de[l + 3 * n] = R(d4); de[l + 4 * n] = R(d5);
+  W.p[l] = R(p);
+  W.mu[l] = R((C.srefp1dre * pow15(d5)) / (d5 + C.srefoo));
+}
+
 template <class R>
 __global__ void k_prim(const BlockDev* __restrict__ bd, const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
-    const Work<R> W = work<R>(B);
     const long long n = B.npad;
-    const CaseConst C = cc[B.case_id];
     const double* q = B.qa;
-    R* de = W.de;
-    const double q0 = q[l], q1 = q[l + n], q2 = q[l + 2 * n], q3 = q[l + 3 * n], q4 = q[l + 4 * n];
-    const double d1 = 1.0 / q0;
-    const double d2 = q1 * d1, d3 = q2 * d1, d4 = q3 * d1;
-    const double p = KGAMM1 * (q4 - 0.5 * ((q1 * d2 + q2 * d3) + q3 * d4));
-    const double d5 = (kGam * p) * d1;
-    de[l] = R(d1); de[l + n] = R(d2); de[l + 2 * n] = R(d3); de[l + 3 * n] = R(d4); de[l + 4 * n] = R(d5);
-    W.p[l] = R(p);
-    W.mu[l] = R((C.srefp1dre * pow15(d5)) / (d5 + C.srefoo));
+    prim_point<R>(work<R>(B), cc[B.case_id], l, n, q[l], q[l + n], q[l + 2 * n], q[l + 3 * n], q[l + 4 * n]);
+  }
+}
+
+// the primitives again at the points junction averaging changed (targets of
+// the three averaging plans), after a fused RK + primitives update
+template <class R>
+__global__ void k_prim_points(const BlockDev* __restrict__ bd, const CaseConst* __restrict__ cc,
+                              const int* __restrict__ tb, const long long* __restrict__ tl, int ntg) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[tb[t]];
+    const long long l = tl[t], n = B.npad;
+    const double* q = B.qa;
+    prim_point<R>(work<R>(B), cc[B.case_id], l, n, q[l], q[l + n], q[l + 2 * n], q[l + 3 * n], q[l + 4 * n]);
   }
 }
 
@@ -1475,12 +1580,27 @@ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long l
 
 // flux components rr(:,d,m) of one point into scr field (m-1)*3 + d and
 // de(:,5) = qa(:,5) + p (src/mo_physics.f90:319-382); t as from visc_point
-template <class R>
+template <class R, bool FROM_PRIM = false>
 __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
                                            long long l, long long n, const R t[9]) {
   const double* q = B.qa;
   R* de = W.de;
   const R p = W.p[l];
+  // FROM_PRIM (FP32 step path): the conserved values come from the primitives
+  // in de (1/rho, u, v, w) and p instead of a second read of the FP64 state
+  R qv[5];
+  if (FROM_PRIM) {
+    const R rho = R(1) / de[l];
+    const R uu = de[l + n], vv = de[l + 2 * n], ww = de[l + 3 * n];
+    qv[0] = rho;
+    qv[1] = rho * uu;
+    qv[2] = rho * vv;
+    qv[3] = rho * ww;
+    qv[4] = p * R(1.0 / KGAMM1) + R(0.5) * rho * ((uu * uu + vv * vv) + ww * ww);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) qv[c] = R(q[l + c * n]);
+  }
   const R* mt[3] = {W.xim, W.etm, W.zem};
   const R um0 = R(S.umf[0]), um1 = R(S.umf[1]), um2 = R(S.umf[2]);
   const R u = de[l + n] + um0, v = de[l + 2 * n] + um1, w = de[l + 3 * n] + um2;
@@ -1491,7 +1611,7 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
     ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
   }
   R* r = W.scr;
-  const R q0 = R(q[l]);
+  const R q0 = qv[0];
 #pragma unroll
   for (int d = 0; d < 3; ++d) r[l + d * n] = q0 * ssd[d];
   R tau[3][3];
@@ -1504,7 +1624,7 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const R qc = R(q[l + (c + 1) * n]);
+    const R qc = qv[c + 1];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       R v1 = qc * ssd[d] + m[d][c] * p;
@@ -1516,7 +1636,7 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
       r[l + (3 * (c + 1) + d) * n] = v1;
     }
   }
-  const R d5 = R(q[l + 4 * n]) + p;
+  const R d5 = qv[4] + p;
   de[l + 4 * n] = d5;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -1587,7 +1707,7 @@ __global__ void k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* 
       R d5;
       visc_point<R>(W, l, n, W.mu[l], t, d5);
     }
-    flux_point<R>(W, B, sp[B.case_id], visc, l, n, t);
+    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t);
   }
 }
 
@@ -1601,6 +1721,37 @@ __global__ void k_flux_sum(const BlockDev* __restrict__ bd) {
 #pragma unroll
     for (int m = 0; m < 5; ++m)
       W.de[l + m * n] = (r[l + (3 * m) * n] + r[l + (3 * m + 1) * n]) + r[l + (3 * m + 2) * n];
+  }
+}
+
+// RK stage update of the step path, with two optional fusions: sum > 0 forms
+// de = sum of the three flux derivatives on the fly (no GCBC or sponge
+// changes de in between; sum == 2 also stores it, so that de holds the last
+// stage's right-hand side after a step), prim computes the next stage's
+// primitives from the new state. Same operations in the same order as k_flux_sum, k_rk and
+// k_prim, so bit-identical to running them one after the other.
+template <class R>
+__global__ void k_rk_next(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                          const CaseConst* __restrict__ cc, int sum, int prim) {
+  FOR_POINTS(bd[blockIdx.y]) {
+    const Work<R> W = work<R>(B);
+    const long long n = B.npad;
+    const double r1 = sp[B.case_id].dtk * B.yaco[l];
+    double q[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      R dv;
+      if (sum) {
+        const R* r = W.scr;
+        dv = (r[l + (3 * c) * n] + r[l + (3 * c + 1) * n]) + r[l + (3 * c + 2) * n];
+        if (sum == 2) W.de[l + c * n] = dv;
+      } else {
+        dv = W.de[l + c * n];
+      }
+      q[c] = B.qo[l + c * n] - r1 * double(dv);
+      B.qa[l + c * n] = q[c];
+    }
+    if (prim) prim_point<R>(W, cc[B.case_id], l, n, q[0], q[1], q[2], q[3], q[4]);
   }
 }
 
@@ -1829,6 +1980,16 @@ void launch_flux_visc(dim3 g, cudaStream_t st, const BlockDev* bd, const StagePa
 template <class R>
 void launch_flux_sum(dim3 g, cudaStream_t st, const BlockDev* bd) {
   k_flux_sum<R><<<g, 256, 0, st>>>(bd);
+}
+template <class R>
+void launch_rk_next(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc, int sum,
+                    int prim) {
+  k_rk_next<R><<<g, 256, 0, st>>>(bd, sp, cc, sum, prim);
+}
+template <class R>
+void launch_prim_points(int grid, cudaStream_t st, const BlockDev* bd, const CaseConst* cc, const int* tb,
+                        const long long* tl, int ntg) {
+  k_prim_points<R><<<grid, 256, 0, st>>>(bd, cc, tb, tl, ntg);
 }
 template <class R>
 void launch_rk(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp) {
