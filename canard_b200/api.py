@@ -92,6 +92,7 @@ def lib():
         L.canard_set_timers.argtypes = [vp, i32]
         L.canard_set_graphs.argtypes = [vp, i32]
         L.canard_autotune.argtypes = [vp, i32, _DP, i32]
+        L.canard_set_line_kind.argtypes = [vp, i32, i32, i32, i32]
         L.canard_line_bench.argtypes = [vp, i32, i32, i32, _DP, _DP, i32, ctypes.POINTER(ctypes.c_double)]
         L.canard_get_timers.argtypes = [vp, _DP, _DP, _DP, i32]
         L.canard_timer_name.restype = ctypes.c_char_p
@@ -217,7 +218,7 @@ class Context:
         if k < 0:
             self._check(-k)
         kinds = {0: "fp64", 1: "fp32-split", 2: "fp64-tile/fp32-split", 3: "fp32-one-lane",
-                 4: "fp64-tile/fp32-one-lane"}
+                 4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem"}
         out = []
         for i in range(k):
             g, d, kd, nc, best, dflt = rep[6 * i:6 * i + 6]
@@ -225,6 +226,17 @@ class Context:
                         "kind": kinds.get(int(kd), str(int(kd))), "chunks": int(nc) or "default",
                         "ms": best, "default_ms": dflt})
         return out
+
+    LINE_KINDS = {"default": -1, "fp64": 0, "fp32-split": 1, "fp64-tile/fp32-split": 2, "fp32-one-lane": 3,
+                  "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5}
+
+    def set_line_kind(self, group, direction, kind, chunks=0):
+        """Pins the line kernel of a group ("filter", "viscous", "flux") and
+        direction ("xi", "eta", "zeta"), by name from LINE_KINDS; every FP64
+        kind gives bit-identical results."""
+        g = ("filter", "viscous", "flux").index(group)
+        d = ("xi", "eta", "zeta").index(direction)
+        self._check(lib().canard_set_line_kind(self.h, g, d, self.LINE_KINDS[kind], chunks))
 
     def line_bench(self, op, nn, fields, reps=10):
         """One direction's derivative (op 0) or filter (op 1) over up to 5

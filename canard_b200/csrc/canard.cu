@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 #include "kernels_f32.h"
 #include "kernels_setup.cuh"
+#include "kernels_tm.cuh"
 
 using namespace canard;
 
@@ -83,7 +84,8 @@ enum LineKind {
   LK_F32 = 1,                  // split
   LK_F64_TILE_F32_SOLVE = 2,   // split
   LK_F32_1L = 3,
-  LK_F64_TILE_F32_SOLVE_1L = 4
+  LK_F64_TILE_F32_SOLVE_1L = 4,
+  LK_F64_TM = 5                // FP64, elimination results in TMEM (eta/zeta, 16 <= L <= 257)
 };
 inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L; }
 inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
@@ -394,7 +396,8 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
   t.out = out;
-  t.lu = (kind == LK_F64) ? static_cast<const void*>(B.lu[nt][dir]) : static_cast<const void*>(B.lu32[nt][dir]);
+  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM;
+  t.lu = f64solve ? static_cast<const void*>(B.lu[nt][dir]) : static_cast<const void*>(B.lu32[nt][dir]);
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
   t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
   t.c0 = B.luc0[nt][dir];
@@ -410,7 +413,7 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
   t.h = t.kg = t.ke = 0;
-  if (kind != LK_F64) {  // FP32 elimination: rounded factors and their constant range
+  if (!f64solve) {  // FP32 elimination: rounded factors and their constant range
     t.cl1 = B.luc32[nt][dir][0]; t.cl2 = B.luc32[nt][dir][1]; t.cu1 = B.luc32[nt][dir][2];
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
     t.c0 = B.luc032[nt][dir];
@@ -421,6 +424,10 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
     t.ke = B.ke32[nt][dir];
   }
   chunking_dir(dir, t.L, t.nbox, t.by, nc_req);
+  if (kind == LK_F64_TM) {  // 32-row boxes streamed through the ring
+    t.by = kTmChunk;
+    t.nbox = (t.L + kTmChunk - 1) / kTmChunk;
+  }
   const int lanes = tile_lanes(kind);
   if (dir == 0) {
     t.ntx = 1;
@@ -433,6 +440,7 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
 
 // dynamic shared memory of one task's tile
 size_t line_smem(int dir, const LineTask& t, int kind) {
+  if (kind == LK_F64_TM) return kTmSmem;
   const size_t es = tile_elem(kind);
   const int lanes = tile_lanes(kind);
   if (dir == 0)
@@ -549,9 +557,30 @@ void launch_line2_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
+int num_sms() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return n;
+}
+
+// persistent: one CTA of kTmWarps tiles per SM
+template <int DIR, int OP>
+void launch_line_tm_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
+  const int grid = std::max(1, std::min(num_sms(), (T.total + kTmWarps - 1) / kTmWarps));
+  launch_line_tm_t<DIR, OP>(grid, c->st, T.tasks, T.first, T.ntasks, T.total, T.maps, c->derr);
+  CK(cudaGetLastError());
+}
+
 template <int DIR, int OP>
 void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   if (T.kind == LK_F64) launch_line_dir<DIR, OP, double, double>(c, T);
+  else if (DIR != 1 && T.kind == LK_F64_TM) launch_line_tm_dir<(DIR == 1 ? 2 : DIR), OP>(c, T);
   else if (OP == 0 && T.kind == LK_F32) launch_line2_dir<DIR, 0, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line2_dir<DIR, 1, double>(c, T);
   else if (OP == 0 && T.kind == LK_F32_1L) launch_line_dir<DIR, 0, float, float>(c, T);
@@ -593,6 +622,10 @@ void set_line_smem_limits() {
   CK((line_smem_limit<1, 1, double, float>(lim)));
   CK((line_smem_limit<2, 1, double, float>(lim)));
   CK((line_smem_limit<3, 1, double, float>(lim)));
+  CK((line_tm_smem_limit<2, 0>()));
+  CK((line_tm_smem_limit<3, 0>()));
+  CK((line_tm_smem_limit<2, 1>()));
+  CK((line_tm_smem_limit<3, 1>()));
   done = true;
 }
 
@@ -1034,14 +1067,24 @@ std::vector<LineTask> group_tasks(canard_ctx* c, int grp, int dir, int m, int ki
   return v;
 }
 
-int default_kind(const canard_ctx* c, int grp) {
+// the TMEM line kernel takes eta/zeta lines of kTmMinL..kTmMaxL points
+bool tm_ok(const canard_ctx* c, int dir) {
+  if (dir == 0 || c->blocks.empty()) return false;
+  for (const auto& b : c->blocks) {
+    const int L = b.g.ijk[0][dir] + 1;
+    if (L < kTmMinL || L > kTmMaxL) return false;
+  }
+  return true;
+}
+
+int default_kind(const canard_ctx* c, int grp, int dir) {
   if (!c->f32()) return LK_F64;
   return grp == 0 ? LK_F64_TILE_F32_SOLVE : LK_F32;
 }
 
 int group_kind(const canard_ctx* c, int grp, int dir) {
   const int k = c->tune[grp][dir].kind;
-  return k >= 0 ? k : default_kind(c, grp);
+  return k >= 0 ? k : default_kind(c, grp, dir);
 }
 
 void free_line_table(Table<LineTask>& T) {
@@ -1063,6 +1106,17 @@ void build_line_tables(canard_ctx* c) {
     k = group_kind(c, 2, dir);
     c->flux[dir] = make_line_table(c, group_tasks(c, 2, dir, 0, k, c->tune[2][dir].nc), dir, false, k);
   }
+}
+
+// the step tables with the current choices; the step graphs used the old ones
+void rebuild_line_tables(canard_ctx* c) {
+  for (int m = 0; m < 5; ++m)
+    for (int i = 0; i < 3; ++i) free_line_table(c->filt[m][i]);
+  for (int d = 0; d < 3; ++d) { free_line_table(c->visc[d]); free_line_table(c->flux[d]); }
+  for (auto& g : c->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  build_line_tables(c);
+  CK(cudaStreamSynchronize(c->st));
 }
 
 void build_tables(canard_ctx* c) {
@@ -1882,7 +1936,7 @@ int canard_line_bench(canard_ctx* c, int32_t op, int32_t nn, int32_t nfields, co
     BlockState& B = c->blocks[block_index(c, 0, 0)];
     const int dir = nn - 1;
     const canard_ctx::TuneChoice& tc = c->tune[op == 0 ? 2 : 0][dir];
-    const int kind = tc.kind >= 0 ? tc.kind : (!c->f32() ? LK_F64 : (op == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE));
+    const int kind = tc.kind >= 0 ? tc.kind : default_kind(c, op == 0 ? 2 : 0, dir);
     const size_t L = (size_t)B.g.X * B.g.Y * B.g.Z;
     std::vector<LineTask> tasks;
     for (int k = 0; k < nfields; ++k) {
@@ -1953,11 +2007,12 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
       for (int dir = 0; dir < 3; ++dir) {
         const int op = grp == 0 ? 1 : 0;
         std::vector<std::pair<int, int>> cand;  // (kind, nc)
-        std::vector<int> kinds{default_kind(c, grp)};
+        std::vector<int> kinds{default_kind(c, grp, dir)};
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
+        else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
         for (int k : kinds) {
           cand.push_back({k, 0});
-          if (dir != 0)
+          if (dir != 0 && k != LK_F64_TM)
             for (int nc : {2, 4, 8}) cand.push_back({k, nc});
         }
         double best = 1e300, def = 0;
@@ -1981,16 +2036,29 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
       }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // rebuild the step tables with the choices; the step graphs used the old ones
-    for (int m = 0; m < 5; ++m)
-      for (int i = 0; i < 3; ++i) free_line_table(c->filt[m][i]);
-    for (int d = 0; d < 3; ++d) { free_line_table(c->visc[d]); free_line_table(c->flux[d]); }
-    for (auto& g : c->graph)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    build_line_tables(c);
-    CK(cudaStreamSynchronize(c->st));
+    rebuild_line_tables(c);
   });
   return rc == CANARD_OK ? rows : -rc;
+}
+
+int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
+  return guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_set_line_kind before canard_setup");
+    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_TM || chunks < 0 ||
+        chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
+      throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
+    if (kind >= 0) {
+      bool fits;
+      if (!c->f32()) fits = kind == LK_F64 || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
+      else if (group == 0) fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L;
+      else fits = kind == LK_F32 || kind == LK_F32_1L;
+      if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
+    }
+    CK(cudaStreamSynchronize(c->st));
+    c->tune[group][dir].kind = kind;
+    c->tune[group][dir].nc = kind >= 0 ? chunks : 0;
+    rebuild_line_tables(c);
+  });
 }
 
 int canard_set_timers(canard_ctx* c, int32_t on) {

@@ -179,13 +179,26 @@ int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, 
  * derivatives) and direction, times the candidate tile shapes on the
  * context's own blocks (filter candidates on scratch copies, the state is not
  * touched): FP64 contexts try TMA staging depths (2, 4, 8 chunks per eta or
- * zeta line); mixed-precision contexts also try the one-lane FP32 sweeps (32
- * lines per tile) against the split solve (16 lines per tile). The fastest
+ * zeta line) and, on eta/zeta lines of 16..257 points, the kernel that keeps
+ * the elimination results in tensor memory; mixed-precision contexts also try
+ * the one-lane FP32 sweeps (32 lines per tile) against the split solve (16
+ * lines per tile). The fastest
  * choice is installed in the step tables. Returns the number of groups
  * (9) and fills up to nmax report rows of 6 doubles: group, direction
  * (0..2), chosen kind, chosen chunk count (0 = default), its ms per launch
  * and the default's. Call after canard_setup. */
 int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax);
+
+/* Pins the line kernel of one group (0 filter, 1 viscous gradients, 2 flux
+ * derivatives) and direction (0..2), as canard_autotune would install it (no
+ * counterpart in the reference): kind 0 FP64 tiles in shared memory (chunks:
+ * 0 default or 2..8 TMA stages), 1 FP32 split, 2 FP64 tile / FP32 split, 3
+ * FP32 one-lane, 4 FP64 tile / FP32 one-lane, 5 FP64 with the elimination
+ * results in tensor memory (eta/zeta, 16..257 points per line); -1 restores
+ * the precision's default. Every FP64 kind gives bit-identical results. A kind
+ * the context's precision or line lengths do not admit returns
+ * CANARD_ERR_ARG. Call after canard_setup. */
+int canard_set_line_kind(canard_ctx* ctx, int32_t group, int32_t dir, int32_t kind, int32_t chunks);
 
 /* Observability (the reference's mo_timer, src/mo_timer.f90:84-133, as CUDA
  * events per kernel family). With timers on, every launch of the family is

@@ -292,3 +292,26 @@ def test_non_finite_state_is_reported():
     with pytest.raises(api.CanardError) as e:
         g.step(2)  # the step with n % 10 == 1 reduces dt
     assert e.value.code == api.ERR_NAN
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (16, 200, 140), (16, 256, 32)])
+def test_tmem_line_kernel_bit_identical(shape):
+    """The FP64 line kernel that keeps the elimination results in tensor
+    memory (eta/zeta lines of 16..257 points) gives the same bits as the
+    default shared-memory tiles. The shapes cover lines whose input boxes all
+    load up front (L <= 128), the input ring's refill (L > 128) and L = 257,
+    whose last row stays in registers."""
+    nx, ny, nz = shape
+    cs = cases.tgv(nx=nx, ny=ny, nz=nz)
+    a = api.Context(cs)
+    b = api.Context(cs)
+    for grp in ("filter", "viscous", "flux"):
+        for d in ("eta", "zeta"):
+            b.set_line_kind(grp, d, "fp64-tmem")
+    with pytest.raises(api.CanardError) as e:
+        b.set_line_kind("flux", "xi", "fp64-tmem")  # xi lines stay in shared memory
+    assert e.value.code == api.ERR_ARG
+    a.step(3)
+    b.step(3)
+    np.testing.assert_array_equal(b.state(0), a.state(0))
+    np.testing.assert_array_equal(b.field(api.F_DE, 0), a.field(api.F_DE, 0))
