@@ -268,10 +268,16 @@ def kernels_mode(args, api, cases, torch):
         o = po.Oracle(cs, setup=False, threads=os.cpu_count() or 1)  # fresh filter send chain
     peak, peak_kind = peaks()
     rows = []
-    for prec, name in ((api.FP64, "fp64"), (api.FP32_MIXED, "fp32")):
+    # fp64-tmem: the FP64 eta/zeta kernel that keeps the elimination results in
+    # tensor memory (an autotuner candidate), pinned for the comparison
+    for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP32_MIXED, "fp32")):
         ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
         for op in (0, 1):
             for nn in (1, 2, 3):
+                if name == "fp64-tmem":
+                    if nn == 1:
+                        continue
+                    ctx.set_line_kind("flux" if op == 0 else "filter", "xi eta zeta".split()[nn - 1], "fp64-tmem")
                 out, ms = ctx.line_bench(op, nn, fields, reps=args.steps)
                 es = 4 if (name == "fp32" and op == 0) else 8
                 gbs = 5 * blk.npts * 2 * es / (ms / 1e3) / 1e9

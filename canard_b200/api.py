@@ -24,7 +24,7 @@ from . import cases as _cases
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libcanard_b200.so")
 
-OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(7)
+OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE, ERR_IO = range(8)
 FP64, FP32_MIXED = 0, 1
 
 F_QA, F_QO, F_DE, F_P, F_SS1, F_XIM, F_ETM, F_ZEM, F_YACO, F_TAU = range(10)
@@ -85,6 +85,12 @@ def lib():
         L.canard_step.argtypes = [vp, i32]
         L.canard_phase.argtypes = [vp, i32, i32]
         L.canard_get_time.argtypes = [vp, i32, _DP]
+        L.canard_restart_write_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
+        L.canard_restart_read_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
+        L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
+                                             ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+        L.canard_write_restart.argtypes = [vp, i32, i32, ctypes.c_char_p]
+        L.canard_read_restart.argtypes = [vp, i32, i32, ctypes.c_char_p]
         L.canard_set_time.argtypes = [vp, i32, _DP]
         L.canard_mpigo.argtypes = [vp, ctypes.POINTER(_DP), i32, i32, i32, i32, i32, i32]
         L.canard_deriv.argtypes = [vp, i32, _DP, _DP, i32, i32]
@@ -127,6 +133,45 @@ def penta(fltk, fltrbc, n, ns, ne, nt):
     if rc:
         raise CanardError(rc, "canard_penta")
     return xu.reshape(3, n), xl.reshape(2, n)
+
+
+def restart_name(mb: int) -> str:
+    """The reference's restart file of block mb, relative to the run directory:
+    'misc/restart' + 'z' + three digits + '.dat' assigned to a character(19)
+    variable, which Fortran truncates to 19 characters (src/mo_io.f90:27,
+    108-116), so the file is misc/restartzNNN.da."""
+    return ("misc/restart" + "z%03d" % mb + ".dat")[:19]
+
+
+def write_restart_file(path, time6, qa):
+    """One block's restart file in the reference's format; qa is (5, ...) in
+    the reference layout (qa(0:lmx, 5))."""
+    q = np.ascontiguousarray(qa, np.float64).reshape(5, -1)
+    t = np.ascontiguousarray(time6, np.float64)
+    rc = lib().canard_restart_write_file(os.fsencode(path), _dp(t), _dp(q), q.shape[1])
+    if rc:
+        raise CanardError(rc, f"canard_restart_write_file {path}")
+
+
+def read_restart_file(path, npts):
+    """(time6, qa (5, npts)) of a restart file of a block of npts points."""
+    t = np.zeros(6)
+    q = np.zeros((5, npts))
+    rc = lib().canard_restart_read_file(os.fsencode(path), _dp(t), _dp(q), npts)
+    if rc:
+        raise CanardError(rc, f"canard_restart_read_file {path}")
+    return t, q
+
+
+def compare_restart(path1, path2, npts, wtol=1e-15, report=None):
+    """dcanard: the number of values whose difference relative to the first
+    file's value exceeds wtol; their lines go to `report` if given."""
+    n = ctypes.c_int64(0)
+    rc = lib().canard_restart_compare(os.fsencode(path1), os.fsencode(path2), npts, wtol,
+                                      os.fsencode(report) if report else None, ctypes.byref(n))
+    if rc:
+        raise CanardError(rc, f"canard_restart_compare {path1} {path2}")
+    return n.value
 
 
 def _structs(case_list: Sequence[_cases.CaseSpec]):
@@ -291,6 +336,20 @@ class Context:
 
     def set_time(self, t6, case=0):
         self._check(lib().canard_set_time(self.h, case, _dp(np.asarray(t6, np.float64))))
+
+    def write_restart(self, directory, case=0):
+        """write_restart_file for every block of a case: the state and the
+        case's time state into directory/misc/restartzNNN.da (NNN = block)."""
+        os.makedirs(os.path.join(directory, "misc"), exist_ok=True)
+        for b in range(len(self.cases[case].blocks)):
+            path = os.path.join(directory, restart_name(b))
+            self._check(lib().canard_write_restart(self.h, case, b, os.fsencode(path)))
+
+    def read_restart(self, directory, case=0):
+        """read_restart_file for every block of a case (pathbase = directory)."""
+        for b in range(len(self.cases[case].blocks)):
+            path = os.path.join(directory, restart_name(b))
+            self._check(lib().canard_read_restart(self.h, case, b, os.fsencode(path)))
 
     # t_numerics
     def mpigo(self, fields, nt, nrt, n45, itag, m, ncols=1):

@@ -1849,6 +1849,38 @@ int canard_get_time(canard_ctx* c, int32_t icase, double* t) {
   });
 }
 
+int canard_write_restart(canard_ctx* c, int32_t icase, int32_t iblock, const char* path) {
+  return guarded(c, [&] {
+    if (!path) throw ApiError(CANARD_ERR_ARG, "null path");
+    const BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    const int64_t npts = (int64_t)B.g.X * B.g.Y * B.g.Z;
+    std::vector<double> qa((size_t)5 * npts);
+    double t[6];
+    int rc = canard_get_state(c, icase, iblock, qa.data());
+    if (rc == CANARD_OK) rc = canard_get_time(c, icase, t);
+    if (rc != CANARD_OK) throw ApiError(rc, c->err);
+    rc = canard_restart_write_file(path, t, qa.data(), npts);
+    if (rc != CANARD_OK) throw ApiError(rc, std::string("cannot write restart file ") + path);
+  });
+}
+
+int canard_read_restart(canard_ctx* c, int32_t icase, int32_t iblock, const char* path) {
+  return guarded(c, [&] {
+    if (!path) throw ApiError(CANARD_ERR_ARG, "null path");
+    const BlockState& B = c->blocks[block_index(c, icase, iblock)];
+    const int64_t npts = (int64_t)B.g.X * B.g.Y * B.g.Z;
+    std::vector<double> qa((size_t)5 * npts);
+    double t[6];
+    int rc = canard_restart_read_file(path, t, qa.data(), npts);
+    if (rc != CANARD_OK)
+      throw ApiError(rc, std::string("cannot read restart file ") + path + " for a block of " +
+                             std::to_string(npts) + " points");
+    rc = canard_set_state(c, icase, iblock, qa.data());
+    if (rc == CANARD_OK) rc = canard_set_time(c, icase, t);
+    if (rc != CANARD_OK) throw ApiError(rc, c->err);
+  });
+}
+
 int canard_set_time(canard_ctx* c, int32_t icase, const double* t) {
   return guarded(c, [&] {
     if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
@@ -2043,7 +2075,6 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
 
 int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
   return guarded(c, [&] {
-    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_set_line_kind before canard_setup");
     if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_TM || chunks < 0 ||
         chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
       throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
@@ -2057,7 +2088,7 @@ int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind
     CK(cudaStreamSynchronize(c->st));
     c->tune[group][dir].kind = kind;
     c->tune[group][dir].nc = kind >= 0 ? chunks : 0;
-    rebuild_line_tables(c);
+    if (c->setup_done) rebuild_line_tables(c);
   });
 }
 

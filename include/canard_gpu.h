@@ -42,6 +42,7 @@ extern "C" {
 #define CANARD_ERR_TIMEOUT 4     /* a bounded device wait gave up */
 #define CANARD_ERR_UNSUPPORTED 5 /* configuration the path does not handle */
 #define CANARD_ERR_STATE 6       /* call order (e.g. step before setup) */
+#define CANARD_ERR_IO 7          /* a file could not be opened, read or written, or has another block's size */
 
 #define CANARD_FP64 0            /* plain FP64 path */
 #define CANARD_FP32_MIXED 1      /* FP32 line solves/fluxes, FP64 state, RK, metrics, LU */
@@ -139,6 +140,27 @@ int canard_phase(canard_ctx* ctx, int32_t phase, int32_t nk);
 int canard_get_time(canard_ctx* ctx, int32_t icase, double* time6);
 int canard_set_time(canard_ctx* ctx, int32_t icase, const double* time6);
 
+/* Restart files in the reference's format: one block per file, Fortran
+ * direct-access records of 5 doubles (write_restart_file / read_restart_file,
+ * src/mo_io.f90:184-271): record 1 = n, ndt, dt, dts, dte; record 2 = timo,
+ * 0, 0, 0, 0; then one record qa(l, 1..5) per stored point l (i fastest,
+ * then j, then k). time6 and qa(0:npts-1, 5) as elsewhere in this header.
+ * canard_write_restart / canard_read_restart move one block's state and its
+ * case's time state between the context and such a file; a file of another
+ * block size returns CANARD_ERR_IO. */
+int canard_restart_write_file(const char* path, const double* time6, const double* qa, int64_t npts);
+int canard_restart_read_file(const char* path, double* time6, double* qa, int64_t npts);
+int canard_write_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
+int canard_read_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
+
+/* The restart comparer (contrib/dcanard.f90:100-126): both files of npts
+ * points are read and every value whose difference, relative to the first
+ * file's value, exceeds wtol is counted in *nreported and, when report_path
+ * is not NULL, written there as dcanard's line " i=<i8> j=<i8> v1=<e15.7>
+ * v2=<e15.7> abs=<e15.7> rel=<e15.7>" (point index from 0, variable 1..5). */
+int canard_restart_compare(const char* path1, const char* path2, int64_t npts, double wtol, const char* report_path,
+                           int64_t* nreported);
+
 /* Unit operations of t_numerics on host arrays, for case 0 (parity tests and
  * drop-in calls). fields[b] = rfield(0:lmx, ncols) of block b. mpigo computes
  * the interface contractions of every block face and exchanges them into the
@@ -197,7 +219,8 @@ int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax)
  * results in tensor memory (eta/zeta, 16..257 points per line); -1 restores
  * the precision's default. Every FP64 kind gives bit-identical results. A kind
  * the context's precision or line lengths do not admit returns
- * CANARD_ERR_ARG. Call after canard_setup. */
+ * CANARD_ERR_ARG. Before canard_setup the choice only applies to
+ * canard_line_bench (the step tables are built by canard_setup). */
 int canard_set_line_kind(canard_ctx* ctx, int32_t group, int32_t dir, int32_t kind, int32_t chunks);
 
 /* Observability (the reference's mo_timer, src/mo_timer.f90:84-133, as CUDA
