@@ -365,6 +365,15 @@ class Clocks:
         except Exception:
             self.p = None
 
+    def wait_first(self, timeout=2.0):
+        """Returns once nvidia-smi has written its first sample (it starts slowly),
+        so that a timed region of a few milliseconds still gets a record."""
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < timeout:
+            if os.path.getsize(self.f.name) > 0:
+                return
+            time.sleep(0.02)
+
     def stop(self):
         if self.p is None:
             return None
@@ -491,10 +500,12 @@ def main():
             dist.barrier()
 
     ctx.step(args.warmup)
+    clk = Clocks(local) if rank == 0 else None
+    if clk:
+        clk.wait_first()
     barrier()
     torch.cuda.synchronize()
     n0 = ctx.launch_count()
-    clk = Clocks(local) if rank == 0 else None
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
