@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -282,6 +283,11 @@ struct canard_ctx {
   // step-path fusions: flux sum inside the RK update (no GCBC, no sponge in
   // the context), next stage's primitives inside the RK update
   bool fuse_sum = false, fuse_prim = true;
+  // wall_condition_update: wall-face points, packed reset kinds (k_wall_update)
+  int wall_n = 0;
+  int* wall_tb = nullptr;
+  long long* wall_tl = nullptr;
+  int* wall_tk = nullptr;
   // timers (mo_timer equivalent) and launch counter
   bool timers = false;
   long long launches = 0;
@@ -913,6 +919,14 @@ void ph_prim_points(canard_ctx* c) {
   CK(cudaGetLastError());
 }
 
+void ph_wall(canard_ctx* c, const StageParams* sp) {
+  if (c->wall_n == 0) return;
+  Timed tm(c, T_RK, 8.0 * 10 * c->wall_n);
+  k_wall_update<<<std::max(1, std::min((c->wall_n + 255) / 256, 1184)), 256, 0, c->st>>>(
+      c->dbd, sp, c->wall_tb, c->wall_tl, c->wall_tk, c->wall_n);
+  CK(cudaGetLastError());
+}
+
 void run_avg(canard_ctx* c, const AvgDev& A, int mode) {
   if (A.ntg == 0) return;
   Timed tm(c, T_AVERAGE, 8.0 * 5 * (A.nsrc + A.ntg));
@@ -977,6 +991,7 @@ void step_body(canard_ctx* c) {
     ph_sponge(c);
     const bool prim = c->fuse_prim && nk < 4;
     ph_rk_next(c, sp, prim);
+    ph_wall(c, sp);
     ph_average(c);
     if (prim) ph_prim_points(c);
   }
@@ -1278,9 +1293,40 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
   upload_avg(P, c->avg_pt);
   upload_avg(Lp, c->avg_ln);
   upload_avg(Sf, c->avg_sf);
+  // wall-face points with their resets in the reference's face order
+  std::map<std::pair<int, long long>, int> wall;
+  for (int b = 0; b < nb; ++b) {
+    const BlockGeom& g = c->blocks[b].g;
+    for (int nn = 1; nn <= 3; ++nn)
+      for (int ip = 0; ip <= 1; ++ip) {
+        const int np = g.nbc[nn - 1][ip];
+        if (np != BC_WALLI && np != BC_WALLV) continue;
+        const int pos = ip * g.ijk[0][nn - 1];
+        for (int k = 0; k <= g.ijk[2][nn - 1]; ++k)
+          for (int j = 0; j <= g.ijk[1][nn - 1]; ++j) {
+            int x, y, z;
+            g.line_xyz(nn, pos, j, k, x, y, z);
+            int& kinds = wall[{b, (long long)g.dev(x, y, z)}];
+            int s = 0;
+            while ((kinds >> (2 * s)) & 3) ++s;
+            kinds |= (np == BC_WALLI ? 1 : 2) << (2 * s);
+          }
+      }
+  }
+  c->wall_n = (int)wall.size();
+  if (c->wall_n) {
+    std::vector<int> wb, wk;
+    std::vector<long long> wl;
+    for (const auto& e : wall) { wb.push_back(e.first.first); wl.push_back(e.first.second); wk.push_back(e.second); }
+    c->wall_tb = dupload(wb, c->st);
+    c->wall_tl = dupload(wl, c->st);
+    c->wall_tk = dupload(wk, c->st);
+  }
+  // the primitives are recomputed at averaged and at reset wall points
   std::vector<std::pair<int, long long>> pts;
   for (const AvgPlan* p : {&P, &Lp, &Sf})
     for (const auto& t : p->targets) pts.emplace_back(t.b, (long long)t.l);
+  for (const auto& e : wall) pts.push_back(e.first);
   std::sort(pts.begin(), pts.end());
   pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
   c->prim_n = (int)pts.size();
@@ -1449,6 +1495,7 @@ void destroy(canard_ctx* c) {
   for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) ft(c->gc_upd[d][s]);
   cudaFree(c->fc_src); cudaFree(c->fc_dst); cudaFree(c->fc_cnt);
   cudaFree(c->prim_tb); cudaFree(c->prim_tl);
+  cudaFree(c->wall_tb); cudaFree(c->wall_tl); cudaFree(c->wall_tk);
   for (AvgDev* A : {&c->avg_pt, &c->avg_ln, &c->avg_sf}) {
     cudaFree(A->tb); cudaFree(A->tl); cudaFree(A->tfirst); cudaFree(A->tcount); cudaFree(A->sb); cudaFree(A->sl);
     cudaFree(A->snap);
@@ -1485,13 +1532,12 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
       for (int d = 0; d < 3; ++d)
         for (int s = 0; s < 2; ++s) {
           const int np = bd.nbc[d][s];
-          if (np == BC_WALLI || np == BC_WALLV)
-            throw ApiError(CANARD_ERR_UNSUPPORTED, "wall boundaries (20/25) are not on this path yet");
           if (np == BC_SUBDOM)
             throw ApiError(CANARD_ERR_UNSUPPORTED, "BC 40 needs nbpc > 1; every block here is one sub-domain");
-          if (!(np == BC_NR || np == BC_CURV || np == BC_STRAIGHT || np == BC_PERIODIC))
+          if (!(np == BC_NR || np == BC_WALLI || np == BC_WALLV || np == BC_CURV || np == BC_STRAIGHT ||
+                np == BC_PERIODIC))
             throw ApiError(CANARD_ERR_ARG, "unknown boundary code " + std::to_string(np));
-          if (np != BC_NR && (bd.mbcd[d][s] < 0 || bd.mbcd[d][s] >= cs.nb))
+          if (np != BC_NR && np != BC_WALLI && np != BC_WALLV && (bd.mbcd[d][s] < 0 || bd.mbcd[d][s] >= cs.nb))
             throw ApiError(CANARD_ERR_ARG, "interface face without a neighbour block in the case");
         }
       make_geom(bd, i, k, B.g);
@@ -1811,7 +1857,8 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
   return guarded(c, [&] {
     if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_phase before canard_setup");
     if ((phase == CANARD_PH_MOVEF_A || phase == CANARD_PH_TIMESTEP || phase == CANARD_PH_VISCOUS ||
-         phase == CANARD_PH_FLUXES || phase == CANARD_PH_GCBC || phase == CANARD_PH_RKUPDATE) &&
+         phase == CANARD_PH_FLUXES || phase == CANARD_PH_GCBC || phase == CANARD_PH_RKUPDATE ||
+         phase == CANARD_PH_WALL) &&
         (nk < 1 || nk > 4))
       throw ApiError(CANARD_ERR_ARG, "stage index nk must be 1..4");
     // parameters of stage nk for the current dt / timo
@@ -1830,7 +1877,7 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
       case CANARD_PH_GCBC: ph_gcbc(c, params()); break;
       case CANARD_PH_SPONGE: ph_sponge(c); break;
       case CANARD_PH_RKUPDATE: ph_rk(c, params()); break;
-      case CANARD_PH_WALL: break;
+      case CANARD_PH_WALL: ph_wall(c, params()); break;
       case CANARD_PH_AVERAGE: ph_average(c); break;
       case CANARD_PH_ADVANCE: time_advance(c); break;
       default: throw ApiError(CANARD_ERR_ARG, "unknown phase");

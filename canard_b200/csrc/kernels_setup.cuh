@@ -234,6 +234,39 @@ __global__ void k_stage_params(const TimeDev* __restrict__ td, const CaseConst* 
   out[g] = p;
 }
 
+// wall_condition_update (src/mo_gcbc.f90:424-459) on the wall-face points of all
+// blocks. npex is 0 everywhere in the reference (gcbc_init sets it once and
+// nothing changes it), so each reset replaces the value; the expressions keep
+// the npex terms so that the arithmetic is the reference's. A point on several
+// wall faces gets their resets in the reference's face order (nn = 1..3, side
+// 0..1): kinds packed two bits each from the low end, 1 inviscid, 2 viscous.
+// The frame velocity is the one after movef of the stage (umfb).
+__global__ void k_wall_update(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                              const int* __restrict__ tb, const long long* __restrict__ tl,
+                              const int* __restrict__ tk, int n) {
+  const double gam = 1.4, hamhamm1 = (1.0 / gam) * (1.0 / (gam - 1.0));
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[tb[t]];
+    const long long l = tl[t], L = B.npad;
+    double* q = B.qa;
+    const double* umf = sp[B.case_id].umfb;
+    const double npx = 0.0;
+    for (int s = 0; s < 3; ++s) {
+      const int kind = (tk[t] >> (2 * s)) & 3;
+      if (kind == 0) break;
+      if (kind == 1) {
+        const double ke = (q[l + L] * q[l + L] + q[l + 2 * L] * q[l + 2 * L]) + q[l + 3 * L] * q[l + 3 * L];
+        q[l + 4 * L] = npx * q[l + 4 * L] + (1.0 - npx) * (hamhamm1 * pow(q[l], gam) + (0.5 * ke) / q[l]);
+      } else {
+        const double fctr = (1.0 - npx) * q[l];
+        for (int d = 0; d < 3; ++d) q[l + (d + 1) * L] = npx * q[l + (d + 1) * L] - fctr * umf[d];
+        const double ke = (q[l + L] * q[l + L] + q[l + 2 * L] * q[l + 2 * L]) + q[l + 3 * L] * q[l + 3 * L];
+        q[l + 4 * L] = npx * q[l + 4 * L] + (1.0 - npx) * (hamhamm1 * q[l] + (0.5 * ke) / q[l]);
+      }
+    }
+  }
+}
+
 // n = n + 1, timo = timo + dt (src/mo_canard_driver.f90:369-370)
 __global__ void k_time_advance(TimeDev* __restrict__ td, int ncases) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -67,9 +67,9 @@ def test_context_without_gpu_reports_an_error():
 
 
 def test_unsupported_configurations_are_rejected_before_device_work():
-    # walls are not on this path; precisions other than FP64 and FP32-mixed
-    # do not exist
-    blk = cases.BlockSpec(16, 16, 16, [[20, 10], [10, 10], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
+    # sub-domain interfaces (BC 40, nbpc > 1) are not on this path; precisions
+    # other than FP64 and FP32-mixed do not exist
+    blk = cases.BlockSpec(16, 16, 16, [[40, 10], [10, 10], [45, 45]], [[0, -1], [-1, -1], [0, 0]])
     cs = cases.CaseSpec([blk])
     h = ctypes.c_void_p()
     c, b = api._structs([cs])

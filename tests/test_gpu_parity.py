@@ -341,3 +341,72 @@ def test_restart_round_trip(tmp_path):
     b.step(3)
     for blk in range(len(cs.blocks)):
         assert rel_l2(b.state(blk), a.state(blk)) <= 1e-12
+
+
+def case_walls():
+    """Walls on three faces: xi side 1 and eta side 0 viscous (25), eta side 1
+    inviscid (20); xi side 0 non-reflecting, zeta periodic. Wall faces meet
+    along two edges (viscous then viscous, viscous then inviscid in the
+    reference's face order), and the frame moves at Mach 0.3 along x, so the
+    no-slip reset uses the frame velocity."""
+    blk = cases.BlockSpec(22, 18, 16, [[10, 25], [25, 20], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
+    Z, Y, X = blk.shape
+    x = np.linspace(-1, 1, X)
+    y = np.linspace(0, 1.2, Y)
+    z = np.linspace(0, 1, Z)
+    Zz, Yy, Xx = np.meshgrid(z, y, x, indexing="ij")
+    xyz = np.stack([Xx + 0.02 * np.sin(3 * Yy), Yy + 0.02 * np.sin(2 * Xx), Zz])
+    rho, u, v, w, p = cases.vortex_state(Xx, Yy, 0.0, 2.0, 0.3, 0.0, 0.6)
+    return cases.CaseSpec([blk], viscous=1, reoo=2000.0, amach=(0.3, 0.0, 0.0), xyz=[xyz],
+                          qa=[cases._conserved(rho, u, v, w, p)], name="walls")
+
+
+def test_wall_phases_match_oracle():
+    """The GCBC wall branch and wall_condition_update phase by phase. Every
+    phase is bit-exact except the inviscid wall's energy reset, which takes
+    rho^1.4 from the device's pow (the oracle: glibc's); there the two may
+    differ by an ulp, so that phase is compared to 2.3e-16 relative and the
+    oracle's state is carried over."""
+    cs = case_walls()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    t6 = [5, 1, 2.0e-3, 1.5e-3, 2.5e-3, 0.31]
+    o.set_time(t6)
+    g.set_time(t6)
+    for ph in (po.PH_FILTER, po.PH_COPYQO):
+        o.phase(ph)
+        g.phase(ph)
+    compare_state(o, g, cs, "filter", fields=(("qa", po.A_QA, api.F_QA),))
+    phases = PHASES[:6] + [(api.PH_WALL, "wall")] + PHASES[6:]
+    for nk in (1, 2):
+        o.phase(po.PH_MOVEF_A, nk)
+        for ph, label in phases:
+            o.phase(ph, nk)
+            g.phase(ph, nk)
+            if ph == api.PH_PRIM:
+                mo = o.get(0, po.A_SS1)
+                g.set_field(api.F_SS1, mo.reshape(g.field(api.F_SS1, 0).shape), 0)
+            if ph == api.PH_WALL:
+                a, c = o.get(0, po.A_QA), g.field(api.F_QA, 0).ravel()
+                assert np.all(np.abs(c - a) <= 2.3e-16 * np.abs(a)), "wall reset beyond 1 ulp"
+                g.set_state(0, a.reshape(g.state(0).shape))
+            compare_state(o, g, cs, f"{label} nk={nk}")
+
+
+def test_wall_steps_match_oracle():
+    cs = case_walls()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    o.step(12)
+    g.step(12)
+    err = rel_l2(g.state(0), o.state(0))
+    assert err <= 1e-10, err
+
+
+def test_wall_steps_fp32_mixed():
+    cs = case_walls()
+    o = po.Oracle(cs)
+    g = api.Context(cs, precision=api.FP32_MIXED)
+    o.step(12)
+    g.step(12)
+    assert rel_l2(g.state(0), o.state(0)) <= 1e-5
