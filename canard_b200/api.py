@@ -59,6 +59,7 @@ class _Case(ctypes.Structure):
 
 _lib = None
 _DP = ctypes.POINTER(ctypes.c_double)
+_FP = ctypes.POINTER(ctypes.c_float)
 
 
 def lib():
@@ -90,6 +91,11 @@ def lib():
         L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.canard_write_restart.argtypes = [vp, i32, i32, ctypes.c_char_p]
+        L.canard_record_enable.argtypes = [vp, i32]
+        L.canard_record_accumulate.argtypes = [vp]
+        L.canard_record_output.argtypes = [vp, i32, ctypes.POINTER(_FP), _DP]
+        L.canard_plt_write.argtypes = [ctypes.c_char_p, i32, i32, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.c_double, ctypes.POINTER(_FP)]
         L.canard_read_restart.argtypes = [vp, i32, i32, ctypes.c_char_p]
         L.canard_set_time.argtypes = [vp, i32, _DP]
         L.canard_mpigo.argtypes = [vp, ctypes.POINTER(_DP), i32, i32, i32, i32, i32, i32]
@@ -161,6 +167,25 @@ def read_restart_file(path, npts):
     if rc:
         raise CanardError(rc, f"canard_restart_read_file {path}")
     return t, q
+
+
+def plt_name(n: int) -> str:
+    """The reference's output file of output n (-1: the grid), relative to the
+    run directory (src/mo_io.f90:96-106)."""
+    return "data/grid.plt" if n == -1 else "data/n%03d.plt" % n
+
+
+def plt_write(path, n, arrays, time=0.0):
+    """write_output_file: one output (n >= 0: rho, u, v, w, p; n = -1: x, y, z)
+    of every block, arrays[b] of shape (nvar, lze+1, let+1, lxi+1) float32."""
+    arrs = [np.ascontiguousarray(a, np.float32) for a in arrays]
+    dims = (ctypes.c_int32 * (3 * len(arrs)))()
+    for b, a in enumerate(arrs):
+        dims[3 * b], dims[3 * b + 1], dims[3 * b + 2] = a.shape[3], a.shape[2], a.shape[1]
+    ptrs = (_FP * len(arrs))(*[a.ctypes.data_as(_FP) for a in arrs])
+    rc = lib().canard_plt_write(os.fsencode(path), n, len(arrs), dims, time, ptrs)
+    if rc:
+        raise CanardError(rc, f"canard_plt_write {path}")
 
 
 def compare_restart(path1, path2, npts, wtol=1e-15, report=None):
@@ -344,6 +369,37 @@ class Context:
         for b in range(len(self.cases[case].blocks)):
             path = os.path.join(directory, restart_name(b))
             self._check(lib().canard_write_restart(self.h, case, b, os.fsencode(path)))
+
+    def record_enable(self, on=True):
+        """Time-averaged recording on (qb = 0, dtsum = 0) or off."""
+        self._check(lib().canard_record_enable(self.h, 1 if on else 0))
+
+    def record_accumulate(self):
+        """qb += (dt/2)(qo + qa), dtsum += dt: after every step of a recorded run."""
+        self._check(lib().canard_record_accumulate(self.h))
+
+    def record_output(self, case=0):
+        """(per block float32 arrays (5, lze+1, let+1, lxi+1) of rho, u, v, w, p
+        of the average, output time); resets the average."""
+        arrs = [np.zeros((5,) + b.shape, np.float32) for b in self.cases[case].blocks]
+        ptrs = (_FP * len(arrs))(*[a.ctypes.data_as(_FP) for a in arrs])
+        t = np.zeros(1)
+        self._check(lib().canard_record_output(self.h, case, ptrs, _dp(t)))
+        return arrs, float(t[0])
+
+    def write_grid_plt(self, directory, case=0):
+        """The grid file written at start-up (data/grid.plt: x, y, z in FP32)."""
+        os.makedirs(os.path.join(directory, "data"), exist_ok=True)
+        cs = self.cases[case]
+        plt_write(os.path.join(directory, plt_name(-1)), -1, [np.asarray(x, np.float32) for x in cs.xyz])
+
+    def write_output(self, directory, n, case=0):
+        """An output of the recording: data/nNNN.plt of every block; returns the
+        output time."""
+        os.makedirs(os.path.join(directory, "data"), exist_ok=True)
+        arrs, t = self.record_output(case)
+        plt_write(os.path.join(directory, plt_name(n)), n, arrs, t)
+        return t
 
     def read_restart(self, directory, case=0):
         """read_restart_file for every block of a case (pathbase = directory)."""

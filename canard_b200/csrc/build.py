@@ -1,10 +1,10 @@
 """Builds libcanard_b200.so in-tree with nvcc for sm_100a.
 
-Four objects: the FP64 unit (canard.cu) with -fmad=false, so its kernels keep
+Five objects: the FP64 unit (canard.cu) with -fmad=false, so its kernels keep
 the reference's rounding order; the FP32 mixed-precision kernels
-(kernels_f32.cu) with multiply-add contraction; host set-up code (host.cpp)
-and the restart files (restart.cpp) with -ffp-contract=off. Objects go to
-csrc/_build.
+(kernels_f32.cu) with multiply-add contraction; host set-up code (host.cpp),
+the restart files (restart.cpp) and the Tecplot writer (plt.cpp) with
+-ffp-contract=off. Objects go to csrc/_build.
 """
 import os
 import subprocess
@@ -16,7 +16,8 @@ ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libcanard_b200.so")
 BUILD = os.path.join(HERE, "_build")
 # (source, FMA contraction allowed)
-UNITS = [("canard.cu", False), ("kernels_f32.cu", True), ("host.cpp", False), ("restart.cpp", False)]
+UNITS = [("canard.cu", False), ("kernels_f32.cu", True), ("host.cpp", False), ("restart.cpp", False),
+         ("plt.cpp", False)]
 DEPS = [u for u, _ in UNITS] + ["kernels.cuh", "kernels_f32.h", "kernels_setup.cuh", "kernels_tm.cuh", "host.h"]
 
 

@@ -178,6 +178,7 @@ struct CaseState {
 struct BlockState {
   BlockGeom g;
   double* arena = nullptr;
+  double* qb = nullptr;  // time-averaged recording (5 fields, padded rows), while recording is on
   BlockDev dev;  // host copy of the device descriptor
   double *lu[2][3] = {};       // [nt][dir]: 5 * L
   double luc[2][3][5] = {};    // bitwise-constant interior factors
@@ -284,6 +285,7 @@ struct canard_ctx {
   // the context), next stage's primitives inside the RK update
   bool fuse_sum = false, fuse_prim = true;
   // wall_condition_update: wall-face points, packed reset kinds (k_wall_update)
+  double* dtsum = nullptr;  // [ncases] recording interval, while recording is on
   int wall_n = 0;
   int* wall_tb = nullptr;
   long long* wall_tl = nullptr;
@@ -1496,6 +1498,8 @@ void destroy(canard_ctx* c) {
   cudaFree(c->fc_src); cudaFree(c->fc_dst); cudaFree(c->fc_cnt);
   cudaFree(c->prim_tb); cudaFree(c->prim_tl);
   cudaFree(c->wall_tb); cudaFree(c->wall_tl); cudaFree(c->wall_tk);
+  cudaFree(c->dtsum);
+  for (auto& b : c->blocks) cudaFree(b.qb);
   for (AvgDev* A : {&c->avg_pt, &c->avg_ln, &c->avg_sf}) {
     cudaFree(A->tb); cudaFree(A->tl); cudaFree(A->tfirst); cudaFree(A->tcount); cudaFree(A->sb); cudaFree(A->sl);
     cudaFree(A->snap);
@@ -1925,6 +1929,80 @@ int canard_read_restart(canard_ctx* c, int32_t icase, int32_t iblock, const char
     rc = canard_set_state(c, icase, iblock, qa.data());
     if (rc == CANARD_OK) rc = canard_set_time(c, icase, t);
     if (rc != CANARD_OK) throw ApiError(rc, c->err);
+  });
+}
+
+int canard_record_enable(canard_ctx* c, int32_t on) {
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    for (auto& b : c->blocks) {
+      cudaFree(b.qb);
+      b.qb = nullptr;
+    }
+    cudaFree(c->dtsum);
+    c->dtsum = nullptr;
+    if (!on) return;
+    for (auto& b : c->blocks) {
+      b.qb = dalloc<double>((size_t)5 * b.g.npad, c->st);
+      CK(cudaMemsetAsync(b.qb, 0, (size_t)5 * b.g.npad * sizeof(double), c->st));
+    }
+    c->dtsum = dalloc<double>(c->cases.size(), c->st);
+    CK(cudaMemsetAsync(c->dtsum, 0, c->cases.size() * sizeof(double), c->st));
+    CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_record_accumulate(canard_ctx* c) {
+  return guarded(c, [&] {
+    if (!c->dtsum) throw ApiError(CANARD_ERR_STATE, "recording is off (canard_record_enable)");
+    for (auto& b : c->blocks) {
+      const long long n = 5 * b.g.npad;
+      const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 8));
+      k_record_acc<<<grid, 256, 0, c->st>>>(b.qb, fptr(b, F_QO), fptr(b, F_QA), b.g.npad, b.g.X, b.g.Xp, c->dtime,
+                                            b.g.case_id);
+      CK(cudaGetLastError());
+    }
+    k_record_dtsum<<<(ncase(c) + 127) / 128, 128, 0, c->st>>>(c->dtsum, c->dtime, ncase(c));
+    CK(cudaGetLastError());
+    c->launches += (long long)c->blocks.size() + 1;
+  });
+}
+
+int canard_record_output(canard_ctx* c, int32_t icase, float* const* vart, double* time_out) {
+  return guarded(c, [&] {
+    if (!c->dtsum) throw ApiError(CANARD_ERR_STATE, "recording is off (canard_record_enable)");
+    if (!vart || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
+    const CaseState& cs = c->cases[icase];
+    size_t most = 0;
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) {
+      if (!vart[b - cs.b0]) throw ApiError(CANARD_ERR_ARG, "null output array");
+      const BlockGeom& g = c->blocks[b].g;
+      most = std::max(most, (size_t)5 * g.X * g.Y * g.Z);
+    }
+    float* dout = dalloc<float>(most, c->st);
+    c->transient.push_back(dout);
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) {
+      const BlockState& B = c->blocks[b];
+      const BlockGeom& g = B.g;
+      const int grid = (int)std::max<long long>(1, std::min<long long>((g.npad + 255) / 256, 148 * 8));
+      k_record_out<<<grid, 256, 0, c->st>>>(B.qb, fptr(B, F_QO), dout, g.X, g.Y, g.Z, g.Xp, g.npad, c->dtime,
+                                            c->dtsum, dev_slot(c, 3), icase);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(vart[b - cs.b0], dout, (size_t)5 * g.X * g.Y * g.Z * sizeof(float),
+                         cudaMemcpyDeviceToHost, c->st));
+    }
+    TimeDev d;
+    double dts = 0;
+    CK(cudaMemcpyAsync(&d, c->dtime + icase, sizeof(d), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&dts, c->dtsum + icase, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (time_out) *time_out = d.timo - 0.5 * dts;  // times(ndati) = timo - dtsum/2
+    // reset the recording of this case (dtsum = 0, qb = 0)
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b)
+      CK(cudaMemsetAsync(c->blocks[b].qb, 0, (size_t)5 * c->blocks[b].g.npad * sizeof(double), c->st));
+    CK(cudaMemsetAsync(c->dtsum + icase, 0, sizeof(double), c->st));
+    CK(cudaStreamSynchronize(c->st));
+    free_transient(c);
   });
 }
 

@@ -234,6 +234,50 @@ __global__ void k_stage_params(const TimeDev* __restrict__ td, const CaseConst* 
   out[g] = p;
 }
 
+// Time-averaged recording (src/mo_canard_driver.f90:373-378): after each step
+// qb = qb + (dt/2)(qo + qa) over the stored points of one block, and dtsum += dt.
+__global__ void k_record_acc(double* __restrict__ qb, const double* __restrict__ qo,
+                             const double* __restrict__ qa, long long npad, int X, int Xp,
+                             const TimeDev* __restrict__ td, int icase) {
+  const double fctr = 0.5 * td[icase].dt;
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < 5 * npad;
+       l += (long long)gridDim.x * blockDim.x)
+    if ((int)(l % Xp) < X) qb[l] = qb[l] + fctr * (qo[l] + qa[l]);
+}
+__global__ void k_record_dtsum(double* dtsum, const TimeDev* __restrict__ td, int ncases) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncases) dtsum[c] = dtsum[c] + td[c].dt;
+}
+
+// An output of the recording (src/mo_canard_driver.f90:379-402): the average
+// qb / dtsum (qo after the first step), written as FP32 rho, u, v, w (plus the
+// frame velocity) and p, variable-major in the reference's point order.
+__global__ void k_record_out(const double* __restrict__ qb, const double* __restrict__ qo,
+                             float* __restrict__ out, int X, int Y, int Z, int Xp, long long npad,
+                             const TimeDev* __restrict__ td, const double* __restrict__ dtsum,
+                             const StageParams* __restrict__ sp, int icase) {
+  const double gamm1 = 1.4 - 1.0;
+  const long long n = td[icase].n;
+  const double ra0 = 1.0 / dtsum[icase];
+  const double* umf = sp[icase].umfb;
+  const long long N = (long long)X * Y * Z;
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < npad;
+       l += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(l % Xp);
+    if (x >= X) continue;
+    const long long row = l / Xp;  // z * Y + y
+    const long long r = row * X + x;
+    double q[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) q[c] = (n == 1) ? qo[l + c * npad] : ra0 * qb[l + c * npad];
+    const double rr = 1.0 / q[0];
+    out[r] = (float)q[0];
+#pragma unroll
+    for (int c = 1; c < 4; ++c) out[r + c * N] = (float)(rr * q[c] + umf[c - 1]);
+    out[r + 4 * N] = (float)(gamm1 * (q[4] - (0.5 * rr) * ((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3])));
+  }
+}
+
 // wall_condition_update (src/mo_gcbc.f90:424-459) on the wall-face points of all
 // blocks. npex is 0 everywhere in the reference (gcbc_init sets it once and
 // nothing changes it), so each reset replaces the value; the expressions keep

@@ -153,6 +153,26 @@ int canard_restart_read_file(const char* path, double* time6, double* qa, int64_
 int canard_write_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 int canard_read_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 
+/* Time-averaged recording and Tecplot output (src/mo_canard_driver.f90:373-425,
+ * src/mo_io.f90:275-562). canard_record_enable(ctx, 1) allocates the average
+ * qb of every block (5 FP64 fields, zeroed; 0 frees it). After each
+ * canard_step(ctx, 1), canard_record_accumulate adds (dt/2)(qo + qa) to qb and
+ * dt to the case's dtsum, as the reference's loop does every step. On an output
+ * step, canard_record_output returns, per block of the case, the FP32 output
+ * variables rho, u, v, w, p (vart[b]: 5 x (lxi+1)(let+1)(lze+1), variable by
+ * variable, i fastest; velocities include the frame velocity) of qb / dtsum (of
+ * qo after the first step) and the output time timo - dtsum/2, then resets qb
+ * and dtsum. canard_plt_write writes one output in the reference's Tecplot
+ * binary layout (data/nNNN.plt, n >= 0, 5 variables; n = -1: data/grid.plt
+ * with x, y, z): dims holds (lxi+1, let+1, lze+1) per block, data[b] the
+ * block's variables in the same layout as vart. The reference's names have
+ * three digits: n <= 999 and at most 1000 blocks, else CANARD_ERR_ARG. */
+int canard_record_enable(canard_ctx* ctx, int32_t on);
+int canard_record_accumulate(canard_ctx* ctx);
+int canard_record_output(canard_ctx* ctx, int32_t icase, float* const* vart, double* time_out);
+int canard_plt_write(const char* path, int32_t n, int32_t nblocks, const int32_t* dims, double time,
+                     const float* const* data);
+
 /* The restart comparer (contrib/dcanard.f90:100-126): both files of npts
  * points are read and every value whose difference, relative to the first
  * file's value, exceeds wtol is counted in *nreported and, when report_path

@@ -410,3 +410,64 @@ def test_wall_steps_fp32_mixed():
     o.step(12)
     g.step(12)
     assert rel_l2(g.state(0), o.state(0)) <= 1e-5
+
+
+def reference_recording(o, cs, nsteps):
+    """The reference's time-averaged recording (src/mo_canard_driver.f90:373-402)
+    restated in numpy over the oracle's steps, for a frame at rest (umf = 0)."""
+    qb = [np.zeros(5 * b.npts) for b in cs.blocks]
+    dtsum = 0.0
+    for _ in range(nsteps):
+        o.step(1)
+        t = o.time()
+        dtsum = dtsum + t[2]
+        fctr = 0.5 * t[2]
+        for b in range(len(cs.blocks)):
+            qb[b] = qb[b] + fctr * (o.get(b, po.A_QO) + o.get(b, po.A_QA))
+    out = []
+    for b, blk in enumerate(cs.blocks):
+        q = (o.get(b, po.A_QO) if int(t[0]) == 1 else (1.0 / dtsum) * qb[b]).reshape(5, -1)
+        rr = 1.0 / q[0]
+        v = np.empty(q.shape, np.float32)
+        v[0] = q[0]
+        v[1:4] = rr * q[1:4] + 0.0
+        v[4] = (1.4 - 1.0) * (q[4] - (0.5 * rr) * ((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]))
+        out.append(v.reshape((5,) + blk.shape))
+    return out, t[5] - 0.5 * dtsum
+
+
+@pytest.mark.parametrize("nsteps", [1, 4])
+def test_recording_matches_the_reference_average(tmp_path, nsteps):
+    """qb accumulated after every step, averaged over dtsum (qo after the first
+    step), the FP32 output variables and the output time; a second output
+    starts from a reset average; the Tecplot file holds what record_output
+    returned."""
+    cs = case_periodic()
+    o = po.Oracle(cs)
+    g = api.Context(cs)
+    g.record_enable()
+    for _ in range(nsteps):
+        g.step(1)
+        g.record_accumulate()
+    arrs, t = g.record_output()
+    ref, tref = reference_recording(o, cs, nsteps)
+    np.testing.assert_allclose(arrs[0], ref[0], rtol=2.0 ** -23, atol=0)
+    assert abs(t - tref) <= 1e-14 * abs(tref)
+    # the next interval starts from zero
+    g.step(2)
+    g.record_accumulate()
+    arrs2, t2 = g.record_output()
+    assert t2 > t and np.all(np.isfinite(arrs2[0]))
+    # file output of a multi-block case
+    mb = api.Context(case_multiblock())
+    mb.record_enable()
+    for _ in range(4):  # dt is 0 for the first two steps (the reference's ramp)
+        mb.step(1)
+        mb.record_accumulate()
+    mb.write_grid_plt(str(tmp_path))
+    tt = mb.write_output(str(tmp_path), 0)
+    data = open(tmp_path / api.plt_name(0), "rb").read()
+    assert data[:8] == b"#!TDV112" and tt > 0
+    npts = sum(b.npts for b in mb.cases[0].blocks)
+    assert len(data) > 5 * 4 * npts
+    assert (tmp_path / api.plt_name(-1)).exists()
