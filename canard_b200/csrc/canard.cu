@@ -286,6 +286,10 @@ struct canard_ctx {
   bool fuse_sum = false, fuse_prim = true;
   // wall_condition_update: wall-face points, packed reset kinds (k_wall_update)
   double* dtsum = nullptr;  // [ncases] recording interval, while recording is on
+  // every block-face point (k_rk_faces)
+  int face_n = 0;
+  int* face_tb = nullptr;
+  long long* face_tl = nullptr;
   int wall_n = 0;
   int* wall_tb = nullptr;
   long long* wall_tl = nullptr;
@@ -905,9 +909,18 @@ void ph_rk(canard_ctx* c, const StageParams* sp) {
 void ph_rk_next(canard_ctx* c, const StageParams* sp, bool prim) {
   // the last stage stores the summed right-hand side (readable after a step)
   const int sum = c->fuse_sum ? (prim ? 1 : 2) : 0;
-  Timed tm(c, T_RK, ew_bytes(c, 11, (sum ? 15 : 5) + (sum == 2 ? 5 : 0) + (prim ? 7 : 0)));
-  if (c->f32()) launch_rk_next<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim);
-  else launch_rk_next<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim);
+  // FP32 stages 1-3 without GCBC, sponge or walls: the stage state only on the
+  // block faces (the FP32 fluxes read the primitives), stored by k_rk_faces
+  const bool faces = c->f32() && prim && c->fuse_sum && c->wall_n == 0 && c->face_n > 0;
+  Timed tm(c, T_RK, ew_bytes(c, 11 - (faces ? 5 : 0), (sum ? 15 : 5) + (sum == 2 ? 5 : 0) + (prim ? 7 : 0)));
+  if (c->f32()) launch_rk_next<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim, faces ? 0 : 1);
+  else launch_rk_next<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim, 1);
+  CK(cudaGetLastError());
+  if (faces) {
+    c->launches += 1;
+    launch_rk_faces<float>(std::max(1, std::min((c->face_n + 255) / 256, 1184)), c->st, c->dbd, sp, c->face_tb,
+                           c->face_tl, c->face_n);
+  }
   CK(cudaGetLastError());
 }
 
@@ -1324,6 +1337,26 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
     c->wall_tl = dupload(wl, c->st);
     c->wall_tk = dupload(wk, c->st);
   }
+  // every block-face point
+  {
+    std::vector<int> fb;
+    std::vector<long long> fl;
+    for (int b = 0; b < nb; ++b) {
+      const BlockGeom& g = c->blocks[b].g;
+      for (int z = 0; z < g.Z; ++z)
+        for (int y = 0; y < g.Y; ++y)
+          for (int x = 0; x < g.X; ++x)
+            if (x == 0 || x == g.X - 1 || y == 0 || y == g.Y - 1 || z == 0 || z == g.Z - 1) {
+              fb.push_back(b);
+              fl.push_back((long long)g.dev(x, y, z));
+            }
+    }
+    c->face_n = (int)fb.size();
+    if (c->face_n) {
+      c->face_tb = dupload(fb, c->st);
+      c->face_tl = dupload(fl, c->st);
+    }
+  }
   // the primitives are recomputed at averaged and at reset wall points
   std::vector<std::pair<int, long long>> pts;
   for (const AvgPlan* p : {&P, &Lp, &Sf})
@@ -1499,6 +1532,7 @@ void destroy(canard_ctx* c) {
   cudaFree(c->prim_tb); cudaFree(c->prim_tl);
   cudaFree(c->wall_tb); cudaFree(c->wall_tl); cudaFree(c->wall_tk);
   cudaFree(c->dtsum);
+  cudaFree(c->face_tb); cudaFree(c->face_tl);
   for (auto& b : c->blocks) cudaFree(b.qb);
   for (AvgDev* A : {&c->avg_pt, &c->avg_ln, &c->avg_sf}) {
     cudaFree(A->tb); cudaFree(A->tl); cudaFree(A->tfirst); cudaFree(A->tcount); cudaFree(A->sb); cudaFree(A->sl);
@@ -2167,6 +2201,9 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         std::vector<int> kinds{default_kind(c, grp, dir)};
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
         else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
+        // the filter acts on the FP64 state with an FP64 right-hand side in every
+        // kind; the FP64 elimination competes with the FP32 ones there
+        if (c->f32() && grp == 0) kinds.push_back(LK_F64);
         for (int k : kinds) {
           cand.push_back({k, 0});
           if (dir != 0 && k != LK_F64_TM)
@@ -2206,7 +2243,8 @@ int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind
     if (kind >= 0) {
       bool fits;
       if (!c->f32()) fits = kind == LK_F64 || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
-      else if (group == 0) fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L;
+      else if (group == 0)
+        fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64;
       else fits = kind == LK_F32 || kind == LK_F32_1L;
       if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
     }

@@ -1729,8 +1729,12 @@ __global__ void k_flux_sum(const BlockDev* __restrict__ bd) {
 // changes de in between; sum == 2 also stores it, so that de holds the last
 // stage's right-hand side after a step), prim computes the next stage's
 // primitives from the new state. Same operations in the same order as k_flux_sum, k_rk and
-// k_prim, so bit-identical to running them one after the other.
-template <class R>
+// k_prim, so bit-identical to running them one after the other. STORE_Q
+// false: the stage state is not stored (k_rk_faces stores it on the block
+// faces, the junction points); the FP32 fluxes of the next stage read the
+// primitives, and nothing else reads the interior state before the last stage
+// rewrites it.
+template <class R, bool STORE_Q = true>
 __global__ void k_rk_next(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
                           const CaseConst* __restrict__ cc, int sum, int prim) {
   FOR_POINTS(bd[blockIdx.y]) {
@@ -1749,7 +1753,7 @@ __global__ void k_rk_next(const BlockDev* __restrict__ bd, const StageParams* __
         dv = W.de[l + c * n];
       }
       q[c] = B.qo[l + c * n] - r1 * double(dv);
-      B.qa[l + c * n] = q[c];
+      if (STORE_Q) B.qa[l + c * n] = q[c];
     }
     if (prim) prim_point<R>(W, cc[B.case_id], l, n, q[0], q[1], q[2], q[3], q[4]);
   }
@@ -1981,10 +1985,34 @@ template <class R>
 void launch_flux_sum(dim3 g, cudaStream_t st, const BlockDev* bd) {
   k_flux_sum<R><<<g, 256, 0, st>>>(bd);
 }
+// the stage state of k_rk_next<R, false> at the listed points (the block
+// faces), with the same expression
+template <class R>
+__global__ void k_rk_faces(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                           const int* __restrict__ tb, const long long* __restrict__ tl, int ntg) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
+    const BlockDev& B = bd[tb[t]];
+    const Work<R> W = work<R>(B);
+    const long long l = tl[t], n = B.npad;
+    const double r1 = sp[B.case_id].dtk * B.yaco[l];
+    const R* r = W.scr;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const R dv = (r[l + (3 * c) * n] + r[l + (3 * c + 1) * n]) + r[l + (3 * c + 2) * n];
+      B.qa[l + c * n] = B.qo[l + c * n] - r1 * double(dv);
+    }
+  }
+}
 template <class R>
 void launch_rk_next(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc, int sum,
-                    int prim) {
-  k_rk_next<R><<<g, 256, 0, st>>>(bd, sp, cc, sum, prim);
+                    int prim, int store_q) {
+  if (store_q) k_rk_next<R, true><<<g, 256, 0, st>>>(bd, sp, cc, sum, prim);
+  else k_rk_next<R, false><<<g, 256, 0, st>>>(bd, sp, cc, sum, prim);
+}
+template <class R>
+void launch_rk_faces(int grid, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const int* tb,
+                     const long long* tl, int ntg) {
+  k_rk_faces<R><<<grid, 256, 0, st>>>(bd, sp, tb, tl, ntg);
 }
 template <class R>
 void launch_prim_points(int grid, cudaStream_t st, const BlockDev* bd, const CaseConst* cc, const int* tb,

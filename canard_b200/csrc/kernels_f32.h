@@ -23,7 +23,9 @@ CANARD_F32_EXTERN template void launch_flux_visc<float>(dim3, cudaStream_t, cons
 CANARD_F32_EXTERN template void launch_flux_sum<float>(dim3, cudaStream_t, const BlockDev*);
 CANARD_F32_EXTERN template void launch_rk<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*);
 CANARD_F32_EXTERN template void launch_rk_next<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*,
-                                                      const CaseConst*, int, int);
+                                                      const CaseConst*, int, int, int);
+CANARD_F32_EXTERN template void launch_rk_faces<float>(int, cudaStream_t, const BlockDev*, const StageParams*,
+                                                       const int*, const long long*, int);
 CANARD_F32_EXTERN template void launch_prim_points<float>(int, cudaStream_t, const BlockDev*, const CaseConst*,
                                                           const int*, const long long*, int);
 CANARD_F32_EXTERN template void launch_gcbc_setup<float>(int, cudaStream_t, const BlockDev*, const GcbcTask*,

@@ -224,8 +224,9 @@ int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, 
  * zeta line) and, on eta/zeta lines of 16..257 points, the kernel that keeps
  * the elimination results in tensor memory; mixed-precision contexts also try
  * the one-lane FP32 sweeps (32 lines per tile) against the split solve (16
- * lines per tile). The fastest
- * choice is installed in the step tables. Returns the number of groups
+ * lines per tile), and for the filter, which filters the FP64 state with an
+ * FP64 right-hand side in every kind, the FP64 elimination as well. The
+ * fastest choice is installed in the step tables. Returns the number of groups
  * (9) and fills up to nmax report rows of 6 doubles: group, direction
  * (0..2), chosen kind, chosen chunk count (0 = default), its ms per launch
  * and the default's. Call after canard_setup. */
