@@ -1453,11 +1453,17 @@ __global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restric
 
 // ---------------------------------------------------------------------------
 // element-wise kernels: blockIdx.y = block
-#define FOR_POINTS(BD)                                                              \
-  const BlockDev& B = BD;                                                           \
-  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < B.npad; \
-       l += (long long)gridDim.x * blockDim.x)                                      \
-    if ((int)(l % B.Xp) < B.X)
+// Grid-stride loop over the stored points of one block (pad columns x >= X
+// skipped). The column x is found by one division per thread and then
+// advanced with the stride, so no point pays an integer division.
+#define FOR_POINTS(BD)                                                                \
+  const BlockDev& B = BD;                                                             \
+  const long long fp_stride_ = (long long)gridDim.x * blockDim.x;                     \
+  const int fp_sx_ = (int)(fp_stride_ % B.Xp);                                        \
+  int fp_x_ = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) % B.Xp);       \
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < B.npad;   \
+       l += fp_stride_, fp_x_ = (fp_x_ + fp_sx_ >= B.Xp) ? fp_x_ + fp_sx_ - B.Xp : fp_x_ + fp_sx_) \
+    if (fp_x_ < B.X)
 
 constexpr double kGam = 1.4;
 #define KGAMM1 (kGam - 1.0)
