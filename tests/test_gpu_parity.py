@@ -471,3 +471,27 @@ def test_recording_matches_the_reference_average(tmp_path, nsteps):
     npts = sum(b.npts for b in mb.cases[0].blocks)
     assert len(data) > 5 * 4 * npts
     assert (tmp_path / api.plt_name(-1)).exists()
+
+
+@pytest.mark.parametrize("name", ["nonperiodic", "multiblock"])
+def test_tmem_line_kernel_with_interfaces_and_gcbc(name):
+    """The tensor-memory kernel where lines end on block interfaces (the
+    receive buffers of the contraction) and on GCBC faces (the line-end values
+    in drva): pinned on every eta/zeta group whose lines it takes, steps stay
+    bit-identical to the default tiles."""
+    cs = CASES[name]()
+    a = api.Context(cs)
+    b = api.Context(cs)
+    pinned = 0
+    for grp in ("filter", "viscous", "flux"):
+        for d in ("eta", "zeta"):
+            try:
+                b.set_line_kind(grp, d, "fp64-tmem")
+                pinned += 1
+            except api.CanardError as e:
+                assert e.code == api.ERR_ARG  # lines shorter than 16 points
+    assert pinned >= 3
+    a.step(4)
+    b.step(4)
+    for blk in range(len(cs.blocks)):
+        np.testing.assert_array_equal(b.state(blk), a.state(blk))
