@@ -910,8 +910,10 @@ void ph_rk_next(canard_ctx* c, const StageParams* sp, bool prim) {
   // the last stage stores the summed right-hand side (readable after a step)
   const int sum = c->fuse_sum ? (prim ? 1 : 2) : 0;
   // FP32 stages 1-3 without GCBC, sponge or walls: the stage state only on the
-  // block faces (the FP32 fluxes read the primitives), stored by k_rk_faces
-  const bool faces = c->f32() && prim && c->fuse_sum && c->wall_n == 0 && c->face_n > 0;
+  // block faces (the FP32 fluxes read the primitives), stored by k_rk_faces;
+  // worth it while the face points are few (large blocks)
+  const bool faces = c->f32() && prim && c->fuse_sum && c->wall_n == 0 && c->face_n > 0 &&
+                     c->face_n < 0.05 * valid_points(c);
   Timed tm(c, T_RK, ew_bytes(c, 11 - (faces ? 5 : 0), (sum ? 15 : 5) + (sum == 2 ? 5 : 0) + (prim ? 7 : 0)));
   if (c->f32()) launch_rk_next<float>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim, faces ? 0 : 1);
   else launch_rk_next<double>(ew_grid(c), c->st, c->dbd, sp, c->dcc, sum, prim, 1);
