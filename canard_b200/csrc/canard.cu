@@ -265,6 +265,12 @@ struct canard_ctx {
   // persistent send chains of all three directions, so field m+1's filter
   // depends on field m's face values between its sweeps.
   Table<LineTask> filt[5][3], visc[3], flux[3];
+  // FP32-mixed: the five fields filtered together along each direction (in
+  // kNnf order). The fields are independent; the one change is the third
+  // contracted value, which takes the send chain's exact value instead of
+  // its rounded running update (a last-bit difference in FP64 face values).
+  Table<LineTask> filt5[3];
+  Table<FaceTask> mp_filt5[3];
   // line-tile choice per [group: 0 filter, 1 viscous gradients, 2 fluxes][direction]
   // (kind < 0: the precision's default); set by canard_autotune
   struct TuneChoice { int kind = -1; int nc = 0; } tune[3][3];
@@ -755,6 +761,13 @@ void stage_params(canard_ctx* c, int nk0, int nk1, int to_slot = -1) {
 // filtering (src/mo_canard_driver.f90:232-251): for each field, the
 // interface contraction and the filter sweep along each direction in turn
 void ph_filter(canard_ctx* c) {
+  if (c->f32()) {
+    for (int inn = 1; inn <= 3; ++inn) {
+      launch_mpigo(c, c->mp_filt5[inn - 1]);
+      launch_line(c, c->filt5[inn - 1], kNnf[inn - 1] - 1, 1);
+    }
+    return;
+  }
   for (int m = 1; m <= 5; ++m)
     for (int inn = 1; inn <= 3; ++inn) {
       launch_mpigo(c, c->mp_filt[m - 1][inn - 1]);
@@ -1126,12 +1139,26 @@ void free_line_table(Table<LineTask>& T) {
   T = Table<LineTask>{};
 }
 
+// the filter tasks of the five fields along one direction (FP32-mixed step)
+std::vector<LineTask> filter_tasks5(canard_ctx* c, int dir, int kind, int nc, bool scratch = false) {
+  std::vector<LineTask> v;
+  for (int m = 1; m <= 5; ++m) {
+    auto w = group_tasks(c, 0, dir, m, kind, nc, scratch);
+    v.insert(v.end(), w.begin(), w.end());
+  }
+  return v;
+}
+
 void build_line_tables(canard_ctx* c) {
-  for (int m = 1; m <= 5; ++m)
-    for (int inn = 1; inn <= 3; ++inn) {
-      const int dir = kNnf[inn - 1] - 1, k = group_kind(c, 0, dir);
-      c->filt[m - 1][inn - 1] = make_line_table(c, group_tasks(c, 0, dir, m, k, c->tune[0][dir].nc), dir, false, k);
-    }
+  for (int inn = 1; inn <= 3; ++inn) {
+    const int dir = kNnf[inn - 1] - 1, k = group_kind(c, 0, dir);
+    if (c->f32())
+      c->filt5[inn - 1] = make_line_table(c, filter_tasks5(c, dir, k, c->tune[0][dir].nc), dir, false, k);
+    else
+      for (int m = 1; m <= 5; ++m)
+        c->filt[m - 1][inn - 1] =
+            make_line_table(c, group_tasks(c, 0, dir, m, k, c->tune[0][dir].nc), dir, false, k);
+  }
   for (int dir = 0; dir < 3; ++dir) {
     int k = group_kind(c, 1, dir);
     c->visc[dir] = make_line_table(c, group_tasks(c, 1, dir, 0, k, c->tune[1][dir].nc), dir, false, k);
@@ -1144,7 +1171,11 @@ void build_line_tables(canard_ctx* c) {
 void rebuild_line_tables(canard_ctx* c) {
   for (int m = 0; m < 5; ++m)
     for (int i = 0; i < 3; ++i) free_line_table(c->filt[m][i]);
-  for (int d = 0; d < 3; ++d) { free_line_table(c->visc[d]); free_line_table(c->flux[d]); }
+  for (int d = 0; d < 3; ++d) {
+    free_line_table(c->filt5[d]);
+    free_line_table(c->visc[d]);
+    free_line_table(c->flux[d]);
+  }
   for (auto& g : c->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   build_line_tables(c);
@@ -1157,12 +1188,24 @@ void build_tables(canard_ctx* c) {
     return f32 ? static_cast<void*>(gptr(c->blocks[b], f32_field)) : static_cast<void*>(fptr(c->blocks[b], f64_field));
   };
   build_line_tables(c);
-  for (int m = 1; m <= 5; ++m)
-    for (int inn = 1; inn <= 3; ++inn) {
-      const int dir = kNnf[inn - 1] - 1;
-      c->mp_filt[m - 1][inn - 1] = make_face_table(
-          c, face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }), false);
+  for (int inn = 1; inn <= 3; ++inn) {
+    const int dir = kNnf[inn - 1] - 1;
+    if (f32) {
+      // the faces of this direction only, no send chain
+      std::vector<FaceTask> all;
+      for (int m = 1; m <= 5; ++m)
+        for (FaceTask t : face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }))
+          if (t.nn == dir + 1) {
+            t.chain = nullptr;
+            all.push_back(t);
+          }
+      c->mp_filt5[inn - 1] = make_face_table(c, all, false);
+    } else {
+      for (int m = 1; m <= 5; ++m)
+        c->mp_filt[m - 1][inn - 1] = make_face_table(
+            c, face_tasks(c, 1, 0, m, dir, [&](int b, int) { return fptr(c->blocks[b], F_QA + m - 1); }), false);
     }
+  }
   {
     std::vector<FaceTask> all;
     for (int m = 2; m <= 5; ++m) {
@@ -1525,9 +1568,9 @@ void destroy(canard_ctx* c) {
   auto ft = [](auto& T) { cudaFree(T.tasks); cudaFree(T.first); };
   auto fl = [](Table<LineTask>& T) { cudaFree(T.maps); };
   for (int m = 0; m < 5; ++m) for (int i = 0; i < 3; ++i) fl(c->filt[m][i]);
-  for (int d = 0; d < 3; ++d) { fl(c->visc[d]); fl(c->flux[d]); }
+  for (int d = 0; d < 3; ++d) { fl(c->filt5[d]); fl(c->visc[d]); fl(c->flux[d]); }
   for (int m = 0; m < 5; ++m) for (int i = 0; i < 3; ++i) { ft(c->filt[m][i]); ft(c->mp_filt[m][i]); }
-  for (int d = 0; d < 3; ++d) { ft(c->visc[d]); ft(c->flux[d]); }
+  for (int d = 0; d < 3; ++d) { ft(c->filt5[d]); ft(c->mp_filt5[d]); ft(c->visc[d]); ft(c->flux[d]); }
   ft(c->mp_visc); ft(c->mp_flux); ft(c->gc_setup); ft(c->sponge);
   for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) ft(c->gc_upd[d][s]);
   cudaFree(c->fc_src); cudaFree(c->fc_dst); cudaFree(c->fc_cnt);
@@ -2214,7 +2257,9 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         double best = 1e300, def = 0;
         canard_ctx::TuneChoice pick;
         for (size_t i = 0; i < cand.size(); ++i) {
-          auto v = group_tasks(c, grp, dir, 1, cand[i].first, cand[i].second, true);
+          // the step's launch shape: FP32-mixed filters the five fields at once
+          auto v = (grp == 0 && c->f32()) ? filter_tasks5(c, dir, cand[i].first, cand[i].second, true)
+                                          : group_tasks(c, grp, dir, 1, cand[i].first, cand[i].second, true);
           if (v.empty()) continue;
           Table<LineTask> T = make_line_table(c, v, dir, true, cand[i].first);
           if (T.smem > 227 * 1024) continue;

@@ -106,6 +106,7 @@ struct FaceTask {
   const void* dstf;     // receiver field column (coordinate-jump correction)
   void* recv;           // receiver buffer [comp][jk] for (direction, side, m)
   double* chain;        // sender's persistent send(:,nt+1,side) of the filter
+                        // (null: the fields are filtered direction-major, no chain)
   const DevScheme* sc;
   int nn, sb, nt, exch, corr, iik;
   double ra0k;
@@ -1431,9 +1432,13 @@ __global__ void k_mpigo(const FaceTask* __restrict__ tasks, const int* __restric
     T snd1 = t1 - resk * T(sc->pbcot[nt][1]);
     T snd2 = 0;
     if (nt == 1) {
-      const T old = T(F.chain[jk]);
-      snd2 = old + ((sap0 - resk) - old);
-      F.chain[jk] = double(snd2);
+      if (F.chain) {
+        const T old = T(F.chain[jk]);
+        snd2 = old + ((sap0 - resk) - old);
+        F.chain[jk] = double(snd2);
+      } else {
+        snd2 = sap0 - resk;  // the chain's exact value, without its rounding
+      }
     }
     if (F.exch) {
       T* recv = static_cast<T*>(F.recv);
