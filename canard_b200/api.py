@@ -110,6 +110,7 @@ def lib():
         L.canard_timer_name.restype = ctypes.c_char_p
         L.canard_timer_name.argtypes = [i32]
         L.canard_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.canard_selftest_wait.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.canard_deriv_noalloc.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, ctypes.c_double,
                                            ctypes.c_double, vp]
         L.canard_coeffs.argtypes = [ctypes.c_double, ctypes.c_double, _DP]
@@ -332,6 +333,13 @@ class Context:
         v = ctypes.c_int64()
         self._check(lib().canard_launch_count(self.h, ctypes.byref(v)))
         return int(v.value)
+
+    def selftest_wait(self):
+        """Runs the bounded-wait self-test: returns (status code, seconds);
+        the code is ERR_TIMEOUT when the device wait gave up as designed."""
+        s = ctypes.c_double()
+        code = lib().canard_selftest_wait(self.h, ctypes.byref(s))
+        return code, s.value
 
     def field(self, which, b=0, case=0):
         blk = self.cases[case].blocks[b]

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -2338,6 +2339,19 @@ int canard_launch_count(canard_ctx* c, int64_t* count) {
   if (!c || !count) return CANARD_ERR_ARG;
   *count = c->launches;
   return CANARD_OK;
+}
+
+int canard_selftest_wait(canard_ctx* c, double* seconds) {
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->st));
+    const auto t0 = std::chrono::steady_clock::now();
+    c->launches += 1;
+    k_wait_selftest<<<1, 32, 0, c->st>>>(c->derr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    sync_check(c);  // reports the flag (CANARD_ERR_TIMEOUT) and clears it
+  });
 }
 
 }  // extern "C"

@@ -20,7 +20,8 @@ namespace canard {
 constexpr int kLanes = 32;            // lines per tile (one warp, one line per lane)
 constexpr int kErrTimeout = 4;
 constexpr int kErrOverflow = 8;  // dt == 0 after step 2 ("Canard: Overflow.")
-constexpr long long kSpinLimit = 1LL << 28;  // bounded mbarrier waits
+constexpr long long kSpinLimit = 1LL << 28;  // bounded mbarrier waits: polls at most
+constexpr unsigned long long kWaitNs = 500000000ull;  // and 0.5 s of %globaltimer
 
 struct DevScheme {
   double pbci[2][2][12];  // [nt][side][i]
@@ -142,17 +143,38 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 // Bounded wait for phase `parity`; returns false if the limit expired.
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// false after kWaitNs (a copy that never completes sets the error flag in the
+// caller instead of holding the GPU)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < 16; ++it)
+    if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
   for (long long it = 0; it < kSpinLimit; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
+}
+// a kernel launched after a bounded wait gave up does no work (the host
+// reports the error at its next synchronisation); uniform over the warp
+__device__ __forceinline__ bool error_pending(const int* err) {
+  int e = 0;
+  if ((threadIdx.x & 31) == 0) e = *reinterpret_cast<const volatile int*>(err);
+  return __shfl_sync(0xffffffffu, e, 0) != 0;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -773,6 +795,7 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   TT* s = reinterpret_cast<TT*>(smem_raw + 128);
   const int lane = threadIdx.x;
   TRACE(0)
+  if (error_pending(err)) return;
   const int ti = find_task(tile0s, ntasks, blockIdx.x);
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
@@ -1236,6 +1259,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   TT* s = reinterpret_cast<TT*>(smem_raw + 128);
   const int lane = threadIdx.x;
   const int half = lane >> 4, li = lane & (kHalf - 1);
+  if (error_pending(err)) return;
   const int ti = find_task(tile0s, ntasks, blockIdx.x);
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);

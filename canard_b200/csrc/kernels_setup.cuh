@@ -311,6 +311,17 @@ __global__ void k_wall_update(const BlockDev* __restrict__ bd, const StageParams
   }
 }
 
+// Self-test of the bounded waits: one warp waits on an mbarrier that nothing
+// arrives at. The wait gives up after kWaitNs and raises the timeout flag, as
+// a line kernel does when a copy never lands; no fault, no trap.
+__global__ void k_wait_selftest(int* __restrict__ err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncwarp();
+  const bool ok = mbar_wait(&bar, 0);
+  if (!ok && threadIdx.x == 0) atomicExch(err, kErrTimeout);
+}
+
 // n = n + 1, timo = timo + dt (src/mo_canard_driver.f90:369-370)
 __global__ void k_time_advance(TimeDev* __restrict__ td, int ncases) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -176,6 +176,14 @@ struct TmStream {
       if (q < g.nch) in.issue_chunk(map, g, q);
     }
   }
+  // every box of the tile lands before the ring is reused (all rows have been
+  // read: each wait first frees the boxes before it, which issues the rest)
+  __device__ __forceinline__ void finish() {
+    while (ok && arrived < g.nch - 1) {
+      release_below((arrived + 1) * kTmChunk);
+      ensure((arrived + 1) * kTmChunk);
+    }
+  }
   __device__ __forceinline__ double S(int r) const { return in.ring[(size_t)(r % kTmRing) * kLanes + in.lane]; }
   __device__ __forceinline__ double TOP(int r) const {
     return in.top[(size_t)(r - (g.L - kTmChunk)) * kLanes + in.lane];
@@ -358,6 +366,7 @@ __device__ __forceinline__ bool tm_forward_deriv(TmStream<DIR>& R, const LuRows<
   });
   if (i < 0) return false;
   for (; i <= last; ++i) {
+    R.release_below(i + 2);  // with a ring of two boxes the last box is issued from here
     R.ensure(i + 2);
     if (!R.ok) return false;
     const double w4 = R.S(i + 2);
@@ -373,7 +382,7 @@ __device__ __forceinline__ bool tm_forward_deriv(TmStream<DIR>& R, const LuRows<
     aN1 = a;
     aN = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
   }
-  R.ensure(N);  // every box of the tile has landed (none left in flight)
+  R.finish();  // every box of the tile has landed (none left in flight)
   return R.ok;
 }
 
@@ -467,6 +476,7 @@ __device__ __forceinline__ bool tm_forward_filter(TmStream<DIR>& R, const LuRows
   });
   if (i < 0) return false;
   for (; i <= last; ++i) {
+    R.release_below(i + 3);
     R.ensure(i + 3);
     if (!R.ok) return false;
     const double w6 = R.S(i + 3);
@@ -486,7 +496,7 @@ __device__ __forceinline__ bool tm_forward_filter(TmStream<DIR>& R, const LuRows
     aN1 = a;
     aN = (bn - __ldg(F.l1 + N) * am2) - __ldg(F.l2 + N) * am1;
   }
-  R.ensure(N);
+  R.finish();
   return R.ok;
 }
 
@@ -502,6 +512,14 @@ __global__ void __launch_bounds__(kTmWarps * 32) k_line_tm(const LineTask* __res
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint32_t* tbase = reinterpret_cast<uint32_t*>(smem_raw);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    // after an earlier bounded wait gave up: no work (uniform over the CTA,
+    // before any barrier or TMEM allocation)
+    __shared__ int stop;
+    if (threadIdx.x == 0) stop = *reinterpret_cast<const volatile int*>(err);
+    __syncthreads();
+    if (stop) return;
+  }
   TmIn<DIR> in;
   in.lane = lane;
   in.bars = reinterpret_cast<uint64_t*>(smem_raw + kTmBarOff) + w * 8;

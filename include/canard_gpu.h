@@ -256,6 +256,14 @@ int canard_get_timers(canard_ctx* ctx, double* ms, double* launches, double* byt
 const char* canard_timer_name(int32_t family);
 int canard_launch_count(canard_ctx* ctx, int64_t* count);
 
+/* Self-test of the bounded device waits (no counterpart in the reference):
+ * runs one kernel whose mbarrier wait can never complete. Like every wait of
+ * the line kernels it gives up after 0.5 s and raises the context's error
+ * flag, so the call returns CANARD_ERR_TIMEOUT, with *seconds (may be NULL)
+ * the host time it took; the flag is cleared and the context stays usable.
+ * Line kernels launched while the flag is up return without work. */
+int canard_selftest_wait(canard_ctx* ctx, double* seconds);
+
 /* Step execution. canard_step runs each time step as one CUDA graph (captured
  * on the first step of each kind: with and without the every-tenth-step dt
  * reduction) whose kernels read the device-resident time state, so a step

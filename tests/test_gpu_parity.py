@@ -294,6 +294,22 @@ def test_non_finite_state_is_reported():
     assert e.value.code == api.ERR_NAN
 
 
+def test_bounded_wait_reports_timeout_and_context_stays_usable():
+    """A device wait that can never complete (an mbarrier nothing arrives at)
+    gives up after about half a second and is reported as ERR_TIMEOUT; the
+    same context then steps exactly like a fresh one."""
+    cs = case_periodic()
+    a = api.Context(cs)
+    b = api.Context(cs)
+    code, sec = b.selftest_wait()
+    assert code == api.ERR_TIMEOUT, code
+    assert 0.3 < sec < 10.0, sec
+    assert "bounded device wait" in api.lib().canard_last_error(b.h).decode()
+    a.step(3)
+    b.step(3)
+    np.testing.assert_array_equal(b.state(0), a.state(0))
+
+
 @pytest.mark.parametrize("shape", [(24, 20, 16), (16, 200, 140), (16, 256, 32)])
 def test_tmem_line_kernel_bit_identical(shape):
     """The FP64 line kernel that keeps the elimination results in tensor
