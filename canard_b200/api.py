@@ -88,6 +88,8 @@ def lib():
         L.canard_get_time.argtypes = [vp, i32, _DP]
         L.canard_restart_write_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
         L.canard_restart_read_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
+        L.canard_grid_write_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
+        L.canard_grid_read_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
         L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.canard_write_restart.argtypes = [vp, i32, i32, ctypes.c_char_p]
@@ -168,6 +170,31 @@ def read_restart_file(path, npts):
     if rc:
         raise CanardError(rc, f"canard_restart_read_file {path}")
     return t, q
+
+
+def grid_name(mb: int) -> str:
+    """The reference's grid file of block mb, relative to the run directory:
+    'misc/grid' + three digits + '.dat', 16 characters, which fit its
+    character(16) variable (src/mo_io.f90:31, 115)."""
+    return "misc/grid%03d.dat" % mb
+
+
+def write_grid_file(path, xyz):
+    """One block's grid file in the reference's format; xyz is (3, ...) in
+    the reference layout (ss(0:lmx, 3))."""
+    g = np.ascontiguousarray(xyz, np.float64).reshape(3, -1)
+    rc = lib().canard_grid_write_file(os.fsencode(path), _dp(g), g.shape[1])
+    if rc:
+        raise CanardError(rc, f"canard_grid_write_file {path}")
+
+
+def read_grid_file(path, npts):
+    """xyz (3, npts) of the grid file of a block of npts points."""
+    g = np.zeros((3, npts))
+    rc = lib().canard_grid_read_file(os.fsencode(path), _dp(g), npts)
+    if rc:
+        raise CanardError(rc, f"canard_grid_read_file {path}")
+    return g
 
 
 def plt_name(n: int) -> str:

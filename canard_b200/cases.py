@@ -274,3 +274,112 @@ def noise_fields(blk: BlockSpec, nfields: int = 5, seed: int = 20261203, kmax: i
         modes = modes + np.sin(kk * 2 * np.pi * i / max(X - 1, 1)) + np.sin(kk * 2 * np.pi * j / max(Y - 1, 1)) \
             + np.sin(kk * 2 * np.pi * k / max(Z - 1, 1))
     return out + modes[None]
+
+
+# ---------------------------------------------------------------------------
+# The reference's own grid generators and initial condition (host code: they
+# run once, before the device holds anything). Coordinates are evaluated with
+# the Fortran expressions in the same order, so the grid files they give
+# (api.write_grid_file) match the reference's byte for byte where libm is not
+# involved (these generators use only +, -, *, /).
+
+def gridtoy(lxi0: int, let0: int, lze0: int, doml0: float, doml1: float, domh: float, span: float) -> np.ndarray:
+    """gridtoy (src/mo_gridgen.f90:510-575): one Cartesian block of
+    (lxi0+1) x (let0+1) x (lze0+1) points, x = -doml0 + i (doml1+doml0)/lxi0,
+    y = -domh + j 2 domh/let0, z = span ((lze0-k)/lze0 - 1/2). Returns xyz
+    (3, lze0+1, let0+1, lxi0+1) in the reference layout."""
+    ra0 = (doml1 + doml0) / lxi0
+    ra1 = 2.0 * domh / let0
+    x = -doml0 + (np.arange(lxi0 + 1, dtype=np.float64) - 0.0) * ra0
+    y = -domh + (np.arange(let0 + 1, dtype=np.float64) - 0.0) * ra1
+    z = span * ((lze0 - np.arange(lze0 + 1, dtype=np.float64)) / lze0 - 0.5)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    return np.stack([X, Y, Z])
+
+
+def gridtoy_multi(lxi0: int, lxi1: int, lxi2: int, let0: int, lze0: int, doml0: float, doml1: float,
+                  domh: float, span: float) -> List[np.ndarray]:
+    """gridtoy_multi (src/mo_gridgen.f90:577-654): six Cartesian blocks, three
+    along x (lxi0, lxi1, lxi2 cells) by two along y (let0 cells each), sharing
+    their interface points. Block mb covers i in its column (mb % 3) and j in
+    its row (mb // 3) of the global (lxi0+lxi1+lxi2+3) x (2 let0+2) point
+    array. Returns xyz (3, lze0+1, let0+1, lxi_mb+1) per block."""
+    lxit = lxi0 + lxi1 + lxi2 + 2
+    lett = 2 * let0 + 1
+    lxis1 = lxi0 + 1
+    lxie1 = lxis1 + lxi1
+    lxis2 = lxie1 + 1
+    cols = [(0, lxi0, 0.0), (lxis1, lxie1, 1.0), (lxis2, lxit, 2.0)]
+    rows = [(0, let0, 0.0), (let0 + 1, lett, 1.0)]
+    ra0 = (doml1 + doml0) / (lxi0 + lxi1 + lxi2)
+    ra1 = domh / (2.0 * let0) * 2.0
+    z = span * ((lze0 - np.arange(lze0 + 1, dtype=np.float64)) / lze0 - 0.5)
+    out = []
+    for mb in range(6):
+        is_, ie, ra2 = cols[mb % 3]
+        js, je, ra3 = rows[mb // 3]
+        x = -doml0 + (np.arange(is_, ie + 1, dtype=np.float64) - ra2) * ra0
+        y = -domh + (np.arange(js, je + 1, dtype=np.float64) - ra3) * ra1
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        out.append(np.stack([X, Y, Z]))
+    return out
+
+
+def initialo(xyz: np.ndarray) -> np.ndarray:
+    """The reference's initial condition (initialo, src/mo_physics.f90:117-140):
+    a vortex at the origin, k1 = 12.5, radius 1, k2 = 1,
+    ao = k2/(2 pi) sqrt(exp(1 - k1^2 (x^2 + y^2))), rho = (1 - (gamma-1)/2 ao^2)^(1/(gamma-1)),
+    u = k1 y ao, v = -k1 x ao, w = 0, rho E = rho^gamma/(gamma(gamma-1)) + rho |u|^2/2.
+    Returns qa (5, ...) on the points of xyz (3, ...)."""
+    x, y = xyz[0], xyz[1]
+    radv, k1, k2 = 1.0, 12.5, 1.0
+    gamm1 = GAM - 1.0
+    ao = k2 / 2.0 / math.pi * np.sqrt(np.exp(1 - k1 * k1 * (x * x + y * y) / (radv * radv)))
+    bo = (1.0 - 0.5 * gamm1 * ao * ao) ** (1.0 / gamm1)
+    v1 = k1 * y * ao / radv
+    v2 = -k1 * x * ao / radv
+    hv2 = 0.5 * ((v1 * v1 + v2 * v2) + 0.0)
+    q = np.empty((5,) + x.shape)
+    q[0] = bo
+    q[1] = bo * v1
+    q[2] = bo * v2
+    q[3] = bo * 0.0
+    q[4] = (1.0 / GAM) * (1.0 / gamm1) * bo ** GAM + hv2 * bo
+    return q
+
+
+def reference_validation(lxi0: int = 50, let0: int = 50, lze0: int = 16) -> CaseSpec:
+    """The reference's validation run (run/exp.validation): one block from
+    gridtoy (doml0 0.5, doml1 1.0, domh 0.5, span 0.1), non-reflecting GCBC on
+    the xi and eta faces, periodic in zeta, initialo's vortex in a Mach 0.3
+    frame, Re 5e5, Tinf 300 K, fltk 0.65, fltrbc 0.9, CFL 1.4. Its input file
+    misspells the sponge namelist (no '&'), so szco keeps its zero default and
+    there is no sponge. The reference splits the block into 2 x 2 sub-domains
+    (nbpc); here it is one sub-domain."""
+    blk = BlockSpec(lxi0, let0, lze0, [[BC_NON_REFLECTIVE] * 2, [BC_NON_REFLECTIVE] * 2, [BC_PERIODIC] * 2],
+                    [[-1, -1], [-1, -1], [0, 0]])
+    xyz = gridtoy(lxi0, let0, lze0, 0.5, 1.0, 0.5, 0.1)
+    return CaseSpec([blk], viscous=1, fltk=0.65, fltrbc=0.9, reoo=500000.0, tempoo=300.0, amach=(0.3, 0.0, 0.0),
+                    nsmf=1, cfl=1.4, doml0=0.5, doml1=1.0, xyz=[xyz], qa=[initialo(xyz)],
+                    name=f"validation{lxi0}x{let0}x{lze0}")
+
+
+def reference_toy(lxi: int = 100, let0: int = 100, lze0: int = 16) -> CaseSpec:
+    """The reference's toy run (run/exp.toy): six blocks from gridtoy_multi
+    (lxi0 = lxi1 = lxi2 = lxi; doml0 0.5, doml1 1.0, domh 0.5, span 0.1),
+    straight interfaces (BC 35) between them, non-reflecting GCBC at the x
+    ends, periodic in eta across the two rows and in zeta, initialo's vortex
+    in a Mach 0.3 frame, Re 5e5, fltk 0.65, fltrbc 0.9, CFL 1.4; no sponge
+    (the input misspells its namelist). The reference splits each block into
+    4 x 2 sub-domains; here each block is one."""
+    nr, st, pe = BC_NON_REFLECTIVE, BC_INTER_STRAIGHT, BC_PERIODIC
+    # nbbc / mbcd of run/exp.toy, per block [direction][side]
+    nbbc = [[[nr, st], [pe, st], [pe, pe]], [[st, st], [pe, st], [pe, pe]], [[st, nr], [pe, st], [pe, pe]],
+            [[nr, st], [st, pe], [pe, pe]], [[st, st], [st, pe], [pe, pe]], [[st, nr], [st, pe], [pe, pe]]]
+    mbcd = [[[-1, 1], [3, 3], [0, 0]], [[0, 2], [4, 4], [1, 1]], [[1, -1], [5, 5], [2, 2]],
+            [[-1, 4], [0, 0], [3, 3]], [[3, 5], [1, 1], [4, 4]], [[4, -1], [2, 2], [5, 5]]]
+    xyz = gridtoy_multi(lxi, lxi, lxi, let0, lze0, 0.5, 1.0, 0.5, 0.1)
+    blocks = [BlockSpec(lxi, let0, lze0, nbbc[m], mbcd[m]) for m in range(6)]
+    return CaseSpec(blocks, viscous=1, fltk=0.65, fltrbc=0.9, reoo=500000.0, tempoo=300.0, amach=(0.3, 0.0, 0.0),
+                    nsmf=1, cfl=1.4, doml0=0.5, doml1=1.0, xyz=xyz, qa=[initialo(g) for g in xyz],
+                    name=f"toy6x{lxi}x{let0}x{lze0}")

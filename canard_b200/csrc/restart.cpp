@@ -1,5 +1,6 @@
-// Restart files in the reference's record format, and the comparer of two
-// restart files (contrib/dcanard.f90). Host code, no device work.
+// Restart files in the reference's record format, the comparer of two
+// restart files (contrib/dcanard.f90), and grid files in the reference's
+// record format. Host code, no device work.
 //
 // A restart file holds one block (misc/restartZZZ.dat, src/mo_io.f90:115-116),
 // written as a Fortran direct-access unformatted file of 40-byte records
@@ -109,6 +110,43 @@ int canard_restart_write_file(const char* path, const double* time6, const doubl
 int canard_restart_read_file(const char* path, double* time6, double* qa, int64_t npts) {
   if (!path || npts < 1) return CANARD_ERR_ARG;
   return read_file(path, time6, qa, npts);
+}
+
+// Grid files (misc/gridZZZ.dat): a Fortran direct-access file read one
+// 24-byte record (x, y, z) per stored point l = i + (lxi+1)(j + (let+1)k)
+// (read_grid_parallel, src/mo_io.f90:151-180, one sub-domain per block) and
+// written one record per k plane holding the plane's (x, y, z) triplets, i
+// fastest (gridtoy / gridtoy_multi / gridaerofoil, src/mo_gridgen.f90:536-570):
+// the same bytes, 3 doubles per point with no markers. xyz is ss(0:npts-1, 3).
+int canard_grid_write_file(const char* path, const double* xyz, int64_t npts) {
+  if (!path || !xyz || npts < 1) return CANARD_ERR_ARG;
+  File out(path, "wb");
+  if (!out.f) return CANARD_ERR_IO;
+  std::vector<double> rec((size_t)3 * 4096);
+  for (int64_t l0 = 0; l0 < npts; l0 += 4096) {
+    const int64_t m = std::min<int64_t>(4096, npts - l0);
+    for (int64_t l = 0; l < m; ++l)
+      for (int c = 0; c < 3; ++c) rec[(size_t)(3 * l + c)] = xyz[(l0 + l) + c * npts];
+    if (std::fwrite(rec.data(), sizeof(double), (size_t)(3 * m), out.f) != (size_t)(3 * m)) return CANARD_ERR_IO;
+  }
+  return std::fflush(out.f) == 0 ? CANARD_OK : CANARD_ERR_IO;
+}
+
+int canard_grid_read_file(const char* path, double* xyz, int64_t npts) {
+  if (!path || !xyz || npts < 1) return CANARD_ERR_ARG;
+  File in(path, "rb");
+  if (!in.f) return CANARD_ERR_IO;
+  if (std::fseek(in.f, 0, SEEK_END) != 0) return CANARD_ERR_IO;
+  if (std::ftell(in.f) != (long)(24 * npts)) return CANARD_ERR_IO;  // another block size
+  std::rewind(in.f);
+  std::vector<double> rec((size_t)3 * 4096);
+  for (int64_t l0 = 0; l0 < npts; l0 += 4096) {
+    const int64_t m = std::min<int64_t>(4096, npts - l0);
+    if (std::fread(rec.data(), sizeof(double), (size_t)(3 * m), in.f) != (size_t)(3 * m)) return CANARD_ERR_IO;
+    for (int64_t l = 0; l < m; ++l)
+      for (int c = 0; c < 3; ++c) xyz[(l0 + l) + c * npts] = rec[(size_t)(3 * l + c)];
+  }
+  return CANARD_OK;
 }
 
 int canard_restart_compare(const char* path1, const char* path2, int64_t npts, double wtol, const char* report_path,

@@ -150,6 +150,15 @@ int canard_set_time(canard_ctx* ctx, int32_t icase, const double* time6);
  * block size returns CANARD_ERR_IO. */
 int canard_restart_write_file(const char* path, const double* time6, const double* qa, int64_t npts);
 int canard_restart_read_file(const char* path, double* time6, double* qa, int64_t npts);
+
+/* Grid files in the reference's format (misc/gridZZZ.dat of block ZZZ): one
+ * 24-byte record (x, y, z) per stored point, i fastest, then j, then k, as
+ * the generators write them plane by plane (src/mo_gridgen.f90:536-570) and
+ * read_grid_parallel reads them point by point (src/mo_io.f90:151-180, which
+ * these replace on the host side; canard_upload_grid takes the result).
+ * xyz is ss(0:npts-1, 3). A file of another size returns CANARD_ERR_IO. */
+int canard_grid_write_file(const char* path, const double* xyz, int64_t npts);
+int canard_grid_read_file(const char* path, double* xyz, int64_t npts);
 int canard_write_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 int canard_read_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 

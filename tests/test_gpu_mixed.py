@@ -56,8 +56,9 @@ CASES = {
     "periodic": lambda: cases.tgv(nx=24, ny=20, nz=16),
     "nonperiodic": case_nonperiodic,
     "multiblock": lambda: cases.curvilinear_4block(24, 16, 14),
+    "toy": lambda: cases.reference_toy(16, 14, 12),
 }
-UREF = {"periodic": 0.1, "nonperiodic": 0.3, "multiblock": 0.4}
+UREF = {"periodic": 0.1, "nonperiodic": 0.3, "multiblock": 0.4, "toy": 0.3}
 
 
 def smooth_fields(cs, seed):

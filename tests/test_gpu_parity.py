@@ -44,7 +44,19 @@ def case_multiblock():
     return cases.curvilinear_4block(24, 16, 14)
 
 
-CASES = {"periodic": case_periodic, "nonperiodic": case_nonperiodic, "multiblock": case_multiblock}
+def case_toy():
+    # the reference's run/exp.toy layout (six blocks from gridtoy_multi, straight
+    # interfaces, periodic across the rows and in zeta, initialo's vortex), small
+    return cases.reference_toy(16, 14, 12)
+
+
+def case_validation():
+    # the reference's run/exp.validation (gridtoy block, GCBC on four faces)
+    return cases.reference_validation(24, 20, 12)
+
+
+CASES = {"periodic": case_periodic, "nonperiodic": case_nonperiodic, "multiblock": case_multiblock,
+         "toy": case_toy, "validation": case_validation}
 
 
 def random_fields(cs, seed, ncols=1):
