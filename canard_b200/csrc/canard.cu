@@ -2341,6 +2341,14 @@ int canard_launch_count(canard_ctx* c, int64_t* count) {
   return CANARD_OK;
 }
 
+#ifdef CANARD_TRACE
+// Trace builds only (-DCANARD_TRACE): the device buffer of 8 int64 per CTA that
+// the line kernels fill with clock64 stamps and the SM id.
+int canard_trace_buffer(void* dev) {
+  return cudaMemcpyToSymbol(g_trace, &dev, sizeof(dev)) == cudaSuccess ? CANARD_OK : CANARD_ERR_CUDA;
+}
+#endif
+
 int canard_selftest_wait(canard_ctx* c, double* seconds) {
   return guarded(c, [&] {
     CK(cudaStreamSynchronize(c->st));
