@@ -506,21 +506,25 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
   Table<LineTask> T;
   T.kind = kind;
   const size_t es = tile_elem(kind);
-  std::vector<int> first;
+  // line tables: `first` holds the task of every tile (one load per CTA
+  // instead of a search over the tasks' first tiles)
+  std::vector<int> tile_task;
   int tot = 0;
   size_t sm = 0;
-  for (auto& t : v) {
+  for (size_t i = 0; i < v.size(); ++i) {
+    LineTask& t = v[i];
     t.tile0 = tot;
-    first.push_back(tot);
+    tile_task.insert(tile_task.end(), (size_t)t.ntiles, (int)i);
     tot += t.ntiles;
     sm = std::max(sm, line_smem(dir, t, kind));
     T.bytes += 2.0 * es * t.X * t.Y * t.Z;  // read the field, write the result
   }
+  if (tile_task.empty()) tile_task.push_back(0);
   T.ntasks = (int)v.size();
   T.total = tot;
   T.smem = sm;
   T.tasks = dupload(v, c->st);
-  T.first = dupload(first, c->st);
+  T.first = dupload(tile_task, c->st);
   std::vector<CUtensorMap> maps(2 * v.size());
   if (dir != 0)
     for (size_t i = 0; i < v.size(); ++i) {
@@ -2380,21 +2384,25 @@ constexpr int kNaMaxLines = 65536;   // lines of the direction (nbsize)
 constexpr int kNaMaxPoints = 1024;   // points per line
 constexpr size_t kNaTask = 0;        // LineTask
 constexpr size_t kNaFace = 512;      // up to 2 FaceTask
-constexpr size_t kNaIdx = 1536;      // tile0 (1 int), line0 (2 ints)
+constexpr size_t kNaIdx = 1536;      // (unused int), line0 of the 2 face tasks
 constexpr size_t kNaErr = 1600;      // device error flag
 constexpr size_t kNaChain = 1608;    // unused third send component (2 doubles)
 constexpr size_t kNaMaps = 1664;     // 2 CUtensorMap, 64-byte aligned
 constexpr size_t kNaScheme = 2048;   // DevScheme
 constexpr size_t kNaLu = 4096;       // 5 x kNaMaxPoints doubles
 constexpr size_t kNaRecv = kNaLu + 5 * kNaMaxPoints * sizeof(double);  // 2 sides x 2 comps x lines
-constexpr size_t kNaBytes = kNaRecv + (size_t)4 * kNaMaxLines * sizeof(double);
+// the line kernel's tile -> task index: every tile belongs to task 0, so this
+// region is never written and keeps the zeros of static initialisation
+constexpr int kNaMaxTiles = 8192;
+constexpr size_t kNaTiles = kNaRecv + (size_t)4 * kNaMaxLines * sizeof(double);
+constexpr size_t kNaBytes = kNaTiles + (size_t)kNaMaxTiles * sizeof(int);
 static_assert(sizeof(LineTask) <= kNaFace - kNaTask, "LineTask slot");
 static_assert(2 * sizeof(FaceTask) <= kNaIdx - kNaFace, "FaceTask slots");
 static_assert(sizeof(DevScheme) <= kNaLu - kNaScheme, "scheme slot");
 static_assert(kNaMaps % 64 == 0 && kNaLu % 256 == 0 && kNaRecv % 256 == 0, "alignment");
 }  // namespace
 
-// about 2.1 MiB per device
+// about 2.1 MiB per device (zero-initialised)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
 namespace {
@@ -2494,6 +2502,7 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
       t.ntiles = t.ntx * (dir == 1 ? g.Z : g.Y);
     }
     t.tile0 = 0;
+    if (t.ntiles > kNaMaxTiles) return fail(CANARD_ERR_ARG, "more than 8192 tiles of 32 lines");
     // periodic on the line itself: each end's contraction feeds the other end
     FaceTask f[2];
     int nf = 0;
@@ -2543,7 +2552,7 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     }
     const size_t smem = line_smem(dir, t, LK_F64);
     const LineTask* dt = reinterpret_cast<const LineTask*>(base + kNaTask);
-    const int* d0 = reinterpret_cast<const int*>(base + kNaIdx);
+    const int* d0 = reinterpret_cast<const int*>(base + kNaTiles);  // zeros: tile -> task 0
     const CUtensorMap* dm = reinterpret_cast<const CUtensorMap*>(base + kNaMaps);
     int* de = reinterpret_cast<int*>(base + kNaErr);
     if (dir == 0) launch_line_t<1, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);

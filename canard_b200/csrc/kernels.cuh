@@ -786,7 +786,7 @@ __host__ __device__ __forceinline__ int dir1_pitch(int L) {
 // the elimination. The tile moves in chunks (see ChunkIn): loads overlap the
 // forward sweep, stores the back substitution.
 template <int DIR, int OP, class TT, class RS>
-__global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
+__global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
                                              int ntasks, const CUtensorMap* __restrict__ maps,
                                              int* __restrict__ err) {
   constexpr int kVec = 16 / (int)sizeof(TT);  // elements per 16 bytes
@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   const int lane = threadIdx.x;
   TRACE(0)
   if (error_pending(err)) return;
-  const int ti = find_task(tile0s, ntasks, blockIdx.x);
+  const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -1250,7 +1250,7 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
 // 3 zeta. OP: 0 derivative, 1 filter (in place). TT: field and tile type;
 // the elimination is FP32.
 template <int DIR, int OP, class TT>
-__global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
+__global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
                                               int ntasks, const CUtensorMap* __restrict__ maps,
                                               int* __restrict__ err) {
   constexpr int kVec = 16 / (int)sizeof(TT);
@@ -1260,7 +1260,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   const int lane = threadIdx.x;
   const int half = lane >> 4, li = lane & (kHalf - 1);
   if (error_pending(err)) return;
-  const int ti = find_task(tile0s, ntasks, blockIdx.x);
+  const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);

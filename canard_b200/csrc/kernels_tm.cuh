@@ -81,10 +81,11 @@ struct TmTile {
 };
 
 template <int DIR>
-__device__ __forceinline__ TmTile tm_tile(const LineTask* __restrict__ tasks, const int* __restrict__ tile0s,
+__device__ __forceinline__ TmTile tm_tile(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
                                           int ntasks, int t) {
   TmTile g;
-  g.ti = find_task(tile0s, ntasks, t);
+  g.ti = __ldg(tile_task + t);
+  (void)ntasks;
   const LineTask& T = tasks[g.ti];
   const int lt = t - T.tile0;
   g.L = T.L;
@@ -506,7 +507,7 @@ __device__ __forceinline__ bool tm_forward_filter(TmStream<DIR>& R, const LuRows
 // and 32-row boxes in their tensor maps.
 template <int DIR, int OP>
 __global__ void __launch_bounds__(kTmWarps * 32) k_line_tm(const LineTask* __restrict__ tasks,
-                                                          const int* __restrict__ tile0s, int ntasks, int ntiles,
+                                                          const int* __restrict__ tile_task, int ntasks, int ntiles,
                                                           const CUtensorMap* __restrict__ maps,
                                                           int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -542,7 +543,7 @@ __global__ void __launch_bounds__(kTmWarps * 32) k_line_tm(const LineTask* __res
   bool ok = true;
   TmTile g;
   if (t < ntiles) {
-    g = tm_tile<DIR>(tasks, tile0s, ntasks, t);
+    g = tm_tile<DIR>(tasks, tile_task, ntasks, t);
     in.issue_tile(maps + 2 * g.ti, g);
   }
   for (; ok && t < ntiles; t += stride) {
@@ -600,7 +601,7 @@ __global__ void __launch_bounds__(kTmWarps * 32) k_line_tm(const LineTask* __res
     const TmTile cur = g;
     const int tn = t + stride;
     if (tn < ntiles) {
-      g = tm_tile<DIR>(tasks, tile0s, ntasks, tn);
+      g = tm_tile<DIR>(tasks, tile_task, ntasks, tn);
       in.issue_tile(maps + 2 * g.ti, g);
     }
     // lanes without a line read lane 0's column (valid memory) and store nothing;
