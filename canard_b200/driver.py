@@ -1,0 +1,136 @@
+"""The reference's program, on the device path: reads ``input.canard``, builds
+the blocks and their grid with the reference's generators, starts from
+``initialo`` or a restart file, and runs the time loop of canard_driver
+(src/mo_canard_driver.f90:99-470) with its stop rule, output schedule,
+time-averaged recording, Tecplot files and final restart file, in the
+reference's file formats and names under the run directory:
+
+* ``data/grid.plt`` at start, ``data/nNNN.plt`` at each of the ``ndata``
+  output times (``ndata < 0``: no output);
+* ``misc/restartzNNN.da`` per block at the end when ``nrestart == 1``; a run
+  with ``nts != 0`` starts from these files.
+
+Every block runs as one sub-domain: an input with ``nbpc > 1`` is run with one
+sub-domain per block (its interface closures then differ from the reference's
+split run at the sub-domain faces), and a warning says so. The reference's
+VISCOUS build flag is the ``viscous`` argument.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import api, cases, namelist
+
+
+def case_from_input(nml, viscous: int = 1, warn=print) -> cases.CaseSpec:
+    """The case an ``input.canard`` describes (namelists as read by
+    namelist.read): blocks and boundary codes from nml_domdcomp, the grid from
+    nml_gridgen's generator, initialo's state, and the physics, numerics and
+    sponge parameters."""
+    drv, can, dd = nml["nml_driver"], nml["nml_canard"], nml["nml_domdcomp"]
+    gg, num, phy, sp = nml["nml_gridgen"], nml["nml_numerics"], nml["nml_physics"], nml["nml_sponge"]
+    nb = int(drv["mbk"]) + 1
+    lxi, let, lze = (dd[k][0] for k in ("lximb", "letmb", "lzemb"))
+    nbbc, mbcd, nbpc = dd["nbbc"][0], dd["mbcd"][0], dd["nbpc"][0]
+    if np.any(nbpc > 1):
+        warn("canard_b200: nbpc > 1 in the input; every block runs as one sub-domain here")
+    gt = int(gg["gridtype"])
+    if gt == 0:
+        xyz = [cases.gridtoy(int(gg["lxi0"]), int(gg["let0"]), int(gg["lze0"]), float(gg["doml0"]),
+                             float(gg["doml1"]), float(gg["domh"]), float(gg["span"]))]
+    elif gt == 1:
+        xyz = cases.gridtoy_multi(int(gg["lxi0"]), int(gg["lxi1"]), int(gg["lxi2"]), int(gg["let0"]),
+                                  int(gg["lze0"]), float(gg["doml0"]), float(gg["doml1"]), float(gg["domh"]),
+                                  float(gg["span"]))
+    else:
+        raise namelist.NamelistError(f"gridtype {gt}: only the reference's gridtoy (0) and gridtoy_multi (1)")
+    if len(xyz) < nb:
+        raise namelist.NamelistError(f"gridtype {gt} makes {len(xyz)} block(s), the input has {nb}")
+    blocks = []
+    for m in range(nb):
+        b = cases.BlockSpec(int(lxi[m]), int(let[m]), int(lze[m]),
+                            [[int(nbbc[m, d, s]) for s in range(2)] for d in range(3)],
+                            [[int(mbcd[m, d, s]) for s in range(2)] for d in range(3)])
+        if xyz[m].shape[1:] != b.shape:
+            raise namelist.NamelistError(f"block {m}: the grid has {xyz[m].shape[1:][::-1]} points per direction, "
+                                         f"nml_domdcomp {b.shape[::-1]}")
+        blocks.append(b)
+    xyz = xyz[:nb]
+    return cases.CaseSpec(blocks, viscous=viscous, fltk=float(num["fltk"]), fltrbc=float(num["fltrbc"]),
+                          reoo=float(phy["reoo"]), tempoo=float(phy["tempoo"]),
+                          amach=(float(phy["amach1"]), float(phy["amach2"]), float(phy["amach3"])),
+                          timf=float(phy["timf"]), nsmf=int(phy["nsmf"]), cfl=float(can["cfl"]),
+                          szco=float(sp["szco"]), szth0=float(gg["szth0"]), szth1=float(gg["szth1"]),
+                          doml0=float(gg["doml0"]), doml1=float(gg["doml1"]), xyz=xyz,
+                          qa=[cases.initialo(g) for g in xyz], name="input.canard")
+
+
+def run(input_path: str = "input.canard", directory: Optional[str] = None, precision: int = api.FP64,
+        viscous: int = 1, max_steps: Optional[int] = None, out=sys.stdout) -> dict:
+    """Runs the case of ``input_path`` in ``directory`` (default: the input's
+    directory) like the reference's program; returns a summary (steps, time,
+    outputs written, whether the run stopped on a zero time step)."""
+    directory = directory or os.path.dirname(os.path.abspath(input_path))
+    nml = namelist.read_file(input_path)
+    cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out))
+    can, drv = nml["nml_canard"], nml["nml_driver"]
+    tmax, ndata = float(can["tmax"]), int(drv["ndata"])
+    loutput = ndata >= 0
+    ctx = api.Context(cs, precision=precision)
+    if int(can["nts"]) != 0:
+        ctx.read_restart(directory)
+    if bool(can["ltimer"]):
+        ctx.set_timers(True)
+    outputs = []
+    if loutput:
+        ctx.write_grid_plt(directory)
+        outputs.append(api.plt_name(-1))
+        ctx.record_enable(True)
+    ndati = -1
+    overflow = False
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        n, _, dt, _, _, timo = ctx.time()
+        # do while (timo < tmax .and. (dt /= 0 .or. n <= 2))
+        if not (timo < tmax and (dt != 0.0 or n <= 2)):
+            break
+        if max_steps is not None and steps >= max_steps:
+            break
+        print(" n =%8d   time =%12.5f" % (int(n), timo), file=out)
+        try:
+            ctx.step(1)
+        except api.CanardError as e:
+            if e.code != api.ERR_NAN:
+                raise
+            overflow = True  # dt == 0 after step 2: the reference's loop ends here
+            break
+        steps += 1
+        if loutput:
+            ctx.record_accumulate()
+            timo_new = ctx.time()[5]  # timo + dt of this step
+            # nout: the output time res falls within [timo, timo + dt]
+            res = (ndati + 1) * tmax / ndata if ndata > 0 else np.inf
+            if (timo - res) * (timo_new - res) <= 0.0:
+                ndati += 1
+                ctx.write_output(directory, ndati)
+                outputs.append(api.plt_name(ndati))
+    if int(can["nrestart"]) == 1:
+        ctx.write_restart(directory)
+    wall = time.perf_counter() - t0
+    n, _, dt, _, _, timo = ctx.time()
+    if overflow or dt == 0.0:
+        print(" Canard: Overflow.", file=out)
+    if bool(can["ltimer"]):
+        for name, v in ctx.timers().items():
+            if v["launches"]:
+                print(" %-18s %10.3f ms %8d launches" % (name, v["ms"], v["launches"]), file=out)
+    print(" Canard: Finished.", file=out)
+    ctx.close()
+    return {"steps": steps, "n": int(n), "time": float(timo), "outputs": outputs, "overflow": overflow,
+            "wall_s": wall, "points": cs.npts}

@@ -1,0 +1,149 @@
+"""The reader of the reference's input file (Fortran namelists) and the case
+it describes, on the CPU (canard_b200.namelist, canard_b200.driver)."""
+import numpy as np
+import pytest
+
+from canard_b200 import cases, driver, namelist
+
+TOY = """&nml_driver
+nio = 0
+mbk = 5
+ndata = 3
+/
+&nml_canard
+nts = 0
+nrestart = 1
+cfl = 1.2d0
+tmax = 0.25e0
+ltimer = .false.
+/
+&nml_domdcomp
+nbpc(:,1) = 2,2,2,2,2,2
+nbpc(:,2) = 6*1
+nbpc(:,3) = 1,1,1,1,1,1
+lximb = 6*16
+letmb = 6*14
+lzemb = 6*12
+nbbc(0,1,:) = 10,35
+nbbc(0,2,:) = 45,35
+nbbc(0,3,:) = 45,45
+mbcd(0,1,:) = -1,1
+mbcd(0,2,:) = 3,3
+mbcd(0,3,:) =  0,0
+nbbc(1,1,:) = 35,35
+nbbc(1,2,:) = 45,35
+nbbc(1,3,:) = 45,45
+mbcd(1,1,:) = 0,2
+mbcd(1,2,:) = 4,4
+mbcd(1,3,:) =  1,1
+nbbc(2,1,:) = 35,10
+nbbc(2,2,:) = 45,35
+nbbc(2,3,:) = 45,45
+mbcd(2,1,:) = 1,-1
+mbcd(2,2,:) = 5,5
+mbcd(2,3,:) =  2,2
+nbbc(3,1,:) = 10,35
+nbbc(3,2,:) = 35,45
+nbbc(3,3,:) = 45,45
+mbcd(3,1,:) = -1,4
+mbcd(3,2,:) = 0,0
+mbcd(3,3,:) =  3,3
+nbbc(4,1,:) = 35,35
+nbbc(4,2,:) = 35,45
+nbbc(4,3,:) = 45,45
+mbcd(4,1,:) = 3,5
+mbcd(4,2,:) = 1,1
+mbcd(4,3,:) =  4,4
+nbbc(5,1,:) = 35,10
+nbbc(5,2,:) = 35,45
+nbbc(5,3,:) = 45,45
+mbcd(5,1,:) = 4,-1
+mbcd(5,2,:) = 2,2
+mbcd(5,3,:) =  5,5
+/
+&nml_numerics
+fltk = 0.65e0
+fltrbc = 0.9e0
+/
+&nml_physics
+reoo = 500000.0e0  ! divided by the frame Mach number in the code
+tempoo = 300.0e0
+amach1 = 0.3e0
+amach2 = 0.0e0
+amach3 = 0.0e0
+timf = 0.0e0
+nsmf = 1
+/
+&nml_gridgen
+gridtype = 1
+lxi0 = 16, lxi1 = 16, lxi2 = 16
+let0 = 14
+lze0 = 12
+doml0 = 0.5e0
+doml1 = 1.0e0
+domh = 0.5e0
+span = 0.1e0
+szth0 = 0.0e0
+szth1 = 0.6e0
+/
+nml_sponge
+szco = 10.0e0
+/
+"""
+
+
+def test_scalars_arrays_and_the_group_without_ampersand():
+    r = namelist.read(TOY)
+    assert r["nml_driver"] == {"nio": 0, "mbk": 5, "ndata": 3}
+    assert r["nml_canard"]["cfl"] == 1.2 and r["nml_canard"]["ltimer"] is False
+    nbpc, lo = r["nml_domdcomp"]["nbpc"]
+    assert lo == [0, 1] and nbpc.shape == (6, 3)
+    np.testing.assert_array_equal(nbpc[:, 0], 2)
+    np.testing.assert_array_equal(nbpc[:, 1:], 1)
+    np.testing.assert_array_equal(r["nml_domdcomp"]["lximb"][0], 16)
+    nbbc = r["nml_domdcomp"]["nbbc"][0]
+    assert nbbc.shape == (6, 3, 2)
+    assert list(nbbc[0, 0]) == [10, 35] and list(nbbc[5, 1]) == [35, 45]
+    assert list(r["nml_domdcomp"]["mbcd"][0][4, 0]) == [3, 5]
+    assert r["nml_gridgen"]["lxi1"] == 16 and r["nml_gridgen"]["span"] == 0.1
+    # "nml_sponge" lacks its '&': the reference's READ never finds the group
+    assert r["nml_sponge"]["szco"] == 0.0
+
+
+def test_sections_repeat_counts_and_logicals():
+    r = namelist.read("&nml_driver mbk = 2 /\n&nml_domdcomp lximb(1:2) = 2*7, letmb(2) = 5 /\n"
+                      "&nml_canard ltimer = T, tmax = 1.5D-1 /")
+    assert list(r["nml_domdcomp"]["lximb"][0]) == [0, 7, 7]
+    assert list(r["nml_domdcomp"]["letmb"][0]) == [0, 0, 5]
+    assert r["nml_canard"]["ltimer"] is True and r["nml_canard"]["tmax"] == 0.15
+
+
+@pytest.mark.parametrize("text", ["&nml_canard cfl = 1.0, bogus = 2 /",
+                                  "&nml_driver mbk = 1 /\n&nml_domdcomp lximb(3) = 5 /",
+                                  "&nml_canard tmax = abc /"])
+def test_errors(text):
+    with pytest.raises(namelist.NamelistError):
+        namelist.read(text)
+
+
+def test_case_from_the_toy_input():
+    warnings = []
+    cs = driver.case_from_input(namelist.read(TOY), warn=warnings.append)
+    assert len(warnings) == 1 and "nbpc" in warnings[0]
+    assert len(cs.blocks) == 6 and cs.cfl == 1.2 and cs.fltk == 0.65 and cs.szco == 0.0
+    ref = cases.reference_toy(16, 14, 12)
+    for a, b in zip(cs.blocks, ref.blocks):
+        assert [list(x) for x in a.nbc] == [list(x) for x in b.nbc]
+        assert [list(x) for x in a.mbcd] == [list(x) for x in b.mbcd]
+    for a, b in zip(cs.xyz, ref.xyz):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(cs.qa, ref.qa):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_grid_sizes_must_match_the_blocks():
+    bad = TOY.replace("lximb = 6*16", "lximb = 6*15")
+    with pytest.raises(namelist.NamelistError):
+        driver.case_from_input(namelist.read(bad), warn=lambda s: None)
+    with pytest.raises(namelist.NamelistError):
+        driver.case_from_input(namelist.read(TOY.replace("gridtype = 1", "gridtype = 2")), warn=lambda s: None)
