@@ -792,10 +792,11 @@ double ew_bytes(const canard_ctx* c, int n64, int nr) {
   return (8.0 * n64 + (c->f32() ? 4.0 : 8.0) * nr) * valid_points(c);
 }
 
-void ph_prim(canard_ctx* c) {
-  Timed tm(c, T_PRIM, ew_bytes(c, 5, 7));
-  if (c->f32()) launch_prim<float>(ew_grid(c), c->st, c->dbd, c->dcc);
-  else launch_prim<double>(ew_grid(c), c->st, c->dbd, c->dcc);
+// with store_qo (the step's first stage) the pass also copies qa to qo
+void ph_prim(canard_ctx* c, bool store_qo = false) {
+  Timed tm(c, T_PRIM, ew_bytes(c, store_qo ? 10 : 5, 7));
+  if (c->f32()) launch_prim<float>(ew_grid(c), c->st, c->dbd, c->dcc, store_qo ? 1 : 0);
+  else launch_prim<double>(ew_grid(c), c->st, c->dbd, c->dcc, store_qo ? 1 : 0);
   CK(cudaGetLastError());
 }
 
@@ -1014,8 +1015,7 @@ void time_advance(canard_ctx* c) {
 // no host synchronisation, so it can be captured as a graph.
 void step_body(canard_ctx* c) {
   ph_filter(c);
-  ph_copyqo(c);
-  ph_prim(c);
+  ph_prim(c, true);  // and qo = qa
   timestep(c);
   stage_params(c, 1, 4);
   for (int nk = 1; nk <= 4; ++nk) {

@@ -1512,12 +1512,19 @@ __device__ __forceinline__ void prim_point(const Work<R>& W, const CaseConst& C,
   W.mu[l] = R((C.srefp1dre * pow15(d5)) / (d5 + C.srefoo));
 }
 
-template <class R>
+// STORE_QO (the step's first stage): also qo = qa (src/mo_canard_driver.f90:
+// 252) from the values this pass reads anyway, instead of a separate copy
+template <class R, bool STORE_QO = false>
 __global__ void k_prim(const BlockDev* __restrict__ bd, const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
     const long long n = B.npad;
     const double* q = B.qa;
-    prim_point<R>(work<R>(B), cc[B.case_id], l, n, q[l], q[l + n], q[l + 2 * n], q[l + 3 * n], q[l + 4 * n]);
+    const double q0 = q[l], q1 = q[l + n], q2 = q[l + 2 * n], q3 = q[l + 3 * n], q4 = q[l + 4 * n];
+    if (STORE_QO) {
+      double* o = B.qo;
+      o[l] = q0; o[l + n] = q1; o[l + 2 * n] = q2; o[l + 3 * n] = q3; o[l + 4 * n] = q4;
+    }
+    prim_point<R>(work<R>(B), cc[B.case_id], l, n, q0, q1, q2, q3, q4);
   }
 }
 
@@ -1992,8 +1999,9 @@ __global__ void k_face_copy(const void* const* __restrict__ src, void* const* __
 // float instantiations are made once, by the FMA-enabled FP32 translation
 // unit, and declared extern everywhere else (kernels_f32.h).
 template <class R>
-void launch_prim(dim3 g, cudaStream_t st, const BlockDev* bd, const CaseConst* cc) {
-  k_prim<R><<<g, 256, 0, st>>>(bd, cc);
+void launch_prim(dim3 g, cudaStream_t st, const BlockDev* bd, const CaseConst* cc, int store_qo) {
+  if (store_qo) k_prim<R, true><<<g, 256, 0, st>>>(bd, cc);
+  else k_prim<R, false><<<g, 256, 0, st>>>(bd, cc);
 }
 template <class R>
 void launch_dtmax(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc,

@@ -11,7 +11,7 @@
 
 namespace canard {
 
-CANARD_F32_EXTERN template void launch_prim<float>(dim3, cudaStream_t, const BlockDev*, const CaseConst*);
+CANARD_F32_EXTERN template void launch_prim<float>(dim3, cudaStream_t, const BlockDev*, const CaseConst*, int);
 CANARD_F32_EXTERN template void launch_dtmax<float>(dim3, cudaStream_t, const BlockDev*, const StageParams*,
                                                     const CaseConst*, unsigned long long*, int*);
 CANARD_F32_EXTERN template void launch_copy_mu<float>(dim3, cudaStream_t, const BlockDev*);
