@@ -1,5 +1,8 @@
 """The reader of the reference's input file (Fortran namelists) and the case
 it describes, on the CPU (canard_b200.namelist, canard_b200.driver)."""
+import os
+import re
+
 import numpy as np
 import pytest
 
@@ -147,3 +150,25 @@ def test_grid_sizes_must_match_the_blocks():
         driver.case_from_input(namelist.read(bad), warn=lambda s: None)
     with pytest.raises(namelist.NamelistError):
         driver.case_from_input(namelist.read(TOY.replace("gridtype = 1", "gridtype = 2")), warn=lambda s: None)
+
+
+REF_RUN = os.path.join(os.environ.get("CANARD_REFERENCE", "/root/reference"), "run")
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_RUN), reason="no reference checkout")
+@pytest.mark.parametrize("script,nblocks,points", [("exp.validation", 1, (17, 51, 51)), ("exp.aio", 1, (17, 51, 51)),
+                                                   ("exp.toy", 6, (17, 101, 101)),
+                                                   ("exp.toy.aio", 6, (17, 101, 101))])
+def test_the_reference_run_inputs(script, nblocks, points):
+    """The input.canard each of the reference's run scripts writes (its here
+    document) reads and gives its case; every one splits blocks (nbpc > 1) and
+    misspells the sponge group, so szco stays 0."""
+    text = open(os.path.join(REF_RUN, script)).read()
+    m = re.search(r"cat > input\.canard << EOF\n(.*?)\nEOF", text, re.S)
+    assert m, script
+    r = namelist.read(m.group(1))
+    warnings = []
+    cs = driver.case_from_input(r, warn=warnings.append)
+    assert len(cs.blocks) == nblocks and all(b.shape == points for b in cs.blocks)
+    assert r["nml_sponge"]["szco"] == 0.0 and len(warnings) == 1
+    assert r["nml_numerics"]["fltk"] == 0.65 and r["nml_physics"]["amach1"] == 0.3
