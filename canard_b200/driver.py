@@ -10,6 +10,11 @@ reference's file formats and names under the run directory:
 * ``misc/restartzNNN.da`` per block at the end when ``nrestart == 1``; a run
   with ``nts != 0`` starts from these files.
 
+The output files are written by a writer thread (OutputWriter), the role of
+the reference's IO server ranks (src/mo_io_server.f90): the stepping thread
+copies an output's averages to the host and carries on while the file is
+written.
+
 Every block runs as one sub-domain: an input with ``nbpc > 1`` is run with one
 sub-domain per block (its interface closures then differ from the reference's
 split run at the sub-domain faces), and a warning says so. The reference's
@@ -18,13 +23,51 @@ VISCOUS build flag is the ``viscous`` argument.
 from __future__ import annotations
 
 import os
+import queue
 import sys
+import threading
 import time
 from typing import Optional
 
 import numpy as np
 
 from . import api, cases, namelist
+
+
+class OutputWriter:
+    """Writes Tecplot outputs (api.plt_write) on a host thread, in the order
+    they are handed over. The library call releases the interpreter lock, so
+    the writes overlap the steps. close() waits for every write and raises the
+    first error."""
+
+    def __init__(self):
+        self._q: "queue.Queue" = queue.Queue()
+        self._err: Optional[BaseException] = None
+        self._t = threading.Thread(target=self._loop, name="canard-output", daemon=True)
+        self._t.start()
+
+    def _loop(self):
+        while True:
+            item = self._q.get()
+            if item is None:
+                return
+            path, n, arrays, t = item
+            if self._err is not None:
+                continue
+            try:
+                os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+                api.plt_write(path, n, arrays, t)
+            except BaseException as e:  # reported by close()
+                self._err = e
+
+    def submit(self, path: str, n: int, arrays, t: float = 0.0):
+        self._q.put((path, n, arrays, t))
+
+    def close(self):
+        self._q.put(None)
+        self._t.join()
+        if self._err is not None:
+            raise self._err
 
 
 def case_from_input(nml, viscous: int = 1, warn=print) -> cases.CaseSpec:
@@ -87,39 +130,16 @@ def run(input_path: str = "input.canard", directory: Optional[str] = None, preci
     if bool(can["ltimer"]):
         ctx.set_timers(True)
     outputs = []
+    writer = OutputWriter()
     if loutput:
-        ctx.write_grid_plt(directory)
+        writer.submit(os.path.join(directory, api.plt_name(-1)), -1, [np.asarray(x, np.float32) for x in cs.xyz])
         outputs.append(api.plt_name(-1))
         ctx.record_enable(True)
-    ndati = -1
-    overflow = False
     t0 = time.perf_counter()
-    steps = 0
-    while True:
-        n, _, dt, _, _, timo = ctx.time()
-        # do while (timo < tmax .and. (dt /= 0 .or. n <= 2))
-        if not (timo < tmax and (dt != 0.0 or n <= 2)):
-            break
-        if max_steps is not None and steps >= max_steps:
-            break
-        print(" n =%8d   time =%12.5f" % (int(n), timo), file=out)
-        try:
-            ctx.step(1)
-        except api.CanardError as e:
-            if e.code != api.ERR_NAN:
-                raise
-            overflow = True  # dt == 0 after step 2: the reference's loop ends here
-            break
-        steps += 1
-        if loutput:
-            ctx.record_accumulate()
-            timo_new = ctx.time()[5]  # timo + dt of this step
-            # nout: the output time res falls within [timo, timo + dt]
-            res = (ndati + 1) * tmax / ndata if ndata > 0 else np.inf
-            if (timo - res) * (timo_new - res) <= 0.0:
-                ndati += 1
-                ctx.write_output(directory, ndati)
-                outputs.append(api.plt_name(ndati))
+    try:
+        steps, _, overflow = _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out)
+    finally:
+        writer.close()  # every output file is complete when run() returns
     if int(can["nrestart"]) == 1:
         ctx.write_restart(directory)
     wall = time.perf_counter() - t0
@@ -134,3 +154,36 @@ def run(input_path: str = "input.canard", directory: Optional[str] = None, preci
     ctx.close()
     return {"steps": steps, "n": int(n), "time": float(timo), "outputs": outputs, "overflow": overflow,
             "wall_s": wall, "points": cs.npts}
+
+
+def _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out):
+    """The time loop of canard_driver; returns (steps, output count - 1,
+    whether it ended on a zero time step)."""
+    ndati = -1
+    steps = 0
+    while True:
+        n, _, dt, _, _, timo = ctx.time()
+        # do while (timo < tmax .and. (dt /= 0 .or. n <= 2))
+        if not (timo < tmax and (dt != 0.0 or n <= 2)):
+            break
+        if max_steps is not None and steps >= max_steps:
+            break
+        print(" n =%8d   time =%12.5f" % (int(n), timo), file=out)
+        try:
+            ctx.step(1)
+        except api.CanardError as e:
+            if e.code != api.ERR_NAN:
+                raise
+            return steps, ndati, True  # dt == 0 after step 2: the reference's loop ends here
+        steps += 1
+        if loutput:
+            ctx.record_accumulate()
+            timo_new = ctx.time()[5]  # timo + dt of this step
+            # nout: the output time res falls within [timo, timo + dt]
+            res = (ndati + 1) * tmax / ndata if ndata > 0 else np.inf
+            if (timo - res) * (timo_new - res) <= 0.0:
+                ndati += 1
+                arrays, t_out = ctx.record_output()
+                writer.submit(os.path.join(directory, api.plt_name(ndati)), ndati, arrays, t_out)
+                outputs.append(api.plt_name(ndati))
+    return steps, ndati, False

@@ -172,3 +172,101 @@ def test_the_reference_run_inputs(script, nblocks, points):
     assert len(cs.blocks) == nblocks and all(b.shape == points for b in cs.blocks)
     assert r["nml_sponge"]["szco"] == 0.0 and len(warnings) == 1
     assert r["nml_numerics"]["fltk"] == 0.65 and r["nml_physics"]["amach1"] == 0.3
+
+
+def test_output_writer_writes_in_order_and_reports_errors(tmp_path):
+    """The writer thread that stands in for the reference's IO server writes
+    the same bytes as a direct call, and a failed write surfaces at close()."""
+    from canard_b200 import api
+    rng = np.random.default_rng(3)
+    outs = [[rng.standard_normal((5, 4, 3, 6)).astype(np.float32)] for _ in range(3)]
+    w = driver.OutputWriter()
+    for n, arrs in enumerate(outs):
+        w.submit(str(tmp_path / "data" / ("n%03d.plt" % n)), n, arrs, 0.5 * n)
+    w.close()
+    for n, arrs in enumerate(outs):
+        ref = tmp_path / ("ref%d.plt" % n)
+        api.plt_write(str(ref), n, arrs, 0.5 * n)
+        assert (tmp_path / "data" / ("n%03d.plt" % n)).read_bytes() == ref.read_bytes()
+    w = driver.OutputWriter()
+    w.submit(str(tmp_path / "x.plt"), 1000, outs[0], 0.0)  # three-digit names only
+    with pytest.raises(api.CanardError):
+        w.close()
+
+
+class _FakeContext:
+    """Stands in for api.Context on the CPU: the reference's dt ramp over a
+    fixed dte (dt = 0 for the first two steps), no device."""
+
+    def __init__(self, cs, precision=0, zero_dt_at=None):
+        self.cs, self.t6, self.steps = cs, [0.0, 0.0, 0.0, 0.0, 0.0, 0.0], 0
+        self.zero_dt_at, self.restarts, self.recorded = zero_dt_at, [], 0
+
+    def time(self, case=0):
+        return np.array(self.t6)
+
+    def step(self, n=1):
+        from canard_b200 import api
+        k = int(self.t6[0])
+        if self.zero_dt_at is not None and k >= self.zero_dt_at:
+            raise api.CanardError(api.ERR_NAN, "Canard: Overflow.")
+        dt = 0.0 if k < 2 else 0.01 * np.sin(0.05 * np.pi * min(k - 1, 10)) ** 2
+        self.t6 = [k + 1, 1, dt, 0.0, 0.01, self.t6[5] + dt]
+        self.steps += 1
+
+    def set_timers(self, on):
+        pass
+
+    def record_enable(self, on=True):
+        pass
+
+    def record_accumulate(self):
+        self.recorded += 1
+
+    def record_output(self, case=0):
+        return [np.zeros((5,) + b.shape, np.float32) for b in self.cs.blocks], self.t6[5]
+
+    def write_restart(self, directory, case=0):
+        self.restarts.append(directory)
+
+    def read_restart(self, directory, case=0):
+        pass
+
+    def timers(self):
+        return {}
+
+    def close(self):
+        pass
+
+
+SMALL = TOY.replace("ndata = 3", "ndata = 4").replace("tmax = 0.25e0", "tmax = 0.05e0")
+
+
+@pytest.mark.parametrize("zero_dt_at", [None, 7])
+def test_driver_loop_on_a_stand_in_context(tmp_path, monkeypatch, zero_dt_at):
+    import io
+    made = []
+
+    def fake(cs, precision=0):
+        made.append(_FakeContext(cs, precision, zero_dt_at))
+        return made[-1]
+
+    monkeypatch.setattr(driver.api, "Context", fake)
+    submitted = []
+    monkeypatch.setattr(driver.OutputWriter, "submit", lambda self, p, n, a, t=0.0: submitted.append((p, n, t)))
+    (tmp_path / "input.canard").write_text(SMALL)
+    log = io.StringIO()
+    res = driver.run(str(tmp_path / "input.canard"), out=log)
+    ctx = made[0]
+    if zero_dt_at is None:
+        # stops at the first step that reaches tmax; outputs at 0, tmax/4, ..., tmax
+        assert ctx.t6[5] >= 0.05 and ctx.t6[5] - ctx.t6[2] < 0.05
+        assert [n for _, n, _ in submitted] == [-1, 0, 1, 2, 3, 4]
+        assert "Overflow" not in log.getvalue()
+        for (_, n, t), lo in zip(submitted[1:], [0.0, 0.0125, 0.025, 0.0375, 0.05]):
+            assert t >= lo  # written at the first step whose end passes n tmax / ndata
+    else:
+        assert res["overflow"] and ctx.steps == zero_dt_at and "Canard: Overflow." in log.getvalue()
+    assert res["outputs"][0] == "data/grid.plt" and len(res["outputs"]) == len(submitted)
+    assert ctx.recorded == ctx.steps and ctx.restarts == [str(tmp_path)]
+    assert "Canard: Finished." in log.getvalue()
