@@ -100,3 +100,36 @@ def test_fortran_e_format_of_negative_and_small_values(tmp_path):
     line = open(rep).read().splitlines()[0]
     assert line == (" i=       0 j=       1 v1= -0.2500000E-02 v2= -0.2000000E-02 abs=  0.5000000E-03"
                     " rel=  0.2000000E+00")
+
+
+def test_dcanard_command_compares_every_block(tmp_path, monkeypatch):
+    """python -m canard_b200.dcanard: block sizes from input.canard, one report
+    file per block under output/, the reference's summary line per block."""
+    import io
+    from canard_b200 import dcanard
+    inp = ("&nml_driver\nmbk = 1\n/\n&nml_domdcomp\nlximb = 12, 13\nletmb = 12, 12\nlzemb = 12, 14\n/\n")
+    (tmp_path / "input.canard").write_text(inp)
+    sizes = [13 * 13 * 13, 14 * 13 * 15]
+    for d in ("a", "b"):
+        (tmp_path / d / "misc").mkdir(parents=True)
+    for mb, npts in enumerate(sizes):
+        t6, qa = sample(npts, 40 + mb)
+        qb = qa.copy()
+        if mb == 1:
+            qb[2, 5] *= 1 + 1e-9
+            qb[4, 7] *= 1 + 1e-12
+        api.write_restart_file(str(tmp_path / "a" / api.restart_name(mb)), t6, qa)
+        api.write_restart_file(str(tmp_path / "b" / api.restart_name(mb)), t6, qb)
+    monkeypatch.chdir(tmp_path)
+    out = io.StringIO()
+    n = dcanard.compare("a", "b", 1e-15, out=out)
+    assert n == 2
+    lines = out.getvalue().splitlines()
+    assert lines[-2] == "Compared %8d elements for %8d variables in block %8d" % (sizes[0], 5, 0)
+    assert lines[-1] == "Compared %8d elements for %8d variables in block %8d" % (sizes[1], 5, 1)
+    assert (tmp_path / "output" / "restart0.dat").read_text() == ""
+    rep = (tmp_path / "output" / "restart1.dat").read_text().splitlines()
+    assert len(rep) == 2 and rep[0].startswith(" i=       5 j=       3") and rep[1].startswith(" i=       7 j=       5")
+    assert dcanard.compare("a", "b", 1e-10, out=io.StringIO()) == 1
+    assert dcanard.compare("a", "b", 1e-8, out=io.StringIO()) == 0
+    assert dcanard.main(["-d", "a", "b", "-t", "1e-15"]) == 0
