@@ -77,6 +77,9 @@ class CaseSpec:
     xyz: Optional[List[np.ndarray]] = None   # per block (3, Z, Y, X)
     qa: Optional[List[np.ndarray]] = None    # per block (5, Z, Y, X)
     name: str = ""
+    # set by decompose(): the blocks above are then sub-domains (ranks) of the
+    # input's blocks; see decompose()
+    sub: Optional[dict] = None
 
     @property
     def npts(self) -> int:
@@ -383,3 +386,96 @@ def reference_toy(lxi: int = 100, let0: int = 100, lze0: int = 16) -> CaseSpec:
     return CaseSpec(blocks, viscous=1, fltk=0.65, fltrbc=0.9, reoo=500000.0, tempoo=300.0, amach=(0.3, 0.0, 0.0),
                     nsmf=1, cfl=1.4, doml0=0.5, doml1=1.0, xyz=xyz, qa=[initialo(g) for g in xyz],
                     name=f"toy6x{lxi}x{let0}x{lze0}")
+
+
+# ---------------------------------------------------------------------------
+# Sub-domains (nbpc > 1): the reference's domain decomposition of its blocks
+# into ranks (domdcomp_init, src/mo_domdcomp.f90:85-232). Only the CPU oracle
+# runs such cases so far; the device context takes one sub-domain per block.
+
+def decompose(cs: CaseSpec, nbpc: Sequence[Sequence[int]]) -> CaseSpec:
+    """Splits block m of cs into nbpc[m] = (n_xi, n_eta, n_zeta) sub-domains as
+    domdcomp_init does: along a direction of l cells split in n, the first
+    sub-domain has l - ((l+1)/n)(n-1) cells and the others (l+1)/n - 1 (points
+    are not shared); inner faces get code 40 (BC_INTER_SUBDOMAINS) and the
+    neighbouring rank, faces on the block's boundary keep its code and face
+    the neighbouring block's sub-domain at that end with the same transverse
+    position. Ranks are numbered rank = mo(m) + (k n_eta + j) n_xi + i for the
+    position (i, j, k). The result's blocks are the ranks; its ``sub`` holds
+    the input's nbpc and mbcd, per rank (block, i, j, k), and per rank the
+    slice of its block's points (z0, y0, x0, nz, ny, nx)."""
+    nb = len(cs.blocks)
+    nbpc = [tuple(int(v) for v in p) for p in nbpc]
+    if len(nbpc) != nb or any(len(p) != 3 or min(p) < 1 for p in nbpc):
+        raise ValueError("nbpc needs three positive counts per block")
+    mo = [0]
+    for p in nbpc:
+        mo.append(mo[-1] + p[0] * p[1] * p[2])
+
+    def rank(m, pos):
+        return mo[m] + (pos[2] * nbpc[m][1] + pos[1]) * nbpc[m][0] + pos[0]
+
+    def idsd3(i, j, k, mm, nn):  # src/mo_domdcomp.f90:588-605
+        pos = [0, 0, 0]
+        pos[nn - 1], pos[nn % 3], pos[(nn + 1) % 3] = i, j, k
+        return rank(mm, pos)
+
+    blocks, xyz, qa, ranks, slices = [], [], [], [], []
+    for m, b in enumerate(cs.blocks):
+        ll = (b.lxi, b.let, b.lze)
+        n = nbpc[m]
+        for kz in range(n[2]):
+            for jy in range(n[1]):
+                for ix in range(n[0]):
+                    pos = (ix, jy, kz)
+                    r = rank(m, pos)
+                    lk, st, nbc, mcd = [0] * 3, [0] * 3, [None] * 3, [None] * 3
+                    for d in range(3):
+                        mak, lpk, mpk = n[d], pos[d], (1, n[0], n[0] * n[1])[d]
+                        face = []
+                        for ip in (0, 1):
+                            mm = b.mbcd[d][ip]
+                            face.append(-1 if mm == -1 else
+                                        idsd3((1 - ip) * (nbpc[mm][d] - 1), pos[(d + 1) % 3], pos[(d + 2) % 3],
+                                              mm, d + 1))
+                        base = (ll[d] + 1) // mak
+                        first = ll[d] - base * (mak - 1)
+                        if mak == 1:
+                            lk[d], nbc[d], mcd[d] = ll[d], [b.nbc[d][0], b.nbc[d][1]], face
+                        elif lpk == 0:
+                            lk[d], nbc[d], mcd[d] = first, [b.nbc[d][0], BC_INTER_SUBDOMAINS], [face[0], r + mpk]
+                        elif lpk < mak - 1:
+                            lk[d], nbc[d], mcd[d] = base - 1, [BC_INTER_SUBDOMAINS] * 2, [r - mpk, r + mpk]
+                        else:
+                            lk[d], nbc[d], mcd[d] = base - 1, [BC_INTER_SUBDOMAINS, b.nbc[d][1]], [r - mpk, face[1]]
+                        st[d] = 0 if lpk == 0 else first + 1 + (lpk - 1) * base
+                    assert r == len(blocks)
+                    if min(lk) < 12:
+                        raise ValueError(f"block {m}, sub-domain {pos}: {[v + 1 for v in lk]} points; the interface "
+                                         "closures need at least 13 per direction")
+                    blocks.append(BlockSpec(lk[0], lk[1], lk[2], nbc, mcd))
+                    sl = (st[2], st[1], st[0], lk[2] + 1, lk[1] + 1, lk[0] + 1)
+                    cut = (slice(None), slice(sl[0], sl[0] + sl[3]), slice(sl[1], sl[1] + sl[4]),
+                           slice(sl[2], sl[2] + sl[5]))
+                    if cs.xyz is not None:
+                        xyz.append(np.ascontiguousarray(cs.xyz[m][cut]))
+                    if cs.qa is not None:
+                        qa.append(np.ascontiguousarray(cs.qa[m][cut]))
+                    ranks.append((m, ix, jy, kz))
+                    slices.append(sl)
+    sub = {"nbpc": [list(p) for p in nbpc], "mbcd": [[list(f) for f in b.mbcd] for b in cs.blocks],
+           "ranks": ranks, "slices": slices, "shapes": [b.shape for b in cs.blocks]}
+    return dataclasses.replace(cs, blocks=blocks, xyz=xyz if cs.xyz is not None else None,
+                               qa=qa if cs.qa is not None else None, sub=sub,
+                               name=cs.name + ":" + "x".join("%d%d%d" % p for p in nbpc))
+
+
+def compose(sub: dict, arrays: Sequence[np.ndarray]) -> List[np.ndarray]:
+    """The input blocks' arrays (ncols, Z, Y, X) from the ranks' arrays of a
+    decomposed case (decompose's ``sub``)."""
+    out = [None] * len(sub["shapes"])
+    for (m, *_), sl, a in zip(sub["ranks"], sub["slices"], arrays):
+        if out[m] is None:
+            out[m] = np.zeros((a.shape[0],) + tuple(sub["shapes"][m]))
+        out[m][:, sl[0]:sl[0] + sl[3], sl[1]:sl[1] + sl[4], sl[2]:sl[2] + sl[5]] = a
+    return out

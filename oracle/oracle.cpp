@@ -360,6 +360,8 @@ struct Block {
   std::vector<double> asz, bsz;
   // junctions: src/mo_domdcomp.f90:17-34
   int njp[8], njl[12];
+  // sub-domain of parent block mb at position ijkp (src/mo_domdcomp.f90:110-119)
+  int mb = 0, ijkp[3] = {0, 0, 0};
   std::vector<int> imjp, jptag, imjl, jltag;
   std::vector<std::vector<int>> jjp, jjl;
   int jpcd[8][101], jlcd[12][101];
@@ -375,9 +377,18 @@ struct Block {
 
 }  // namespace
 
+// A block of the input (nbbc / mbcd / nbpc of nml_domdcomp) whose sub-domains
+// are ranks mo .. mo + nbpc[0] nbpc[1] nbpc[2] - 1.
+struct Parent {
+  int nbpc[3] = {1, 1, 1};
+  int mbcd[3][2];
+  int mo = 0;
+};
+
 struct orc_solver {
   orc_case_desc cs;
-  std::vector<Block> B;
+  std::vector<Block> B;       // ranks (sub-domains)
+  std::vector<Parent> P;      // blocks; by default every rank is its own block
   Coeffs C;
   double srefoo, srefp1dre, reoo, amachoo, uoo[3];
   double umf[3] = {0, 0, 0}, dudtmf[3] = {0, 0, 0};
@@ -1133,8 +1144,26 @@ void trimm(std::vector<int>& it, int& lene, int lens) {
     }
 }
 
+int idsd3_rank(const Parent& p, const int* pos) {
+  return p.mo + (pos[2] * p.nbpc[1] + pos[1]) * p.nbpc[0] + pos[0];
+}
+
+// rank of block mm's sub-domain at position (i along nn, j along nn+1, k
+// along nn+2, cyclically): src/mo_domdcomp.f90:588-605
+int idsd3(const S& s, int i, int j, int k, int mm, int nn) {
+  const Parent& p = s.P[mm];
+  int pos[3];
+  pos[nn - 1] = i;
+  pos[nn % 3] = j;
+  pos[(nn + 1) % 3] = k;
+  return p.mo + (pos[2] * p.nbpc[1] + pos[1]) * p.nbpc[0] + pos[0];
+}
+
+// search_point / search_line (src/mo_domdcomp.f90:269-437): the junctions of
+// block corners / edges over the blocks' neighbour graph, then per rank the
+// corners / edge segments it owns and the ranks owning the partners
 void search_junctions(S& s, bool points) {
-  const int mbki = s.nblk() - 1;
+  const int mbki = (int)s.P.size() - 1;
   const int per = points ? 8 : 12;
   const int lp = per * mbki + per - 1;
   std::vector<int> imj(lp + 1, 0);
@@ -1160,8 +1189,7 @@ void search_junctions(S& s, bool points) {
   for (int mm = 0; mm <= mbki; ++mm)
     for (int nn = 1; nn <= 3; ++nn)
       for (int ip = 0; ip <= 1; ++ip) {
-        // mbcd of block mm; with nbpc = 1 everywhere mcd == mbcd
-        int mp = s.B[mm].mcd[nn - 1][ip];
+        int mp = s.P[mm].mbcd[nn - 1][ip];
         if (mp == -1) continue;
         for (int i = 0; i <= 3; ++i) {
           int is = per * mm + ij[i][nn - 1][ip];
@@ -1192,8 +1220,10 @@ void search_junctions(S& s, bool points) {
     for (int c = 1; c <= imj[i]; ++c) mn = std::min(mn, jj[i][c]);
     tag[i] = mn;
   }
-  for (int mb = 0; mb <= mbki; ++mb) {
-    Block& k = s.B[mb];
+  for (int r = 0; r < s.nblk(); ++r) {
+    Block& k = s.B[r];
+    const int mb = k.mb;
+    const Parent& pb = s.P[mb];
     if (points) {
       k.imjp = imj; k.jptag = tag; k.jjp = jj;
       for (int i = 0; i < 8; ++i) {
@@ -1201,10 +1231,17 @@ void search_junctions(S& s, bool points) {
         for (int c = 0; c < 101; ++c) k.jpcd[i][c] = -1;
       }
       for (int i = 0; i <= 7; ++i) {
-        int l = 8 * mb + i;
-        if (imj[l] >= 3) {
+        const int ip = i % 2, jp = (i % 4) / 2, kp = i / 4;
+        const int l = 8 * mb + i;
+        if (k.ijkp[0] == ip * (pb.nbpc[0] - 1) && k.ijkp[1] == jp * (pb.nbpc[1] - 1) &&
+            k.ijkp[2] == kp * (pb.nbpc[2] - 1) && imj[l] >= 3) {
           k.njp[i] = l;
-          for (int c = 1; c <= imj[l]; ++c) k.jpcd[i][c] = jj[l][c] / 8;  // idsd3 with nbpc = 1
+          for (int c = 1; c <= imj[l]; ++c) {
+            const int mm = jj[l][c] / 8, j = jj[l][c] - 8 * mm;
+            const Parent& pm = s.P[mm];
+            k.jpcd[i][c] = idsd3(s, (j % 2) * (pm.nbpc[0] - 1), ((j % 4) / 2) * (pm.nbpc[1] - 1),
+                                 (j / 4) * (pm.nbpc[2] - 1), mm, 1);
+          }
         }
       }
     } else {
@@ -1214,10 +1251,19 @@ void search_junctions(S& s, bool points) {
         for (int c = 0; c < 101; ++c) k.jlcd[i][c] = -1;
       }
       for (int i = 0; i <= 11; ++i) {
-        int l = 12 * mb + i;
-        if (imj[l] >= 2) {
+        const int nn = i / 4 + 1, ns = nn % 3 + 1, ne = ns % 3 + 1;
+        const int ip = (i % 4) / 2, jp = (i % 4) % 2;
+        const int l = 12 * mb + i;
+        if (k.ijkp[nn - 1] == ip * (pb.nbpc[nn - 1] - 1) && k.ijkp[ns - 1] == jp * (pb.nbpc[ns - 1] - 1) &&
+            imj[l] >= 2) {
           k.njl[i] = l;
-          for (int c = 1; c <= imj[l]; ++c) k.jlcd[i][c] = jj[l][c] / 12;
+          for (int c = 1; c <= imj[l]; ++c) {
+            const int mm = jj[l][c] / 12, j = jj[l][c] - 12 * mm;
+            const int np = j / 4 + 1, nq = np % 3 + 1;
+            const Parent& pm = s.P[mm];
+            k.jlcd[i][c] = idsd3(s, ((j % 4) / 2) * (pm.nbpc[np - 1] - 1), ((j % 4) % 2) * (pm.nbpc[nq - 1] - 1),
+                                 k.ijkp[ne - 1], mm, np);
+          }
         }
       }
     }
@@ -1718,6 +1764,14 @@ orc_solver* orc_create(const orc_case_desc* c, const orc_block_desc* bd) {
       k.p.assign(L, 0); k.ss.assign(3 * L, 0); k.rr.assign(3 * L, 0);
       for (auto* v : {&k.txx, &k.tyy, &k.tzz, &k.txy, &k.tyz, &k.tzx, &k.hxx, &k.hyy, &k.hzz}) v->assign(L, 0);
       k.xyz.assign(3 * L, 0);
+      k.mb = b;
+    }
+    // without orc_set_subdomains every rank is a block of its own (nbpc = 1)
+    s->P.resize(c->nblocks);
+    for (int b = 0; b < c->nblocks; ++b) {
+      s->P[b].mo = b;
+      for (int d = 0; d < 3; ++d)
+        for (int ip = 0; ip < 2; ++ip) s->P[b].mbcd[d][ip] = bd[b].mbcd[d][ip];
     }
     return s;
   } catch (...) {
@@ -1726,6 +1780,34 @@ orc_solver* orc_create(const orc_case_desc* c, const orc_block_desc* bd) {
 }
 
 void orc_destroy(orc_solver* s) { delete s; }
+
+int orc_set_subdomains(orc_solver* s, int nblocks, const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub) {
+  if (!s || nblocks < 1 || !nbpc || !mbcd || !sub) return -1;
+  std::vector<Parent> P(nblocks);
+  int mo = 0;
+  for (int m = 0; m < nblocks; ++m) {
+    P[m].mo = mo;
+    for (int d = 0; d < 3; ++d) {
+      P[m].nbpc[d] = nbpc[3 * m + d];
+      if (P[m].nbpc[d] < 1) return -1;
+      for (int ip = 0; ip < 2; ++ip) P[m].mbcd[d][ip] = mbcd[6 * m + 2 * d + ip];
+    }
+    mo += P[m].nbpc[0] * P[m].nbpc[1] * P[m].nbpc[2];
+  }
+  if (mo != s->nblk()) return -1;  // one rank per sub-domain
+  for (int r = 0; r < s->nblk(); ++r) {
+    Block& k = s->B[r];
+    k.mb = sub[4 * r];
+    if (k.mb < 0 || k.mb >= nblocks) return -1;
+    for (int d = 0; d < 3; ++d) {
+      k.ijkp[d] = sub[4 * r + 1 + d];
+      if (k.ijkp[d] < 0 || k.ijkp[d] >= P[k.mb].nbpc[d]) return -1;
+    }
+    if (idsd3_rank(P[k.mb], k.ijkp) != r) return -1;  // ranks numbered as domdcomp_init numbers them
+  }
+  s->P = P;
+  return 0;
+}
 
 int orc_lmx(orc_solver* s, int b) { return s->B[b].lmx; }
 

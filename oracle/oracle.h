@@ -56,6 +56,12 @@ void orc_set_threads(int n);
 int orc_lmx(orc_solver* s, int b);
 int orc_set_grid(orc_solver* s, int b, const double* xyz);  /* (0:lmx,3) */
 int orc_setup(orc_solver* s);   /* metrics, gcbc_init, junction search, sponge */
+/* Ranks as sub-domains of split blocks (nbpc > 1; src/mo_domdcomp.f90:85-232):
+ * the create call's blocks are then the ranks, with their BC 40 faces and
+ * neighbour ranks; here the input's blocks: nbpc[m][3], mbcd[m][3][2] (block
+ * neighbours), and per rank sub[r] = (block, position along xi, eta, zeta),
+ * ranks numbered as the reference numbers them. Call before orc_setup. */
+int orc_set_subdomains(orc_solver* s, int nblocks, const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub);
 int orc_set_state(orc_solver* s, int b, const double* qa);  /* (0:lmx,5) */
 /* array ids: see ORC_A_* below; returns number of doubles written or <0 */
 long orc_get_array(orc_solver* s, int b, int which, double* out);

@@ -54,6 +54,7 @@ def lib():
             build()
         L = ctypes.CDLL(LIB)
         dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_set_subdomains.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int32)] * 3
         L.orc_create.restype = ctypes.c_void_p
         L.orc_create.argtypes = [ctypes.POINTER(_Case), ctypes.POINTER(_Block)]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
@@ -129,6 +130,16 @@ class Oracle:
         self.h = L.orc_create(ctypes.byref(self._c), self._b)
         if not self.h:
             raise RuntimeError("orc_create failed")
+        if getattr(cs, "sub", None):
+            sub = cs.sub
+            nbpc = np.ascontiguousarray(sub["nbpc"], dtype=np.int32)
+            mbcd = np.ascontiguousarray(sub["mbcd"], dtype=np.int32)
+            ranks = np.ascontiguousarray(sub["ranks"], dtype=np.int32)
+            i32p = ctypes.POINTER(ctypes.c_int32)
+            rc = L.orc_set_subdomains(self.h, len(sub["nbpc"]), nbpc.ctypes.data_as(i32p),
+                                      mbcd.ctypes.data_as(i32p), ranks.ctypes.data_as(i32p))
+            if rc != 0:
+                raise RuntimeError("orc_set_subdomains failed")
         if cs.xyz is not None:
             for i, x in enumerate(cs.xyz):
                 self.set_grid(i, x)
