@@ -7,7 +7,8 @@ src/mo_numerics.f90:97-110, src/mo_sponge.f90:210-220, src/mo_gridgen.f90:49-71)
 plus the grid coordinates and the initial conserved state of every block.
 
 Every block is one sub-domain with ``nbpc = 1`` (one rank per block in the
-reference). Field arrays use the reference layout: a NumPy array of shape
+reference); ``decompose`` splits blocks into the reference's sub-domains for
+the oracle. Field arrays use the reference layout: a NumPy array of shape
 ``(ncols, lze+1, let+1, lxi+1)`` in C order is exactly the Fortran array
 ``q(0:lmx, ncols)`` with ``l = (k*(let+1)+j)*(lxi+1)+i`` (src/mo_utils.f90:54-69).
 

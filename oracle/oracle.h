@@ -14,7 +14,8 @@
  * wavenumber, filter transfer function, constant preservation, coefficient
  * identities) in tests/test_oracle_kat.py.
  *
- * Every block is one "rank" of the reference (nbpc = 1 per block); the MPI
+ * Every block is one "rank" of the reference (nbpc = 1 per block), or, after
+ * orc_set_subdomains, every rank is a sub-domain of a split block; the MPI
  * point-to-point exchanges are reproduced by a message-matching simulator with
  * MPI's non-overtaking rule (per source/destination/tag FIFO).
  */
