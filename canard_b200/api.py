@@ -89,6 +89,8 @@ def lib():
         L.canard_restart_write_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
         L.canard_restart_read_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
         L.canard_grid_write_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.canard_average_host.argtypes = [i32, ctypes.c_void_p, i32, i32p, i32p, i32p, ctypes.POINTER(_DP)]
         L.canard_grid_read_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
         L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
@@ -246,6 +248,29 @@ def _structs(case_list: Sequence[_cases.CaseSpec]):
                 b_arr[i].nbc[d][s] = int(b.nbc[d][s])
                 b_arr[i].mbcd[d][s] = int(b.mbcd[d][s])
     return cs_arr, b_arr
+
+
+def average_host(cs: _cases.CaseSpec, qa):
+    """The junction averaging of one case (average_point, average_line,
+    average_surface) on the host, through the plans the device builds and the
+    device's arithmetic, for a case of blocks or of sub-domains
+    (cases.decompose). qa: per block / rank (5, ...); returns the averaged
+    copies."""
+    _, blocks = _structs([cs])
+    arrs = [np.ascontiguousarray(q, np.float64).copy() for q in qa]
+    ptrs = (_DP * len(arrs))(*[_dp(a) for a in arrs])
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    keep = []
+    if cs.sub:
+        for k in ("nbpc", "mbcd", "ranks"):
+            keep.append(np.ascontiguousarray(cs.sub[k], np.int32))
+        args = [len(cs.sub["nbpc"])] + [a.ctypes.data_as(i32p) for a in keep]
+    else:
+        args = [0, None, None, None]
+    rc = lib().canard_average_host(len(arrs), ctypes.cast(blocks, ctypes.c_void_p), *args, ptrs)
+    if rc:
+        raise CanardError(rc, "canard_average_host")
+    return arrs
 
 
 class Context:

@@ -334,8 +334,46 @@ std::string face_links(const std::vector<BlockGeom>& B, std::vector<FaceLink>& o
   return "";
 }
 
+Decomp unsplit(const std::vector<BlockGeom>& B) {
+  Decomp d;
+  for (int b = 0; b < (int)B.size(); ++b) {
+    Decomp::Parent p;
+    for (int a = 0; a < 3; ++a) {
+      p.nbpc[a] = 1;
+      for (int s = 0; s < 2; ++s) p.nbr[a][s] = B[b].nbr[a][s];
+    }
+    p.mo = b;
+    d.parents.push_back(p);
+    d.mb.push_back(b);
+    d.pos.push_back({0, 0, 0});
+  }
+  return d;
+}
+
+std::string check_decomp(const std::vector<BlockGeom>& B, const Decomp& d) {
+  int mo = 0;
+  for (const auto& p : d.parents) {
+    if (p.mo != mo) return "sub-domains: ranks of a block must follow the previous block's";
+    for (int a = 0; a < 3; ++a)
+      if (p.nbpc[a] < 1) return "sub-domains: nbpc must be positive";
+    mo += p.nbpc[0] * p.nbpc[1] * p.nbpc[2];
+  }
+  if (mo != (int)B.size() || d.mb.size() != B.size() || d.pos.size() != B.size())
+    return "sub-domains: one rank per sub-domain of the blocks";
+  for (int r = 0; r < (int)B.size(); ++r) {
+    const int m = d.mb[r];
+    if (m < 0 || m >= (int)d.parents.size()) return "sub-domains: rank in no block";
+    for (int a = 0; a < 3; ++a)
+      if (d.pos[r][a] < 0 || d.pos[r][a] >= d.parents[m].nbpc[a]) return "sub-domains: position outside the split";
+    if (d.idsd3(d.pos[r][0], d.pos[r][1], d.pos[r][2], m, 1) != r)
+      return "sub-domains: ranks must be numbered as the reference numbers them";
+  }
+  return "";
+}
+
 namespace {
-// Junction search of src/mo_domdcomp.f90:269-437 for nbpc = 1 (rank = block).
+// Junction search of src/mo_domdcomp.f90:269-437 over the blocks of a case
+// (the parents when they are split into sub-domains).
 struct Junction {
   std::vector<int> cnt;                 // imjp / imjl
   std::vector<std::vector<int>> list;   // jjp / jjl
@@ -355,9 +393,9 @@ void compact(std::vector<int>& it, int& lene, int lens) {  // trimm, src/mo_domd
     }
 }
 
-std::string search(const std::vector<BlockGeom>& B, bool points, Junction& J) {
+std::string search(const Decomp& D, bool points, Junction& J) {
   const int per = points ? 8 : 12;
-  const int nbl = (int)B.size();
+  const int nbl = (int)D.parents.size();
   const int lp = per * nbl - 1;
   J.cnt.assign(lp + 1, 0);
   J.list.assign(lp + 1, std::vector<int>(102, -1));
@@ -378,7 +416,7 @@ std::string search(const std::vector<BlockGeom>& B, bool points, Junction& J) {
   for (int mm = 0; mm < nbl; ++mm)
     for (int nn = 0; nn < 3; ++nn)
       for (int s = 0; s < 2; ++s) {
-        const int mp = B[mm].nbr[nn][s];
+        const int mp = D.parents[mm].nbr[nn][s];
         if (mp == -1) continue;
         for (int i = 0; i < 4; ++i) {
           const int is = per * mm + on_face[nn][s][i];
@@ -411,12 +449,50 @@ std::string search(const std::vector<BlockGeom>& B, bool points, Junction& J) {
 }  // namespace
 
 std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan& Lp) {
+  return junction_plans(B, unsplit(B), P, Lp);
+}
+
+std::string junction_plans(const std::vector<BlockGeom>& B, const Decomp& D, AvgPlan& P, AvgPlan& Lp) {
+  std::string e = check_decomp(B, D);
+  if (!e.empty()) return e;
   Junction JP, JL;
-  std::string e = search(B, true, JP);
+  e = search(D, true, JP);
   if (!e.empty()) return e;
-  e = search(B, false, JL);
+  e = search(D, false, JL);
   if (!e.empty()) return e;
-  const int nbl = (int)B.size();
+  const int nbl = (int)B.size();  // ranks
+  // search_point's owner test and partner ranks: rank b averages block corner i
+  // of its block if it holds that corner and three or more corners meet there
+  auto point_partner = [&](int b, int i, int j) -> int {
+    const int g = 8 * D.mb[b] + i;
+    if (j == 0) {
+      const Decomp::Parent& p = D.parents[D.mb[b]];
+      const int c[3] = {i % 2, (i % 4) / 2, i / 4};
+      for (int a = 0; a < 3; ++a)
+        if (D.pos[b][a] != c[a] * (p.nbpc[a] - 1)) return -1;
+      return JP.cnt[g] >= 3 ? b : -1;
+    }
+    const int mm = JP.list[g][j] / 8, jc = JP.list[g][j] - 8 * mm;
+    const Decomp::Parent& q = D.parents[mm];
+    return D.idsd3((jc % 2) * (q.nbpc[0] - 1), ((jc % 4) / 2) * (q.nbpc[1] - 1), (jc / 4) * (q.nbpc[2] - 1), mm, 1);
+  };
+  // search_line's: rank b averages its segment of block edge i if it touches
+  // the edge and two or more edges meet there; partners hold the same segment
+  auto line_partner = [&](int b, int i, int j) -> int {
+    const int g = 12 * D.mb[b] + i;
+    const int nn = i / 4 + 1, ns = nn % 3 + 1, ne = ns % 3 + 1;
+    if (j == 0) {
+      const Decomp::Parent& p = D.parents[D.mb[b]];
+      if (D.pos[b][nn - 1] != ((i % 4) / 2) * (p.nbpc[nn - 1] - 1)) return -1;
+      if (D.pos[b][ns - 1] != ((i % 4) % 2) * (p.nbpc[ns - 1] - 1)) return -1;
+      return JL.cnt[g] >= 2 ? b : -1;
+    }
+    const int mm = JL.list[g][j] / 12, jc = JL.list[g][j] - 12 * mm;
+    const int np = jc / 4 + 1, nq = np % 3 + 1;
+    const Decomp::Parent& q = D.parents[mm];
+    return D.idsd3(((jc % 4) / 2) * (q.nbpc[np - 1] - 1), ((jc % 4) % 2) * (q.nbpc[nq - 1] - 1), D.pos[b][ne - 1],
+                   mm, np);
+  };
   // ---- points (average_point, src/mo_domdcomp.f90:439-490)
   {
     Matcher M;
@@ -425,10 +501,10 @@ std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan&
     std::vector<std::vector<int>> recv_ids(nbl * 8);
     for (int b = 0; b < nbl; ++b)
       for (int i = 0; i < 8; ++i) {
-        const int g = 8 * b + i;
-        if (JP.cnt[g] < 3) continue;
+        if (point_partner(b, i, 0) < 0) continue;
+        const int g = 8 * D.mb[b] + i;
         for (int j = 1; j <= JP.cnt[g]; ++j) {
-          const int dst = JP.list[g][j] / 8;
+          const int dst = point_partner(b, i, j);
           const int64_t mid = (int64_t)owners.size();
           owners.push_back({b, i});
           M.send(b, dst, JP.tag[g], mid);
@@ -447,8 +523,8 @@ std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan&
     P = AvgPlan();
     for (int b = 0; b < nbl; ++b)
       for (int i = 0; i < 8; ++i) {
-        const int g = 8 * b + i;
-        if (JP.cnt[g] < 3) continue;
+        if (point_partner(b, i, 0) < 0) continue;
+        const int g = 8 * D.mb[b] + i;
         AvgTarget t{b, corner_l(b, i), (int)P.src_b.size(), JP.cnt[g] + 1};
         P.src_b.push_back(b);
         P.src_l.push_back(t.l);
@@ -467,10 +543,10 @@ std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan&
     std::vector<Slot> owners;
     for (int b = 0; b < nbl; ++b)
       for (int i = 0; i < 12; ++i) {
-        const int g = 12 * b + i;
-        if (JL.cnt[g] < 2) continue;
+        if (line_partner(b, i, 0) < 0) continue;
+        const int g = 12 * D.mb[b] + i;
         for (int j = 1; j <= JL.cnt[g]; ++j) {
-          const int dst = JL.list[g][j] / 12;
+          const int dst = line_partner(b, i, j);
           const int64_t mid = (int64_t)owners.size();
           owners.push_back({b, i});
           M.send(b, dst, JL.tag[g], mid);
@@ -493,8 +569,8 @@ std::string junction_plans(const std::vector<BlockGeom>& B, AvgPlan& P, AvgPlan&
     Lp = AvgPlan();
     for (int b = 0; b < nbl; ++b)
       for (int i = 0; i < 12; ++i) {
-        const int g = 12 * b + i;
-        if (JL.cnt[g] < 2) continue;
+        if (line_partner(b, i, 0) < 0) continue;
+        const int g = 12 * D.mb[b] + i;
         const int len = edge_len(b, i);
         std::vector<Slot> src;
         for (int j = 1; j <= JL.cnt[g]; ++j) {
@@ -641,3 +717,91 @@ void sponge_list(const BlockGeom& g, const canard_case_desc& c, const double* xy
 }
 
 }  // namespace canard
+
+// Junction averaging of one case on the host, through the plans the device
+// applies (k_avg_snapshot / k_avg_combine, same arithmetic in the same order):
+// the check of the plan builder against the oracle without a GPU.
+extern "C" int canard_average_host(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks,
+                                   const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub,
+                                   double* const* qa) {
+  using namespace canard;
+  if (nranks < 1 || !ranks || !qa) return CANARD_ERR_ARG;
+  std::vector<BlockGeom> B(nranks);
+  for (int r = 0; r < nranks; ++r) {
+    if (!qa[r]) return CANARD_ERR_ARG;
+    make_geom(ranks[r], 0, r, B[r]);
+  }
+  Decomp D;
+  if (nbpc) {
+    if (nblocks < 1 || !mbcd || !sub) return CANARD_ERR_ARG;
+    int mo = 0;
+    for (int m = 0; m < nblocks; ++m) {
+      Decomp::Parent p;
+      for (int a = 0; a < 3; ++a) {
+        p.nbpc[a] = nbpc[3 * m + a];
+        for (int s2 = 0; s2 < 2; ++s2) p.nbr[a][s2] = mbcd[6 * m + 2 * a + s2];
+      }
+      p.mo = mo;
+      mo += p.nbpc[0] * p.nbpc[1] * p.nbpc[2];
+      D.parents.push_back(p);
+    }
+    for (int r = 0; r < nranks; ++r) {
+      D.mb.push_back(sub[4 * r]);
+      D.pos.push_back({sub[4 * r + 1], sub[4 * r + 2], sub[4 * r + 3]});
+    }
+  } else {
+    D = unsplit(B);
+  }
+  std::vector<FaceLink> links;
+  AvgPlan P, L, S;
+  if (!face_links(B, links).empty() || !junction_plans(B, D, P, L).empty() || !surface_plan(B, links, S).empty())
+    return CANARD_ERR_UNSUPPORTED;
+  std::vector<std::vector<double>> q(nranks);
+  for (int r = 0; r < nranks; ++r) {
+    const BlockGeom& g = B[r];
+    q[r].assign((size_t)5 * g.npad, 0.0);
+    for (int c = 0; c < 5; ++c)
+      for (int z = 0; z < g.Z; ++z)
+        for (int y = 0; y < g.Y; ++y)
+          for (int x = 0; x < g.X; ++x)
+            q[r][(size_t)c * g.npad + g.dev(x, y, z)] = qa[r][(size_t)c * g.X * g.Y * g.Z + g.ref_index(x, y, z)];
+  }
+  auto apply = [&](const AvgPlan& p, int mode) {
+    std::vector<double> snap((size_t)5 * p.src_b.size());
+    for (size_t e = 0; e < p.src_b.size(); ++e)
+      for (int c = 0; c < 5; ++c) snap[5 * e + c] = q[p.src_b[e]][(size_t)c * B[p.src_b[e]].npad + p.src_l[e]];
+    for (const AvgTarget& t : p.targets) {
+      std::vector<double>& v = q[t.b];
+      const size_t np = (size_t)B[t.b].npad;
+      for (int c = 0; c < 5; ++c) {
+        if (mode == 0) {
+          double acc = snap[(size_t)t.first * 5 + c];
+          for (int j = 1; j < t.count; ++j) acc = acc + snap[(size_t)(t.first + j) * 5 + c];
+          v[t.l + c * np] = (1.0 / (double)t.count) * acc;
+        } else {
+          double x = v[t.l + c * np];
+          double r1 = 1.0;
+          for (int j = 0; j < t.count; ++j) {
+            r1 = r1 + 1.0;
+            const double r2 = 1.0 / r1;
+            x = r2 * ((r1 - 1.0) * x + snap[(size_t)(t.first + j) * 5 + c]) + 0.0 * x;
+          }
+          v[t.l + c * np] = x;
+        }
+      }
+    }
+  };
+  apply(P, 0);
+  apply(L, 0);
+  apply(S, 1);
+  for (int r = 0; r < nranks; ++r) {
+    const BlockGeom& g = B[r];
+    for (int c = 0; c < 5; ++c)
+      for (int z = 0; z < g.Z; ++z)
+        for (int y = 0; y < g.Y; ++y)
+          for (int x = 0; x < g.X; ++x)
+            qa[r][(size_t)c * g.X * g.Y * g.Z + g.ref_index(x, y, z)] = q[r][(size_t)c * g.npad + g.dev(x, y, z)];
+  }
+  return CANARD_OK;
+}
+

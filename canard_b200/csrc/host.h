@@ -4,6 +4,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "canard_gpu.h"
@@ -65,7 +66,30 @@ struct AvgPlan {
   std::vector<int> src_b;       // per source entry
   std::vector<int64_t> src_l;   // device index
 };
+// The blocks of a case split into sub-domains (nbpc > 1, src/mo_domdcomp.f90:
+// 85-232): the BlockGeoms are then the ranks. parents[m]: the split of input
+// block m and its neighbour blocks; mb[r], pos[r]: rank r's block and position.
+struct Decomp {
+  struct Parent { int nbpc[3]; int nbr[3][2]; int mo; };
+  std::vector<Parent> parents;
+  std::vector<int> mb;
+  std::vector<std::array<int, 3>> pos;
+  // rank of block mm's sub-domain at (i along nn, j along nn+1, k along nn+2)
+  // (idsd3, src/mo_domdcomp.f90:588-605); nn = 1..3
+  int idsd3(int i, int j, int k, int mm, int nn) const {
+    const Parent& p = parents[mm];
+    int q[3];
+    q[nn - 1] = i; q[nn % 3] = j; q[(nn + 1) % 3] = k;
+    return p.mo + (q[2] * p.nbpc[1] + q[1]) * p.nbpc[0] + q[0];
+  }
+};
+// Every rank its own block (nbpc = 1): the decomposition of unsplit blocks.
+Decomp unsplit(const std::vector<BlockGeom>& blocks);
+// Checks a decomposition against the ranks' geometry; empty string if sound.
+std::string check_decomp(const std::vector<BlockGeom>& ranks, const Decomp& d);
+
 std::string junction_plans(const std::vector<BlockGeom>& blocks, AvgPlan& points, AvgPlan& lines);
+std::string junction_plans(const std::vector<BlockGeom>& ranks, const Decomp& d, AvgPlan& points, AvgPlan& lines);
 
 // average_surface plan: per averaged point, its ordered list of snapshot sources.
 std::string surface_plan(const std::vector<BlockGeom>& blocks, const std::vector<FaceLink>& links,

@@ -158,6 +158,17 @@ int canard_restart_read_file(const char* path, double* time6, double* qa, int64_
  * these replace on the host side; canard_upload_grid takes the result).
  * xyz is ss(0:npts-1, 3). A file of another size returns CANARD_ERR_IO. */
 int canard_grid_write_file(const char* path, const double* xyz, int64_t npts);
+
+/* Junction averaging of one case on the host (average_point, average_line,
+ * average_surface: src/mo_domdcomp.f90:439-559, src/mo_gcbc.f90:342-422),
+ * through the same averaging plans the device builds and applies, in the same
+ * arithmetic; no device is used. ranks: the blocks, or with nbpc != NULL the
+ * sub-domains of nblocks split blocks (nbpc[m][3], mbcd[m][3][2] of the
+ * input's blocks, sub[r] = block, position along xi, eta, zeta; ranks
+ * numbered as src/mo_domdcomp.f90:588-605 numbers them). qa[r]: rank r's state
+ * (0:lmx, 5), averaged in place. For checking the plans without a GPU. */
+int canard_average_host(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks, const int32_t* nbpc,
+                        const int32_t* mbcd, const int32_t* sub, double* const* qa);
 int canard_grid_read_file(const char* path, double* xyz, int64_t npts);
 int canard_write_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 int canard_read_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);

@@ -82,3 +82,32 @@ def test_split_runs_stay_close_to_one_subdomain_per_block(make, nbpc, steps):
     rels = split_vs_plain(make(), nbpc, steps)
     print("split vs one sub-domain per block, relative L2:", rels)
     assert max(rels) < 1e-5 and min(rels) > 0, rels
+
+
+@pytest.mark.parametrize("make,nbpc", [
+    (lambda: cases.tgv(nx=24, ny=20, nz=16), None),
+    (lambda: cases.curvilinear_4block(24, 16, 14), None),
+    (lambda: cases.reference_toy(16, 14, 12), None),
+    (lambda: cases.tgv(nx=48, ny=40, nz=32), [(2, 2, 2)]),
+    (lambda: cases.reference_validation(48, 40, 12), [(2, 2, 1)]),
+    (lambda: cases.reference_toy(52, 26, 12), [(4, 2, 1)] * 6),
+    (lambda: cases.curvilinear_4block(40, 30, 28), [(2, 1, 2)] * 4),
+])
+def test_device_averaging_plans_match_the_oracle(make, nbpc):
+    """The device's junction-averaging plans (point, line, surface), built by
+    the library's plan builder and applied on the host with the device's
+    arithmetic, give the oracle's averaging phase bit for bit, for plain and
+    split cases."""
+    from canard_b200 import api
+    cs = make()
+    if nbpc:
+        cs = cases.decompose(cs, nbpc)
+    rng = np.random.default_rng(len(cs.blocks))
+    qa = [q * (1 + 1e-3 * rng.standard_normal(q.shape)) for q in cs.qa]
+    o = po.Oracle(cs)
+    for r, q in enumerate(qa):
+        o.set_state(r, q)
+    o.phase(po.PH_AVERAGE, 1)
+    got = api.average_host(cs, qa)
+    for r in range(len(cs.blocks)):
+        np.testing.assert_array_equal(got[r].reshape(-1), o.state(r).reshape(-1), err_msg=f"rank {r}")
