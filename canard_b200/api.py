@@ -91,6 +91,7 @@ def lib():
         L.canard_grid_write_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
         i32p = ctypes.POINTER(ctypes.c_int32)
         L.canard_average_host.argtypes = [i32, ctypes.c_void_p, i32, i32p, i32p, i32p, ctypes.POINTER(_DP)]
+        L.canard_set_subdomains.argtypes = [vp, i32, i32, i32p, i32p, i32p]
         L.canard_grid_read_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
         L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
@@ -286,6 +287,12 @@ class Context:
         if rc:
             raise CanardError(rc, "canard_ctx_create failed")
         self.h = h
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        for ci, cs in enumerate(self.cases):
+            if cs.sub:  # sub-domains of split blocks (cases.decompose)
+                a = [np.ascontiguousarray(cs.sub[k], np.int32) for k in ("nbpc", "mbcd", "ranks")]
+                self._check(lib().canard_set_subdomains(self.h, ci, len(cs.sub["nbpc"]),
+                                                        *[x.ctypes.data_as(i32p) for x in a]))
         if setup:
             for ci, cs in enumerate(self.cases):
                 for bi, x in enumerate(cs.xyz):

@@ -174,6 +174,9 @@ struct CaseState {
   int b0 = 0, nb = 0;
   double reoo, srefoo, srefp1dre, uoo[3];
   long long n = 0;  // host mirror of the device step counter (decides the dt-reduction launch)
+  // the case's blocks are sub-domains of split blocks (canard_set_subdomains)
+  bool split = false;
+  Decomp dec;
 };
 
 struct BlockState {
@@ -1332,7 +1335,13 @@ void build_gcbc_sponge_avg(canard_ctx* c) {
     std::string e = face_links(gs, lk);
     if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
     AvgPlan p1, l1, s1;
-    e = junction_plans(gs, p1, l1);
+    bool sub40 = false;
+    for (const auto& g : gs)
+      for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < 2; ++s) sub40 = sub40 || g.nbc[d][s] == BC_SUBDOM;
+    if (sub40 && !cs.split)
+      throw ApiError(CANARD_ERR_UNSUPPORTED, "faces with code 40 need the case's split (canard_set_subdomains)");
+    e = cs.split ? junction_plans(gs, cs.dec, p1, l1) : junction_plans(gs, p1, l1);
     if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
     e = surface_plan(gs, lk, s1);
     if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
@@ -1620,9 +1629,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
       for (int d = 0; d < 3; ++d)
         for (int s = 0; s < 2; ++s) {
           const int np = bd.nbc[d][s];
-          if (np == BC_SUBDOM)
-            throw ApiError(CANARD_ERR_UNSUPPORTED, "BC 40 needs nbpc > 1; every block here is one sub-domain");
-          if (!(np == BC_NR || np == BC_WALLI || np == BC_WALLV || np == BC_CURV || np == BC_STRAIGHT ||
+          if (!(np == BC_SUBDOM || np == BC_NR || np == BC_WALLI || np == BC_WALLV || np == BC_CURV || np == BC_STRAIGHT ||
                 np == BC_PERIODIC))
             throw ApiError(CANARD_ERR_ARG, "unknown boundary code " + std::to_string(np));
           if (np != BC_NR && np != BC_WALLI && np != BC_WALLV && (bd.mbcd[d][s] < 0 || bd.mbcd[d][s] >= cs.nb))
@@ -1827,6 +1834,38 @@ int canard_upload_grid(canard_ctx* c, int32_t icase, int32_t iblock, const doubl
     B.xyz_host.assign(xyz, xyz + 3 * L);
     h2d_field(c, B, fptr(B, F_XYZ), xyz, 3);
     CK(cudaStreamSynchronize(c->st));
+  });
+}
+
+int canard_set_subdomains(canard_ctx* c, int32_t icase, int32_t nblocks, const int32_t* nbpc, const int32_t* mbcd,
+                          const int32_t* sub) {
+  return guarded(c, [&] {
+    if (c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_set_subdomains after canard_setup");
+    if (icase < 0 || icase >= (int)c->cases.size() || nblocks < 1 || !nbpc || !mbcd || !sub)
+      throw ApiError(CANARD_ERR_ARG, "bad sub-domain argument");
+    CaseState& cs = c->cases[icase];
+    Decomp d;
+    int mo = 0;
+    for (int m = 0; m < nblocks; ++m) {
+      Decomp::Parent p;
+      for (int a = 0; a < 3; ++a) {
+        p.nbpc[a] = nbpc[3 * m + a];
+        for (int s = 0; s < 2; ++s) p.nbr[a][s] = mbcd[6 * m + 2 * a + s];
+      }
+      p.mo = mo;
+      mo += p.nbpc[0] * p.nbpc[1] * p.nbpc[2];
+      d.parents.push_back(p);
+    }
+    for (int r = 0; r < cs.nb; ++r) {
+      d.mb.push_back(sub[4 * r]);
+      d.pos.push_back({sub[4 * r + 1], sub[4 * r + 2], sub[4 * r + 3]});
+    }
+    std::vector<BlockGeom> gs;
+    for (int b = cs.b0; b < cs.b0 + cs.nb; ++b) gs.push_back(c->blocks[b].g);
+    const std::string e = check_decomp(gs, d);
+    if (!e.empty()) throw ApiError(CANARD_ERR_ARG, e);
+    cs.dec = d;
+    cs.split = true;
   });
 }
 

@@ -123,6 +123,15 @@ int canard_set_stream(canard_ctx* ctx, void* cuda_stream);
  * grid_metrics on the device, then gcbc_init, the junction searches and
  * spongeup; call it once after every block's grid is uploaded. */
 int canard_upload_grid(canard_ctx* ctx, int32_t icase, int32_t iblock, const double* xyz);
+/* Sub-domains (the reference's nbpc > 1, src/mo_domdcomp.f90:85-232): the
+ * case's blocks are then the ranks of its split input blocks, with code-40
+ * faces between sub-domains of one block; nbpc[m][3] and mbcd[m][3][2] are the
+ * input blocks' split and neighbours, sub[r] = (block, position along xi, eta,
+ * zeta) of rank r, numbered as src/mo_domdcomp.f90:588-605 numbers them.
+ * The junction averaging then follows search_point / search_line over the
+ * input blocks. Call before canard_setup; a case with code-40 faces needs it. */
+int canard_set_subdomains(canard_ctx* ctx, int32_t icase, int32_t nblocks, const int32_t* nbpc,
+                          const int32_t* mbcd, const int32_t* sub);
 int canard_setup(canard_ctx* ctx);
 int canard_set_state(canard_ctx* ctx, int32_t icase, int32_t iblock, const double* qa);
 int canard_get_state(canard_ctx* ctx, int32_t icase, int32_t iblock, double* qa);

@@ -67,14 +67,14 @@ def test_context_without_gpu_reports_an_error():
 
 
 def test_unsupported_configurations_are_rejected_before_device_work():
-    # sub-domain interfaces (BC 40, nbpc > 1) are not on this path; precisions
-    # other than FP64 and FP32-mixed do not exist
-    blk = cases.BlockSpec(16, 16, 16, [[40, 10], [10, 10], [45, 45]], [[0, -1], [-1, -1], [0, 0]])
+    # boundary codes the reference does not have; precisions other than FP64
+    # and FP32-mixed do not exist
+    blk = cases.BlockSpec(16, 16, 16, [[50, 10], [10, 10], [45, 45]], [[0, -1], [-1, -1], [0, 0]])
     cs = cases.CaseSpec([blk])
     h = ctypes.c_void_p()
     c, b = api._structs([cs])
     for prec in (api.FP64, api.FP32_MIXED):
         rc = api.lib().canard_ctx_create(c, 1, b, prec, ctypes.byref(h))
-        assert rc in (api.ERR_UNSUPPORTED, api.ERR_CUDA)
+        assert rc in (api.ERR_ARG, api.ERR_CUDA)
     c, b = api._structs([cases.tgv(16)])
     assert api.lib().canard_ctx_create(c, 1, b, 7, ctypes.byref(h)) == api.ERR_UNSUPPORTED
