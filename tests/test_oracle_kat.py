@@ -239,3 +239,20 @@ def test_golden_fixtures(name):
     o.step(nsteps)
     for b in range(len(cs.blocks)):
         np.testing.assert_array_equal(o.state(b), ref[f"qa{b}"])
+
+
+@pytest.mark.parametrize("name", __import__("golden_cases").DIGEST_CASES)
+def test_golden_digests(name):
+    """The oracle's states after 1, 10 and 100 steps and on split layouts equal
+    the frozen digests bit for bit."""
+    import hashlib
+    import json
+    from golden_cases import golden_case
+    ref = json.load(open(os.path.join(GOLDEN, "digests.json")))[name]
+    cs, nsteps = golden_case(name)
+    o = po.Oracle(cs)
+    o.step(nsteps)
+    got = [hashlib.sha256(np.ascontiguousarray(o.state(b), np.float64).tobytes()).hexdigest()
+           for b in range(len(cs.blocks))]
+    assert got == ref
+
