@@ -9,8 +9,7 @@ import pytest
 import pyoracle as po
 from canard_b200 import api, cases
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skip(reason="the device path for sub-domains has not had its first GPU run yet")]
+pytestmark = pytest.mark.gpu
 
 SPLITS = {
     "tgv_box": (lambda: cases.tgv(nx=48, ny=40, nz=32), [(2, 2, 2)]),
