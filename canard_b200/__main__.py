@@ -12,9 +12,10 @@ def main():
     p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     p.add_argument("--inviscid", action="store_true", help="the reference built without VISCOUS")
     p.add_argument("--max-steps", type=int, default=None)
+    p.add_argument("--split", action="store_true", help="run the input's sub-domains (nbpc) as its ranks")
     a = p.parse_args()
     driver.run(a.input, a.dir, precision=api.FP32_MIXED if a.precision == "fp32" else api.FP64,
-               viscous=0 if a.inviscid else 1, max_steps=a.max_steps)
+               viscous=0 if a.inviscid else 1, max_steps=a.max_steps, split=a.split)
 
 
 if __name__ == "__main__":

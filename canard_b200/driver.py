@@ -15,10 +15,13 @@ the reference's IO server ranks (src/mo_io_server.f90): the stepping thread
 copies an output's averages to the host and carries on while the file is
 written.
 
-Every block runs as one sub-domain: an input with ``nbpc > 1`` is run with one
-sub-domain per block (its interface closures then differ from the reference's
-split run at the sub-domain faces), and a warning says so. The reference's
-VISCOUS build flag is the ``viscous`` argument.
+By default every block runs as one sub-domain: an input with ``nbpc > 1`` is
+run with one sub-domain per block (its interface closures then differ from the
+reference's split run at the sub-domain faces), and a warning says so. With
+``split=True`` the blocks are split as the input says (cases.decompose): the
+ranks run as the reference's ranks do, and the restart and output files are
+still per input block, assembled from its ranks. The reference's VISCOUS build
+flag is the ``viscous`` argument.
 """
 from __future__ import annotations
 
@@ -70,17 +73,17 @@ class OutputWriter:
             raise self._err
 
 
-def case_from_input(nml, viscous: int = 1, warn=print) -> cases.CaseSpec:
+def case_from_input(nml, viscous: int = 1, warn=print, split: bool = False) -> cases.CaseSpec:
     """The case an ``input.canard`` describes (namelists as read by
     namelist.read): blocks and boundary codes from nml_domdcomp, the grid from
     nml_gridgen's generator, initialo's state, and the physics, numerics and
-    sponge parameters."""
+    sponge parameters; with ``split``, its blocks split into the ranks of nbpc."""
     drv, can, dd = nml["nml_driver"], nml["nml_canard"], nml["nml_domdcomp"]
     gg, num, phy, sp = nml["nml_gridgen"], nml["nml_numerics"], nml["nml_physics"], nml["nml_sponge"]
     nb = int(drv["mbk"]) + 1
     lxi, let, lze = (dd[k][0] for k in ("lximb", "letmb", "lzemb"))
     nbbc, mbcd, nbpc = dd["nbbc"][0], dd["mbcd"][0], dd["nbpc"][0]
-    if np.any(nbpc > 1):
+    if np.any(nbpc > 1) and not split:
         warn("canard_b200: nbpc > 1 in the input; every block runs as one sub-domain here")
     gt = int(gg["gridtype"])
     if gt == 0:
@@ -104,44 +107,86 @@ def case_from_input(nml, viscous: int = 1, warn=print) -> cases.CaseSpec:
                                          f"nml_domdcomp {b.shape[::-1]}")
         blocks.append(b)
     xyz = xyz[:nb]
-    return cases.CaseSpec(blocks, viscous=viscous, fltk=float(num["fltk"]), fltrbc=float(num["fltrbc"]),
-                          reoo=float(phy["reoo"]), tempoo=float(phy["tempoo"]),
-                          amach=(float(phy["amach1"]), float(phy["amach2"]), float(phy["amach3"])),
-                          timf=float(phy["timf"]), nsmf=int(phy["nsmf"]), cfl=float(can["cfl"]),
-                          szco=float(sp["szco"]), szth0=float(gg["szth0"]), szth1=float(gg["szth1"]),
-                          doml0=float(gg["doml0"]), doml1=float(gg["doml1"]), xyz=xyz,
-                          qa=[cases.initialo(g) for g in xyz], name="input.canard")
+    cs = cases.CaseSpec(blocks, viscous=viscous, fltk=float(num["fltk"]), fltrbc=float(num["fltrbc"]),
+                        reoo=float(phy["reoo"]), tempoo=float(phy["tempoo"]),
+                        amach=(float(phy["amach1"]), float(phy["amach2"]), float(phy["amach3"])),
+                        timf=float(phy["timf"]), nsmf=int(phy["nsmf"]), cfl=float(can["cfl"]),
+                        szco=float(sp["szco"]), szth0=float(gg["szth0"]), szth1=float(gg["szth1"]),
+                        doml0=float(gg["doml0"]), doml1=float(gg["doml1"]), xyz=xyz,
+                        qa=[cases.initialo(g) for g in xyz], name="input.canard")
+    if split and np.any(nbpc > 1):
+        cs = cases.decompose(cs, [tuple(int(v) for v in nbpc[m]) for m in range(nb)])
+    return cs
+
+
+class _Files:
+    """The per-input-block restart and output files of a case whose context
+    blocks may be ranks of split blocks (cs.sub): states and outputs are
+    assembled per input block, restart states split back to the ranks."""
+
+    def __init__(self, cs):
+        self.cs, self.sub = cs, cs.sub
+
+    def per_block(self, arrays):
+        return cases.compose(self.sub, arrays) if self.sub else list(arrays)
+
+    def grid(self):
+        return [np.asarray(x, np.float32) for x in self.per_block(self.cs.xyz)]
+
+    def write_restart(self, ctx, directory):
+        if not self.sub:
+            ctx.write_restart(directory)
+            return
+        os.makedirs(os.path.join(directory, "misc"), exist_ok=True)
+        t6 = ctx.time()
+        for m, q in enumerate(self.per_block([ctx.state(r) for r in range(len(self.cs.blocks))])):
+            api.write_restart_file(os.path.join(directory, api.restart_name(m)), t6, q)
+
+    def read_restart(self, ctx, directory):
+        if not self.sub:
+            ctx.read_restart(directory)
+            return
+        blocks = []
+        for m, shape in enumerate(self.sub["shapes"]):
+            t6, q = api.read_restart_file(os.path.join(directory, api.restart_name(m)), int(np.prod(shape)))
+            blocks.append(q.reshape((5,) + tuple(shape)))
+        for r, ((m, *_), sl) in enumerate(zip(self.sub["ranks"], self.sub["slices"])):
+            ctx.set_state(r, np.ascontiguousarray(blocks[m][:, sl[0]:sl[0] + sl[3], sl[1]:sl[1] + sl[4],
+                                                               sl[2]:sl[2] + sl[5]]))
+        ctx.set_time(t6)
 
 
 def run(input_path: str = "input.canard", directory: Optional[str] = None, precision: int = api.FP64,
-        viscous: int = 1, max_steps: Optional[int] = None, out=sys.stdout) -> dict:
+        viscous: int = 1, max_steps: Optional[int] = None, out=sys.stdout, split: bool = False) -> dict:
     """Runs the case of ``input_path`` in ``directory`` (default: the input's
     directory) like the reference's program; returns a summary (steps, time,
-    outputs written, whether the run stopped on a zero time step)."""
+    outputs written, whether the run stopped on a zero time step). ``split``:
+    run the input's sub-domains (nbpc) as the reference's ranks."""
     directory = directory or os.path.dirname(os.path.abspath(input_path))
     nml = namelist.read_file(input_path)
-    cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out))
+    cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out), split=split)
+    files = _Files(cs)
     can, drv = nml["nml_canard"], nml["nml_driver"]
     tmax, ndata = float(can["tmax"]), int(drv["ndata"])
     loutput = ndata >= 0
     ctx = api.Context(cs, precision=precision)
     if int(can["nts"]) != 0:
-        ctx.read_restart(directory)
+        files.read_restart(ctx, directory)
     if bool(can["ltimer"]):
         ctx.set_timers(True)
     outputs = []
     writer = OutputWriter()
     if loutput:
-        writer.submit(os.path.join(directory, api.plt_name(-1)), -1, [np.asarray(x, np.float32) for x in cs.xyz])
+        writer.submit(os.path.join(directory, api.plt_name(-1)), -1, files.grid())
         outputs.append(api.plt_name(-1))
         ctx.record_enable(True)
     t0 = time.perf_counter()
     try:
-        steps, _, overflow = _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out)
+        steps, _, overflow = _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out, files)
     finally:
         writer.close()  # every output file is complete when run() returns
     if int(can["nrestart"]) == 1:
-        ctx.write_restart(directory)
+        files.write_restart(ctx, directory)
     wall = time.perf_counter() - t0
     n, _, dt, _, _, timo = ctx.time()
     if overflow or dt == 0.0:
@@ -156,7 +201,7 @@ def run(input_path: str = "input.canard", directory: Optional[str] = None, preci
             "wall_s": wall, "points": cs.npts}
 
 
-def _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out):
+def _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out, files):
     """The time loop of canard_driver; returns (steps, output count - 1,
     whether it ended on a zero time step)."""
     ndati = -1
@@ -184,6 +229,7 @@ def _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out)
             if (timo - res) * (timo_new - res) <= 0.0:
                 ndati += 1
                 arrays, t_out = ctx.record_output()
+                arrays = [np.asarray(a, np.float32) for a in files.per_block(arrays)]
                 writer.submit(os.path.join(directory, api.plt_name(ndati)), ndati, arrays, t_out)
                 outputs.append(api.plt_name(ndati))
     return steps, ndati, False

@@ -270,3 +270,73 @@ def test_driver_loop_on_a_stand_in_context(tmp_path, monkeypatch, zero_dt_at):
     assert res["outputs"][0] == "data/grid.plt" and len(res["outputs"]) == len(submitted)
     assert ctx.recorded == ctx.steps and ctx.restarts == [str(tmp_path)]
     assert "Canard: Finished." in log.getvalue()
+
+
+class _SplitFake(_FakeContext):
+    """The stand-in with per-rank states."""
+
+    def __init__(self, cs, precision=0, zero_dt_at=None):
+        super().__init__(cs, precision, zero_dt_at)
+        self.q = [np.array(q) for q in cs.qa]
+        self.t_set = None
+
+    def step(self, n=1):
+        super().step(n)
+        for q in self.q:
+            q *= 1.0 + 1e-3
+
+    def state(self, b, case=0):
+        return self.q[b].copy()
+
+    def set_state(self, b, q, case=0):
+        self.q[b] = np.array(q).reshape(self.q[b].shape)
+
+    def set_time(self, t6, case=0):
+        self.t_set = list(t6)
+        self.t6 = list(t6)
+
+    def record_output(self, case=0):
+        return [q.astype(np.float32) for q in self.q], self.t6[5]
+
+
+def test_driver_split_files_are_per_input_block(tmp_path, monkeypatch):
+    """With split=True the context runs the input's ranks, and the restart and
+    output files stay one per input block, assembled from its ranks; a restart
+    read splits the block files back to the ranks."""
+    import io
+    from canard_b200 import api
+    text = SMALL.replace("lximb = 6*16", "lximb = 6*26").replace("lxi0 = 16, lxi1 = 16, lxi2 = 16",
+                                                                  "lxi0 = 26, lxi1 = 26, lxi2 = 26")
+    (tmp_path / "input.canard").write_text(text)
+    made = []
+
+    def fake(cs, precision=0):
+        made.append(_SplitFake(cs, precision))
+        return made[-1]
+
+    monkeypatch.setattr(driver.api, "Context", fake)
+    submitted = []
+    monkeypatch.setattr(driver.OutputWriter, "submit", lambda self, p, n, a, t=0.0: submitted.append((n, a)))
+    log = io.StringIO()
+    driver.run(str(tmp_path / "input.canard"), out=log, split=True)
+    ctx = made[0]
+    assert len(ctx.cs.blocks) == 12 and "nbpc > 1" not in log.getvalue()
+    # restart files: per input block, equal to its ranks' states assembled
+    blocks = cases.compose(ctx.cs.sub, ctx.q)
+    assert len(blocks) == 6
+    for m, q in enumerate(blocks):
+        t6, got = api.read_restart_file(str(tmp_path / api.restart_name(m)), q[0].size)
+        np.testing.assert_array_equal(got, q.reshape(5, -1))
+    assert not (tmp_path / api.restart_name(6)).exists()
+    # the grid and every output hold the six input blocks
+    n, grid = submitted[0]
+    assert n == -1 and len(grid) == 6 and grid[0].shape == (3, 13, 15, 27)
+    for n, arrs in submitted[1:]:
+        assert len(arrs) == 6 and arrs[1].shape == (5, 13, 15, 27)
+    # restart: the block files split back to the ranks
+    (tmp_path / "input.canard").write_text(text.replace("nts = 0", "nts = 1").replace("tmax = 0.05e0", "tmax = 0.07e0"))
+    driver.run(str(tmp_path / "input.canard"), out=io.StringIO(), split=True, max_steps=0)
+    ctx2 = made[1]
+    assert ctx2.t_set is not None and ctx2.t_set[0] == ctx.t6[0]
+    for r in range(12):
+        np.testing.assert_array_equal(ctx2.q[r], ctx.q[r])
