@@ -84,10 +84,33 @@ def test_split_runs_stay_close_to_one_subdomain_per_block(make, nbpc, steps):
     assert max(rels) < 1e-5 and min(rels) > 0, rels
 
 
+def _nonperiodic():
+    blk = cases.BlockSpec(23, 18, 16, [[10, 10], [10, 10], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
+    Z, Y, X = blk.shape
+    Zz, Yy, Xx = np.meshgrid(np.linspace(0, 1, Z), np.linspace(-0.8, 0.9, Y), np.linspace(-1, 1, X), indexing="ij")
+    rho, u, v, w, p = cases.vortex_state(Xx, Yy, 0.3, 3.0, 0.3)
+    return cases.CaseSpec([blk], viscous=1, reoo=2000.0, xyz=[np.stack([Xx, Yy, Zz])],
+                          qa=[cases._conserved(rho, u, v, w, p)])
+
+
+def _walls():
+    blk = cases.BlockSpec(22, 18, 16, [[10, 25], [25, 20], [45, 45]], [[-1, -1], [-1, -1], [0, 0]])
+    Z, Y, X = blk.shape
+    Zz, Yy, Xx = np.meshgrid(np.linspace(0, 1, Z), np.linspace(0, 1.2, Y), np.linspace(-1, 1, X), indexing="ij")
+    rho, u, v, w, p = cases.vortex_state(Xx, Yy, 0.0, 2.0, 0.3, 0.0, 0.6)
+    return cases.CaseSpec([blk], viscous=1, reoo=2000.0, amach=(0.3, 0.0, 0.0), xyz=[np.stack([Xx, Yy, Zz])],
+                          qa=[cases._conserved(rho, u, v, w, p)])
+
+
 @pytest.mark.parametrize("make,nbpc", [
     (lambda: cases.tgv(nx=24, ny=20, nz=16), None),
+    (lambda: cases.tgv(64), None),
     (lambda: cases.curvilinear_4block(24, 16, 14), None),
     (lambda: cases.reference_toy(16, 14, 12), None),
+    (lambda: cases.reference_validation(24, 20, 12), None),
+    (_nonperiodic, None),
+    (_walls, None),
+    (lambda: cases.batched(4, lo=16, hi=24)[1], None),
     (lambda: cases.tgv(nx=48, ny=40, nz=32), [(2, 2, 2)]),
     (lambda: cases.reference_validation(48, 40, 12), [(2, 2, 1)]),
     (lambda: cases.reference_toy(52, 26, 12), [(4, 2, 1)] * 6),
