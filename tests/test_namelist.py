@@ -340,3 +340,33 @@ def test_driver_split_files_are_per_input_block(tmp_path, monkeypatch):
     assert ctx2.t_set is not None and ctx2.t_set[0] == ctx.t6[0]
     for r in range(12):
         np.testing.assert_array_equal(ctx2.q[r], ctx.q[r])
+
+
+@pytest.mark.parametrize("ndata,nrestart,expect_outputs,expect_restart", [
+    (-1, 1, [], True),          # ndata < 0: no output at all (loutput = .false.)
+    (0, 0, ["data/grid.plt"], False),  # ndata = 0: the grid only; nrestart = 0: no restart file
+])
+def test_driver_output_and_restart_switches(tmp_path, monkeypatch, ndata, nrestart, expect_outputs, expect_restart):
+    import io
+    made = []
+    monkeypatch.setattr(driver.api, "Context", lambda cs, precision=0: made.append(_FakeContext(cs)) or made[-1])
+    submitted = []
+    monkeypatch.setattr(driver.OutputWriter, "submit", lambda self, p, n, a, t=0.0: submitted.append(n))
+    text = SMALL.replace("ndata = 4", "ndata = %d" % ndata).replace("nrestart = 1", "nrestart = %d" % nrestart)
+    (tmp_path / "input.canard").write_text(text)
+    res = driver.run(str(tmp_path / "input.canard"), out=io.StringIO())
+    assert res["outputs"] == expect_outputs and len(submitted) == len(expect_outputs)
+    assert bool(made[0].restarts) == expect_restart
+    assert made[0].steps > 5  # the loop ran to tmax
+
+
+def test_driver_restart_start_without_files_is_an_io_error(tmp_path):
+    """nts /= 0 reads misc/restartzNNN.da; without them the run stops before
+    its first step with the I/O error (the real context is needed for the
+    read, so this runs the read path of the split-file helper on the CPU)."""
+    from canard_b200 import api
+    cs = cases.decompose(cases.reference_validation(26, 26, 12), [(2, 2, 1)])
+    files = driver._Files(cs)
+    with pytest.raises(api.CanardError) as e:
+        files.read_restart(_SplitFake(cs), str(tmp_path))
+    assert e.value.code == api.ERR_IO
