@@ -170,33 +170,36 @@ def run(input_path: str = "input.canard", directory: Optional[str] = None, preci
     tmax, ndata = float(can["tmax"]), int(drv["ndata"])
     loutput = ndata >= 0
     ctx = api.Context(cs, precision=precision)
-    if int(can["nts"]) != 0:
-        files.read_restart(ctx, directory)
-    if bool(can["ltimer"]):
-        ctx.set_timers(True)
-    outputs = []
-    writer = OutputWriter()
-    if loutput:
-        writer.submit(os.path.join(directory, api.plt_name(-1)), -1, files.grid())
-        outputs.append(api.plt_name(-1))
-        ctx.record_enable(True)
-    t0 = time.perf_counter()
     try:
-        steps, _, overflow = _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out, files)
+        if int(can["nts"]) != 0:
+            files.read_restart(ctx, directory)
+        if bool(can["ltimer"]):
+            ctx.set_timers(True)
+        outputs = []
+        writer = OutputWriter()
+        if loutput:
+            writer.submit(os.path.join(directory, api.plt_name(-1)), -1, files.grid())
+            outputs.append(api.plt_name(-1))
+            ctx.record_enable(True)
+        t0 = time.perf_counter()
+        try:
+            steps, _, overflow = _loop(ctx, tmax, ndata, loutput, max_steps, directory, writer, outputs, out, files)
+        finally:
+            writer.close()  # every output file is complete when run() returns
+        if int(can["nrestart"]) == 1:
+            files.write_restart(ctx, directory)
+        wall = time.perf_counter() - t0
+        n, _, dt, _, _, timo = ctx.time()
+        # the loop ends on a zero time step only after step 2 (dt is 0 before)
+        if overflow or (dt == 0.0 and n > 2):
+            print(" Canard: Overflow.", file=out)
+        if bool(can["ltimer"]):
+            for name, v in ctx.timers().items():
+                if v["launches"]:
+                    print(" %-18s %10.3f ms %8d launches" % (name, v["ms"], v["launches"]), file=out)
+        print(" Canard: Finished.", file=out)
     finally:
-        writer.close()  # every output file is complete when run() returns
-    if int(can["nrestart"]) == 1:
-        files.write_restart(ctx, directory)
-    wall = time.perf_counter() - t0
-    n, _, dt, _, _, timo = ctx.time()
-    if overflow or dt == 0.0:
-        print(" Canard: Overflow.", file=out)
-    if bool(can["ltimer"]):
-        for name, v in ctx.timers().items():
-            if v["launches"]:
-                print(" %-18s %10.3f ms %8d launches" % (name, v["ms"], v["launches"]), file=out)
-    print(" Canard: Finished.", file=out)
-    ctx.close()
+        ctx.close()
     return {"steps": steps, "n": int(n), "time": float(timo), "outputs": outputs, "overflow": overflow,
             "wall_s": wall, "points": cs.npts}
 

@@ -370,3 +370,13 @@ def test_driver_restart_start_without_files_is_an_io_error(tmp_path):
     with pytest.raises(api.CanardError) as e:
         files.read_restart(_SplitFake(cs), str(tmp_path))
     assert e.value.code == api.ERR_IO
+
+
+def test_driver_stopped_early_is_not_an_overflow(tmp_path, monkeypatch):
+    import io
+    monkeypatch.setattr(driver.api, "Context", lambda cs, precision=0: _FakeContext(cs))
+    monkeypatch.setattr(driver.OutputWriter, "submit", lambda self, p, n, a, t=0.0: None)
+    (tmp_path / "input.canard").write_text(SMALL)
+    log = io.StringIO()
+    res = driver.run(str(tmp_path / "input.canard"), out=log, max_steps=1)  # dt is 0 for steps 0 and 1
+    assert res["steps"] == 1 and "Overflow" not in log.getvalue()
