@@ -67,7 +67,7 @@ const int kNnf[3] = {2, 3, 1};  // filter direction order (src/mo_numerics.f90:2
 template <class T>
 struct Table {
   T* tasks = nullptr;
-  int* first = nullptr;
+  int* first = nullptr;  // line tables: the task of every tile; others: each task's first line
   int ntasks = 0;
   int total = 0;  // tiles or lines
   size_t smem = 0;
