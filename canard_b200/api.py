@@ -92,6 +92,9 @@ def lib():
         i32p = ctypes.POINTER(ctypes.c_int32)
         L.canard_average_host.argtypes = [i32, ctypes.c_void_p, i32, i32p, i32p, i32p, ctypes.POINTER(_DP)]
         L.canard_set_subdomains.argtypes = [vp, i32, i32, i32p, i32p, i32p]
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        L.canard_plan_export.argtypes = [i32, ctypes.c_void_p, i32, i32p, i32p, i32p, i32, i64p, ctypes.c_int64,
+                                         i64p]
         L.canard_grid_read_file.argtypes = [ctypes.c_char_p, _DP, ctypes.c_int64]
         L.canard_restart_compare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
@@ -272,6 +275,41 @@ def average_host(cs: _cases.CaseSpec, qa):
     if rc:
         raise CanardError(rc, "canard_average_host")
     return arrs
+
+
+def _sub_args(cs: _cases.CaseSpec):
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    if not cs.sub:
+        return [], [0, None, None, None]
+    keep = [np.ascontiguousarray(cs.sub[k], np.int32) for k in ("nbpc", "mbcd", "ranks")]
+    return keep, [len(cs.sub["nbpc"])] + [a.ctypes.data_as(i32p) for a in keep]
+
+
+PLAN_FACES, PLAN_POINTS, PLAN_LINES, PLAN_SURFACE = 0, 1, 2, 3
+_PLAN_WIDTH = (7, 4, 4, 4, 2, 2, 2)
+
+
+def plan_export(cs: _cases.CaseSpec, kind: int) -> np.ndarray:
+    """One exchange list of a case (canard_plan_export) as an int64 array of
+    rows: kind 0 the face links (receiving rank, nn, receiving side, sending
+    rank, sending side, lines, sending face's code); 1-3 the point, line and
+    surface averaging targets (rank, l, first, count); 4-6 their sources
+    (rank, l). Host only."""
+    _, blocks = _structs([cs])
+    keep, args = _sub_args(cs)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    n = ctypes.c_int64(0)
+    call = lambda out, cap: lib().canard_plan_export(len(cs.blocks), ctypes.cast(blocks, ctypes.c_void_p), *args,
+                                                     kind, out, cap, ctypes.byref(n))
+    rc = call(None, 0)
+    if rc:
+        raise CanardError(rc, "canard_plan_export")
+    out = np.zeros(max(n.value, 1), np.int64)
+    if n.value:
+        rc = call(out.ctypes.data_as(i64p), out.size)
+        if rc:
+            raise CanardError(rc, "canard_plan_export")
+    return out[:n.value].reshape(-1, _PLAN_WIDTH[kind])
 
 
 class Context:

@@ -718,19 +718,18 @@ void sponge_list(const BlockGeom& g, const canard_case_desc& c, const double* xy
 
 }  // namespace canard
 
-// Junction averaging of one case on the host, through the plans the device
-// applies (k_avg_snapshot / k_avg_combine, same arithmetic in the same order):
-// the check of the plan builder against the oracle without a GPU.
-extern "C" int canard_average_host(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks,
-                                   const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub,
-                                   double* const* qa) {
+namespace {
+
+// Ranks, decomposition and the face-link and averaging plans of one case, from
+// the arguments canard_average_host and canard_plan_export share.
+int case_plans(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks, const int32_t* nbpc,
+               const int32_t* mbcd, const int32_t* sub, std::vector<canard::BlockGeom>& B,
+               std::vector<canard::FaceLink>& links, canard::AvgPlan& P, canard::AvgPlan& L,
+               canard::AvgPlan& S) {
   using namespace canard;
-  if (nranks < 1 || !ranks || !qa) return CANARD_ERR_ARG;
-  std::vector<BlockGeom> B(nranks);
-  for (int r = 0; r < nranks; ++r) {
-    if (!qa[r]) return CANARD_ERR_ARG;
-    make_geom(ranks[r], 0, r, B[r]);
-  }
+  if (nranks < 1 || !ranks) return CANARD_ERR_ARG;
+  B.assign(nranks, BlockGeom{});
+  for (int r = 0; r < nranks; ++r) make_geom(ranks[r], 0, r, B[r]);
   Decomp D;
   if (nbpc) {
     if (nblocks < 1 || !mbcd || !sub) return CANARD_ERR_ARG;
@@ -752,10 +751,27 @@ extern "C" int canard_average_host(int32_t nranks, const canard_block_desc* rank
   } else {
     D = unsplit(B);
   }
-  std::vector<FaceLink> links;
-  AvgPlan P, L, S;
   if (!face_links(B, links).empty() || !junction_plans(B, D, P, L).empty() || !surface_plan(B, links, S).empty())
     return CANARD_ERR_UNSUPPORTED;
+  return CANARD_OK;
+}
+
+}  // namespace
+
+// Junction averaging of one case on the host, through the plans the device
+// applies (k_avg_snapshot / k_avg_combine, same arithmetic in the same order):
+// the check of the plan builder against the oracle without a GPU.
+extern "C" int canard_average_host(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks,
+                                   const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub,
+                                   double* const* qa) {
+  using namespace canard;
+  if (nranks < 1 || !ranks || !qa) return CANARD_ERR_ARG;
+  for (int r = 0; r < nranks; ++r)
+    if (!qa[r]) return CANARD_ERR_ARG;
+  std::vector<BlockGeom> B;
+  std::vector<FaceLink> links;
+  AvgPlan P, L, S;
+  if (int rc = case_plans(nranks, ranks, nblocks, nbpc, mbcd, sub, B, links, P, L, S)) return rc;
   std::vector<std::vector<double>> q(nranks);
   for (int r = 0; r < nranks; ++r) {
     const BlockGeom& g = B[r];
@@ -805,3 +821,48 @@ extern "C" int canard_average_host(int32_t nranks, const canard_block_desc* rank
   return CANARD_OK;
 }
 
+
+// Face links and averaging plans of one case, exported for placing its ranks
+// on several devices: the pieces of every exchange a rank takes part in.
+extern "C" int canard_plan_export(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks,
+                                  const int32_t* nbpc, const int32_t* mbcd, const int32_t* sub, int32_t kind,
+                                  int64_t* out, int64_t cap, int64_t* n) {
+  using namespace canard;
+  if (kind < 0 || kind > 6 || !n || cap < 0 || (cap > 0 && !out)) return CANARD_ERR_ARG;
+  std::vector<BlockGeom> B;
+  std::vector<FaceLink> links;
+  AvgPlan plans[3];
+  if (int rc = case_plans(nranks, ranks, nblocks, nbpc, mbcd, sub, B, links, plans[0], plans[1], plans[2]))
+    return rc;
+  // device index of rank b -> index in the reference's (0:lmx) layout
+  auto ref = [&](int b, int64_t l) {
+    const BlockGeom& g = B[b];
+    const int64_t x = l % g.Xp, y = l / g.Xp % g.Y, z = l / ((int64_t)g.Xp * g.Y);
+    return g.ref_index((int)x, (int)y, (int)z);
+  };
+  std::vector<int64_t> v;
+  if (kind == 0) {
+    for (const FaceLink& L : links) {
+      const BlockGeom& g = B[L.src_b];
+      const int64_t row[7] = {L.dst_b, L.nn + 1, L.dst_side, L.src_b, L.src_side, g.nbs[L.nn],
+                              g.nbc[L.nn][L.src_side]};
+      v.insert(v.end(), row, row + 7);
+    }
+  } else if (kind <= 3) {
+    for (const AvgTarget& t : plans[kind - 1].targets) {
+      const int64_t row[4] = {t.b, ref(t.b, t.l), t.first, t.count};
+      v.insert(v.end(), row, row + 4);
+    }
+  } else {
+    const AvgPlan& p = plans[kind - 4];
+    for (size_t e = 0; e < p.src_b.size(); ++e) {
+      v.push_back(p.src_b[e]);
+      v.push_back(ref(p.src_b[e], p.src_l[e]));
+    }
+  }
+  *n = (int64_t)v.size();
+  if (cap == 0) return CANARD_OK;
+  if (cap < *n) return CANARD_ERR_ARG;
+  std::copy(v.begin(), v.end(), out);
+  return CANARD_OK;
+}

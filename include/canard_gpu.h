@@ -178,6 +178,23 @@ int canard_grid_write_file(const char* path, const double* xyz, int64_t npts);
  * (0:lmx, 5), averaged in place. For checking the plans without a GPU. */
 int canard_average_host(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks, const int32_t* nbpc,
                         const int32_t* mbcd, const int32_t* sub, double* const* qa);
+/* The exchanges of one case as lists, for placing its ranks on several
+ * devices (arguments as canard_average_host; no device is used). They are the
+ * reference's message pattern between ranks: the interface contractions and
+ * the drva exchange of mpigo / gcbc_comm (src/mo_numerics.f90:429-705,
+ * src/mo_gcbc.f90:186-220) and the sources of average_point / average_line /
+ * average_surface (src/mo_domdcomp.f90:439-559, src/mo_gcbc.f90:342-422).
+ * kind 0: face links, 7 values each: receiving rank, direction nn (1..3),
+ *   receiving side (0 start, 1 end), sending rank, sending side, lines, the
+ *   sending face's boundary code;
+ * kind 1, 2, 3: targets of the point, line and surface averaging, 4 values
+ *   each: rank, point l (reference layout), first source, source count;
+ * kind 4, 5, 6: their sources, 2 values each: rank, point l.
+ * *n receives the number of values; with cap = 0 nothing else is written, else
+ * out (cap values) receives them, CANARD_ERR_ARG if cap < *n. */
+int canard_plan_export(int32_t nranks, const canard_block_desc* ranks, int32_t nblocks, const int32_t* nbpc,
+                       const int32_t* mbcd, const int32_t* sub, int32_t kind, int64_t* out, int64_t cap,
+                       int64_t* n);
 int canard_grid_read_file(const char* path, double* xyz, int64_t npts);
 int canard_write_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);
 int canard_read_restart(canard_ctx* ctx, int32_t icase, int32_t iblock, const char* path);

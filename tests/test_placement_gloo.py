@@ -1,0 +1,192 @@
+"""A case's ranks placed on several devices (canard_b200.placement), with the
+devices played by gloo processes on the CPU. Each process holds only the states
+of its own ranks, receives the averaging sources that live on the other
+processes through the plan's send lists, and applies the junction averaging
+(average_point, average_line, average_surface: src/mo_domdcomp.f90:439-559,
+src/mo_gcbc.f90:342-422) with the device kernels' arithmetic. Together the
+processes must give the single-process result (canard_average_host) bit for
+bit. Face links are checked as a partition of the reference's message pattern."""
+import os
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from canard_b200 import api, cases, placement
+
+
+CASES = {
+    "tgv_box": (lambda: cases.tgv(nx=26, ny=24, nz=26), [(2, 1, 2)]),
+    "validation": (lambda: cases.reference_validation(48, 40, 12), [(2, 2, 1)]),
+    "curv4": (lambda: cases.curvilinear_4block(40, 30, 28), [(2, 1, 2)] * 4),
+    "toy": (lambda: cases.reference_toy(52, 26, 12), [(4, 2, 1)] * 6),
+}
+
+
+def make_case(name):
+    make, nbpc = CASES[name]
+    cs = cases.decompose(make(), nbpc)
+    rng = np.random.default_rng(len(cs.blocks))
+    qa = [np.ascontiguousarray(q * (1 + 1e-3 * rng.standard_normal(q.shape))) for q in cs.qa]
+    return cs, qa
+
+
+def apply_pass(p, d, local, recv):
+    """One averaging pass on device d: local[r] = rank r's (5, npts) state,
+    recv = (n, 5) values from the other devices in slot order. Arithmetic as
+    canard_average_host: a snapshot of every source first, then per target the
+    mean of its sources (mode 0: ordered sum times 1/count) or the running
+    average onto the point (mode 1), targets in plan order."""
+    t = p.targets
+    mine = np.flatnonzero(np.isin(t[:, 0], list(local)))
+    snap = np.zeros((len(p.sources), 5))
+    slot = p.slots[d]
+    for ent in np.concatenate([np.arange(t[i, 2], t[i, 2] + t[i, 3]) for i in mine]) if len(mine) else []:
+        r, l = p.sources[ent]
+        snap[ent] = local[r][:, l] if slot[ent] < 0 else recv[slot[ent]]
+    for i in mine:  # sequential: a point may be a target more than once
+        r, l, first, count = t[i]
+        src = snap[first:first + count]
+        if p.mode == 0:
+            acc = src[0].copy()
+            for j in range(1, count):
+                acc = acc + src[j]
+            local[r][:, l] = (1.0 / float(count)) * acc
+        else:
+            x = local[r][:, l].copy()
+            r1 = 1.0
+            for j in range(count):
+                r1 = r1 + 1.0
+                r2 = 1.0 / r1
+                x = r2 * ((r1 - 1.0) * x + src[j]) + 0.0 * x
+            local[r][:, l] = x
+
+
+def _worker(w, world, port, name, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=w, world_size=world)
+    cs, qa = make_case(name)
+    dev = placement.contiguous(cs, world)
+    plan = placement.ExchangePlan(cs, dev)
+    local = {r: qa[r].reshape(5, -1).copy() for r in np.flatnonzero(dev == w)}
+    sent = 0
+    for p in plan.passes:
+        reqs = []
+        for d in range(world):
+            pts = p.sends.get((w, d))
+            if d == w or pts is None:
+                continue
+            vals = np.stack([local[r][:, l] for r, l in pts]) if len(pts) else np.zeros((0, 5))
+            reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(vals)), d))
+            sent += vals.size
+        parts = []
+        for e in range(world):
+            pts = p.sends.get((e, w))
+            if e == w or pts is None:
+                continue
+            buf = torch.zeros((len(pts), 5), dtype=torch.float64)
+            dist.recv(buf, e)
+            parts.append(buf.numpy())
+        for q in reqs:
+            q.wait()
+        recv = np.concatenate(parts) if parts else np.zeros((0, 5))
+        apply_pass(p, w, local, recv)
+    out.put((w, {int(r): v for r, v in local.items()}, sent))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def run_world(name, world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29600 + (os.getpid() + 37 * world + len(name)) % 800
+    procs = [ctx.Process(target=_worker, args=(w, world, port, name, q)) for w in range(world)]
+    for p in procs:
+        p.start()
+    got, sent = {}, 0
+    for _ in range(world):
+        w, loc, s = q.get(timeout=300)
+        got.update(loc)
+        sent += s
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    return got, sent
+
+
+@pytest.mark.parametrize("name,world", [("tgv_box", 2), ("curv4", 2), ("curv4", 3), ("toy", 3)])
+def test_distributed_averaging_equals_the_single_process_plans(name, world):
+    cs, qa = make_case(name)
+    ref = api.average_host(cs, qa)
+    got, sent = run_world(name, world)
+    assert sorted(got) == list(range(len(cs.blocks)))
+    for r in range(len(cs.blocks)):
+        np.testing.assert_array_equal(got[r].reshape(-1), ref[r].reshape(-1), err_msg=f"rank {r}")
+    plan = placement.ExchangePlan(cs, placement.contiguous(cs, world))
+    assert sent == 5 * plan.summary()["averaging_remote_points"]
+    assert sent > 0  # the placement does cut junctions
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_face_links_are_the_reference_message_pattern(name):
+    """Every interface or curved face of every rank receives from exactly one
+    face, the one its neighbour entry names, over the same line count; the
+    placement's crossing links are the links whose two ranks sit on different
+    devices."""
+    cs, _ = make_case(name)
+    links = api.plan_export(cs, api.PLAN_FACES)
+    want = set()
+    for r, b in enumerate(cs.blocks):
+        for d in range(3):
+            for s in range(2):
+                if b.nbc[d][s] in (30, 35, 40, 45):
+                    want.add((r, d + 1, s))
+    assert sorted(map(tuple, links[:, :3].tolist())) == sorted(want)
+    for dst, nn, ds, src, ss, lines, code in links:
+        assert cs.blocks[dst].mbcd[nn - 1][ds] == src and ss == 1 - ds
+        assert code == cs.blocks[src].nbc[nn - 1][ss]
+        ext = [(q.lxi + 1, q.let + 1, q.lze + 1) for q in (cs.blocks[src], cs.blocks[dst])]
+        tr = [a for a in range(3) if a != nn - 1]
+        assert lines == ext[0][tr[0]] * ext[0][tr[1]] and ext[0][tr[0]] == ext[1][tr[0]]
+    for ndev in (2, 3):
+        dev = placement.contiguous(cs, ndev)
+        plan = placement.ExchangePlan(cs, dev)
+        cross = {tuple(x) for x in plan.cross_links.tolist()}
+        assert cross == {tuple(x) for x in links.tolist() if dev[x[0]] != dev[x[3]]}
+
+
+def test_contiguous_placement_balances_points():
+    cs = cases.decompose(cases.tgv(nx=64, ny=64, nz=64), [(1, 2, 4)])
+    for ndev in (1, 2, 4, 8):
+        dev = placement.contiguous(cs, ndev)
+        assert sorted(set(dev.tolist())) == list(range(ndev))
+        assert np.all(np.diff(dev) >= 0)  # runs of consecutive ranks
+        pts = placement.rank_points(cs)
+        load = np.array([pts[dev == d].sum() for d in range(ndev)])
+        assert load.max() - load.min() <= pts.max()
+    with pytest.raises(ValueError):
+        placement.contiguous(cs, 9)
+
+
+def test_bytes_of_one_zeta_cut():
+    """TGV box split once along zeta on 2 devices: the periodic face and the
+    sub-domain face each cross in both directions. Per crossing link and step:
+    lines x (4 stages x 9 viscous fields x 2 values x 8 B + 5 filtered fields
+    x 3 values x 8 B); averaging: the periodic face's points, 5 values per
+    stage."""
+    n = 32
+    cs = cases.decompose(cases.tgv(nx=n, ny=n, nz=n), [(1, 1, 2)])
+    plan = placement.ExchangePlan(cs, placement.contiguous(cs, 2))
+    lines = (n + 1) ** 2
+    assert len(plan.cross_links) == 4
+    m = plan.bytes_per_step(viscous=True)
+    per_link = lines * (4 * 9 * 2 * 8 + 5 * 3 * 8)
+    avg_pts = sum(len(v) for p in plan.passes for (e, d), v in p.sends.items() if e == 0)
+    assert m[0, 1] == 2 * per_link + 4 * 5 * 8 * avg_pts
+    assert avg_pts >= lines  # the periodic face's points (and its edges and corners)
+    m32 = plan.bytes_per_step(viscous=True, deriv_bytes=4)
+    assert m[0, 1] - m32[0, 1] == 2 * lines * 4 * 9 * 2 * 4
+    assert plan.bytes_per_step(viscous=False)[0, 1] == 2 * lines * (4 * 5 * 2 * 8 + 5 * 3 * 8) + 4 * 5 * 8 * avg_pts
