@@ -190,3 +190,91 @@ def test_bytes_of_one_zeta_cut():
     m32 = plan.bytes_per_step(viscous=True, deriv_bytes=4)
     assert m[0, 1] - m32[0, 1] == 2 * lines * 4 * 9 * 2 * 4
     assert plan.bytes_per_step(viscous=False)[0, 1] == 2 * lines * (4 * 5 * 2 * 8 + 5 * 3 * 8) + 4 * 5 * 8 * avg_pts
+
+
+def _mpigo_fields(cs):
+    rng = np.random.default_rng(99)
+    return [rng.standard_normal((b.lxi + 1) * (b.let + 1) * (b.lze + 1)) for b in cs.blocks]
+
+
+def _recv(o, r, nt):
+    """Rank r's receive buffers of the oracle, per direction (5 fields, 2 sides,
+    2 or 3 values, lines)."""
+    import pyoracle as po
+    flat = o.get(r, po.A_RECV0 if nt == 0 else po.A_RECV1).reshape(-1)
+    b = o.cs.blocks[r]
+    out, at = [], 0
+    for d in range(3):
+        ext = [b.lxi + 1, b.let + 1, b.lze + 1]
+        nb = ext[(d + 1) % 3] * ext[(d + 2) % 3]
+        size = 5 * 2 * (2 + nt) * nb
+        out.append(flat[at:at + size].reshape(5, 2, 2 + nt, nb))
+        at += size
+    return out
+
+
+def _mpigo_worker(w, world, port, name, nt, out):
+    import pyoracle as po
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=w, world_size=world)
+    cs, _ = make_case(name)
+    dev = placement.contiguous(cs, world)
+    plan = placement.ExchangePlan(cs, dev)
+    # this device's ranks only; the others' fields are unknown here
+    f = [x if dev[r] == w else np.full_like(x, np.nan) for r, x in enumerate(_mpigo_fields(cs))]
+    o = po.Oracle(cs, setup=False, threads=1)  # one process per device shares the cores
+    m = 2
+    o.mpigo(f, nt, 1, 0, 7, m)
+    mine = {int(r): _recv(o, r, nt) for r in np.flatnonzero(dev == w)}
+    reqs, sends = [], 0
+    for dst, nn, ds, src, ss, lines, code in plan.cross_links:
+        if code not in placement.INTERFACE_CODES:
+            continue
+        if dev[src] == w:  # computed here from this device's sender, owed to the receiver's device
+            blk = np.ascontiguousarray(_recv(o, dst, nt)[nn - 1][m - 1, ds])
+            reqs.append(dist.isend(torch.from_numpy(blk), int(dev[dst]), tag=int(dst * 6 + (nn - 1) * 2 + ds)))
+            sends += 1
+    for dst, nn, ds, src, ss, lines, code in plan.cross_links:
+        if code in placement.INTERFACE_CODES and dev[dst] == w:
+            buf = torch.zeros(mine[dst][nn - 1][m - 1, ds].shape, dtype=torch.float64)
+            dist.recv(buf, int(dev[src]), tag=int(dst * 6 + (nn - 1) * 2 + ds))
+            mine[dst][nn - 1][m - 1, ds] = buf.numpy()
+    for q in reqs:
+        q.wait()
+    out.put((w, {r: [a.copy() for a in v] for r, v in mine.items()}, sends))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,world,nt", [("tgv_box", 2, 0), ("curv4", 3, 1), ("toy", 2, 0)])
+def test_distributed_interface_contractions(name, world, nt):
+    """mpigo (src/mo_numerics.f90:429-705) with the ranks on gloo processes:
+    each process forms the contractions of its own ranks' faces (the oracle
+    stands in for the device kernel), sends those of the crossing links to the
+    receiver's process, and then holds every receive buffer of its ranks as
+    the single-process exchange fills it, bit for bit (derivative nt = 0 and
+    filter nt = 1)."""
+    import pyoracle as po
+    cs, _ = make_case(name)
+    o = po.Oracle(cs, setup=False)
+    o.mpigo(_mpigo_fields(cs), nt, 1, 0, 7, 2)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + (os.getpid() + 41 * world + 3 * nt) % 800
+    procs = [ctx.Process(target=_mpigo_worker, args=(w, world, port, name, nt, q)) for w in range(world)]
+    for p in procs:
+        p.start()
+    got, sends = {}, 0
+    for _ in range(world):
+        _, loc, s = q.get(timeout=300)
+        got.update(loc)
+        sends += s
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sends > 0
+    for r in range(len(cs.blocks)):
+        want = _recv(o, r, nt)
+        for d in range(3):
+            np.testing.assert_array_equal(got[r][d][1], want[d][1], err_msg=f"rank {r} direction {d + 1}")
