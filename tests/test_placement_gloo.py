@@ -7,6 +7,7 @@ src/mo_gcbc.f90:342-422) with the device kernels' arithmetic. Together the
 processes must give the single-process result (canard_average_host) bit for
 bit. Face links are checked as a partition of the reference's message pattern."""
 import os
+import socket
 
 import numpy as np
 import pytest
@@ -23,6 +24,12 @@ CASES = {
     "curv4": (lambda: cases.curvilinear_4block(40, 30, 28), [(2, 1, 2)] * 4),
     "toy": (lambda: cases.reference_toy(52, 26, 12), [(4, 2, 1)] * 6),
 }
+
+
+def free_port():
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
 
 
 def make_case(name):
@@ -102,7 +109,7 @@ def _worker(w, world, port, name, out):
 def run_world(name, world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29600 + (os.getpid() + 37 * world + len(name)) % 800
+    port = free_port()
     procs = [ctx.Process(target=_worker, args=(w, world, port, name, q)) for w in range(world)]
     for p in procs:
         p.start()
@@ -261,7 +268,7 @@ def test_distributed_interface_contractions(name, world, nt):
     o.mpigo(_mpigo_fields(cs), nt, 1, 0, 7, 2)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29700 + (os.getpid() + 41 * world + 3 * nt) % 800
+    port = free_port()
     procs = [ctx.Process(target=_mpigo_worker, args=(w, world, port, name, nt, q)) for w in range(world)]
     for p in procs:
         p.start()
