@@ -1,5 +1,6 @@
 """``python -m canard_b200 [input.canard] [--precision fp32] [--dir D]``: runs
-the reference's input file on the device path (canard_b200.driver)."""
+the reference's input file on the device path (canard_b200.driver).
+``--plan-devices N`` prints its ranks placed on N devices instead."""
 import argparse
 
 from . import api, driver
@@ -13,7 +14,13 @@ def main():
     p.add_argument("--inviscid", action="store_true", help="the reference built without VISCOUS")
     p.add_argument("--max-steps", type=int, default=None)
     p.add_argument("--split", action="store_true", help="run the input's sub-domains (nbpc) as its ranks")
+    p.add_argument("--plan-devices", type=int, default=0, metavar="N",
+                   help="print the input's ranks placed on N devices and the bytes they exchange; no run")
     a = p.parse_args()
+    prec = api.FP32_MIXED if a.precision == "fp32" else api.FP64
+    if a.plan_devices:
+        driver.plan_devices(a.input, a.plan_devices, viscous=0 if a.inviscid else 1, precision=prec)
+        return
     driver.run(a.input, a.dir, precision=api.FP32_MIXED if a.precision == "fp32" else api.FP64,
                viscous=0 if a.inviscid else 1, max_steps=a.max_steps, split=a.split)
 

@@ -156,6 +156,25 @@ class _Files:
         ctx.set_time(t6)
 
 
+def plan_devices(input_path: str, ndev: int, viscous: int = 1, precision: int = api.FP64,
+                 out=sys.stdout) -> dict:
+    """The input's ranks (its blocks split by nbpc) placed on ndev devices
+    (placement.contiguous) and the bytes each device would send the others per
+    time step (placement.ExchangePlan); printed and returned. No device is used."""
+    from . import placement
+    nml = namelist.read_file(input_path)
+    cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out), split=True)
+    plan = placement.ExchangePlan(cs, placement.contiguous(cs, ndev))
+    res = plan.summary(viscous=bool(viscous), deriv_bytes=4 if precision == api.FP32_MIXED else 8)
+    res["device_of_rank"] = plan.device.tolist()
+    print(f" {res['ranks']} ranks on {ndev} devices: {res['cross_links']} face links cross devices", file=out)
+    for d in range(ndev):
+        ranks = [r for r, e in enumerate(res["device_of_rank"]) if e == d]
+        print(f" device {d}: ranks {ranks[0]}-{ranks[-1]}, {res['points_per_device'][d]} points, "
+              f"{res['bytes_per_step_out'][d] / 1e6:.3f} MB out per step", file=out)
+    return res
+
+
 def run(input_path: str = "input.canard", directory: Optional[str] = None, precision: int = api.FP64,
         viscous: int = 1, max_steps: Optional[int] = None, out=sys.stdout, split: bool = False) -> dict:
     """Runs the case of ``input_path`` in ``directory`` (default: the input's

@@ -380,3 +380,20 @@ def test_driver_stopped_early_is_not_an_overflow(tmp_path, monkeypatch):
     log = io.StringIO()
     res = driver.run(str(tmp_path / "input.canard"), out=log, max_steps=1)  # dt is 0 for steps 0 and 1
     assert res["steps"] == 1 and "Overflow" not in log.getvalue()
+
+
+def test_plan_devices_of_an_input(tmp_path):
+    """--plan-devices: the input's ranks (nbpc) placed on devices, with the
+    bytes per step that cross between them; no device is used."""
+    import io
+    text = SMALL.replace("lximb = 6*16", "lximb = 6*26").replace("lxi0 = 16, lxi1 = 16, lxi2 = 16",
+                                                                  "lxi0 = 26, lxi1 = 26, lxi2 = 26")
+    (tmp_path / "input.canard").write_text(text)
+    log = io.StringIO()
+    res = driver.plan_devices(str(tmp_path / "input.canard"), 3, out=log)
+    assert res["ranks"] == 12 and res["devices"] == 3
+    assert sorted(set(res["device_of_rank"])) == [0, 1, 2]
+    assert all(b > 0 for b in res["bytes_per_step_out"])
+    assert "12 ranks on 3 devices" in log.getvalue()
+    f32 = driver.plan_devices(str(tmp_path / "input.canard"), 3, precision=1, out=io.StringIO())
+    assert all(a < b for a, b in zip(f32["bytes_per_step_out"], res["bytes_per_step_out"]))
