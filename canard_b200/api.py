@@ -254,6 +254,14 @@ def _structs(case_list: Sequence[_cases.CaseSpec]):
     return cs_arr, b_arr
 
 
+def _sub_args(cs: _cases.CaseSpec):
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    if not cs.sub:
+        return [], [0, None, None, None]
+    keep = [np.ascontiguousarray(cs.sub[k], np.int32) for k in ("nbpc", "mbcd", "ranks")]
+    return keep, [len(cs.sub["nbpc"])] + [a.ctypes.data_as(i32p) for a in keep]
+
+
 def average_host(cs: _cases.CaseSpec, qa):
     """The junction averaging of one case (average_point, average_line,
     average_surface) on the host, through the plans the device builds and the
@@ -263,26 +271,11 @@ def average_host(cs: _cases.CaseSpec, qa):
     _, blocks = _structs([cs])
     arrs = [np.ascontiguousarray(q, np.float64).copy() for q in qa]
     ptrs = (_DP * len(arrs))(*[_dp(a) for a in arrs])
-    i32p = ctypes.POINTER(ctypes.c_int32)
-    keep = []
-    if cs.sub:
-        for k in ("nbpc", "mbcd", "ranks"):
-            keep.append(np.ascontiguousarray(cs.sub[k], np.int32))
-        args = [len(cs.sub["nbpc"])] + [a.ctypes.data_as(i32p) for a in keep]
-    else:
-        args = [0, None, None, None]
+    keep, args = _sub_args(cs)
     rc = lib().canard_average_host(len(arrs), ctypes.cast(blocks, ctypes.c_void_p), *args, ptrs)
     if rc:
         raise CanardError(rc, "canard_average_host")
     return arrs
-
-
-def _sub_args(cs: _cases.CaseSpec):
-    i32p = ctypes.POINTER(ctypes.c_int32)
-    if not cs.sub:
-        return [], [0, None, None, None]
-    keep = [np.ascontiguousarray(cs.sub[k], np.int32) for k in ("nbpc", "mbcd", "ranks")]
-    return keep, [len(cs.sub["nbpc"])] + [a.ctypes.data_as(i32p) for a in keep]
 
 
 PLAN_FACES, PLAN_POINTS, PLAN_LINES, PLAN_SURFACE = 0, 1, 2, 3
