@@ -415,7 +415,6 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v_steps = []
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle as po
         from canard_b200 import cases
@@ -438,7 +437,6 @@ def main():
                 "cpu_baseline": {"value": v, "unit": "Mpoint-steps/s", "cores": threads, "kind": "port",
                                  "sample": sample},
                 "e2e": {"value": v, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        del v_steps
         print(json.dumps(line), flush=True)
         return 0
 
