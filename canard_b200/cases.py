@@ -409,6 +409,14 @@ def decompose(cs: CaseSpec, nbpc: Sequence[Sequence[int]]) -> CaseSpec:
     nbpc = [tuple(int(v) for v in p) for p in nbpc]
     if len(nbpc) != nb or any(len(p) != 3 or min(p) < 1 for p in nbpc):
         raise ValueError("nbpc needs three positive counts per block")
+    # a face's sub-domains meet the neighbouring block's at equal transverse
+    # positions (idsd3 below), so both blocks split the face alike
+    for m, b in enumerate(cs.blocks):
+        for d in range(3):
+            for mm in b.mbcd[d]:
+                if mm >= 0 and any(nbpc[mm][t] != nbpc[m][t] for t in ((d + 1) % 3, (d + 2) % 3)):
+                    raise ValueError(f"blocks {m} and {mm} split their shared face differently "
+                                     f"({nbpc[m]} and {nbpc[mm]})")
     mo = [0]
     for p in nbpc:
         mo.append(mo[-1] + p[0] * p[1] * p[2])

@@ -285,3 +285,46 @@ def test_distributed_interface_contractions(name, world, nt):
         want = _recv(o, r, nt)
         for d in range(3):
             np.testing.assert_array_equal(got[r][d][1], want[d][1], err_msg=f"rank {r} direction {d + 1}")
+
+
+def _emulate(cs, qa, dev):
+    """The devices of a placement one after the other in this process: each
+    gets exactly its plan's send lists from the others' pre-pass states."""
+    plan = placement.ExchangePlan(cs, dev)
+    local = [{r: qa[r].reshape(5, -1).copy() for r in np.flatnonzero(dev == d)} for d in range(plan.ndev)]
+    for p in plan.passes:
+        recv = []
+        for d in range(plan.ndev):
+            parts = [np.stack([local[e][r][:, l] for r, l in p.sends[(e, d)]])
+                     for e in range(plan.ndev) if e != d and (e, d) in p.sends]
+            recv.append(np.concatenate(parts) if parts else np.zeros((0, 5)))
+        for d in range(plan.ndev):
+            apply_pass(p, d, local[d], recv[d])
+    out = {}
+    for loc in local:
+        out.update(loc)
+    return out
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_splits_and_placements(seed):
+    """Random box sizes, splits and device counts (periodic TGV boxes and the
+    4-block curvilinear case): the placed averaging equals the single-process
+    plans bit for bit, and the crossing links are exactly the links between
+    devices."""
+    rng = np.random.default_rng(seed)
+    if seed % 2 == 0:
+        nbpc = [tuple(int(v) for v in rng.integers(1, 4, 3))]
+        n = [int(26 + rng.integers(0, 8)) * k for k in nbpc[0]]
+        base = cases.tgv(nx=max(n[0], 16), ny=max(n[1], 16), nz=max(n[2], 16))
+    else:
+        nbpc = [tuple(int(v) for v in rng.integers(1, 3, 3))] * 4
+        base = cases.curvilinear_4block(44, 30, 28)
+    cs = cases.decompose(base, nbpc)
+    qa = [np.ascontiguousarray(q * (1 + 1e-3 * rng.standard_normal(q.shape))) for q in cs.qa]
+    ndev = int(rng.integers(1, min(len(cs.blocks), 5) + 1))
+    dev = placement.contiguous(cs, ndev) if seed < 4 else rng.permutation(np.arange(len(cs.blocks)) % ndev)
+    got = _emulate(cs, qa, np.asarray(dev))
+    ref = api.average_host(cs, qa)
+    for r in range(len(cs.blocks)):
+        np.testing.assert_array_equal(got[r].reshape(-1), ref[r].reshape(-1), err_msg=f"rank {r}")

@@ -49,6 +49,8 @@ def test_decomposition_bookkeeping():
     np.testing.assert_array_equal(cases.compose(d.sub, d.qa)[2], cs.qa[2])
     with pytest.raises(ValueError):
         cases.decompose(cases.tgv(nx=24, ny=20, nz=16), [(2, 2, 2)])  # 12-point sub-domains
+    with pytest.raises(ValueError, match="shared face"):  # blocks 0 and 1 meet along xi, split along eta
+        cases.decompose(cs, [(1, 2, 1), (1, 1, 1), (1, 1, 1), (1, 1, 1)])
 
 
 def split_vs_plain(cs, nbpc, steps):
