@@ -935,10 +935,12 @@ void gcbc_init(S& s, Block& k) {
 }
 
 // src/mo_gcbc.f90:133-340 (setup, comm, update)
-void gcbc_all(S& s, int nk_unused, double dt) {
+// part 0: the whole of gcbc_setup, gcbc_comm and gcbc_update; 1: setup only;
+// 2: comm and update only (a test places ranks on several processes in between)
+void gcbc_all(S& s, int nk_unused, double dt, int part = 0) {
   (void)nk_unused;
   // setup
-  for (int b = 0; b < s.nblk(); ++b) {
+  for (int b = 0; b < s.nblk() && part != 2; ++b) {
     Block& k = s.B[b];
     size_t L = k.L();
     for (int nn = 1; nn <= 3; ++nn) {
@@ -971,6 +973,7 @@ void gcbc_all(S& s, int nk_unused, double dt) {
       }
     }
   }
+  if (part == 1) return;
   // comm (BC_INTER_CURV faces)
   MpiSim mpi;
   for (int b = 0; b < s.nblk(); ++b) {
@@ -1652,6 +1655,8 @@ int run_phase(S& s, int phase, int nk) {
     case ORC_PH_VISCOUS: if (s.cs.viscous) calc_viscous(s); break;
     case ORC_PH_FLUXES: calc_fluxes(s); break;
     case ORC_PH_GCBC: gcbc_all(s, nk, s.dt); break;
+    case ORC_PH_GCBC_SETUP: gcbc_all(s, nk, s.dt, 1); break;
+    case ORC_PH_GCBC_COMM_UPDATE: gcbc_all(s, nk, s.dt, 2); break;
     case ORC_PH_SPONGE: spongego(s); break;
     case ORC_PH_RKUPDATE: {
       double dtko = (s.dt * std::min(nk - 1, 1)) / (nkrk - nk + 2);

@@ -94,7 +94,8 @@ enum {
   ORC_PH_FILTER = 0, ORC_PH_COPYQO = 1, ORC_PH_PRIM = 2, ORC_PH_TIMESTEP = 3,
   ORC_PH_VISCOUS = 4, ORC_PH_FLUXES = 5, ORC_PH_GCBC = 6, ORC_PH_SPONGE = 7,
   ORC_PH_RKUPDATE = 8, ORC_PH_WALL = 9, ORC_PH_AVERAGE = 10, ORC_PH_ADVANCE = 11,
-  ORC_PH_MOVEF_A = 12
+  ORC_PH_MOVEF_A = 12,
+  ORC_PH_GCBC_SETUP = 13, ORC_PH_GCBC_COMM_UPDATE = 14 /* ORC_PH_GCBC in two parts */
 };
 
 #ifdef __cplusplus

@@ -23,6 +23,7 @@ A_RECV0, A_RECV1, A_SEND1, A_SBCC, A_SPONGE = 16, 17, 18, 19, 20
 
 PH_FILTER, PH_COPYQO, PH_PRIM, PH_TIMESTEP, PH_VISCOUS, PH_FLUXES = 0, 1, 2, 3, 4, 5
 PH_GCBC, PH_SPONGE, PH_RKUPDATE, PH_WALL, PH_AVERAGE, PH_ADVANCE, PH_MOVEF_A = 6, 7, 8, 9, 10, 11, 12
+PH_GCBC_SETUP, PH_GCBC_COMM_UPDATE = 13, 14  # PH_GCBC in two parts
 
 
 class _Block(ctypes.Structure):

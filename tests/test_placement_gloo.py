@@ -328,3 +328,80 @@ def test_random_splits_and_placements(seed):
     ref = api.average_host(cs, qa)
     for r in range(len(cs.blocks)):
         np.testing.assert_array_equal(got[r].reshape(-1), ref[r].reshape(-1), err_msg=f"rank {r}")
+
+
+def _stage_before_gcbc(cs):
+    """An oracle one step into the case, then stage 1 up to the GCBC update
+    (primitives, time step, viscous stresses, fluxes)."""
+    import pyoracle as po
+    o = po.Oracle(cs, threads=1)
+    o.step(1)
+    for ph in (po.PH_FILTER, po.PH_COPYQO, po.PH_PRIM, po.PH_TIMESTEP, po.PH_VISCOUS, po.PH_FLUXES):
+        o.phase(ph, 1)
+    return o
+
+
+def _gcbc_worker(w, world, port, name, out):
+    import pyoracle as po
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=w, world_size=world)
+    cs, _ = make_case(name)
+    dev = placement.contiguous(cs, world)
+    plan = placement.ExchangePlan(cs, dev)
+    o = _stage_before_gcbc(cs)
+    # this device knows nothing of the other devices' ranks from here on
+    for r in np.flatnonzero(dev != w):
+        for a in (po.A_QA, po.A_DE, po.A_P) + po.A_DRVA:
+            o.set(int(r), a, np.full(o.get(int(r), a).size, np.nan))
+    o.phase(po.PH_GCBC_SETUP, 1)
+    curved = [x for x in plan.cross_links.tolist() if x[6] == placement.CURVED_CODE]
+    reqs = []
+    for dst, nn, ds, src, ss, lines, code in curved:
+        if dev[src] == w:  # the sender's characteristic values, (5, lines) of its side
+            drva = o.get(src, po.A_DRVA[nn - 1]).reshape(2, 5, lines)
+            reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(drva[ss])), int(dev[dst]),
+                                   tag=int(dst * 6 + (nn - 1) * 2 + ds)))
+    for dst, nn, ds, src, ss, lines, code in curved:
+        if dev[dst] == w:  # into this device's mirror of the remote sender
+            buf = torch.zeros((5, lines), dtype=torch.float64)
+            dist.recv(buf, int(dev[src]), tag=int(dst * 6 + (nn - 1) * 2 + ds))
+            drva = o.get(src, po.A_DRVA[nn - 1]).reshape(2, 5, lines)
+            drva[ss] = buf.numpy()
+            o.set(src, po.A_DRVA[nn - 1], drva.reshape(-1))
+    for q in reqs:
+        q.wait()
+    o.phase(po.PH_GCBC_COMM_UPDATE, 1)
+    out.put((w, {int(r): o.get(int(r), po.A_DE) for r in np.flatnonzero(dev == w)}, len(reqs)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_gcbc_exchange(world):
+    """gcbc_comm (src/mo_gcbc.f90:186-220) with the ranks on gloo processes: each
+    process forms the characteristic values (drva) of its own ranks' faces, the
+    crossing curved-interface links carry them to the receiver's process, and
+    the GCBC update of every rank then equals the single-process phase bit for
+    bit (the 4-block curvilinear case, split 2 x 1 x 2 per block)."""
+    import pyoracle as po
+    cs, _ = make_case("curv4")
+    o = _stage_before_gcbc(cs)
+    o.phase(po.PH_GCBC, 1)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_gcbc_worker, args=(w, world, port, "curv4", q)) for w in range(world)]
+    for p in procs:
+        p.start()
+    got, sends = {}, 0
+    for _ in range(world):
+        _, loc, s = q.get(timeout=300)
+        got.update(loc)
+        sends += s
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sends > 0
+    for r in range(len(cs.blocks)):
+        np.testing.assert_array_equal(got[r], o.get(r, po.A_DE), err_msg=f"rank {r}")
