@@ -386,6 +386,11 @@ struct Parent {
 };
 
 struct orc_solver {
+  orc_hook_fn hook = nullptr;  // exchange hook (orc_set_hook)
+  void* hook_user = nullptr;
+  void call_hook(int kind, int a, int b, double* data = nullptr, int n = 0) {
+    if (hook) hook(hook_user, kind, a, b, data, n);
+  }
   orc_case_desc cs;
   std::vector<Block> B;       // ranks (sub-domains)
   std::vector<Parent> P;      // blocks; by default every rank is its own block
@@ -454,6 +459,7 @@ void mpigo(S& s, double* const* cols, int nt, int nrt, int n45, int itag, int m)
     }
   }
   mpi.waitall();
+  s.call_hook(0, nt, m);
   if (n45 == 1) {
     for (int b = 0; b < s.nblk(); ++b) {
       Block& k = s.B[b];
@@ -974,6 +980,7 @@ void gcbc_all(S& s, int nk_unused, double dt, int part = 0) {
     }
   }
   if (part == 1) return;
+  s.call_hook(1, 0, 0);
   // comm (BC_INTER_CURV faces)
   MpiSim mpi;
   for (int b = 0; b < s.nblk(); ++b) {
@@ -1049,6 +1056,7 @@ void gcbc_all(S& s, int nk_unused, double dt, int part = 0) {
 
 // src/mo_gcbc.f90:342-422
 void average_surface(S& s) {
+  s.call_hook(2, 2, 0);
   MpiSim mpi;
   for (int b = 0; b < s.nblk(); ++b) {
     Block& k = s.B[b];
@@ -1275,6 +1283,7 @@ void search_junctions(S& s, bool points) {
 
 // src/mo_domdcomp.f90:439-490
 void average_point(S& s) {
+  s.call_hook(2, 0, 0);
   MpiSim mpi;
   std::vector<std::vector<double>> r1(s.nblk()), r2(s.nblk());
   for (int b = 0; b < s.nblk(); ++b) {
@@ -1320,6 +1329,7 @@ void average_point(S& s) {
 
 // src/mo_domdcomp.f90:493-559
 void average_line(S& s) {
+  s.call_hook(2, 1, 0);
   MpiSim mpi;
   std::vector<std::vector<double>> r1(s.nblk()), r2(s.nblk());
   for (int b = 0; b < s.nblk(); ++b) {
@@ -1456,8 +1466,11 @@ void primitives(S& s) {  // src/mo_canard_driver.f90:267-275
 }
 
 void calc_time_step(S& s) {  // src/mo_physics.f90:171-211
-  double res1 = -1e300, res2 = -1e300;
-  for (auto& k : s.B) {
+  const int nb = s.nblk();
+  std::vector<double> res(2 * nb, -1e300);  // per rank: res1, then res2
+  for (int b = 0; b < nb; ++b) {
+    Block& k = s.B[b];
+    double res1 = -1e300, res2 = -1e300;
     size_t L = k.L();
     const double *de = k.de.data(), *xi = k.xim.data(), *et = k.etm.data(), *ze = k.zem.data();
     for (size_t l = 0; l < L; ++l) {
@@ -1478,6 +1491,15 @@ void calc_time_step(S& s) {  // src/mo_physics.f90:171-211
       res1 = std::max(res1, (std::sqrt(de[l + 4 * L] * r1) + r2) * ssi);
       if (s.cs.viscous) res2 = std::max(res2, (((de[l] * k.ss[l]) * r1) * ssi) * ssi);
     }
+    res[b] = res1;
+    res[nb + b] = res2;
+  }
+  s.call_hook(3, 0, 0, res.data(), nb);
+  // the maximum does not depend on the order of the ranks
+  double res1 = -1e300, res2 = -1e300;
+  for (int b = 0; b < nb; ++b) {
+    res1 = std::max(res1, res[b]);
+    res2 = std::max(res2, res[nb + b]);
   }
   double ra0 = s.cs.cfl / res1;
   double ra1 = ra0;
@@ -1913,11 +1935,12 @@ int orc_set_array(orc_solver* s, int b, int which, const double* in) {
     for (int i = 0; i < 9; ++i) std::copy(in + i * k.L(), in + (i + 1) * k.L(), v[i]->begin());
     return 0;
   }
-  if (which == ORC_A_SEND1) {
+  if (which == ORC_A_SEND1 || which == ORC_A_RECV0 || which == ORC_A_RECV1) {
+    std::vector<double>* v = which == ORC_A_SEND1 ? k.send1 : which == ORC_A_RECV0 ? k.recv0 : k.recv1;
     long p = 0;
     for (int d = 0; d < 3; ++d) {
-      std::copy(in + p, in + p + k.send1[d].size(), k.send1[d].begin());
-      p += (long)k.send1[d].size();
+      std::copy(in + p, in + p + v[d].size(), v[d].begin());
+      p += (long)v[d].size();
     }
     return 0;
   }
@@ -1935,6 +1958,11 @@ int orc_step(orc_solver* s, int nsteps) {
     std::fprintf(stderr, "orc_step: %s\n", e.what());
     return -2;
   }
+}
+
+void orc_set_hook(orc_solver* s, orc_hook_fn fn, void* user) {
+  s->hook = fn;
+  s->hook_user = user;
 }
 
 int orc_phase(orc_solver* s, int phase, int nk) {

@@ -72,6 +72,16 @@ int orc_phase(orc_solver* s, int phase, int nk);
 int orc_get_time(orc_solver* s, double* out6); /* n, ndt, dt, dts, dte, timo */
 int orc_set_time(orc_solver* s, const double* in6);
 
+/* Exchange hook, for tests that hold a case's ranks in several processes: it
+ * is called where one rank's step reads another rank's data. kind 0: after
+ * mpigo's messages arrived (a = nt, b = m), before the periodic correction;
+ * kind 1: after gcbc_setup, before gcbc_comm; kind 2: before average_point
+ * (a = 0), average_line (1) and average_surface (2); kind 3: in
+ * calc_time_step, data = the per-rank maxima res1[0:n] then res2[0:n], which
+ * the hook may overwrite before they are reduced. NULL removes the hook. */
+typedef void (*orc_hook_fn)(void* user, int kind, int a, int b, double* data, int n);
+void orc_set_hook(orc_solver* s, orc_hook_fn fn, void* user);
+
 /* unit operations (mirror t_numerics) */
 int orc_mpigo(orc_solver* s, double* const* fields, int ncols, int nt, int nrt,
               int n45, int itag, int m);

@@ -42,6 +42,9 @@ class _Case(ctypes.Structure):
 
 
 _lib = None
+# orc_hook_fn: (user, kind, a, b, data, n)
+HOOK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                        ctypes.POINTER(ctypes.c_double), ctypes.c_int)
 
 
 def build():
@@ -74,6 +77,7 @@ def lib():
                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_deriv.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int]
         L.orc_filte.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int]
+        L.orc_set_hook.argtypes = [ctypes.c_void_p, HOOK, ctypes.c_void_p]
         L.orc_coeffs.argtypes = [ctypes.c_double, ctypes.c_double, dp]
         L.orc_penta.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_int, dp, dp]
@@ -204,6 +208,22 @@ class Oracle:
         rc = lib().orc_mpigo(self.h, arr, 1, nt, nrt, n45, itag, m)
         if rc != 0:
             raise RuntimeError("orc_mpigo")
+
+    def set_hook(self, fn):
+        """fn(kind, a, b, data) at the oracle's exchange points (orc_set_hook);
+        data is a NumPy view of the hook's doubles (empty for kinds 0-2).
+        None removes it."""
+        if fn is None:
+            self._hook = None
+            lib().orc_set_hook(self.h, HOOK(), None)
+            return
+
+        def tramp(_user, kind, a, b, data, n):
+            view = np.ctypeslib.as_array(data, shape=(2 * n,)) if n else np.zeros(0)
+            fn(kind, a, b, view)
+
+        self._hook = HOOK(tramp)  # kept alive while registered
+        lib().orc_set_hook(self.h, self._hook, None)
 
     def deriv(self, b, fin, fout, nn, m):
         rc = lib().orc_deriv(self.h, b, _dp(fin), _dp(fout), nn, m)

@@ -405,3 +405,159 @@ def test_distributed_gcbc_exchange(world):
     assert sends > 0
     for r in range(len(cs.blocks)):
         np.testing.assert_array_equal(got[r], o.get(r, po.A_DE), err_msg=f"rank {r}")
+
+
+class _DeviceHook:
+    """Exchange hook of one process holding the ranks of one device: at each
+    point where the single-process oracle reads another rank's data it moves
+    exactly what the placement's plan says crosses devices, and no more. The
+    other devices' ranks are mirrors whose state is NaN."""
+
+    def __init__(self, o, plan, w):
+        import pyoracle as po
+        self.po, self.o, self.plan, self.w = po, o, plan, w
+        self.dev = plan.device
+        self.rounds = 0
+
+    def _swap(self, items):
+        """items: (src rank, dst rank, tag, get(), put(value)) of crossing
+        pieces; sends those this device owns, receives those it needs."""
+        reqs = []
+        for src, dst, tag, get, _ in items:
+            if self.dev[src] == self.w and self.dev[dst] != self.w:
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(get())), int(self.dev[dst]), tag=tag))
+        for src, dst, tag, get, put in items:
+            if self.dev[dst] == self.w and self.dev[src] != self.w:
+                buf = torch.from_numpy(np.zeros_like(get()))
+                dist.recv(buf, int(self.dev[src]), tag=tag)
+                put(buf.numpy())
+        for q in reqs:
+            q.wait()
+        self.rounds += 1
+
+    def __call__(self, kind, a, b, data):
+        po, o = self.po, self.o
+        links = self.plan.cross_links
+        if kind == 0:  # mpigo: the receiver's buffer slot, filled on the sender's device
+            nt, m, which = a, b, (po.A_RECV0 if a == 0 else po.A_RECV1)
+            cache = {}
+
+            def buf(r):
+                if r not in cache:
+                    cache[r] = o.get(r, which)
+                return cache[r]
+
+            def slot(r, nn, side):
+                blk = o.cs.blocks[r]
+                ext = [blk.lxi + 1, blk.let + 1, blk.lze + 1]
+                sizes = [5 * 2 * (2 + nt) * ext[(d + 1) % 3] * ext[(d + 2) % 3] for d in range(3)]
+                at = sum(sizes[:nn - 1])
+                return buf(r)[at:at + sizes[nn - 1]].reshape(5, 2, 2 + nt, -1)[m - 1, side]
+
+            items = []
+            for dst, nn, ds, src, ss, lines, code in links.tolist():
+                if code in placement.INTERFACE_CODES:
+                    def put(v, dst=dst, nn=nn, ds=ds):
+                        slot(dst, nn, ds)[...] = v
+                    items.append((src, dst, dst * 6 + (nn - 1) * 2 + ds, lambda dst=dst, nn=nn, ds=ds: slot(dst, nn, ds),
+                                  put))
+            self._swap(items)
+            for r in cache:
+                if self.dev[r] == self.w:
+                    o.set(r, which, cache[r])
+        elif kind == 1:  # gcbc_comm: the sender's drva, into this device's mirror of it
+            items = []
+            for dst, nn, ds, src, ss, lines, code in links.tolist():
+                if code != placement.CURVED_CODE:
+                    continue
+
+                def get(src=src, nn=nn, ss=ss, lines=lines):
+                    return o.get(src, po.A_DRVA[nn - 1]).reshape(2, 5, lines)[ss]
+
+                def put(v, src=src, nn=nn, ss=ss, lines=lines):
+                    d = o.get(src, po.A_DRVA[nn - 1]).reshape(2, 5, lines)
+                    d[ss] = v
+                    o.set(src, po.A_DRVA[nn - 1], d.reshape(-1))
+                items.append((src, dst, dst * 6 + (nn - 1) * 2 + ds, get, put))
+            self._swap(items)
+        elif kind == 2:  # an averaging pass: the remote sources, into the mirrors
+            p = self.plan.passes[a]
+            reqs = []
+            for (e, d), pts in p.sends.items():
+                if e == self.w:
+                    q = {r: o.get(int(r), po.A_QA).reshape(5, -1) for r in np.unique(pts[:, 0])}
+                    vals = np.stack([q[r][:, l] for r, l in pts])
+                    reqs.append(dist.isend(torch.from_numpy(vals), int(d), tag=100 + a))
+            for (e, d), pts in p.sends.items():
+                if d == self.w:
+                    buf = torch.zeros((len(pts), 5), dtype=torch.float64)
+                    dist.recv(buf, int(e), tag=100 + a)
+                    for r in np.unique(pts[:, 0]):
+                        q = o.get(int(r), po.A_QA).reshape(5, -1)
+                        sel = pts[:, 0] == r
+                        q[:, pts[sel, 1]] = buf.numpy()[sel].T
+                        o.set(int(r), po.A_QA, q.reshape(-1))
+            for q in reqs:
+                q.wait()
+            self.rounds += 1
+        elif kind == 3:  # the time step's maxima: this device's ranks, then MAX over devices
+            n = len(data) // 2
+            mine = self.dev == self.w
+            t = torch.tensor([data[:n][mine].max(), data[n:][mine].max()], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            data[:n] = t[0].item()
+            data[n:] = t[1].item()
+            self.rounds += 1
+
+
+def _step_worker(w, world, port, name, steps, out):
+    import pyoracle as po
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=w, world_size=world)
+    cs, qa = make_case(name)
+    dev = placement.contiguous(cs, world)
+    plan = placement.ExchangePlan(cs, dev)
+    o = po.Oracle(cs, threads=1)
+    for r in range(len(cs.blocks)):
+        o.set_state(r, qa[r] if dev[r] == w else np.full_like(qa[r], np.nan))
+    hook = _DeviceHook(o, plan, w)
+    o.set_hook(hook)
+    o.step(steps)
+    o.set_hook(None)
+    out.put((w, {int(r): o.state(int(r)) for r in np.flatnonzero(dev == w)}, hook.rounds))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,world", [("tgv_box", 2), ("curv4", 3)])
+def test_distributed_time_steps(name, world):
+    """Whole time steps with the ranks on gloo processes: each process holds
+    the state of its own device's ranks only (the others are NaN), and the
+    plan's exchanges (interface contractions, curved-interface drva, averaging
+    sources, the time step's maxima) are all that crosses between processes.
+    After 4 steps every rank equals the single-process run bit for bit."""
+    import pyoracle as po
+    cs, qa = make_case(name)
+    o = po.Oracle(cs)
+    for r in range(len(cs.blocks)):
+        o.set_state(r, qa[r])
+    o.step(4)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_step_worker, args=(w, world, port, name, 4, q)) for w in range(world)]
+    for p in procs:
+        p.start()
+    got, rounds = {}, []
+    for _ in range(world):
+        _, loc, n = q.get(timeout=600)
+        got.update(loc)
+        rounds.append(n)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert len(set(rounds)) == 1 and rounds[0] > 0  # every process took the same exchange steps
+    for r in range(len(cs.blocks)):
+        assert np.all(np.isfinite(got[r]))
+        np.testing.assert_array_equal(got[r], o.state(r), err_msg=f"rank {r}")
