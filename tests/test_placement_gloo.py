@@ -530,7 +530,7 @@ def _step_worker(w, world, port, name, steps, out):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name,world", [("tgv_box", 2), ("curv4", 3)])
+@pytest.mark.parametrize("name,world", [("tgv_box", 2), ("curv4", 3), ("toy", 3), ("validation", 2)])
 def test_distributed_time_steps(name, world):
     """Whole time steps with the ranks on gloo processes: each process holds
     the state of its own device's ranks only (the others are NaN), and the
