@@ -156,13 +156,32 @@ class _Files:
         ctx.set_time(t6)
 
 
-def plan_devices(input_path: str, ndev: int, viscous: int = 1, precision: int = api.FP64,
+def gpu_options(nml, precision=None, viscous=None, max_steps=None, split=None) -> dict:
+    """The run's options: each argument that is not None, else the input's
+    &nml_gpu value (defaults: FP64, viscous, no step limit, no split)."""
+    g = nml["nml_gpu"]
+    if precision is None:
+        if int(g["nprecision"]) not in (api.FP64, api.FP32_MIXED):
+            raise namelist.NamelistError(f"&nml_gpu: nprecision {int(g['nprecision'])} (0 FP64, 1 FP32-mixed)")
+        precision = int(g["nprecision"])
+    if viscous is None:
+        viscous = 0 if bool(g["linviscid"]) else 1
+    if max_steps is None and int(g["nsteps"]) > 0:
+        max_steps = int(g["nsteps"])
+    if split is None:
+        split = bool(g["lsplit"])
+    return {"precision": precision, "viscous": viscous, "max_steps": max_steps, "split": split}
+
+
+def plan_devices(input_path: str, ndev: int, viscous: Optional[int] = None, precision: Optional[int] = None,
                  out=sys.stdout) -> dict:
     """The input's ranks (its blocks split by nbpc) placed on ndev devices
     (placement.contiguous) and the bytes each device would send the others per
     time step (placement.ExchangePlan); printed and returned. No device is used."""
     from . import placement
     nml = namelist.read_file(input_path)
+    opt = gpu_options(nml, precision=precision, viscous=viscous)
+    viscous, precision = opt["viscous"], opt["precision"]
     cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out), split=True)
     plan = placement.ExchangePlan(cs, placement.contiguous(cs, ndev))
     res = plan.summary(viscous=bool(viscous), deriv_bytes=4 if precision == api.FP32_MIXED else 8)
@@ -175,14 +194,18 @@ def plan_devices(input_path: str, ndev: int, viscous: int = 1, precision: int = 
     return res
 
 
-def run(input_path: str = "input.canard", directory: Optional[str] = None, precision: int = api.FP64,
-        viscous: int = 1, max_steps: Optional[int] = None, out=sys.stdout, split: bool = False) -> dict:
+def run(input_path: str = "input.canard", directory: Optional[str] = None, precision: Optional[int] = None,
+        viscous: Optional[int] = None, max_steps: Optional[int] = None, out=sys.stdout,
+        split: Optional[bool] = None) -> dict:
     """Runs the case of ``input_path`` in ``directory`` (default: the input's
     directory) like the reference's program; returns a summary (steps, time,
     outputs written, whether the run stopped on a zero time step). ``split``:
-    run the input's sub-domains (nbpc) as the reference's ranks."""
+    run the input's sub-domains (nbpc) as the reference's ranks. Options left
+    at None come from the input's &nml_gpu group (gpu_options)."""
     directory = directory or os.path.dirname(os.path.abspath(input_path))
     nml = namelist.read_file(input_path)
+    opt = gpu_options(nml, precision=precision, viscous=viscous, max_steps=max_steps, split=split)
+    precision, viscous, max_steps, split = opt["precision"], opt["viscous"], opt["max_steps"], opt["split"]
     cs = case_from_input(nml, viscous=viscous, warn=lambda s: print(s, file=out), split=split)
     files = _Files(cs)
     can, drv = nml["nml_canard"], nml["nml_driver"]

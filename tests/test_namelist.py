@@ -397,3 +397,35 @@ def test_plan_devices_of_an_input(tmp_path):
     assert "12 ranks on 3 devices" in log.getvalue()
     f32 = driver.plan_devices(str(tmp_path / "input.canard"), 3, precision=1, out=io.StringIO())
     assert all(a < b for a, b in zip(f32["bytes_per_step_out"], res["bytes_per_step_out"]))
+
+
+def test_nml_gpu_options(tmp_path, monkeypatch):
+    """&nml_gpu carries this implementation's options (precision, split, a step
+    limit, inviscid) in a group the reference never reads; arguments given to
+    run() win over it; an input without the group keeps the defaults."""
+    import io
+    base = SMALL.replace("lximb = 6*16", "lximb = 6*26").replace("lxi0 = 16, lxi1 = 16, lxi2 = 16",
+                                                                  "lxi0 = 26, lxi1 = 26, lxi2 = 26")
+    text = base + "\n&nml_gpu nprecision = 1, lsplit = .true., nsteps = 3, linviscid = .true. /\n"
+    r = namelist.read(text)
+    assert int(r["nml_gpu"]["nprecision"]) == 1 and bool(r["nml_gpu"]["lsplit"]) and int(r["nml_gpu"]["nsteps"]) == 3
+    assert driver.gpu_options(namelist.read(base)) == {"precision": 0, "viscous": 1, "max_steps": None,
+                                                       "split": False}
+    made = []
+
+    def fake(cs, precision=0):
+        made.append(_SplitFake(cs, precision))
+        made[-1].precision = precision
+        return made[-1]
+
+    monkeypatch.setattr(driver.api, "Context", fake)
+    monkeypatch.setattr(driver.OutputWriter, "submit", lambda self, p, n, a, t=0.0: None)
+    (tmp_path / "input.canard").write_text(text)
+    driver.run(str(tmp_path / "input.canard"), out=io.StringIO())
+    ctx = made[-1]
+    assert ctx.precision == 1 and len(ctx.cs.blocks) == 12 and ctx.steps == 3 and ctx.cs.viscous == 0
+    driver.run(str(tmp_path / "input.canard"), out=io.StringIO(), precision=0, split=False, max_steps=2, viscous=1)
+    ctx = made[-1]
+    assert ctx.precision == 0 and len(ctx.cs.blocks) == 6 and ctx.steps == 2 and ctx.cs.viscous == 1
+    with pytest.raises(namelist.NamelistError):
+        driver.gpu_options(namelist.read(base + "\n&nml_gpu nprecision = 2 /\n"))
