@@ -15,7 +15,8 @@ memory copied in and out every step. Multi-GPU runs are independent replicas
 (the single-block case has no partition on this path), so scaling is weak.
 
 `--impl reference` times the reference algorithm on the host CPU cores (the
-oracle restatement: the Fortran reference cannot be compiled in this image).
+oracle restatement: the Fortran reference cannot be compiled in this image)
+on the same workload, --warmup untimed and --steps timed full steps.
 """
 import argparse
 import json
@@ -49,11 +50,10 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                    help="fp64: plain FP64 path (bit-exact with the oracle); fp32: FP32 line solves, fluxes, "
                         "viscous stresses and GCBC with the FP64 state, RK update, metrics and LU factors")
-    p.add_argument("--cpu-n", type=int, default=128, help="cells per direction of the CPU sample")
     p.add_argument("--acc-nx", type=int, default=384)
     p.add_argument("--acc-ny", type=int, default=256)
     p.add_argument("--acc-nz", type=int, default=128)
-    p.add_argument("--cpu-steps", type=int, default=2)
+    p.add_argument("--cpu-steps", type=int, default=5)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--mode", default="step", choices=["step", "kernels", "accuracy", "cpu"],
@@ -77,26 +77,6 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def cpu_arm(n, steps, warmup=0):
-    """Oracle (CPU restatement of the reference) on a TGV sample; returns
-    Mpoint-steps/s, thread count, sample description."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-    from canard_b200 import cases
-    threads = os.cpu_count() or 1
-    cs = cases.tgv(n)
-    o = po.Oracle(cs, threads=threads)
-    if warmup:
-        o.step(warmup)
-    t0 = time.perf_counter()
-    o.step(steps)
-    dt = time.perf_counter() - t0
-    v = cs.npts * steps / dt / 1e6
-    sample = (f"TGV {n}^3 cells ({n + 1}^3 points), viscous FP64, {steps} full steps after set-up"
-              f"{' and ' + str(warmup) + ' warm-up steps' if warmup else ''}, OpenMP over lines")
-    return v, threads, sample, dt
 
 
 def state_errors(qg, qr, uref):
@@ -202,6 +182,61 @@ def batched_extra(args, api, cases, torch, stream):
     return out
 
 
+def workload_cases(args, cases, world=1, rank=0):
+    """The timed cases of this rank, all cases of the job and the workload's
+    description (one for both arms, so that the reference arm runs the same
+    config)."""
+    if args.config == "tgv":
+        case_list = all_cases = [cases.tgv(args.n)]
+        workload = (f"tgv{args.n}: Taylor-Green vortex {args.n}^3 cells ({args.n + 1}^3 points), Re 1600, "
+                    "Mach 0.1, viscous, FP64 plain, full time step")
+    elif args.config == "batched":
+        from canard_b200 import shard
+        all_cases = cases.batched(64, seed=11)
+        mine = shard.my_cases([c.npts for c in all_cases], world, rank)
+        case_list = [all_cases[i] for i in mine]
+        workload = ("batched: 64 independent single-block cases (sides 32..96, TGV / periodic vortex, "
+                    "Mach 0.1-0.5, Re 400-3200), FP64, one launch per phase and direction for all cases"
+                    + (f", sharded over {world} ranks by point count" if world > 1 else ""))
+    elif args.config == "curv4":
+        case_list = all_cases = [cases.curvilinear_4block()]
+        workload = "curv4: 4 blocks of 192x128x64 cells, curvilinear, GCBC in/outflow, sponge, Re 1e5, FP64"
+    else:
+        case_list = all_cases = [cases.vortex()]
+        workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
+    if args.precision == "fp32":
+        workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
+    return case_list, all_cases, workload
+
+
+def config_dict(args, workload, ncases, job_points, npts, world):
+    """The bench line's config, the same for the device arm and the reference arm."""
+    return {"workload": workload, "cases": ncases, "points": job_points, "precision": args.precision,
+            "l2": "inputs larger than L2 (state, metrics and work fields ~"
+                  f"{(54 * 8 + (41 * 4 if args.precision == 'fp32' else 0)) * npts / 1e9:.1f} GB resident on the "
+                  "device; larger than the host caches on the CPU arm too)",
+            "parallelism": ("case shards" if args.config == "batched" else "replicas") if world > 1 else "single"}
+
+
+def oracle_rate(case_list, steps, warmup, threads):
+    """The oracle (CPU restatement of the reference) over the cases, one after
+    the other: Mpoint-steps/s of `steps` timed steps after `warmup` untimed
+    ones, and the timed seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    npts, secs = 0, 0.0
+    for cs in case_list:
+        o = po.Oracle(cs, threads=threads)
+        if warmup:
+            o.step(warmup)
+        t0 = time.perf_counter()
+        o.step(steps)
+        secs += time.perf_counter() - t0
+        npts += cs.npts
+        del o
+    return npts * steps / secs / 1e6, secs
+
+
 def config_cases(args, cases):
     if args.config == "tgv":
         return [cases.tgv(args.n)], f"tgv{args.n}"
@@ -268,18 +303,25 @@ def kernels_mode(args, api, cases, torch):
     rows = []
     # fp64-tmem: the FP64 eta/zeta kernel that keeps the elimination results in
     # tensor memory (an autotuner candidate), pinned for the comparison
-    for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP32_MIXED, "fp32")):
+    # fp32-stream: the mixed filter that streams the FP64 state into FP32
+    # right-hand sides (an autotuner candidate), pinned for the comparison
+    for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP32_MIXED, "fp32"),
+                       (api.FP32_MIXED, "fp32-stream")):
         ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
         for op in (0, 1):
+            if name == "fp32-stream" and op == 0:
+                continue
             for nn in (1, 2, 3):
                 if name == "fp64-tmem" and nn > 1:
                     ctx.set_line_kind("flux" if op == 0 else "filter", "xi eta zeta".split()[nn - 1], "fp64-tmem")
+                if name == "fp32-stream":
+                    ctx.set_line_kind("filter", "xi eta zeta".split()[nn - 1], "fp64-stream/fp32-split")
                 # xi runs on the shared-memory tiles here too: the filter's interface calls
                 # advance the send chains of all directions in the oracle's order
                 out, ms = ctx.line_bench(op, nn, fields, reps=args.steps)
                 if name == "fp64-tmem" and nn == 1:
                     continue
-                es = 4 if (name == "fp32" and op == 0) else 8
+                es = 4 if (name.startswith("fp32") and op == 0) else 8
                 gbs = 5 * blk.npts * 2 * es / (ms / 1e3) / 1e9
                 r = ref[(op, nn)]
                 err = float(np.linalg.norm((out - r).ravel()) / np.linalg.norm(r.ravel()))
@@ -415,27 +457,21 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle as po
         from canard_b200 import cases
         threads = os.cpu_count() or 1
-        cs = cases.tgv(args.cpu_n)
-        o = po.Oracle(cs, threads=threads)
-        o.step(args.warmup)
-        t0 = time.perf_counter()
-        o.step(args.steps)
-        dt = time.perf_counter() - t0
-        v = cs.npts * args.steps / dt / 1e6
-        sample = (f"each step = one full reference time step of TGV {args.cpu_n}^3 cells "
-                  f"({args.cpu_n + 1}^3 points), viscous FP64, on the host CPU")
+        case_list, all_cases, workload = workload_cases(args, cases)
+        v, secs = oracle_rate(case_list, args.steps, args.warmup, threads)
+        npts = sum(c.npts for c in case_list)
+        sample = (f"the whole workload ({len(case_list)} case(s), {npts} points): {args.warmup} warm-up and "
+                  f"{args.steps} timed full reference time steps, FP64, OpenMP over lines on the host CPU")
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpoint-steps/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded TGV initial condition)",
-                "config": {"workload": f"tgv{args.n}: Taylor-Green vortex, viscous, FP64 plain, full step",
-                           "cpu_sample": f"tgv{args.cpu_n}"},
-                "cpu_baseline": {"value": v, "unit": "Mpoint-steps/s", "cores": threads, "kind": "port",
-                                 "sample": sample},
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak" if args.config != "batched" else "strong",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
+                "config": config_dict(args, workload, len(case_list), npts, npts, 1),
+                "cpu_baseline": {"value": v, "unit": "Mpoint-steps/s", "cores": threads,
+                                 "kind": "port", "sample": sample},
                 "e2e": {"value": v, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -457,29 +493,10 @@ def main():
         return 0
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
-    if args.config == "tgv":
-        case_list = [cases.tgv(args.n)]
-        workload = (f"tgv{args.n}: Taylor-Green vortex {args.n}^3 cells ({args.n + 1}^3 points), Re 1600, "
-                    "Mach 0.1, viscous, FP64 plain, full time step")
-    elif args.config == "batched":
-        from canard_b200 import shard
-        all_cases = cases.batched(64, seed=11)
-        mine = shard.my_cases([c.npts for c in all_cases], world, rank)
-        case_list = [all_cases[i] for i in mine]
-        workload = ("batched: 64 independent single-block cases (sides 32..96, TGV / periodic vortex, "
-                    "Mach 0.1-0.5, Re 400-3200), FP64, one launch per phase and direction for all cases"
-                    + (f", sharded over {world} ranks by point count" if world > 1 else ""))
-    elif args.config == "curv4":
-        case_list = [cases.curvilinear_4block()]
-        workload = "curv4: 4 blocks of 192x128x64 cells, curvilinear, GCBC in/outflow, sponge, Re 1e5, FP64"
-    else:
-        case_list = [cases.vortex()]
-        workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
+    case_list, all_cases, workload = workload_cases(args, cases, world, rank)
     prec = api.FP32_MIXED if args.precision == "fp32" else api.FP64
     ctx = api.Context(case_list, precision=prec)
     tuning = None if args.no_autotune else ctx.autotune(reps=3)
-    if args.precision == "fp32":
-        workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
     # a non-default stream: the library launches on it and the CUDA events
     # below are recorded on it (handle 0 would mean the context's own stream)
     stream = torch.cuda.Stream()
@@ -524,28 +541,40 @@ def main():
     fam = ctx.timers()
     ctx.set_timers(False)
     tot = sum(f["ms"] for f in fam.values())
-    dom_name, dom = max(((k, v) for k, v in fam.items() if k.startswith(("deriv", "filter"))),
-                        key=lambda kv: kv[1]["ms"])
-    line_fams = {k: v for k, v in fam.items() if k.startswith(("deriv", "filter"))}
-    lb = sum(v["bytes"] for v in line_fams.values())
-    lms = sum(v["ms"] for v in line_fams.values())
     peak, peak_kind = peaks()
-    achieved = dom["bytes"] / dom["launches"] / (dom["ms"] / dom["launches"] / 1e3) / 1e9
-    # DRAM bytes per launch from the ncu capture of a smaller case, scaled by the
-    # algorithmic bytes of this launch (the capture covers the FP64 kernels)
-    traffic = None
+    # DRAM bytes per algorithmic byte of each family's kernel from an ncu
+    # capture of a smaller case (FP64 kernels), scaled to this launch
+    ratios = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath) and args.precision == "fp64":
         try:
-            r = json.load(open(tpath)).get(dom_name)
-            if r:
-                traffic = r["dram_bytes_per_algorithmic_byte"] * dom["bytes"] / dom["launches"]
+            ratios = {k: v["dram_bytes_per_algorithmic_byte"] for k, v in json.load(open(tpath)).items()}
         except Exception:
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": f"k_line ({dom_name})", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": dom["bytes"] / dom["launches"],
-                "all_line_solves_gbs": lb / (lms / 1e3) / 1e9}
+            ratios = {}
+
+    def family_roofline(name, kernel):
+        f = fam[name]
+        per = f["bytes"] / f["launches"]
+        achieved = per / (f["ms"] / f["launches"] / 1e3) / 1e9
+        return {"bound": "hbm", "kernel": f"{kernel} ({name})", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": ratios[name] * per if name in ratios else None,
+                "algorithmic_bytes_per_launch": per, "share_of_step": f["ms"] / tot if tot else 0.0}
+
+    # the dominant kernel: the single kernel with the largest share of the step
+    # (each family is one kernel; the line solves are one kernel per direction)
+    kernel_of = {"flux_components": "k_flux_visc", "rk_update": "k_rk_next", "primitives": "k_prim"}
+    cands = [(k, v) for k, v in fam.items() if v["launches"] and v["bytes"] > 0
+             and (k in kernel_of or k.startswith(("deriv", "filter")))]
+    dom_name = max(cands, key=lambda kv: kv[1]["ms"])[0]
+    roofline = family_roofline(dom_name, kernel_of.get(dom_name, "k_line"))
+    line_fams = {k: v for k, v in fam.items() if k.startswith(("deriv", "filter")) and v["launches"]}
+    ln = max(line_fams, key=lambda k: line_fams[k]["ms"])
+    roofline_line = family_roofline(ln, "k_line")
+    lb = sum(v["bytes"] for v in line_fams.values())
+    lms = sum(v["ms"] for v in line_fams.values())
+    roofline_line["all_line_solves_gbs"] = lb / (lms / 1e3) / 1e9
+    roofline_line["all_line_solves_share"] = lms / tot if tot else 0.0
 
     # end to end through the C ABI: pinned host state in and out every step
     hosts = []
@@ -591,7 +620,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         ctx.close()
         torch.cuda.empty_cache()
-        v, th, sample, _ = cpu_arm(args.cpu_n, args.cpu_steps)
+        th = os.cpu_count() or 1
+        v, _ = oracle_rate(case_list, args.cpu_steps, 1, th)
+        sample = (f"the timed workload itself ({npts} points): 1 warm-up and {args.cpu_steps} timed full reference "
+                  "time steps, FP64, OpenMP over lines")
         cpu = {"value": v, "unit": "Mpoint-steps/s", "cores": th, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -599,14 +631,10 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": scaling, "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
-                "config": {"workload": workload, "cases": len(case_list), "points": job_points, "precision": args.precision,
-                           "autotuned": not args.no_autotune,
-                           "l2": "inputs larger than L2 (state, metrics and work fields ~"
-                                 f"{(54 * 8 + (41 * 4 if args.precision == 'fp32' else 0)) * npts / 1e9:.1f} GB "
-                                 "resident)",
-                           "parallelism": ("case shards" if args.config == "batched" else "replicas")
-                           if world > 1 else "single"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "config": config_dict(args, workload, len(case_list), job_points, npts, world),
+                "autotuned": not args.no_autotune,
+                "roofline": roofline, "roofline_line_solve": roofline_line,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks,
                 "families": {k: {"ms_per_step": v["ms"], "share": v["ms"] / tot if tot else 0.0,
                                  "launches": v["launches"]} for k, v in fam.items() if v["launches"]}}

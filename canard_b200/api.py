@@ -85,6 +85,7 @@ def lib():
         L.canard_set_field.argtypes = [vp, i32, i32, i32, _DP, ctypes.c_int64]
         L.canard_step.argtypes = [vp, i32]
         L.canard_phase.argtypes = [vp, i32, i32]
+        L.canard_phase_with.argtypes = [vp, i32, i32, ctypes.c_double, _DP, _DP]
         L.canard_get_time.argtypes = [vp, i32, _DP]
         L.canard_restart_write_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
         L.canard_restart_read_file.argtypes = [ctypes.c_char_p, _DP, _DP, ctypes.c_int64]
@@ -121,6 +122,7 @@ def lib():
         L.canard_selftest_wait.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.canard_deriv_noalloc.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, ctypes.c_double,
                                            ctypes.c_double, vp]
+        L.canard_deriv_noalloc_status.argtypes = [vp]
         L.canard_coeffs.argtypes = [ctypes.c_double, ctypes.c_double, _DP]
         L.canard_penta.argtypes = [ctypes.c_double, ctypes.c_double, i32, i32, i32, i32, _DP, _DP]
         _lib = L
@@ -379,7 +381,7 @@ class Context:
         if k < 0:
             self._check(-k)
         kinds = {0: "fp64", 1: "fp32-split", 2: "fp64-tile/fp32-split", 3: "fp32-one-lane",
-                 4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem"}
+                 4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem", 6: "fp64-stream/fp32-split"}
         out = []
         for i in range(k):
             g, d, kd, nc, best, dflt = rep[6 * i:6 * i + 6]
@@ -389,7 +391,7 @@ class Context:
         return out
 
     LINE_KINDS = {"default": -1, "fp64": 0, "fp32-split": 1, "fp64-tile/fp32-split": 2, "fp32-one-lane": 3,
-                  "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5}
+                  "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5, "fp64-stream/fp32-split": 6}
 
     def set_line_kind(self, group, direction, kind, chunks=0):
         """Pins the line kernel of a group ("filter", "viscous", "flux") and
@@ -451,6 +453,13 @@ class Context:
 
     def phase(self, ph, nk=0):
         self._check(lib().canard_phase(self.h, ph, nk))
+
+    def phase_with(self, ph, nk, dt, umf, dudtmf=(0.0, 0.0, 0.0)):
+        """A fluxes / GCBC / RK update / wall phase with the stage's dt and
+        moving frame given as the reference's routines receive them."""
+        u = np.ascontiguousarray(umf, dtype=np.float64)
+        a = np.ascontiguousarray(dudtmf, dtype=np.float64)
+        self._check(lib().canard_phase_with(self.h, ph, nk, float(dt), _dp(u), _dp(a)))
 
     def time(self, case=0):
         out = np.zeros(6)

@@ -3,7 +3,7 @@
 A case is the content of the reference's ``input.canard`` namelists for one run
 (``nml_domdcomp``, ``nml_numerics``, ``nml_physics``, ``nml_canard``,
 ``nml_sponge``; see src/mo_io.f90:35-66, src/mo_physics.f90:86-111,
-src/mo_numerics.f90:97-110, src/mo_sponge.f90:210-220, src/mo_gridgen.f90:49-71)
+src/mo_numerics.f90:97-110, src/mo_sponge.f90:20-30, src/mo_gridgen.f90:49-71)
 plus the grid coordinates and the initial conserved state of every block.
 
 Every block is one sub-domain with ``nbpc = 1`` (one rank per block in the
@@ -171,7 +171,7 @@ def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, v
 
 
 def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, seed=7,
-                       viscous=1, sponge_cells=20) -> CaseSpec:
+                       viscous=1, sponge_cells=20, inflow_sponge_cells=None) -> CaseSpec:
     """Four blocks tiled 2x2 in (xi, eta) on x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta),
     y = eta + 0.05 sin(2 pi xi), z = zeta with unit index spacing h = 1/128.
 
@@ -184,8 +184,13 @@ def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, s
     The uniform stream (Mach ``mach`` along x) is carried by the moving frame
     (amach1 = mach, nsmf = 1), with 1% seeded velocity noise. The sponge covers
     the last ``sponge_cells`` cells before the outflow (szth1 = half of it,
-    src/mo_sponge.f90:238-249)."""
-    h = 1.0 / 128.0
+    src/mo_sponge.f90:46-51)."""
+    # x and y spacing 1/nyb (1/128 at the stated size): the two block rows span
+    # eta in [0, 2], whole periods of sin(2 pi eta); zeta spans [0, 1] over the
+    # nzb cells, one period of sin(2 pi zeta), so the grid is smooth across
+    # both periodic seams
+    h = 1.0 / nyb
+    hz = 1.0 / nzb
     NX, NY, NZ = 2 * nxb, 2 * nyb, nzb
     blocks = []
     for bj in range(2):
@@ -215,7 +220,7 @@ def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, s
             j = bj * nyb + np.arange(nyb + 1)
             k = np.arange(nzb + 1)
             Kz, Jy, Ix = np.meshgrid(k, j, i, indexing="ij")
-            xi, eta, zeta = Ix * h, Jy * h, Kz * h
+            xi, eta, zeta = Ix * h, Jy * h, Kz * hz
             X = xi + 0.05 * np.sin(2 * np.pi * eta) * np.sin(2 * np.pi * zeta)
             Y = eta + 0.05 * np.sin(2 * np.pi * xi)
             Z = zeta
@@ -228,8 +233,9 @@ def curvilinear_4block(nxb=192, nyb=128, nzb=64, mach=0.4, re=1e5, noise=0.01, s
             w = noise * mach * rng.standard_normal(shape)
             qa.append(_conserved(rho, u, v, w, p))
     xmax = NX * h
+    ni = sponge_cells if inflow_sponge_cells is None else inflow_sponge_cells
     return CaseSpec(blocks, viscous=viscous, reoo=re, amach=(mach, 0.0, 0.0), nsmf=1,
-                    szco=1.0, szth0=0.0, szth1=0.5 * sponge_cells * h, doml0=0.0, doml1=xmax,
+                    szco=1.0, szth0=0.5 * ni * h, szth1=0.5 * sponge_cells * h, doml0=0.0, doml1=xmax,
                     xyz=xyz, qa=qa, name=f"curv4x{nxb}x{nyb}x{nzb}")
 
 

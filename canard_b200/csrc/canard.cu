@@ -87,11 +87,14 @@ enum LineKind {
   LK_F64_TILE_F32_SOLVE = 2,   // split
   LK_F32_1L = 3,
   LK_F64_TILE_F32_SOLVE_1L = 4,
-  LK_F64_TM = 5                // FP64, elimination results in TMEM (eta/zeta, 16 <= L <= 257)
+  LK_F64_TM = 5,               // FP64, elimination results in TMEM (eta/zeta, 16 <= L <= 257)
+  LK_F64_STREAM_F32 = 6        // filter: FP64 field streamed into FP32 right-hand sides, split FP32 solve
 };
 inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L; }
 inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
-inline int tile_lanes(int kind) { return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE) ? kHalf : kLanes; }
+inline int tile_lanes(int kind) {
+  return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_STREAM_F32) ? kHalf : kLanes;
+}
 
 // First row of the second half of a split solve: balances the two halves'
 // register-constant rows (the first half's rows below c0 use the tables
@@ -460,14 +463,54 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   }
 }
 
+// the largest dynamic shared memory a line kernel's CTA may request (sm_100a:
+// 227 KiB per block)
+constexpr int kLineSmemMax = 227 * 1024;
+
 // dynamic shared memory of one task's tile
 size_t line_smem(int dir, const LineTask& t, int kind) {
   if (kind == LK_F64_TM) return kTmSmem;
+  if (kind == LK_F64_STREAM_F32)  // FP32 right-hand-side tile only (no copies in flight)
+    return (size_t)kHalf * (dir == 0 ? dir1_pitch<float>(t.L) : t.L) * sizeof(float);
   const size_t es = tile_elem(kind);
   const int lanes = tile_lanes(kind);
   if (dir == 0)
     return 128 + (size_t)lanes * (kind_f32_fields(kind) ? dir1_pitch<float>(t.L) : dir1_pitch<double>(t.L)) * es;
   return 128 + (size_t)t.nbox * t.by * lanes * es;
+}
+
+// shared memory of a default-chunked tile of lines of L points
+size_t tile_smem_for(int dir, int L, int kind) {
+  LineTask t{};
+  t.L = L;
+  chunking_dir(dir, L, t.nbox, t.by);
+  return line_smem(dir, t, kind);
+}
+
+// the longest line of direction dir whose tile of this kind fits in a CTA
+int max_tile_points(int dir, int kind) {
+  int L = 13;
+  while (L < 8192 && tile_smem_for(dir, L + 1, kind) <= (size_t)kLineSmemMax) ++L;
+  return L;
+}
+
+// Lines too long for the shared-memory tile of any kind the context's step
+// uses are rejected up front (a launch would fail and lose the context).
+void check_line_lengths(const BlockGeom& g, bool f32) {
+  static const char* dn[3] = {"xi", "eta", "zeta"};
+  for (int dir = 0; dir < 3; ++dir) {
+    const int L = g.ijk[0][dir] + 1;
+    const int kinds64[1] = {LK_F64};
+    const int kinds32[2] = {LK_F64_TILE_F32_SOLVE, LK_F32};
+    const int* ks = f32 ? kinds32 : kinds64;
+    const int nk = f32 ? 2 : 1;
+    for (int i = 0; i < nk; ++i)
+      if (tile_smem_for(dir, L, ks[i]) > (size_t)kLineSmemMax)
+        throw ApiError(CANARD_ERR_UNSUPPORTED,
+                       std::string("lines of ") + std::to_string(L) + " points along " + dn[dir] +
+                           " do not fit the shared-memory line tile (at most " +
+                           std::to_string(max_tile_points(dir, ks[i])) + " points in this precision)");
+  }
 }
 
 // cuTensorMapEncodeTiled from the driver, found at run time (the library does
@@ -603,6 +646,14 @@ void launch_line_tm_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
+template <int DIR>
+void launch_filt2s_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, T_FILTER_XI + DIR - 1, T.bytes);
+  launch_filt2s_t<DIR>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, c->derr);
+  CK(cudaGetLastError());
+}
+
 template <int DIR, int OP>
 void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   if (T.kind == LK_F64) launch_line_dir<DIR, OP, double, double>(c, T);
@@ -611,6 +662,7 @@ void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE) launch_line2_dir<DIR, 1, double>(c, T);
   else if (OP == 0 && T.kind == LK_F32_1L) launch_line_dir<DIR, 0, float, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE_1L) launch_line_dir<DIR, 1, double, float>(c, T);
+  else if (OP == 1 && T.kind == LK_F64_STREAM_F32) launch_filt2s_dir<DIR>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -626,10 +678,17 @@ void launch_line(canard_ctx* c, const Table<LineTask>& T, int dir, int op) {
   }
 }
 
+// The dynamic shared memory limit is a per-device function attribute: it is
+// raised once for every device this process uses (with that device current).
 void set_line_smem_limits() {
-  static bool done = false;
-  if (done) return;
-  const int lim = 227 * 1024;
+  static std::mutex mu;
+  static bool done_dev[256] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) throw ApiError(CANARD_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (done_dev[dev]) return;
+  const int lim = kLineSmemMax;
   CK((line_smem_limit<1, 0, double, double>(lim)));
   CK((line_smem_limit<2, 0, double, double>(lim)));
   CK((line_smem_limit<3, 0, double, double>(lim)));
@@ -652,7 +711,10 @@ void set_line_smem_limits() {
   CK((line_tm_smem_limit<3, 0>()));
   CK((line_tm_smem_limit<2, 1>()));
   CK((line_tm_smem_limit<3, 1>()));
-  done = true;
+  CK((filt2s_smem_limit<1>(lim)));
+  CK((filt2s_smem_limit<2>(lim)));
+  CK((filt2s_smem_limit<3>(lim)));
+  done_dev[dev] = true;
 }
 
 // ---- mpigo face tasks ----------------------------------------------------------
@@ -1603,8 +1665,6 @@ void destroy(canard_ctx* c) {
 
 void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const canard_block_desc* blocks) {
   if (!cases || !blocks || ncases <= 0) throw ApiError(CANARD_ERR_ARG, "null or empty case list");
-  CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
-  c->st = c->own;
   int b0 = 0;
   for (int i = 0; i < ncases; ++i) {
     CaseState cs;
@@ -1636,6 +1696,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
             throw ApiError(CANARD_ERR_ARG, "interface face without a neighbour block in the case");
         }
       make_geom(bd, i, k, B.g);
+      check_line_lengths(B.g, c->precision == CANARD_FP32_MIXED);
       // remap neighbours to global indices for the links
       c->blocks.push_back(B);
     }
@@ -1651,7 +1712,9 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
     if (!e.empty()) throw ApiError(CANARD_ERR_UNSUPPORTED, e);
     for (FaceLink L : lk) { L.dst_b += cs.b0; L.src_b += cs.b0; c->links.push_back(L); }
   }
-  // device memory
+  // device memory (everything above is host-side argument checking)
+  CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  c->st = c->own;
   std::vector<BlockDev> bdv;
   for (auto& B : c->blocks) {
     const BlockGeom& g = B.g;
@@ -2013,6 +2076,34 @@ int canard_phase(canard_ctx* c, int32_t phase, int32_t nk) {
   });
 }
 
+int canard_phase_with(canard_ctx* c, int32_t phase, int32_t nk, double dt, const double* umf,
+                      const double* dudtmf) {
+  return guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_phase_with before canard_setup");
+    if (!umf || !dudtmf) throw ApiError(CANARD_ERR_ARG, "null frame velocity or acceleration");
+    if (nk < 1 || nk > 4) throw ApiError(CANARD_ERR_ARG, "stage index nk must be 1..4");
+    if (phase != CANARD_PH_FLUXES && phase != CANARD_PH_GCBC && phase != CANARD_PH_RKUPDATE &&
+        phase != CANARD_PH_WALL)
+      throw ApiError(CANARD_ERR_ARG, "canard_phase_with takes the fluxes, GCBC, RK update and wall phases");
+    // the stage scalars of every case as the caller's movef gave them
+    // (src/mo_canard_driver.f90:261-263, 336-338): dtk = dt / (nkrk - nk + 1)
+    StageParams sp{};
+    for (int k = 0; k < 3; ++k) { sp.umf[k] = umf[k]; sp.dudtmf[k] = dudtmf[k]; sp.umfb[k] = umf[k]; }
+    sp.dt = dt;
+    sp.dtk = dt / (4 - nk + 1);
+    std::vector<StageParams> v(c->cases.size(), sp);
+    CK(cudaMemcpyAsync(dev_slot(c, 4), v.data(), v.size() * sizeof(StageParams), cudaMemcpyHostToDevice, c->st));
+    const StageParams* d = dev_slot(c, 4);
+    switch (phase) {
+      case CANARD_PH_FLUXES: ph_fluxes(c, d); break;
+      case CANARD_PH_GCBC: ph_gcbc(c, d); break;
+      case CANARD_PH_RKUPDATE: ph_rk(c, d); break;
+      default: ph_wall(c, d); break;
+    }
+    sync_check(c);
+  });
+}
+
 int canard_get_time(canard_ctx* c, int32_t icase, double* t) {
   return guarded(c, [&] {
     if (!t || icase < 0 || icase >= (int)c->cases.size()) throw ApiError(CANARD_ERR_ARG, "bad case / pointer");
@@ -2289,13 +2380,14 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         std::vector<std::pair<int, int>> cand;  // (kind, nc)
         std::vector<int> kinds{default_kind(c, grp, dir)};
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
+        if (c->f32() && grp == 0) kinds.push_back(LK_F64_STREAM_F32);
         else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
         // the filter acts on the FP64 state with an FP64 right-hand side in every
         // kind; the FP64 elimination competes with the FP32 ones there
         if (c->f32() && grp == 0) kinds.push_back(LK_F64);
         for (int k : kinds) {
           cand.push_back({k, 0});
-          if (dir != 0 && k != LK_F64_TM)
+          if (dir != 0 && k != LK_F64_TM && k != LK_F64_STREAM_F32)
             for (int nc : {2, 4, 8}) cand.push_back({k, nc});
         }
         double best = 1e300, def = 0;
@@ -2328,14 +2420,15 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
 
 int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
   return guarded(c, [&] {
-    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_TM || chunks < 0 ||
+    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_STREAM_F32 || chunks < 0 ||
         chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
       throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
     if (kind >= 0) {
       bool fits;
       if (!c->f32()) fits = kind == LK_F64 || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
       else if (group == 0)
-        fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64;
+        fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64 ||
+               (kind == LK_F64_STREAM_F32 && chunks == 0);
       else fits = kind == LK_F32 || kind == LK_F32_1L;
       if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
     }
@@ -2420,7 +2513,8 @@ int canard_selftest_wait(canard_ctx* c, double* seconds) {
 // fixed size that every GPU loading this library holds until the process exits.
 namespace {
 constexpr int kNaMaxLines = 65536;   // lines of the direction (nbsize)
-constexpr int kNaMaxPoints = 1024;   // points per line
+constexpr int kNaMaxPoints = 1024;   // points per line the scratch's factor table holds (the FP64
+                                     // tile allows fewer: 906 along xi, 896 along eta or zeta)
 constexpr size_t kNaTask = 0;        // LineTask
 constexpr size_t kNaFace = 512;      // up to 2 FaceTask
 constexpr size_t kNaIdx = 1536;      // (unused int), line0 of the 2 face tasks
@@ -2498,7 +2592,9 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
   g.Xp = pitch;
   g.npad = (int64_t)pitch * g.Y * g.Z;
   const int L = g.ijk[0][dir] + 1, nbs = g.nbs[dir];
-  if (L > kNaMaxPoints) return fail(CANARD_ERR_ARG, "more than 1024 points per line");
+  if (L > kNaMaxPoints || tile_smem_for(dir, L, LK_F64) > (size_t)kLineSmemMax)
+    return fail(CANARD_ERR_ARG, "line too long for the shared-memory tile (at most 906 points along xi, "
+                                "896 along eta or zeta)");
   if (nbs > kNaMaxLines) return fail(CANARD_ERR_ARG, "more than 65536 lines in this direction");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   try {
@@ -2581,7 +2677,6 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, &ds, sizeof(ds), kNaScheme, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyToSymbolAsync(g_noalloc_scratch, lu.data(), lu.size() * sizeof(double), kNaLu,
                                cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(base + kNaErr, 0, sizeof(int), st));
     if (nf) {
       const int tot = nf * nbs;
       launch_mpigo_t<double>(std::max(1, std::min((tot + 127) / 128, 148 * 16)), st,
@@ -2604,4 +2699,30 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     return fail(CANARD_ERR_CUDA, e.what());
   }
   return CANARD_OK;
+}
+
+// Reads and clears the error flag of the allocation-free derivative after the
+// work queued on `stream` has finished. The flag is raised by a line kernel
+// whose bounded wait for its input copies gave up; it stays up, and makes later
+// calls skip their work, until this function clears it.
+extern "C" int canard_deriv_noalloc_status(void* stream) {
+  try {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    unsigned char* base = noalloc_scratch(dev);
+    CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, base + kNaErr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag == 0) return CANARD_OK;
+    const int zero = 0;
+    CK(cudaMemcpy(base + kNaErr, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    std::fprintf(stderr, "canard_deriv_noalloc_status: a bounded device wait gave up (flag %d)\n", flag);
+    return (flag & kErrTimeout) ? CANARD_ERR_TIMEOUT : CANARD_ERR_CUDA;
+  } catch (const ApiError& e) {
+    std::fprintf(stderr, "canard_deriv_noalloc_status: %s\n", e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "canard_deriv_noalloc_status: %s\n", e.what());
+    return CANARD_ERR_CUDA;
+  }
 }

@@ -15,7 +15,7 @@ namespace canard {
 namespace {
 
 const double kPi = std::acos(-1.0);
-// src/mo_parameters.f90:61-79
+// src/mo_parameters.f90:52-70
 const double kAlpha = 4 / 9.0, kBeta = 1 / 36.0, kAa = 20 / 27.0, kAb = 25 / 216.0;
 const double kAlpha10 = 0.09166666665902128, kAlpha12 = 1.3500000000438646, kBeta13 = 0.2666666666794667;
 const double kA10 = -0.3506944444280639, kA12 = 0.8249999999974599, kA13 = 0.7444444444773477,

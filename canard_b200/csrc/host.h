@@ -101,7 +101,7 @@ struct GcbcFace { int nn, side, bc; int64_t first; };  // first entry = line 0, 
 void gcbc_tables(const BlockGeom& g, const double* yaco_ref, std::vector<GcbcFace>& faces,
                  std::vector<int64_t>& pts, std::vector<double>& w);
 
-// Sponge list (spongeup, src/mo_sponge.f90:224-261).
+// Sponge list (spongeup, src/mo_sponge.f90:34-71).
 void sponge_list(const BlockGeom& g, const canard_case_desc& c, const double* xyz_ref,
                  const double* yaco_ref, std::vector<int64_t>& pts, std::vector<double>& asz,
                  std::vector<double>& bsz);

@@ -221,7 +221,7 @@ __device__ __forceinline__ double pow15(double x) {
 }
 
 // ---------------------------------------------------------------------------
-// scheme constants (src/mo_parameters.f90:61-79)
+// scheme constants (src/mo_parameters.f90:52-70)
 #define CA_ALPHA (4 / 9.0)
 #define CA_BETA (1 / 36.0)
 #define CA_AA (20 / 27.0)
@@ -1409,6 +1409,238 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
 }
 
 // ---------------------------------------------------------------------------
+// Mixed-precision filter of the FP64 state on an FP32 tile (split solve, 16
+// lines per warp, two lanes per line as in k_line2). The FP64 field never
+// sits in shared memory: each lane streams its half of its line from global
+// memory (16 lines of one x-tile: 128-byte rows for eta and zeta), forms the
+// filter's right-hand sides in FP64 from a 7-point register window and the
+// closures (src/mo_numerics.f90:922-950), and stores them rounded to FP32 in
+// the tile, which is half the size of an FP64 tile. The FP32 split
+// elimination then runs on the tile (as sweep2, right-hand sides given), and
+// each row is written back as original (FP64, read again: it was read moments
+// before and is still in L2) + increment.
+
+// forward elimination of rows [ib, ie) from right-hand sides held in the tile
+template <int ST, class CF>
+__device__ __forceinline__ void fwd_rows_rhs(float* s, int ib, int ie, const CF& cf, float& am2, float& am1) {
+  int i = ib;
+  for (; i + 7 < ie; i += 8) {
+    float r[8], l1[8], l2[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { r[k] = s[(i + k) * ST]; l1[k] = cf.L1(i + k); l2[k] = cf.L2(i + k); }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float a = (r[k] - l1[k] * am2) - l2[k] * am1;
+      s[(i + k) * ST] = a;
+      am2 = am1;
+      am1 = a;
+    }
+  }
+  for (; i < ie; ++i) {
+    const float a = (s[i * ST] - cf.L1(i) * am2) - cf.L2(i) * am1;
+    s[i * ST] = a;
+    am2 = am1;
+    am1 = a;
+  }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(32) k_filt2s(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
+                                               int ntasks, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* s = reinterpret_cast<float*>(smem_raw);
+  const int lane = threadIdx.x;
+  const int half = lane >> 4, li = lane & (kHalf - 1);
+  const unsigned full = 0xffffffffu;
+  if (error_pending(err)) return;
+  const int ti = __ldg(tile_task + blockIdx.x);
+  const LineTask& T = tasks[ti];
+  const double* __restrict__ in = static_cast<const double*>(T.in);
+  double* out = static_cast<double*>(T.out);
+  const int lt = blockIdx.x - T.tile0;
+  const int L = T.L, h = T.h, N = L - 1;
+  const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
+  int nval, x0 = 0, r0 = 0, fix = 0;
+  if (DIR == 1) {
+    r0 = lt * kHalf;
+    nval = min(kHalf, Y * Z - r0);
+  } else {
+    fix = lt / T.ntx;
+    x0 = (lt % T.ntx) * kHalf;
+    nval = min(kHalf, X - x0);
+  }
+  const bool has = li < nval;
+  const int P = dir1_pitch<float>(L);
+  constexpr int ST = (DIR == 1) ? 1 : kHalf;
+  float* sl = (DIR == 1) ? s + li * P : s + li;
+  // element r of this lane's line: in[lb + r * rs] (lanes past the block's
+  // edge read line 0 of the tile and store nothing)
+  const long long rs = (DIR == 1) ? 1 : ((DIR == 2) ? (long long)Xp : (long long)Xp * Y);
+  const int lc = has ? li : 0;
+  const long long lb = (DIR == 1) ? (long long)(r0 + lc) * Xp
+                                  : ((DIR == 2) ? (long long)fix * Y * Xp + x0 + lc : (long long)fix * Xp + x0 + lc);
+  auto F = [&](int r) { return __ldg(in + lb + (long long)r * rs); };
+  int jk = 0;
+  if (DIR == 1) jk = r0 + lc;
+  else if (DIR == 2) jk = (x0 + lc) * Z + fix;
+  else jk = fix * X + x0 + lc;
+  const int nbs = T.nbs;
+  const DevScheme* __restrict__ sc = T.sc;
+  const double fa = sc->fa, fb = sc->fb, fc = sc->fc;
+  const double* recv = static_cast<const double*>(T.recv);
+  // ---- right-hand sides in FP64, stored as FP32
+  const int ndf = half == 0 ? T.ndf0 : T.ndf1;
+  {
+    // the three closure rows of the own end: rows 0, 1, 2 (first half) or
+    // N, N-1, N-2 (second half), e(k) = the k-th value from that end
+    const int e0 = half == 0 ? 0 : N, de = half == 0 ? 1 : -1;
+    auto E = [&](int k) { return F(e0 + de * k); };
+    double b0, b1, b2;
+    if (ndf == 0) {
+      const double v0 = E(0), v1 = E(1), v2 = E(2), v3 = E(3), v4 = E(4), v5 = E(5);
+      auto fbc = [&](int r, int k) { return sc->fbc[r][k]; };
+      b0 = (((fbc(0, 0) * (v1 - v0) + fbc(0, 1) * (v2 - v0)) + fbc(0, 2) * (v3 - v0)) + fbc(0, 3) * (v4 - v0)) +
+           fbc(0, 4) * (v5 - v0);
+      b1 = (((fbc(1, 0) * (v0 - v1) + fbc(1, 1) * (v2 - v1)) + fbc(1, 2) * (v3 - v1)) + fbc(1, 3) * (v4 - v1)) +
+           fbc(1, 4) * (v5 - v1);
+      b2 = (((fbc(2, 0) * (v0 - v2) + fbc(2, 1) * (v1 - v2)) + fbc(2, 2) * (v3 - v2)) + fbc(2, 3) * (v4 - v2)) +
+           fbc(2, 4) * (v5 - v2);
+    } else {
+      // interface closure: contraction with pbci plus the received sums; the
+      // third row takes the neighbour's raw value in place of the missing one
+      const int so = half == 0 ? 0 : 3;  // recv components of the side
+      const double q0 = recv[(so + 0) * nbs + jk], q1 = recv[(so + 1) * nbs + jk], q2 = recv[(so + 2) * nbs + jk];
+      double v[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) v[k] = E(k);
+      double t0 = 0, t1 = 0;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        t0 = t0 + sc->pbci[1][0][k] * v[k];
+        t1 = t1 + sc->pbci[1][1][k] * v[k];
+      }
+      const double ra2 = v[2] + v[2];
+      b0 = t0 + q0;
+      b1 = t1 + q1;
+      b2 = (fa * ((v[1] + v[3]) - ra2) + fb * ((v[0] + v[4]) - ra2)) + fc * ((q2 + v[5]) - ra2);
+    }
+    sl[e0 * ST] = float(b0);
+    sl[(e0 + de) * ST] = float(b1);
+    sl[(e0 + 2 * de) * ST] = float(b2);
+  }
+  {
+    // interior rows [a, b) of the own half: rows 3..h-1 or h..N-3
+    const int a = half == 0 ? 3 : h, b = half == 0 ? h : N - 2;
+    double w0 = F(a - 3), w1 = F(a - 2), w2 = F(a - 1), w3 = F(a), w4 = F(a + 1), w5 = F(a + 2);
+    auto rhs8 = [&](int r, const double (&v)[8]) {
+      double win[14] = {w0, w1, w2, w3, w4, w5, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double rk = win[k + 3] + win[k + 3];
+        const double q = (fa * ((win[k + 2] + win[k + 4]) - rk) + fb * ((win[k + 1] + win[k + 5]) - rk)) +
+                         fc * ((win[k] + win[k + 6]) - rk);
+        sl[(r + k) * ST] = float(q);
+      }
+      w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11]; w4 = win[12]; w5 = win[13];
+    };
+    int r = a;
+    if (r + 8 <= b) {
+      double nx[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) nx[k] = F(r + 3 + k);  // rows up to b + 2 <= N
+      while (r + 16 <= b) {
+        double cu[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cu[k] = nx[k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) nx[k] = F(r + 11 + k);
+        rhs8(r, cu);
+        r += 8;
+      }
+      rhs8(r, nx);
+      r += 8;
+    }
+    for (; r < b; ++r) {
+      const double w6 = F(r + 3);
+      const double rk = w3 + w3;
+      const double q = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+      sl[r * ST] = float(q);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    }
+  }
+  __syncwarp();
+  // ---- FP32 split elimination (see sweep2)
+  const float* lu = static_cast<const float*>(T.lu);
+  const CoefTable<float> ct{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
+  const CoefConst<float> cc{float(T.cl1), float(T.cl2), float(T.cu1), float(T.cu2), float(T.cu3)};
+  const float* hb = lu + 5 * L;
+  const int LT = L + 8;
+  const SplitTables H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke};
+  const int c0 = T.c0, c1 = L - 4;
+  float am2 = 0.f, am1 = 0.f;
+  int fb0;
+  if (half == 0) {
+    am2 = sl[0];
+    am1 = sl[ST] - ct.L2(1) * am2;
+    sl[ST] = am1;
+    fb0 = 2;
+  } else {
+    fb0 = h;
+  }
+  const int fe0 = half == 0 ? h : L;
+  {
+    const int m0 = max(fb0, c0), m1 = min(fe0, c1 + 1);
+    fwd_rows_rhs<ST>(sl, fb0, min(fe0, m0), ct, am2, am1);
+    fwd_rows_rhs<ST>(sl, m0, m1, cc, am2, am1);
+    fwd_rows_rhs<ST>(sl, max(fb0, c1 + 1), fe0, ct, am2, am1);
+  }
+  const int src = lane & (kHalf - 1);
+  const float A0 = __shfl_sync(full, am2, src), A1 = __shfl_sync(full, am1, src);
+  __syncwarp();
+  float cp1 = 0.f, cp2 = 0.f;
+  if (half == 1) {
+    cp1 = ct.U1(N) * sl[N * ST];
+    sl[N * ST] = cp1;
+    const float c = ct.U1(N - 1) * sl[(N - 1) * ST] - ct.U2(N - 1) * cp1;
+    sl[(N - 1) * ST] = c;
+    cp2 = cp1;
+    cp1 = c;
+  }
+  bwd3<ST, float, float>(sl, half == 0 ? h - 1 : N - 2, half == 0 ? 0 : h, c0, c1, ct, cc, cp1, cp2);
+  float ch0 = 0.f, ch1 = 0.f;
+  if (half == 1) {
+    ch0 = cp1 + (__ldg(H.h0) * A0 + __ldg(H.h1) * A1);
+    ch1 = cp2 + (__ldg(H.h0 + 1) * A0 + __ldg(H.h1 + 1) * A1);
+  }
+  const float C0 = __shfl_sync(full, ch0, src + kHalf), C1 = __shfl_sync(full, ch1, src + kHalf);
+  __syncwarp();
+  {
+    const float* t0 = half == 0 ? H.e0 : H.h0;
+    const float* t1 = half == 0 ? H.e1 : H.h1;
+    const float s0 = half == 0 ? C0 : A0, s1 = half == 0 ? C1 : A1;
+    const int cnt = half == 0 ? min(H.ke, h) : min(H.kh, L - h);
+    const int i0 = half == 0 ? h - 1 : h, di = half == 0 ? -1 : 1;
+    for (int j = 0; j < cnt; ++j) {
+      const int i = i0 + di * j;
+      sl[i * ST] = sl[i * ST] + (__ldg(t0 + j) * s0 + __ldg(t1 + j) * s1);
+    }
+  }
+  // ---- originals + increments of the own half, written back
+  if (has) {
+    const int lo = half == 0 ? 0 : h, hi = half == 0 ? h : L;
+    int r = lo;
+    for (; r + 8 <= hi; r += 8) {
+      double v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = F(r + k);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) out[lb + (long long)(r + k) * rs] = v[k] + double(sl[(r + k) * ST]);
+    }
+    for (; r < hi; ++r) out[lb + (long long)r * rs] = F(r) + double(sl[r * ST]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ void line_xyz(int nn, int pos, int j, int k, int& x, int& y, int& z) {
   if (nn == 1) { x = pos; y = j; z = k; }
   else if (nn == 2) { x = k; y = pos; z = j; }
@@ -1965,7 +2197,7 @@ __global__ void k_gcbc_update(const BlockDev* __restrict__ bd, const GcbcTask* _
   }
 }
 
-// sponge (src/mo_sponge.f90:265-278): the forcing is formed in FP64 from the
+// sponge (src/mo_sponge.f90:75-88): the forcing is formed in FP64 from the
 // FP64 state and added to de in the flux type
 template <class R>
 __global__ void k_sponge(const BlockDev* __restrict__ bd, const SpongeTask* __restrict__ tasks,
@@ -2098,6 +2330,14 @@ template <int DIR, int OP, class TT>
 void launch_line2_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
                     const CUtensorMap* maps, int* err) {
   k_line2<DIR, OP, TT><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR>
+void launch_filt2s_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt, int* err) {
+  k_filt2s<DIR><<<grid, kLanes, smem, st>>>(t, f, nt, err);
+}
+template <int DIR>
+cudaError_t filt2s_smem_limit(int bytes) {
+  return cudaFuncSetAttribute(k_filt2s<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 template <int DIR, int OP, class TT>
 cudaError_t line2_smem_limit(int bytes) {

@@ -62,5 +62,14 @@ CANARD_F32_LINE1(1, 1, double)
 CANARD_F32_LINE1(2, 1, double)
 CANARD_F32_LINE1(3, 1, double)
 #undef CANARD_F32_LINE1
+// the filter of the FP64 state streamed into FP32 right-hand sides (split FP32 solve)
+#define CANARD_F32_FILT(DIR)                                                                              \
+  CANARD_F32_EXTERN template void launch_filt2s_t<DIR>(int, size_t, cudaStream_t, const LineTask*, const int*, \
+                                                       int, int*);                                        \
+  CANARD_F32_EXTERN template cudaError_t filt2s_smem_limit<DIR>(int);
+CANARD_F32_FILT(1)
+CANARD_F32_FILT(2)
+CANARD_F32_FILT(3)
+#undef CANARD_F32_FILT
 
 }  // namespace canard

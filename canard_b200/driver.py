@@ -1,7 +1,7 @@
 """The reference's program, on the device path: reads ``input.canard``, builds
 the blocks and their grid with the reference's generators, starts from
 ``initialo`` or a restart file, and runs the time loop of canard_driver
-(src/mo_canard_driver.f90:99-470) with its stop rule, output schedule,
+(src/mo_canard_driver.f90:34-459) with its stop rule, output schedule,
 time-averaged recording, Tecplot files and final restart file, in the
 reference's file formats and names under the run directory:
 

@@ -10,10 +10,10 @@
  *   gcbc_setup / gcbc_comm / gcbc_update     src/mo_gcbc.f90:133-340
  *   average_surface                         src/mo_gcbc.f90:342-422
  *   t_domdcomp%average_point / average_line src/mo_domdcomp.f90:439-559
- *   spongego                                src/mo_sponge.f90:265-278
+ *   spongego                                src/mo_sponge.f90:75-88
  *   the time loop body (filter, RK stages)  src/mo_canard_driver.f90:226-431
  * and the set-up they depend on (t_grid%grid_metrics src/mo_grid.f90:52-189,
- * gcbc_init src/mo_gcbc.f90:40-131, spongeup src/mo_sponge.f90:224-261,
+ * gcbc_init src/mo_gcbc.f90:40-131, spongeup src/mo_sponge.f90:34-71,
  * search_point / search_line src/mo_domdcomp.f90:269-437, init_extra / init
  * src/mo_numerics.f90:114-249).
  *
@@ -146,6 +146,16 @@ int canard_set_field(canard_ctx* ctx, int32_t icase, int32_t iblock, int32_t fie
  * time6 = (n, ndt, dt, dts, dte, timo) of one case. */
 int canard_step(canard_ctx* ctx, int32_t nsteps);
 int canard_phase(canard_ctx* ctx, int32_t phase, int32_t nk);
+/* The fluxes, GCBC, RK update or wall phase of stage nk with the stage's
+ * scalars given by the caller, as the reference's routines receive them
+ * (calc_fluxes reads this%umf, src/mo_physics.f90:319-321; gcbc_update takes
+ * dt, umf, dudtmf, src/mo_gcbc.f90:222; the RK update uses dtk = dt/(5-nk),
+ * src/mo_canard_driver.f90:336-345; wall_condition_update takes umf,
+ * src/mo_gcbc.f90:424), for every case of the context, instead of the frame
+ * motion and dt the device derives from its own time state. For per-routine
+ * drop-in where the caller's time loop owns the time state. */
+int canard_phase_with(canard_ctx* ctx, int32_t phase, int32_t nk, double dt, const double* umf,
+                      const double* dudtmf);
 int canard_get_time(canard_ctx* ctx, int32_t icase, double* time6);
 int canard_set_time(canard_ctx* ctx, int32_t icase, const double* time6);
 
@@ -331,17 +341,27 @@ int canard_set_graphs(canard_ctx* ctx, int32_t on);
  *   nbc0, nbc1    end closures: 10/20/25/30 one-sided, 45 periodic on the line
  *                 itself (both ends)
  *   fltk, fltrbc  nml_numerics values (fix the interface coefficients)
- * Limits: at most 1024 points per line and 65536 lines in the direction;
- * larger sizes return CANARD_ERR_ARG. The scratch is one static device array
- * of about 2.1 MiB that every GPU loading the library holds until the process
- * exits. Every call reuses it and leaves its last contents there, so calls
- * that overlap on the GPU (on different streams) race. The first call on a
- * device looks up the array's device address with that device current and
- * caches it; make that first call before any stream capture. No cudaMalloc,
- * cudaFree or other allocating routine is called. */
+ * Limits: a line of the direction must fit the FP64 shared-memory tile, at
+ * most 906 points along xi and 896 along eta or zeta, and the direction may
+ * have at most 65536 lines; larger sizes return CANARD_ERR_ARG before any
+ * work is queued. The scratch is one static device array of about 2.1 MiB
+ * that every GPU loading the library holds until the process exits. Every
+ * call reuses it and leaves its last contents there, so calls that overlap on
+ * the GPU (on different streams) race. The first call on a device looks up
+ * the array's device address with that device current and caches it; make
+ * that first call before any stream capture. No cudaMalloc, cudaFree or other
+ * allocating routine is called. The return code covers the arguments and the
+ * queuing; the kernels' own status is read with canard_deriv_noalloc_status. */
 int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t lxi, int32_t let, int32_t lze,
                          int32_t pitch, int32_t nn, int32_t nbc0, int32_t nbc1, double fltk,
                          double fltrbc, void* stream);
+/* Status of the allocation-free derivative's kernels (no counterpart in the
+ * reference): waits for `stream`, then returns CANARD_ERR_TIMEOUT if a line
+ * kernel's bounded wait for its input copies gave up since the last status
+ * call (its output is then incomplete), else CANARD_OK, and clears the flag.
+ * While the flag is up, later canard_deriv_noalloc calls skip their line
+ * solve. Allocates nothing. */
+int canard_deriv_noalloc_status(void* stream);
 
 #ifdef __cplusplus
 }

@@ -78,3 +78,25 @@ def test_unsupported_configurations_are_rejected_before_device_work():
         assert rc in (api.ERR_ARG, api.ERR_CUDA)
     c, b = api._structs([cases.tgv(16)])
     assert api.lib().canard_ctx_create(c, 1, b, 7, ctypes.byref(h)) == api.ERR_UNSUPPORTED
+
+
+def test_noalloc_rejects_lines_beyond_the_tile_before_any_work():
+    # the FP64 line tile holds at most 906 points along xi and 896 along eta or
+    # zeta; longer lines are refused by the argument checks, before any device
+    # call (the pointers are never touched)
+    lib = api.lib()
+    p = ctypes.c_void_p(256)
+    assert lib.canard_deriv_noalloc(p, p, 906, 12, 12, 908, 1, 10, 10, 0.85, 0.85, None) == api.ERR_ARG
+    assert lib.canard_deriv_noalloc(p, p, 12, 896, 12, 16, 2, 10, 10, 0.85, 0.85, None) == api.ERR_ARG
+    assert lib.canard_deriv_noalloc(p, p, 12, 12, 896, 16, 3, 10, 10, 0.85, 0.85, None) == api.ERR_ARG
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_context_rejects_lines_longer_than_the_tile(prec):
+    # FP64 tiles hold 906 points along xi and 896 along eta/zeta; the mixed
+    # precision's tiles are half as wide and take longer lines
+    h = ctypes.c_void_p()
+    for dims in ((906, 12, 12), (12, 896, 12), (12, 12, 896)) if prec == 0 else ((1900, 12, 12),):
+        blk = cases.BlockSpec(*dims, [[10, 10]] * 3, [[-1, -1]] * 3)
+        c, b = api._structs([cases.CaseSpec([blk])])
+        assert api.lib().canard_ctx_create(c, 1, b, prec, ctypes.byref(h)) == api.ERR_UNSUPPORTED, dims

@@ -19,15 +19,16 @@ def run(args, env=None):
 
 
 def test_reference_arm_line():
-    (line,) = run(["--impl", "reference", "--steps", "1", "--warmup", "1", "--cpu-n", "24"])
+    (line,) = run(["--impl", "reference", "--steps", "1", "--warmup", "1", "--n", "24"])
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
               "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert k in line, k
     assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 1
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["unit"] == line["unit"]
+    assert line["config"]["workload"].startswith("tgv24:") and line["config"]["points"] == 25 ** 3
 
 
 def test_reference_arm_other_ranks_print_nothing():
-    assert run(["--impl", "reference", "--steps", "1", "--warmup", "0", "--cpu-n", "24"],
+    assert run(["--impl", "reference", "--steps", "1", "--warmup", "0", "--n", "24"],
                env={"RANK": "1", "WORLD_SIZE": "2"}) == []

@@ -1,0 +1,98 @@
+"""The benchmark configurations at their stated sizes against the oracle.
+
+Each config is run on the device (FP64 plain and FP32-mixed) and by the CPU
+oracle from the same initial condition for the same number of full time
+steps; the error is the relative L2 distance per conserved variable (rho,
+rho u, rho v, rho w, rho E), the momenta measured against ||rho|| * U where
+that exceeds their own norm (U the case's velocity scale: a component that is
+zero by symmetry has no relative error of its own). Bounds: <= 1e-10 for the
+FP64 path (the Sutherland power is the one place its rounding may differ from
+the oracle's by an ulp), <= 1e-5 for FP32-mixed.
+
+* C1: Taylor-Green vortex, 64^3 cells, 100 steps.
+* C2: the same at 256^3 cells (257^3 stored points), 10 steps.
+* C3: four curvilinear blocks of 192 x 128 x 64 cells with GCBC in/outflow,
+  curved and straight interfaces and a sponge, 12 steps; FP32-mixed against
+  FP64 after 200 steps on the device.
+* C4: the isentropic vortex through a GCBC outflow on a 96 x 64 x 32 copy,
+  50 steps.
+
+The oracle runs on every host thread; C2 takes it a couple of minutes.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from canard_b200 import api, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def errors(qg, qr, uref):
+    rho = np.linalg.norm(qr[0].ravel())
+    out = []
+    for v in range(5):
+        den = np.linalg.norm(qr[v].ravel())
+        if 1 <= v <= 3:
+            den = max(den, rho * uref)
+        out.append(float(np.linalg.norm((qg[v] - qr[v]).ravel()) / den))
+    return out
+
+
+def run_device(cs, steps, precision):
+    g = api.Context(cs, precision=precision)
+    g.step(steps)
+    q = [g.state(b) for b in range(len(cs.blocks))]
+    g.close()
+    return q
+
+
+def run_oracle(cs, steps):
+    o = po.Oracle(cs, threads=os.cpu_count() or 1)
+    o.step(steps)
+    q = [o.state(b) for b in range(len(cs.blocks))]
+    del o
+    return q
+
+
+def check(cs, steps, uref, fp32=True):
+    ref = run_oracle(cs, steps)
+    worst = {}
+    for name, prec, tol in (("fp64", api.FP64, 1e-10), ("fp32", api.FP32_MIXED, 1e-5)):
+        if name == "fp32" and not fp32:
+            continue
+        got = run_device(cs, steps, prec)
+        errs = [errors(a, b, uref) for a, b in zip(got, ref)]
+        worst[name] = max(max(e) for e in errs)
+        print(cs.name, name, steps, "steps, per block", errs)
+        assert all(np.isfinite(a).all() for a in got)
+        assert worst[name] <= tol, (name, errs)
+    return worst
+
+
+def test_c1_tgv64_100_steps():
+    check(cases.tgv(64), 100, 0.1)
+
+
+def test_c2_tgv256_10_steps():
+    check(cases.tgv(256), 10, 0.1)
+
+
+def test_c3_curvilinear_4block_12_steps():
+    check(cases.curvilinear_4block(), 12, 0.4)
+
+
+def test_c3_fp32_mixed_against_fp64_after_200_steps():
+    cs = cases.curvilinear_4block()
+    a = run_device(cs, 200, api.FP64)
+    b = run_device(cs, 200, api.FP32_MIXED)
+    errs = [errors(x, y, 0.4) for x, y in zip(b, a)]
+    print("C3 FP32-mixed vs FP64 after 200 steps, per block", errs)
+    assert all(np.isfinite(x).all() for x in a + b)
+    assert max(max(e) for e in errs) <= 1e-5, errs
+
+
+def test_c4_vortex_small_copy_50_steps():
+    check(cases.vortex(96, 64, 32), 50, 0.5)

@@ -173,3 +173,41 @@ def test_face_only_stage_state_on_a_large_block():
     g.step(10)
     errs = state_errors(g.state(0), a.state(0), 0.1)
     assert max(errs) <= TOL_STEPS, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_streamed_filter_steps_within_1e_5(name):
+    """The filter kind that streams the FP64 state into FP32 right-hand sides
+    (k_filt2s), pinned on every direction: 12 steps within the tolerance."""
+    cs = CASES[name]()
+    o = po.Oracle(cs)
+    g = api.Context(cs, precision=api.FP32_MIXED)
+    for d in ("xi", "eta", "zeta"):
+        g.set_line_kind("filter", d, "fp64-stream/fp32-split")
+    o.step(12)
+    g.step(12)
+    for b in range(len(cs.blocks)):
+        errs = state_errors(g.state(b), o.state(b), UREF[name])
+        print(name, b, ["%.2e" % e for e in errs])
+        assert max(errs) <= TOL_STEPS, (name, b, errs)
+
+
+@pytest.mark.parametrize("nn", [1, 2, 3])
+@pytest.mark.parametrize("name", ["periodic", "nonperiodic"])
+def test_streamed_filter_unit(name, nn):
+    """One filter pass of 5 smooth fields through canard_line_bench with the
+    streamed kind, against the oracle's filte: the FP64 field carries an FP32
+    increment, so the agreement is far below FP32 rounding of the field."""
+    cs = CASES[name]()
+    blk = cs.blocks[0]
+    fields = np.stack([f.reshape(blk.shape) for f in (smooth_fields(cs, 11 + k)[0] for k in range(5))])
+    g = api.Context(cs, precision=api.FP32_MIXED, setup=False, upload_state=False)
+    g.set_line_kind("filter", "xi eta zeta".split()[nn - 1], "fp64-stream/fp32-split")
+    out, ms = g.line_bench(1, nn, fields, reps=2)
+    o = po.Oracle(cs, setup=False)
+    inn = {2: 1, 3: 2, 1: 3}[nn]
+    for k in range(5):
+        f = fields[k].ravel().copy()
+        o.mpigo([f], 1, 1, 0, k + 1, k + 1)
+        o.filte(0, f, inn, k + 1)
+        assert rel_l2(out[k].ravel(), f) <= 1e-8, (k, rel_l2(out[k].ravel(), f))

@@ -523,3 +523,34 @@ def test_tmem_line_kernel_with_interfaces_and_gcbc(name):
     b.step(4)
     for blk in range(len(cs.blocks)):
         np.testing.assert_array_equal(b.state(blk), a.state(blk))
+
+
+def test_phase_with_caller_stage_scalars_equals_device_stage():
+    """canard_phase_with takes dt, umf and dudtmf from the caller, as the
+    reference's calc_fluxes / gcbc_update / RK update receive them; with the
+    values the device's own movef gives (a constant moving frame, Mach 0.4
+    along x) the phases give the same bits as canard_phase."""
+    cs = case_multiblock()
+    a, b = api.Context(cs), api.Context(cs)
+    t6 = [5, 1, 2.0e-3, 1.5e-3, 2.5e-3, 0.31]
+    umf = (cs.amach[0], cs.amach[1], cs.amach[2])
+    for g in (a, b):
+        g.set_time(t6)
+        g.phase(api.PH_FILTER)
+        g.phase(api.PH_COPYQO)
+    for nk in (1, 2, 3):
+        for g in (a, b):
+            g.phase(api.PH_PRIM, nk)
+            g.phase(api.PH_VISCOUS, nk)
+        a.phase(api.PH_FLUXES, nk)
+        b.phase_with(api.PH_FLUXES, nk, t6[2], umf)
+        a.phase(api.PH_GCBC, nk)
+        b.phase_with(api.PH_GCBC, nk, t6[2], umf)
+        for g in (a, b):
+            g.phase(api.PH_SPONGE, nk)
+        a.phase(api.PH_RKUPDATE, nk)
+        b.phase_with(api.PH_RKUPDATE, nk, t6[2], umf)
+        for g in (a, b):
+            g.phase(api.PH_AVERAGE, nk)
+        for blk in range(len(cs.blocks)):
+            np.testing.assert_array_equal(a.state(blk), b.state(blk), err_msg=f"nk={nk} block {blk}")

@@ -106,7 +106,7 @@ def test_periodic_derivative_modified_wavenumber(nn):
 def test_derivative_solves_the_compact_system(nn, periodic):
     """The output satisfies every row of the pentadiagonal system of the
     reference (interior: src/mo_numerics.f90:761-763 with alpha, beta; one-sided
-    closures: src/mo_parameters.f90:66-79), to rounding."""
+    closures: src/mo_parameters.f90:57-70), to rounding."""
     blk = periodic_block(26, 22) if periodic else nonperiodic_block(26, 22)
     o = make_oracle(blk)
     rng = np.random.default_rng(1)
