@@ -47,8 +47,9 @@ def parse():
                    help="tgv: single TGV block (default); batched: 64 independent cases with sides "
                         "in 32..96; curv4: 4-block curvilinear grid with GCBC and sponge; vortex: "
                         "isentropic vortex through a GCBC outflow")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                   help="fp64: plain FP64 path (bit-exact with the oracle); fp32: FP32 line solves, fluxes, "
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fast", "fp32"],
+                   help="fp64: plain FP64 path (bit-exact with the oracle); fast: FP64 throughout with the split "
+                        "line solves and FMA (within 1e-10 of the oracle); fp32: FP32 line solves, fluxes, "
                         "viscous stresses and GCBC with the FP64 state, RK update, metrics and LU factors")
     p.add_argument("--acc-nx", type=int, default=384)
     p.add_argument("--acc-ny", type=int, default=256)
@@ -134,13 +135,15 @@ def fp32_extra(args, api, cases, torch, stream, value64):
 def batched_extra(args, api, cases, torch, stream):
     """64 independent cases (sides 32..96): one context, one launch per phase
     and direction for all cases, each step one CUDA graph, FP32-mixed and
-    FP64; against the per-case FP64 plain path (one context per case, kernels
-    launched one by one, case after case)."""
+    FP64; against the per-case FP64 plain path (one context per case, case
+    after case: kernels launched one by one, and with each case's own step
+    graph)."""
     allc = cases.batched(64, seed=11)
     npts = sum(c.npts for c in allc)
     out = {"workload": "64 cases, sides 32..96 (seed 11), TGV / periodic vortex, Mach 0.1-0.5, Re 400-3200",
            "points": npts, "steps": args.steps}
     states = {}
+    gaps = {}
     for key, prec in (("fp32_mixed_graph", api.FP32_MIXED), ("fp64_graph", api.FP64)):
         g = api.Context(allc, precision=prec)
         if not args.no_autotune:
@@ -150,7 +153,18 @@ def batched_extra(args, api, cases, torch, stream):
         ms = time_steps(g, args.steps, stream, torch)
         out[key] = npts * args.steps / (ms / 1e3) / 1e6
         states[key] = [g.state(0, i) for i in range(len(allc))]
+        # the step's kernels alone (each bracketed by CUDA events, launched one
+        # by one) against the graph's step: what launch gaps and kernel tails
+        # cost, the most a persistent kernel per stage could take back without
+        # fusing work
+        g.set_timers(True)
+        g.step(1)
+        kms = sum(f["ms"] for f in g.timers().values())
+        g.set_timers(False)
+        gaps[key] = {"graph_ms_per_step": ms / args.steps, "kernels_ms_per_step": kms,
+                     "outside_kernels_fraction": max(0.0, 1.0 - kms / (ms / args.steps))}
         g.close()
+    out["graph_vs_kernel_time"] = gaps
     ctxs = []
     for c in allc:
         x = api.Context(c)
@@ -170,10 +184,25 @@ def batched_extra(args, api, cases, torch, stream):
     ms = max(a.elapsed_time(b), (time.perf_counter() - t0) * 1e3)
     out["fp64_per_case_plain"] = npts * args.steps / (ms / 1e3) / 1e6
     ref = [x.state(0) for x in ctxs]
+    # the same per-case contexts with their own step graphs on (one graph
+    # launch per case and step)
+    for x in ctxs:
+        x.set_graphs(True)
+        x.step(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    for x in ctxs:
+        x.step(args.steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = max(a.elapsed_time(b), (time.perf_counter() - t0) * 1e3)
+    out["fp64_per_case_graphs"] = npts * args.steps / (ms / 1e3) / 1e6
     for x in ctxs:
         x.close()
     out["speedup_fp32_graph_vs_fp64_per_case"] = out["fp32_mixed_graph"] / out["fp64_per_case_plain"]
     out["speedup_fp64_graph_vs_fp64_per_case"] = out["fp64_graph"] / out["fp64_per_case_plain"]
+    out["speedup_fp32_graph_vs_fp64_per_case_graphs"] = out["fp32_mixed_graph"] / out["fp64_per_case_graphs"]
     out["fp64_graph_bit_identical_to_per_case"] = bool(all(np.array_equal(s, r)
                                                             for s, r in zip(states["fp64_graph"], ref)))
     errs = [state_errors(s, r, 0.5) for s, r in zip(states["fp32_mixed_graph"], ref)]
@@ -206,6 +235,8 @@ def workload_cases(args, cases, world=1, rank=0):
         workload = "vortex: 384x256x128 cells, isentropic vortex, GCBC outflow, FP64"
     if args.precision == "fp32":
         workload = workload.replace("FP64 plain", "FP32-mixed").replace(", FP64", ", FP32-mixed")
+    elif args.precision == "fast":
+        workload = workload.replace("FP64 plain", "FP64 fast mode").replace(", FP64", ", FP64 fast mode")
     return case_list, all_cases, workload
 
 
@@ -305,8 +336,8 @@ def kernels_mode(args, api, cases, torch):
     # tensor memory (an autotuner candidate), pinned for the comparison
     # fp32-stream: the mixed filter that streams the FP64 state into FP32
     # right-hand sides (an autotuner candidate), pinned for the comparison
-    for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP32_MIXED, "fp32"),
-                       (api.FP32_MIXED, "fp32-stream")):
+    for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP64_FAST, "fp64-fast"),
+                       (api.FP32_MIXED, "fp32"), (api.FP32_MIXED, "fp32-stream")):
         ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
         for op in (0, 1):
             if name == "fp32-stream" and op == 0:
@@ -336,17 +367,21 @@ def kernels_mode(args, api, cases, torch):
 
 
 def accuracy_mode(args, api, cases, torch):
-    """FP32-mixed against FP64 on the isentropic vortex through a GCBC outflow:
-    the 384x256x128 case on the GPU after 50 ... 1000 steps (relative L2 per
-    conserved variable, momenta against ||rho|| * 0.5, and whether each state
-    is still finite), and a 96x64x32 copy against the oracle after 50 steps
-    (both precisions)."""
+    """The C4 study: the isentropic vortex through a GCBC outflow.
+
+    * The 384x256x128 case on the GPU after 50 ... 1000 steps: FP32-mixed and
+      the fast FP64 mode against the bit-exact FP64 path (relative L2 per
+      conserved variable, momenta against ||rho|| * 0.5), and whether each
+      state is still finite.
+    * A 96x64x32 copy against the oracle after 50, 200 and 1000 steps, in all
+      three precisions (the oracle's 1000 steps take a few minutes on the
+      host cores)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     out = {"mode": "accuracy"}
     big = cases.vortex(nx=args.acc_nx, ny=args.acc_ny, nz=args.acc_nz)
-    a = api.Context(big)
-    b = api.Context(big, precision=api.FP32_MIXED)
+    ctxs = {"fp64": api.Context(big), "fast": api.Context(big, precision=api.FP64_FAST),
+            "fp32": api.Context(big, precision=api.FP32_MIXED)}
     done, rows = 0, []
     stopped = {}
 
@@ -360,30 +395,39 @@ def accuracy_mode(args, api, cases, torch):
             stopped[key] = f"stopped between steps {done} and {done + k}: {e}"
 
     for n in (50, 100, 200, 400, 1000):
-        advance(a, "fp64", n - done)
-        advance(b, "fp32", n - done)
-        qa, qb = a.state(0), b.state(0)
+        for key, ctx in ctxs.items():
+            advance(ctx, key, n - done)
+        q = {key: ctx.state(0) for key, ctx in ctxs.items()}
         done = n
-        row = {"steps": n, "time": a.time()[5], "fp64_finite": "fp64" not in stopped and bool(np.isfinite(qa).all()),
-               "fp32_finite": "fp32" not in stopped and bool(np.isfinite(qb).all())}
-        if row["fp64_finite"] and row["fp32_finite"]:
-            row["rel_l2_fp32_vs_fp64"] = state_errors(qb, qa, 0.5)
+        row = {"steps": n, "time": ctxs["fp64"].time()[5]}
+        for key in ctxs:
+            row[f"{key}_finite"] = key not in stopped and bool(np.isfinite(q[key]).all())
+        for key in ("fast", "fp32"):
+            if row["fp64_finite"] and row[f"{key}_finite"]:
+                row[f"rel_l2_{key}_vs_fp64"] = state_errors(q[key], q["fp64"], 0.5)
         rows.append(row)
     out["stopped"] = stopped
-    a.close()
-    b.close()
+    for ctx in ctxs.values():
+        ctx.close()
     out["vortex_gpu"] = {"case": big.name, "points": big.npts, "rows": rows}
     small = cases.vortex(nx=96, ny=64, nz=32)
     o = po.Oracle(small, threads=os.cpu_count() or 1)
-    o.step(50)
-    qo = o.state(0)
-    res = {}
-    for prec, name in ((api.FP64, "fp64"), (api.FP32_MIXED, "fp32")):
-        g = api.Context(small, precision=prec)
-        g.step(50)
-        res[name] = state_errors(g.state(0), qo, 0.5)
+    gs = {"fp64": api.Context(small), "fast": api.Context(small, precision=api.FP64_FAST),
+          "fp32": api.Context(small, precision=api.FP32_MIXED)}
+    res, done = [], 0
+    for n in (50, 200, 1000):
+        o.step(n - done)
+        qo = o.state(0)
+        row = {"steps": n}
+        for key, g in gs.items():
+            g.step(n - done)
+            row[key] = state_errors(g.state(0), qo, 0.5)
+        done = n
+        res.append(row)
+    for g in gs.values():
         g.close()
-    out["vortex_vs_oracle_50_steps"] = {"case": small.name, "points": small.npts, "rel_l2": res}
+    out["vortex_vs_oracle"] = {"case": small.name, "points": small.npts, "rows": res,
+                               "oracle_finite_at_1000": bool(np.isfinite(o.state(0)).all())}
     out["note"] = ("per conserved variable (rho, rho u, rho v, rho w, rho E); momentum components against "
                    "||rho|| * 0.5 where that exceeds their own norm (rho w is zero by symmetry)")
     return out
@@ -494,7 +538,7 @@ def main():
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
     case_list, all_cases, workload = workload_cases(args, cases, world, rank)
-    prec = api.FP32_MIXED if args.precision == "fp32" else api.FP64
+    prec = {"fp32": api.FP32_MIXED, "fast": api.FP64_FAST}.get(args.precision, api.FP64)
     ctx = api.Context(case_list, precision=prec)
     tuning = None if args.no_autotune else ctx.autotune(reps=3)
     # a non-default stream: the library launches on it and the CUDA events
@@ -629,7 +673,7 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": scaling, "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "scaling": scaling, "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32" else "f64",
                 "data": "synthetic (seeded analytic initial conditions; curv4 adds seeded velocity noise)",
                 "config": config_dict(args, workload, len(case_list), job_points, npts, world),
                 "autotuned": not args.no_autotune,

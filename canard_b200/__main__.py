@@ -11,7 +11,7 @@ def main():
     p = argparse.ArgumentParser(prog="python -m canard_b200")
     p.add_argument("input", nargs="?", default="input.canard")
     p.add_argument("--dir", default=None, help="run directory (default: the input's directory)")
-    p.add_argument("--precision", default=None, choices=["fp64", "fp32"],
+    p.add_argument("--precision", default=None, choices=["fp64", "fast", "fp32"],
                    help="default: &nml_gpu nprecision, else fp64")
     p.add_argument("--inviscid", action="store_true", default=None,
                    help="the reference built without VISCOUS (default: &nml_gpu linviscid)")
@@ -21,7 +21,7 @@ def main():
     p.add_argument("--plan-devices", type=int, default=0, metavar="N",
                    help="print the input's ranks placed on N devices and the bytes they exchange; no run")
     a = p.parse_args()
-    prec = None if a.precision is None else (api.FP32_MIXED if a.precision == "fp32" else api.FP64)
+    prec = None if a.precision is None else {"fp32": api.FP32_MIXED, "fast": api.FP64_FAST}.get(a.precision, api.FP64)
     visc = None if a.inviscid is None else 0
     if a.plan_devices:
         driver.plan_devices(a.input, a.plan_devices, viscous=visc, precision=prec)

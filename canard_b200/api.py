@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libcanard_b200.so")
 
 OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE, ERR_IO = range(8)
-FP64, FP32_MIXED = 0, 1
+FP64, FP32_MIXED, FP64_FAST = 0, 1, 2
 
 F_QA, F_QO, F_DE, F_P, F_SS1, F_XIM, F_ETM, F_ZEM, F_YACO, F_TAU = range(10)
 F_DRVA = (10, 11, 12)
@@ -381,7 +381,7 @@ class Context:
         if k < 0:
             self._check(-k)
         kinds = {0: "fp64", 1: "fp32-split", 2: "fp64-tile/fp32-split", 3: "fp32-one-lane",
-                 4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem", 6: "fp64-stream/fp32-split"}
+                 4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem", 6: "fp64-stream/fp32-split", 7: "fp64-split"}
         out = []
         for i in range(k):
             g, d, kd, nc, best, dflt = rep[6 * i:6 * i + 6]
@@ -391,12 +391,13 @@ class Context:
         return out
 
     LINE_KINDS = {"default": -1, "fp64": 0, "fp32-split": 1, "fp64-tile/fp32-split": 2, "fp32-one-lane": 3,
-                  "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5, "fp64-stream/fp32-split": 6}
+                  "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5, "fp64-stream/fp32-split": 6, "fp64-split": 7}
 
     def set_line_kind(self, group, direction, kind, chunks=0):
         """Pins the line kernel of a group ("filter", "viscous", "flux") and
-        direction ("xi", "eta", "zeta"), by name from LINE_KINDS; every FP64
-        kind gives bit-identical results."""
+        direction ("xi", "eta", "zeta"), by name from LINE_KINDS; "fp64",
+        "fp64-tmem" give results bit-identical to the reference's order,
+        "fp64-split" (the fast FP64 mode's kind) differs at rounding level."""
         g = ("filter", "viscous", "flux").index(group)
         d = ("xi", "eta", "zeta").index(direction)
         self._check(lib().canard_set_line_kind(self.h, g, d, self.LINE_KINDS[kind], chunks))

@@ -88,21 +88,30 @@ enum LineKind {
   LK_F32_1L = 3,
   LK_F64_TILE_F32_SOLVE_1L = 4,
   LK_F64_TM = 5,               // FP64, elimination results in TMEM (eta/zeta, 16 <= L <= 257)
-  LK_F64_STREAM_F32 = 6        // filter: FP64 field streamed into FP32 right-hand sides, split FP32 solve
+  LK_F64_STREAM_F32 = 6,       // filter: FP64 field streamed into FP32 right-hand sides, split FP32 solve
+  LK_F64_SPLIT = 7             // FP64 fields, split FP64 solve with FMA (fast FP64 mode)
 };
 inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L; }
 inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
 inline int tile_lanes(int kind) {
-  return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_STREAM_F32) ? kHalf : kLanes;
+  return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_STREAM_F32 || kind == LK_F64_SPLIT)
+             ? kHalf
+             : kLanes;
 }
 
 // First row of the second half of a split solve: balances the two halves'
 // register-constant rows (the first half's rows below c0 use the tables
-// alone), with a parity that puts their lock-step rows into different banks.
-int split_row(int L, int dir, int nt, int c0) {
+// alone), with a parity that puts their lock-step rows into different banks
+// (es: tile element size).
+int split_row(int L, int dir, int nt, int c0, int es = 4) {
   const int first = nt == 0 ? 2 : 3;   // first interior row of the elimination
   int h = (L - 3 + first + std::max(c0, first)) / 2;
   auto good = [&](int x) {
+    if (es == 8) {
+      // row-major FP64 tile (pitch 2 mod 4): an odd offset puts the second
+      // half on the odd 8-byte words; a [row][16] FP64 row fills all banks
+      return dir != 0 || ((x - first) % 2 + 2) % 2 == 1;
+    }
     if (dir == 0) return ((x - first) % 4 + 4) % 4 == 2;  // row-major tile, 16-byte units of 4 floats
     return ((x - first) % 2 + 2) % 2 == 1;                // [row][16] tile
   };
@@ -115,9 +124,11 @@ int split_row(int L, int dir, int nt, int c0) {
 // H0, H1 = the second half's back substitution (rows L-1..h) of the
 // homogeneous forward solutions started at rows h-2, h-1 (index row - h);
 // E0, E1 = the homogeneous backward solutions started at rows h, h+1 (index
-// h-1-row); each L + 8 entries; returns the lengths beyond which every entry
-// stays below 1e-12 (set to zero).
-void split_tables(const std::vector<double>& lu, int L, int h, std::vector<float>& out, int& kg, int& ke) {
+// h-1-row); each L + 8 entries of type T; returns the lengths beyond which
+// every entry stays below thr (set to zero): 1e-12 for the FP32
+// eliminations, 1e-18 for the FP64 ones.
+template <class T>
+void split_tables(const std::vector<double>& lu, int L, int h, double thr, std::vector<T>& out, int& kg, int& ke) {
   const double* l1 = lu.data();
   const double* l2 = l1 + L;
   const double* u1 = l1 + 2 * L;
@@ -159,15 +170,15 @@ void split_tables(const std::vector<double>& lu, int L, int h, std::vector<float
   auto len = [&](const std::vector<double>& a, const std::vector<double>& b, int n) {
     int k = 0;
     for (int j = 0; j < n; ++j)
-      if (std::fabs(a[j]) > 1e-12 || std::fabs(b[j]) > 1e-12) k = j + 1;
+      if (std::fabs(a[j]) > thr || std::fabs(b[j]) > thr) k = j + 1;
     return k;
   };
   kg = std::max(2, len(H0, H1, L - h));  // c(h), c(h+1) always read H at 0 and 1
   ke = len(E0, E1, h);
   const int LT = L + 8;  // padded: the kernel reads the tables in blocks of eight
-  out.assign((size_t)4 * LT, 0.0f);
-  for (int j = 0; j < kg; ++j) { out[j] = (float)H0[j]; out[LT + j] = (float)H1[j]; }
-  for (int j = 0; j < ke; ++j) { out[2 * LT + j] = (float)E0[j]; out[3 * LT + j] = (float)E1[j]; }
+  out.assign((size_t)4 * LT, T(0));
+  for (int j = 0; j < kg; ++j) { out[j] = (T)H0[j]; out[LT + j] = (T)H1[j]; }
+  for (int j = 0; j < ke; ++j) { out[2 * LT + j] = (T)E0[j]; out[3 * LT + j] = (T)E1[j]; }
 }
 
 struct CaseState {
@@ -211,6 +222,10 @@ struct BlockState {
   float* recv32[3] = {};  // derivative receive buffers of the FP32 fields
   float* drva32[3] = {};
   float* drvb32[3] = {};
+  // FP64 factors (5 L) followed by the FP64 split-solve tables (4 (L + 8)):
+  // the fast FP64 mode's line kind, also a filter candidate of the mixed path
+  double* lu64s[2][3] = {};
+  int h64[2][3] = {}, kg64[2][3] = {}, ke64[2][3] = {};
   double* recv_ptr(int nt, int dir, int m, int side) const {
     const int nc = nt == 0 ? 2 : 3;
     return recv[nt][dir] + ((size_t)(m - 1) * 2 + side) * nc * g.nbs[dir];
@@ -248,6 +263,13 @@ struct canard_ctx {
   std::string err;
   int precision = CANARD_FP64;
   bool f32() const { return precision == CANARD_FP32_MIXED; }
+  // fast FP64 mode: FP64 fields with the split FP64 line solves (FMA)
+  bool fast() const { return precision == CANARD_FP64_FAST; }
+  // the filter runs direction by direction over all five fields (one
+  // contraction and one line launch per direction; the send chain's third
+  // value is the field value itself, which the reference's running update
+  // equals up to one rounding): every context except the bit-exact FP64 one
+  bool filter5() const { return precision != CANARD_FP64; }
   cudaStream_t own = nullptr, st = nullptr;
   std::vector<CaseState> cases;
   std::vector<BlockState> blocks;
@@ -418,11 +440,16 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
                     void* out, int m, bool with_drva, LineTask& t, int kind = LK_F64, bool allow_selfp = false,
                     int nc_req = 0) {
   const BlockGeom& g = B.g;
+  // the filter kernels add the increment to the field they read (FP64
+  // reduce-add stores): in place only
+  if (nt == 1 && in != out) throw ApiError(CANARD_ERR_ARG, "the filter runs in place");
   t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
   t.out = out;
-  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM;
-  t.lu = f64solve ? static_cast<const void*>(B.lu[nt][dir]) : static_cast<const void*>(B.lu32[nt][dir]);
+  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM || kind == LK_F64_SPLIT;
+  t.lu = kind == LK_F64_SPLIT ? static_cast<const void*>(B.lu64s[nt][dir])
+         : f64solve          ? static_cast<const void*>(B.lu[nt][dir])
+                             : static_cast<const void*>(B.lu32[nt][dir]);
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
   t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
   t.c0 = B.luc0[nt][dir];
@@ -443,7 +470,11 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
     t.c0 = B.luc032[nt][dir];
   }
-  if (tile_lanes(kind) == kHalf) {
+  if (kind == LK_F64_SPLIT) {
+    t.h = B.h64[nt][dir];
+    t.kg = B.kg64[nt][dir];
+    t.ke = B.ke64[nt][dir];
+  } else if (tile_lanes(kind) == kHalf) {
     t.h = B.h32[nt][dir];
     t.kg = B.kg32[nt][dir];
     t.ke = B.ke32[nt][dir];
@@ -496,11 +527,12 @@ int max_tile_points(int dir, int kind) {
 
 // Lines too long for the shared-memory tile of any kind the context's step
 // uses are rejected up front (a launch would fail and lose the context).
-void check_line_lengths(const BlockGeom& g, bool f32) {
+void check_line_lengths(const BlockGeom& g, int precision) {
   static const char* dn[3] = {"xi", "eta", "zeta"};
+  const bool f32 = precision == CANARD_FP32_MIXED;
   for (int dir = 0; dir < 3; ++dir) {
     const int L = g.ijk[0][dir] + 1;
-    const int kinds64[1] = {LK_F64};
+    const int kinds64[1] = {precision == CANARD_FP64_FAST ? LK_F64_SPLIT : LK_F64};
     const int kinds32[2] = {LK_F64_TILE_F32_SOLVE, LK_F32};
     const int* ks = f32 ? kinds32 : kinds64;
     const int nk = f32 ? 2 : 1;
@@ -618,11 +650,11 @@ void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
-template <int DIR, int OP, class TT>
+template <int DIR, int OP, class TT, class RS = float>
 void launch_line2_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  launch_line2_t<DIR, OP, TT>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line2_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -663,6 +695,7 @@ void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   else if (OP == 0 && T.kind == LK_F32_1L) launch_line_dir<DIR, 0, float, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE_1L) launch_line_dir<DIR, 1, double, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_STREAM_F32) launch_filt2s_dir<DIR>(c, T);
+  else if (T.kind == LK_F64_SPLIT) launch_line2_dir<DIR, OP, double, double>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -711,6 +744,12 @@ void set_line_smem_limits() {
   CK((line_tm_smem_limit<3, 0>()));
   CK((line_tm_smem_limit<2, 1>()));
   CK((line_tm_smem_limit<3, 1>()));
+  CK((line2_smem_limit<1, 0, double, double>(lim)));
+  CK((line2_smem_limit<2, 0, double, double>(lim)));
+  CK((line2_smem_limit<3, 0, double, double>(lim)));
+  CK((line2_smem_limit<1, 1, double, double>(lim)));
+  CK((line2_smem_limit<2, 1, double, double>(lim)));
+  CK((line2_smem_limit<3, 1, double, double>(lim)));
   CK((filt2s_smem_limit<1>(lim)));
   CK((filt2s_smem_limit<2>(lim)));
   CK((filt2s_smem_limit<3>(lim)));
@@ -831,7 +870,7 @@ void stage_params(canard_ctx* c, int nk0, int nk1, int to_slot = -1) {
 // filtering (src/mo_canard_driver.f90:232-251): for each field, the
 // interface contraction and the filter sweep along each direction in turn
 void ph_filter(canard_ctx* c) {
-  if (c->f32()) {
+  if (c->filter5()) {
     for (int inn = 1; inn <= 3; ++inn) {
       launch_mpigo(c, c->mp_filt5[inn - 1]);
       launch_line(c, c->filt5[inn - 1], kNnf[inn - 1] - 1, 1);
@@ -1193,6 +1232,7 @@ bool tm_ok(const canard_ctx* c, int dir) {
 }
 
 int default_kind(const canard_ctx* c, int grp, int dir) {
+  if (c->fast()) return LK_F64_SPLIT;
   if (!c->f32()) return LK_F64;
   return grp == 0 ? LK_F64_TILE_F32_SOLVE : LK_F32;
 }
@@ -1222,7 +1262,7 @@ std::vector<LineTask> filter_tasks5(canard_ctx* c, int dir, int kind, int nc, bo
 void build_line_tables(canard_ctx* c) {
   for (int inn = 1; inn <= 3; ++inn) {
     const int dir = kNnf[inn - 1] - 1, k = group_kind(c, 0, dir);
-    if (c->f32())
+    if (c->filter5())
       c->filt5[inn - 1] = make_line_table(c, filter_tasks5(c, dir, k, c->tune[0][dir].nc), dir, false, k);
     else
       for (int m = 1; m <= 5; ++m)
@@ -1260,7 +1300,7 @@ void build_tables(canard_ctx* c) {
   build_line_tables(c);
   for (int inn = 1; inn <= 3; ++inn) {
     const int dir = kNnf[inn - 1] - 1;
-    if (f32) {
+    if (c->filter5()) {
       // the faces of this direction only, no send chain
       std::vector<FaceTask> all;
       for (int m = 1; m <= 5; ++m)
@@ -1631,7 +1671,7 @@ void destroy(canard_ctx* c) {
     for (int d = 0; d < 3; ++d) { cudaFree(b.chain[d]); cudaFree(b.drva[d]); cudaFree(b.drvb[d]); cudaFree(b.cm[d]); }
     cudaFree(b.arena32);
     for (int nt = 0; nt < 2; ++nt)
-      for (int d = 0; d < 3; ++d) cudaFree(b.lu32[nt][d]);
+      for (int d = 0; d < 3; ++d) { cudaFree(b.lu32[nt][d]); cudaFree(b.lu64s[nt][d]); }
     for (int d = 0; d < 3; ++d) { cudaFree(b.recv32[d]); cudaFree(b.drva32[d]); cudaFree(b.drvb32[d]); }
     cudaFree(b.gc_pts); cudaFree(b.gc_w); cudaFree(b.sp_pts); cudaFree(b.sp_a); cudaFree(b.sp_b);
   }
@@ -1696,7 +1736,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
             throw ApiError(CANARD_ERR_ARG, "interface face without a neighbour block in the case");
         }
       make_geom(bd, i, k, B.g);
-      check_line_lengths(B.g, c->precision == CANARD_FP32_MIXED);
+      check_line_lengths(B.g, c->precision);
       // remap neighbours to global indices for the links
       c->blocks.push_back(B);
     }
@@ -1753,7 +1793,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
           for (int k = 0; k < 5; ++k) B.luc32[nt][dir][k] = lu32[(size_t)k * L + e];
           B.luc032[nt][dir] = c0f;
           const int h = split_row(L, dir, nt, c0f);
-          split_tables(lu, L, h, hom, B.kg32[nt][dir], B.ke32[nt][dir]);
+          split_tables(lu, L, h, 1e-12, hom, B.kg32[nt][dir], B.ke32[nt][dir]);
           B.h32[nt][dir] = h;
           lu32.insert(lu32.end(), hom.begin(), hom.end());
           B.lu32[nt][dir] = dupload(lu32, c->st);
@@ -1772,6 +1812,14 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
           for (int k = 0; k < 5; ++k) B.luc[nt][dir][k] = lu[(size_t)k * L + e];
         }
         B.luc0[nt][dir] = i0;
+        {  // the split FP64 solve: factors followed by FP64 correction tables
+          std::vector<double> lus(lu), hom;
+          const int h = split_row(L, dir, nt, i0, (int)sizeof(double));
+          split_tables(lu, L, h, 1e-18, hom, B.kg64[nt][dir], B.ke64[nt][dir]);
+          B.h64[nt][dir] = h;
+          lus.insert(lus.end(), hom.begin(), hom.end());
+          B.lu64s[nt][dir] = dupload(lus, c->st);
+        }
         B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs, c->st);
       }
       B.chain[dir] = dalloc<double>((size_t)2 * nbs, c->st);
@@ -1859,7 +1907,8 @@ int canard_ctx_create(const canard_case_desc* cases, int32_t ncases, const canar
                       int32_t precision, canard_ctx** out) {
   if (!out) return CANARD_ERR_ARG;
   *out = nullptr;
-  if (precision != CANARD_FP64 && precision != CANARD_FP32_MIXED) return CANARD_ERR_UNSUPPORTED;
+  if (precision != CANARD_FP64 && precision != CANARD_FP32_MIXED && precision != CANARD_FP64_FAST)
+    return CANARD_ERR_UNSUPPORTED;
   canard_ctx* c = new canard_ctx();
   c->precision = precision;
   int rc = guarded(c, [&] { create(c, cases, ncases, blocks); });
@@ -2269,7 +2318,7 @@ static void unit_line(canard_ctx* c, int iblock, const double* in, double* out, 
   BlockState& B = c->blocks[b];
   double* f = fptr(B, F_SCR + 11);
   h2d_field(c, B, f, in, 1);
-  const int kind = !c->f32() ? LK_F64 : (nt == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
+  const int kind = c->fast() ? LK_F64_SPLIT : !c->f32() ? LK_F64 : (nt == 0 ? LK_F32 : LK_F64_TILE_F32_SOLVE);
   void* fd = f;
   if (kind_f32_fields(kind)) {
     fd = gptr(B, G_SCR + 11);
@@ -2379,12 +2428,16 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         const int op = grp == 0 ? 1 : 0;
         std::vector<std::pair<int, int>> cand;  // (kind, nc)
         std::vector<int> kinds{default_kind(c, grp, dir)};
+        if (c->fast()) kinds.push_back(LK_F64);  // the one-lane FP64 sweeps compete in the fast mode
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
         if (c->f32() && grp == 0) kinds.push_back(LK_F64_STREAM_F32);
         else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
         // the filter acts on the FP64 state with an FP64 right-hand side in every
-        // kind; the FP64 elimination competes with the FP32 ones there
-        if (c->f32() && grp == 0) kinds.push_back(LK_F64);
+        // kind; the FP64 eliminations (one-lane and split) compete with the FP32 ones there
+        if (c->f32() && grp == 0) {
+          kinds.push_back(LK_F64);
+          kinds.push_back(LK_F64_SPLIT);
+        }
         for (int k : kinds) {
           cand.push_back({k, 0});
           if (dir != 0 && k != LK_F64_TM && k != LK_F64_STREAM_F32)
@@ -2394,7 +2447,7 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         canard_ctx::TuneChoice pick;
         for (size_t i = 0; i < cand.size(); ++i) {
           // the step's launch shape: FP32-mixed filters the five fields at once
-          auto v = (grp == 0 && c->f32()) ? filter_tasks5(c, dir, cand[i].first, cand[i].second, true)
+          auto v = (grp == 0 && c->filter5()) ? filter_tasks5(c, dir, cand[i].first, cand[i].second, true)
                                           : group_tasks(c, grp, dir, 1, cand[i].first, cand[i].second, true);
           if (v.empty()) continue;
           Table<LineTask> T = make_line_table(c, v, dir, true, cand[i].first);
@@ -2420,15 +2473,16 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
 
 int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
   return guarded(c, [&] {
-    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_STREAM_F32 || chunks < 0 ||
+    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_SPLIT || chunks < 0 ||
         chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
       throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
     if (kind >= 0) {
       bool fits;
-      if (!c->f32()) fits = kind == LK_F64 || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
+      if (!c->f32())
+        fits = kind == LK_F64 || kind == LK_F64_SPLIT || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
       else if (group == 0)
         fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64 ||
-               (kind == LK_F64_STREAM_F32 && chunks == 0);
+               kind == LK_F64_SPLIT || (kind == LK_F64_STREAM_F32 && chunks == 0);
       else fits = kind == LK_F32 || kind == LK_F32_1L;
       if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
     }

@@ -188,6 +188,14 @@ __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t by
                "r"(bytes)
                : "memory");
 }
+// dst[k] = dst[k] + src[k] over bytes / 8 doubles, one FP64 add with
+// round-to-nearest per element done at the memory side: the filter's
+// in-place f = f + increment without reading f back into the SM
+__device__ __forceinline__ void bulk_s2g_add_f64(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
 // TMA tile copies of a 3-D box (coordinates x, y, z in elements)
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
   asm volatile(
@@ -649,13 +657,14 @@ __device__ __forceinline__ bool sweep_deriv(TT* __restrict__ s, int L, const LuR
 // Compact filter of one line (src/mo_numerics.f90:922-977): the increment is
 // solved for and each row stored as original + increment, the original read
 // from og[row * ogs] (this lane's line in the unfiltered field).
-template <int ST, class TT, class RS, class Done>
+// ADD 1: every row is stored as original (og, stride ogs) + increment; ADD 0:
+// the tile receives the increment alone (the caller adds it to the field).
+template <int ST, class TT, class RS, int ADD, class Done>
 __device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const LuRows<RS>& F, int ndf0, int ndf1,
                                              const DevScheme* __restrict__ sc, TT r00, TT r10, TT r20, TT r01,
                                              TT r11, TT r21, const TT* __restrict__ og, int ogs,
                                              ChunkIn& CI, int* err, Done&& done) {
 #define S(i) s[(i)*ST]
-  constexpr int ADD = 1;
   const int N = L - 1;
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
   auto fbc = [&](int r, int k) { return TT(sc->fbc[r][k]); };
@@ -786,7 +795,7 @@ __host__ __device__ __forceinline__ int dir1_pitch(int L) {
 // the elimination. The tile moves in chunks (see ChunkIn): loads overlap the
 // forward sweep, stores the back substitution.
 template <int DIR, int OP, class TT, class RS>
-__global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
+__global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
                                              int ntasks, const CUtensorMap* __restrict__ maps,
                                              int* __restrict__ err) {
   constexpr int kVec = 16 / (int)sizeof(TT);  // elements per 16 bytes
@@ -854,12 +863,32 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
   while (CI.ready < L) CI.wait_next(err);
   TRACE(7)
 #endif
-  // chunk c is final (the filter added the originals row by row): store it
+  // The filter of FP64 fields (in place) leaves the increment in the tile and
+  // adds it to the field with bulk FP64 reduce-adds; other filters add the
+  // originals row by row.
+  constexpr bool kRedAdd = OP == 1 && sizeof(TT) == 8;
+  if (kRedAdd && DIR == 1 && (L & 1)) s[lane * P + L] = TT(0);  // the 16-byte tail's pad element adds 0
+  // chunk c is final: store it
   auto done = [&](int c) {
     const int lo = c * CR, len = chunk_len(c);
     fence_proxy_async();
     __syncwarp();
-    if (DIR == 1) {
+    if (kRedAdd) {
+      if (DIR == 1) {
+        if (lane < nval) {
+          bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                           (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
+          bulk_commit();
+        }
+      } else {
+        // one reduce-add per row of the chunk (nval columns rounded up to 16
+        // bytes: the extra column is the row's pad, whose increment is 0)
+        const uint32_t rb = (uint32_t)((nval + 1) / 2 * 2 * sizeof(TT));
+        for (int r = lo + lane; r < lo + len; r += kLanes)
+          bulk_s2g_add_f64(out + base + (long long)r * pstride, s + r * kLanes, rb);
+        bulk_commit();
+      }
+    } else if (DIR == 1) {
       if (lane < nval) {
         bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
                  (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
@@ -921,8 +950,8 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
     // lane 0's, whose results are not stored)
     const TT* og = (DIR == 1) ? in + base + (long long)(has ? lane : 0) * Xp : in + base + (has ? lane : 0);
     const int ogs = (DIR == 1) ? 1 : (int)pstride;
-    ok = sweep_filter<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21, og, ogs, CI, err,
-                                  done);
+    ok = sweep_filter<ST, TT, RS, kRedAdd ? 0 : 1>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r20, r01, r11, r21,
+                                                   og, ogs, CI, err, done);
   }
   // every issued bulk store has to finish reading shared memory before exit;
   // after a timeout, wait for the chunks still in flight (bounded) instead
@@ -957,21 +986,25 @@ __global__ void __launch_bounds__(32) k_line(const LineTask* __restrict__ tasks,
 // forward solutions started at rows h-2, h-1, and E0, E1 the homogeneous
 // backward solutions started at rows h, h+1. They depend only on the LU
 // factors and decay geometrically away from h; the host tabulates them in
-// FP64 (stored FP32) as far as they exceed 1e-12. Algebraically this is the
-// same elimination; the rounding differs from the one-lane order, which is
-// why only the FP32 path uses it.
+// FP64 as far as they exceed a threshold below the elimination type's
+// rounding (stored FP32 for the FP32 eliminations, FP64 for the fast FP64
+// mode). Algebraically this is the same elimination; the rounding differs
+// from the one-lane order, which is why the bit-exact FP64 path does not use
+// it.
 constexpr int kHalf = 16;
 
 // Correction tables of one (block, direction, system): H0, H1 indexed by
 // row - h, E0, E1 indexed by h-1-row, each L + 8 long (zero past kh / ke,
 // so blocks of eight read past the end without a bound).
-struct SplitTables {
-  const float* __restrict__ h0;
-  const float* __restrict__ h1;
-  const float* __restrict__ e0;
-  const float* __restrict__ e1;
+template <class RS>
+struct SplitTab {
+  const RS* __restrict__ h0;
+  const RS* __restrict__ h1;
+  const RS* __restrict__ e0;
+  const RS* __restrict__ e1;
   int kh, ke;
 };
+using SplitTables = SplitTab<float>;
 
 // Forward elimination of rows [ib, ie) with per-lane bounds (window w0..w3 =
 // s[i-2..i+1] on entry), blocks of eight.
@@ -1050,11 +1083,10 @@ __device__ __forceinline__ void bwd3(TT* s, int ihi, int ilo, int c0, int c1, co
 // On return (after a warp-wide barrier) the tile holds the derivative or the
 // increment. q0, q1 (, q2): interface values received by the lane's own end
 // (side 0 for the first half, side 1 for the second).
-template <int OP, int ST, class TT>
-__device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int half, const CoefTable<float>& cf,
-                                       const CoefConst<float>& cc, int c0, const SplitTables& H, int ndf0,
+template <int OP, int ST, class TT, class RS = float>
+__device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int half, const CoefTable<RS>& cf,
+                                       const CoefConst<RS>& cc, int c0, const SplitTab<RS>& H, int ndf0,
                                        int ndf1, const DevScheme* __restrict__ sc, TT q0, TT q1, TT q2) {
-  using RS = float;
   constexpr int NE = OP == 0 ? 2 : 3;  // closure rows at each end
   const int N = L - 1;
   const unsigned full = 0xffffffffu;
@@ -1221,14 +1253,14 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
   // ---- both corrections in one loop: first half rows h-1, h-2, ... with
   // (E0, E1; c(h), c(h+1)), second half rows h, h+1, ... with (H0, H1; a(h-2), a(h-1))
   {
-    const float* t0 = half == 0 ? H.e0 : H.h0;
-    const float* t1 = half == 0 ? H.e1 : H.h1;
+    const RS* t0 = half == 0 ? H.e0 : H.h0;
+    const RS* t1 = half == 0 ? H.e1 : H.h1;
     const RS s0 = half == 0 ? C0 : A0, s1 = half == 0 ? C1 : A1;
     const int cnt = half == 0 ? min(H.ke, h) : min(H.kh, L - h);
     const int i0 = half == 0 ? h - 1 : h, di = half == 0 ? -1 : 1;
     const int kmax = max(min(H.ke, h), min(H.kh, L - h));
     for (int j0 = 0; j0 < kmax; j0 += 8) {
-      float g0[8], g1[8];
+      RS g0[8], g1[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         g0[k] = __ldg(t0 + j0 + k);
@@ -1248,11 +1280,13 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
 
 // One CTA = one warp = 16 lines, split solve (see above). DIR: 1 xi, 2 eta,
 // 3 zeta. OP: 0 derivative, 1 filter (in place). TT: field and tile type;
-// the elimination is FP32.
-template <int DIR, int OP, class TT>
+// RS: elimination type (FP32 for the mixed path; FP64 for the fast FP64
+// mode, whose factors and correction tables are FP64).
+template <int DIR, int OP, class TT, class RS = float>
 __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
                                               int ntasks, const CUtensorMap* __restrict__ maps,
                                               int* __restrict__ err) {
+  static_assert(OP == 0 || sizeof(TT) == 8, "the split filter acts on FP64 fields (reduce-add stores)");
   constexpr int kVec = 16 / (int)sizeof(TT);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
@@ -1314,11 +1348,11 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   else if (DIR == 2) jk = (x0 + li) * Z + fix;
   else jk = fix * X + x0 + li;
   const int nbs = T.nbs, N = L - 1;
-  const float* lu = static_cast<const float*>(T.lu);
-  const CoefTable<float> cf{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
-  const float* hb = lu + 5 * L;  // correction tables follow the factors
+  const RS* lu = static_cast<const RS*>(T.lu);
+  const CoefTable<RS> cf{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
+  const RS* hb = lu + 5 * L;  // correction tables follow the factors
   const int LT = L + 8;
-  const SplitTables H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke};
+  const SplitTab<RS> H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke};
   const TT* recv = static_cast<const TT*>(T.recv);
   // interface sums received by the own end
   TT q0 = 0, q1 = 0, q2 = 0;
@@ -1342,59 +1376,34 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
       if (OP == 1) q2 = recv[(nc + 2) * nbs + jk];
     }
   }
-  const CoefConst<float> cc{float(T.cl1), float(T.cl2), float(T.cu1), float(T.cu2), float(T.cu3)};
-  sweep2<OP, ST, TT>(sl, L, h, half, cf, cc, T.c0, H, T.ndf0, T.ndf1, T.sc, q0, q1, q2);
+  const CoefConst<RS> cc{RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3)};
+  sweep2<OP, ST, TT, RS>(sl, L, h, half, cf, cc, T.c0, H, T.ndf0, T.ndf1, T.sc, q0, q1, q2);
   if (OP == 0 && has && T.drva) {
     TT* drva = static_cast<TT*>(T.drva);
     if (half == 0) drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
     else drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[N * ST];
   }
-  // filter: add the originals; then store every chunk
-  if (OP == 1) {
-    if (DIR != 1) {
-      // lanes of both halves split the rows of the 16 columns
-      if (has) {
-        const TT* g = in + base + li;
-        TT* col = s + li;
-        const int lo = half == 0 ? 0 : h, hi = half == 0 ? h : L;
-        int i = lo;
-        for (; i + 16 <= hi; i += 16) {
-          TT v[16];
-#pragma unroll
-          for (int k = 0; k < 16; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
-#pragma unroll
-          for (int k = 0; k < 16; ++k) col[(i + k) * kHalf] = v[k] + col[(i + k) * kHalf];
-        }
-        for (; i < hi; ++i) col[i * kHalf] = __ldg(g + (long long)i * pstride) + col[i * kHalf];
-      }
-    } else {
-      const int tot = nval * L;
-      int e = lane;
-      for (; e + 15 * kLanes < tot; e += 16 * kLanes) {
-        TT v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const int q = e + k * kLanes, r = q / L, i = q - r * L;
-          v[k] = __ldg(in + base + (long long)r * Xp + i);
-        }
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const int q = e + k * kLanes, r = q / L, i = q - r * L;
-          s[r * P + i] = v[k] + s[r * P + i];
-        }
-      }
-      for (; e < tot; e += kLanes) {
-        const int r = e / L, i = e - r * L;
-        s[r * P + i] = __ldg(in + base + (long long)r * Xp + i) + s[r * P + i];
-      }
-    }
-    __syncwarp();
-  }
+  // filter (in place on FP64 fields): the tile holds the increment, added to
+  // the field by bulk FP64 reduce-adds; the derivative's chunks are stored
+  if (OP == 1 && DIR == 1 && (L & 1)) s[li * P + L] = TT(0);  // the 16-byte tail's pad element adds 0
   fence_proxy_async();
   __syncwarp();
   for (int c = 0; c < NC; ++c) {
     const int lo = c * CR, len = chunk_len(c);
-    if (DIR == 1) {
+    if (OP == 1) {
+      if (DIR == 1) {
+        if (lane < nval) {
+          bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                           (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
+        }
+      } else {
+        // one reduce-add per row (nval columns rounded up to 16 bytes: the
+        // extra column is the row's pad, whose increment is 0)
+        const uint32_t rb = (uint32_t)((nval + 1) / 2 * 2 * sizeof(TT));
+        for (int r = lo + lane; r < lo + len; r += kLanes)
+          bulk_s2g_add_f64(out + base + (long long)r * pstride, s + r * kHalf, rb);
+      }
+    } else if (DIR == 1) {
       if (lane < nval) {
         bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
                  (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
@@ -2326,10 +2335,10 @@ void launch_line_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, co
                    const CUtensorMap* maps, int* err) {
   k_line<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
 }
-template <int DIR, int OP, class TT>
+template <int DIR, int OP, class TT, class RS = float>
 void launch_line2_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
                     const CUtensorMap* maps, int* err) {
-  k_line2<DIR, OP, TT><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+  k_line2<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
 }
 template <int DIR>
 void launch_filt2s_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt, int* err) {
@@ -2339,9 +2348,9 @@ template <int DIR>
 cudaError_t filt2s_smem_limit(int bytes) {
   return cudaFuncSetAttribute(k_filt2s<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
-template <int DIR, int OP, class TT>
+template <int DIR, int OP, class TT, class RS = float>
 cudaError_t line2_smem_limit(int bytes) {
-  return cudaFuncSetAttribute(k_line2<DIR, OP, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return cudaFuncSetAttribute(k_line2<DIR, OP, TT, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 template <int DIR, int OP, class TT, class RS>
 cudaError_t line_smem_limit(int bytes) {

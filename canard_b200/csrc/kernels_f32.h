@@ -1,7 +1,9 @@
-// The float instantiations of the kernel launchers. kernels_f32.cu defines
-// them (CANARD_F32_EXTERN empty) in a translation unit compiled with FMA
+// The instantiations of the kernel launchers that are compiled with FMA
+// contraction: the FP32 kernels of the mixed-precision path and the FP64
+// split solves of the fast FP64 mode. kernels_f32.cu defines them
+// (CANARD_F32_EXTERN empty) in a translation unit compiled with FMA
 // contraction; every other unit declares them extern, so it neither
-// instantiates nor compiles the FP32 kernels itself.
+// instantiates nor compiles these kernels itself.
 #pragma once
 #include "kernels.cuh"
 
@@ -50,6 +52,20 @@ CANARD_F32_LINE(1, 1, double)
 CANARD_F32_LINE(2, 1, double)
 CANARD_F32_LINE(3, 1, double)
 #undef CANARD_F32_LINE
+// split solves in FP64 with FMA contraction: the fast FP64 mode (not
+// bit-identical to the reference's order; held to its tolerance)
+#define CANARD_F64S_LINE(DIR, OP)                                                                              \
+  CANARD_F32_EXTERN template void launch_line2_t<DIR, OP, double, double>(int, size_t, cudaStream_t,            \
+                                                                          const LineTask*, const int*, int,    \
+                                                                          const CUtensorMap*, int*);           \
+  CANARD_F32_EXTERN template cudaError_t line2_smem_limit<DIR, OP, double, double>(int);
+CANARD_F64S_LINE(1, 0)
+CANARD_F64S_LINE(2, 0)
+CANARD_F64S_LINE(3, 0)
+CANARD_F64S_LINE(1, 1)
+CANARD_F64S_LINE(2, 1)
+CANARD_F64S_LINE(3, 1)
+#undef CANARD_F64S_LINE
 // one-lane sweeps with an FP32 elimination (the autotuner's alternative)
 #define CANARD_F32_LINE1(DIR, OP, TT)                                                                         \
   CANARD_F32_EXTERN template void launch_line_t<DIR, OP, TT, float>(int, size_t, cudaStream_t, const LineTask*, \

@@ -161,8 +161,9 @@ def gpu_options(nml, precision=None, viscous=None, max_steps=None, split=None) -
     &nml_gpu value (defaults: FP64, viscous, no step limit, no split)."""
     g = nml["nml_gpu"]
     if precision is None:
-        if int(g["nprecision"]) not in (api.FP64, api.FP32_MIXED):
-            raise namelist.NamelistError(f"&nml_gpu: nprecision {int(g['nprecision'])} (0 FP64, 1 FP32-mixed)")
+        if int(g["nprecision"]) not in (api.FP64, api.FP32_MIXED, api.FP64_FAST):
+            raise namelist.NamelistError(f"&nml_gpu: nprecision {int(g['nprecision'])} "
+                                         "(0 FP64, 1 FP32-mixed, 2 fast FP64)")
         precision = int(g["nprecision"])
     if viscous is None:
         viscous = 0 if bool(g["linviscid"]) else 1

@@ -45,7 +45,7 @@ SCHEMA: Dict[str, Dict[str, Tuple[str, tuple]]] = {
     "nml_sponge": {"szco": ("r", _SCALAR)},
     # Options of this implementation, in a group of its own that the reference's
     # READs never look for (they search their groups by name): nprecision 0
-    # FP64, 1 FP32-mixed; lsplit: run nbpc's sub-domains as the reference's
+    # FP64, 1 FP32-mixed, 2 fast FP64; lsplit: run nbpc's sub-domains as the reference's
     # ranks; nsteps > 0: stop after that many steps as well; linviscid: the
     # reference built without VISCOUS.
     "nml_gpu": {"nprecision": ("i", _SCALAR), "lsplit": ("l", _SCALAR), "nsteps": ("i", _SCALAR),

@@ -44,8 +44,12 @@ extern "C" {
 #define CANARD_ERR_STATE 6       /* call order (e.g. step before setup) */
 #define CANARD_ERR_IO 7          /* a file could not be opened, read or written, or has another block's size */
 
-#define CANARD_FP64 0            /* plain FP64 path */
+#define CANARD_FP64 0            /* plain FP64 path, bit-identical to the reference's operation order */
 #define CANARD_FP32_MIXED 1      /* FP32 line solves/fluxes, FP64 state, RK, metrics, LU */
+#define CANARD_FP64_FAST 2       /* FP64 throughout, line solves split in two halves per line with FMA,
+                                    the filter direction by direction over the five fields: not
+                                    bit-identical, rounding-level differences (<= 1e-10 relative L2
+                                    after 10 steps is the bound its tests hold) */
 
 typedef struct canard_ctx canard_ctx;
 
@@ -281,7 +285,9 @@ int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, 
  * the elimination results in tensor memory; mixed-precision contexts also try
  * the one-lane FP32 sweeps (32 lines per tile) against the split solve (16
  * lines per tile), and for the filter, which filters the FP64 state with an
- * FP64 right-hand side in every kind, the FP64 elimination as well. The
+ * FP64 right-hand side in every kind, the FP64 eliminations (one-lane and
+ * split) as well; fast FP64 contexts try the split FP64 solve against the
+ * one-lane FP64 sweeps. The
  * fastest choice is installed in the step tables. Returns the number of groups
  * (9) and fills up to nmax report rows of 6 doubles: group, direction
  * (0..2), chosen kind, chosen chunk count (0 = default), its ms per launch
@@ -293,8 +299,12 @@ int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax)
  * counterpart in the reference): kind 0 FP64 tiles in shared memory (chunks:
  * 0 default or 2..8 TMA stages), 1 FP32 split, 2 FP64 tile / FP32 split, 3
  * FP32 one-lane, 4 FP64 tile / FP32 one-lane, 5 FP64 with the elimination
- * results in tensor memory (eta/zeta, 16..257 points per line); -1 restores
- * the precision's default. Every FP64 kind gives bit-identical results. A kind
+ * results in tensor memory (eta/zeta, 16..257 points per line), 6 the filter
+ * of the FP64 state streamed into FP32 right-hand sides (mixed precision), 7
+ * FP64 split solve with FMA (FP64 and fast FP64 contexts; the fast mode's
+ * default); -1 restores the precision's default. Kinds 0 and 5 give results
+ * bit-identical to the reference's operation order; kind 7 differs from them
+ * at the rounding level. A kind
  * the context's precision or line lengths do not admit returns
  * CANARD_ERR_ARG. Before canard_setup the choice only applies to
  * canard_line_bench (the step tables are built by canard_setup). */

@@ -24,7 +24,7 @@ module mo_canard_gpu
    integer(c_int), parameter :: CANARD_OK = 0, CANARD_ERR_ARG = 1, CANARD_ERR_CUDA = 2, CANARD_ERR_NAN = 3, &
                                 CANARD_ERR_TIMEOUT = 4, CANARD_ERR_UNSUPPORTED = 5, CANARD_ERR_STATE = 6, &
                                 CANARD_ERR_IO = 7
-   integer(c_int32_t), parameter :: CANARD_FP64 = 0, CANARD_FP32_MIXED = 1
+   integer(c_int32_t), parameter :: CANARD_FP64 = 0, CANARD_FP32_MIXED = 1, CANARD_FP64_FAST = 2
    ! field ids of canard_get_field / canard_set_field
    integer(c_int32_t), parameter :: CANARD_F_QA = 0, CANARD_F_QO = 1, CANARD_F_DE = 2, CANARD_F_P = 3, &
                                     CANARD_F_SS1 = 4, CANARD_F_XIM = 5, CANARD_F_ETM = 6, CANARD_F_ZEM = 7, &

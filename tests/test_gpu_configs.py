@@ -1,13 +1,13 @@
 """The benchmark configurations at their stated sizes against the oracle.
 
-Each config is run on the device (FP64 plain and FP32-mixed) and by the CPU
-oracle from the same initial condition for the same number of full time
-steps; the error is the relative L2 distance per conserved variable (rho,
+Each config is run on the device (FP64 plain, fast FP64 and FP32-mixed) and
+by the CPU oracle from the same initial condition for the same number of full
+time steps; the error is the relative L2 distance per conserved variable (rho,
 rho u, rho v, rho w, rho E), the momenta measured against ||rho|| * U where
 that exceeds their own norm (U the case's velocity scale: a component that is
 zero by symmetry has no relative error of its own). Bounds: <= 1e-10 for the
 FP64 path (the Sutherland power is the one place its rounding may differ from
-the oracle's by an ulp), <= 1e-5 for FP32-mixed.
+the oracle's by an ulp) and the fast FP64 mode, <= 1e-5 for FP32-mixed.
 
 * C1: Taylor-Green vortex, 64^3 cells, 100 steps.
 * C2: the same at 256^3 cells (257^3 stored points), 10 steps.
@@ -60,7 +60,8 @@ def run_oracle(cs, steps):
 def check(cs, steps, uref, fp32=True):
     ref = run_oracle(cs, steps)
     worst = {}
-    for name, prec, tol in (("fp64", api.FP64, 1e-10), ("fp32", api.FP32_MIXED, 1e-5)):
+    for name, prec, tol in (("fp64", api.FP64, 1e-10), ("fast", api.FP64_FAST, 1e-10),
+                            ("fp32", api.FP32_MIXED, 1e-5)):
         if name == "fp32" and not fp32:
             continue
         got = run_device(cs, steps, prec)

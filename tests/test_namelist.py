@@ -429,4 +429,4 @@ def test_nml_gpu_options(tmp_path, monkeypatch):
     ctx = made[-1]
     assert ctx.precision == 0 and len(ctx.cs.blocks) == 6 and ctx.steps == 2 and ctx.cs.viscous == 1
     with pytest.raises(namelist.NamelistError):
-        driver.gpu_options(namelist.read(base + "\n&nml_gpu nprecision = 2 /\n"))
+        driver.gpu_options(namelist.read(base + "\n&nml_gpu nprecision = 3 /\n"))
