@@ -139,7 +139,7 @@ def vortex_state(X, Y, mach, strength=5.0, radius=1.0, xc=0.0, yc=0.0):
 
 
 def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, viscous=1,
-           sponge_cells=20) -> CaseSpec:
+           sponge_cells=20, xc=0.0, cfl=0.8) -> CaseSpec:
     """Isentropic vortex carried by a Mach ``mach`` stream through a
     non-reflecting (GCBC) outflow, in Canard's moving-frame form: the state
     holds the vortex around fluid at rest, the frame moves at Mach ``mach``
@@ -162,9 +162,9 @@ def vortex(nx=384, ny=256, nz=128, mach=0.5, strength=5.0, radius=1.0, re=1e5, v
     y = -0.5 * ny * dx + dx * np.arange(ny + 1)  # periodic: the last point repeats the first
     z = dx * np.arange(nz + 1)
     Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    rho, u, v, w, p = vortex_state(X, Y, mach, strength, radius)
+    rho, u, v, w, p = vortex_state(X, Y, mach, strength, radius, xc=xc)
     szth = 0.5 * sponge_cells * dx
-    return CaseSpec([blk], viscous=viscous, reoo=re, amach=(mach, 0.0, 0.0), nsmf=1,
+    return CaseSpec([blk], viscous=viscous, reoo=re, amach=(mach, 0.0, 0.0), nsmf=1, cfl=cfl,
                     szco=1.0, szth0=szth, szth1=szth, doml0=8.0, doml1=8.0,
                     xyz=[np.stack([X, Y, Z])], qa=[_conserved(rho, u - mach, v, w, p)],
                     name=f"vortex{nx}x{ny}x{nz}")

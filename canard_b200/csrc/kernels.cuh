@@ -863,29 +863,21 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   while (CI.ready < L) CI.wait_next(err);
   TRACE(7)
 #endif
-  // The filter of FP64 fields (in place) leaves the increment in the tile and
-  // adds it to the field with bulk FP64 reduce-adds; other filters add the
-  // originals row by row.
-  constexpr bool kRedAdd = OP == 1 && sizeof(TT) == 8;
-  if (kRedAdd && DIR == 1 && (L & 1)) s[lane * P + L] = TT(0);  // the 16-byte tail's pad element adds 0
+  // The xi filter of FP64 fields (in place) leaves the increment in the tile
+  // and adds it to the field with one bulk FP64 reduce-add per line chunk; the
+  // eta/zeta filters add the originals row by row (a reduce-add per 256-byte
+  // row costs more than the re-read, measured).
+  constexpr bool kRedAdd = OP == 1 && sizeof(TT) == 8 && DIR == 1;
+  if (kRedAdd && (L & 1)) s[lane * P + L] = TT(0);  // the 16-byte tail's pad element adds 0
   // chunk c is final: store it
   auto done = [&](int c) {
     const int lo = c * CR, len = chunk_len(c);
     fence_proxy_async();
     __syncwarp();
     if (kRedAdd) {
-      if (DIR == 1) {
-        if (lane < nval) {
-          bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
-                           (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
-          bulk_commit();
-        }
-      } else {
-        // one reduce-add per row of the chunk (nval columns rounded up to 16
-        // bytes: the extra column is the row's pad, whose increment is 0)
-        const uint32_t rb = (uint32_t)((nval + 1) / 2 * 2 * sizeof(TT));
-        for (int r = lo + lane; r < lo + len; r += kLanes)
-          bulk_s2g_add_f64(out + base + (long long)r * pstride, s + r * kLanes, rb);
+      if (lane < nval) {
+        bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
+                         (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
         bulk_commit();
       }
     } else if (DIR == 1) {
@@ -1007,12 +999,31 @@ struct SplitTab {
 using SplitTables = SplitTab<float>;
 
 // Forward elimination of rows [ib, ie) with per-lane bounds (window w0..w3 =
-// s[i-2..i+1] on entry), blocks of eight.
+// s[i-2..i+1] on entry), blocks of eight, software-pipelined: the next block's
+// factors and right-hand sides are formed while the current block's chain runs
+// (they read rows the chain does not write).
 template <int ST, class TT, class RS, class CF>
 __device__ __forceinline__ void fwd_rows_deriv(TT* s, int ib, int ie, const CF& cf, TT& w0, TT& w1, TT& w2,
                                                TT& w3, RS& am2, RS& am1) {
   int i = ib;
-  for (; i + 7 < ie; i += 8) fwd8_deriv<ST, TT, RS>(s, i, cf, w0, w1, w2, w3, am2, am1);
+  if (i + 7 < ie) {
+    F8<RS> nx;
+    nx.load(cf, i);
+    TT rr[8];
+    rhs8_deriv<ST, TT>(s, i, w0, w1, w2, w3, rr);
+    while (i + 15 < ie) {
+      const F8<RS> cu = nx;
+      TT rc[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) rc[k] = rr[k];
+      nx.load(cf, i + 8);
+      rhs8_deriv<ST, TT>(s, i + 8, w0, w1, w2, w3, rr);
+      chain8_fwd<ST, TT, RS>(s, i, cu, rc, am2, am1);
+      i += 8;
+    }
+    chain8_fwd<ST, TT, RS>(s, i, nx, rr, am2, am1);
+    i += 8;
+  }
   for (; i < ie; ++i) {
     const TT w4 = s[(i + 2) * ST];
     const TT rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4 - w0);
@@ -1027,7 +1038,24 @@ template <int ST, class TT, class RS, class CF>
 __device__ __forceinline__ void fwd_rows_filter(TT* s, int ib, int ie, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
                                                 TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
   int i = ib;
-  for (; i + 7 < ie; i += 8) fwd8_filter<ST, TT, RS>(s, i, cf, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  if (i + 7 < ie) {
+    F8<RS> nx;
+    nx.load(cf, i);
+    TT rr[8];
+    rhs8_filter<ST, TT>(s, i, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr);
+    while (i + 15 < ie) {
+      const F8<RS> cu = nx;
+      TT rc[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) rc[k] = rr[k];
+      nx.load(cf, i + 8);
+      rhs8_filter<ST, TT>(s, i + 8, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr);
+      chain8_fwd<ST, TT, RS>(s, i, cu, rc, am2, am1);
+      i += 8;
+    }
+    chain8_fwd<ST, TT, RS>(s, i, nx, rr, am2, am1);
+    i += 8;
+  }
   for (; i < ie; ++i) {
     const TT w6 = s[(i + 3) * ST];
     const TT rk = w3 + w3;
@@ -1039,11 +1067,31 @@ __device__ __forceinline__ void fwd_rows_filter(TT* s, int ib, int ie, const CF&
   }
 }
 
-// back substitution of rows ihi down to ilo (inclusive), per-lane bounds
+// back substitution of rows ihi down to ilo (inclusive), per-lane bounds;
+// the next block's factors and u1 products are formed during the current
+// block's chain (they read rows below the ones it writes)
 template <int ST, class TT, class RS, class CF>
 __device__ __forceinline__ void bwd_rows(TT* s, int ihi, int ilo, const CF& cf, RS& cp1, RS& cp2) {
   int i = ihi;
-  for (; i - 7 >= ilo; i -= 8) bwd8<ST, TT, RS>(s, i, cf, cp1, cp2);
+  if (i - 7 >= ilo) {
+    B8<RS> bn;
+    O8<TT> on;
+    RS pn[8];
+    bn.load(cf, i);
+    bwd_p8<ST, TT, RS>(s, i, bn, pn);
+    while (i - 15 >= ilo) {
+      const B8<RS> bu = bn;
+      RS pu[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) pu[k] = pn[k];
+      bn.load(cf, i - 8);
+      bwd_p8<ST, TT, RS>(s, i - 8, bn, pn);
+      bwd_chain8<ST, TT, RS, 0>(s, i, bu, pu, on, cp1, cp2);
+      i -= 8;
+    }
+    bwd_chain8<ST, TT, RS, 0>(s, i, bn, pn, on, cp1, cp2);
+    i -= 8;
+  }
   for (; i >= ilo; --i) {
     const RS c = (cf.U1(i) * RS(s[i * ST]) - cf.U2(i) * cp1) - cf.U3(i) * cp2;
     s[i * ST] = TT(c);
@@ -1231,6 +1279,17 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
   const int src = threadIdx.x & (kHalf - 1);
   const RS A0 = __shfl_sync(full, am2, src), A1 = __shfl_sync(full, am1, src);
   __syncwarp();
+  TRACE(3)
+  // the correction tables' first entries load under the back substitution
+  const RS* t0 = half == 0 ? H.e0 : H.h0;
+  const RS* t1 = half == 0 ? H.e1 : H.h1;
+  RS g0[8], g1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    g0[k] = __ldg(t0 + k);
+    g1[k] = __ldg(t1 + k);
+  }
+  const RS hh00 = __ldg(H.h0), hh01 = __ldg(H.h0 + 1), hh10 = __ldg(H.h1), hh11 = __ldg(H.h1 + 1);
   // ---- back substitution: two end rows (second half), then the shared loop
   RS cp1 = 0, cp2 = 0;
   if (half == 1) {
@@ -1243,28 +1302,30 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
   }
   bwd3<ST, TT, RS>(s, half == 0 ? h - 1 : N - 2, half == 0 ? 0 : h, c0, c1, cf, cc, cp1, cp2);
   // the second half's true c(h), c(h+1), needed by the first half's correction
+  TRACE(4)
   RS ch0 = 0, ch1 = 0;
   if (half == 1) {
-    ch0 = cp1 + (__ldg(H.h0) * A0 + __ldg(H.h1) * A1);
-    ch1 = cp2 + (__ldg(H.h0 + 1) * A0 + __ldg(H.h1 + 1) * A1);
+    ch0 = cp1 + (hh00 * A0 + hh10 * A1);
+    ch1 = cp2 + (hh01 * A0 + hh11 * A1);
   }
   const RS C0 = __shfl_sync(full, ch0, src + kHalf), C1 = __shfl_sync(full, ch1, src + kHalf);
   __syncwarp();
   // ---- both corrections in one loop: first half rows h-1, h-2, ... with
-  // (E0, E1; c(h), c(h+1)), second half rows h, h+1, ... with (H0, H1; a(h-2), a(h-1))
+  // (E0, E1; c(h), c(h+1)), second half rows h, h+1, ... with (H0, H1;
+  // a(h-2), a(h-1)); the next block's table entries load during the current
+  // block (the tables hold L + 8 entries, zero past their length)
   {
-    const RS* t0 = half == 0 ? H.e0 : H.h0;
-    const RS* t1 = half == 0 ? H.e1 : H.h1;
     const RS s0 = half == 0 ? C0 : A0, s1 = half == 0 ? C1 : A1;
     const int cnt = half == 0 ? min(H.ke, h) : min(H.kh, L - h);
     const int i0 = half == 0 ? h - 1 : h, di = half == 0 ? -1 : 1;
     const int kmax = max(min(H.ke, h), min(H.kh, L - h));
     for (int j0 = 0; j0 < kmax; j0 += 8) {
-      RS g0[8], g1[8];
+      RS n0[8], n1[8];
+      const bool more = j0 + 8 < kmax;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        g0[k] = __ldg(t0 + j0 + k);
-        g1[k] = __ldg(t1 + j0 + k);
+        n0[k] = more ? __ldg(t0 + j0 + 8 + k) : RS(0);
+        n1[k] = more ? __ldg(t1 + j0 + 8 + k) : RS(0);
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -1272,6 +1333,11 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
           const int i = i0 + di * (j0 + k);
           s[i * ST] = TT(RS(s[i * ST]) + (g0[k] * s0 + g1[k] * s1));
         }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        g0[k] = n0[k];
+        g1[k] = n1[k];
       }
     }
   }
@@ -1293,6 +1359,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   TT* s = reinterpret_cast<TT*>(smem_raw + 128);
   const int lane = threadIdx.x;
   const int half = lane >> 4, li = lane & (kHalf - 1);
+  TRACE(0)
   if (error_pending(err)) return;
   const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
   const LineTask& T = tasks[ti];
@@ -1333,6 +1400,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
       else tma_load_3d(s + c * CR * kHalf, map_in, x0, fix, c * CR, bars + c);
     }
   }
+  TRACE(1)
   bool ok = true;
   for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
   if (!ok) {
@@ -1340,6 +1408,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
     return;
   }
   __syncwarp();
+  TRACE(2)
   constexpr int ST = (DIR == 1) ? 1 : kHalf;
   TT* sl = (DIR == 1) ? s + li * P : s + li;
   const bool has = li < nval;
@@ -1378,35 +1447,43 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   }
   const CoefConst<RS> cc{RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3)};
   sweep2<OP, ST, TT, RS>(sl, L, h, half, cf, cc, T.c0, H, T.ndf0, T.ndf1, T.sc, q0, q1, q2);
+  TRACE(5)
   if (OP == 0 && has && T.drva) {
     TT* drva = static_cast<TT*>(T.drva);
     if (half == 0) drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
     else drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[N * ST];
   }
-  // filter (in place on FP64 fields): the tile holds the increment, added to
-  // the field by bulk FP64 reduce-adds; the derivative's chunks are stored
+  // filter (in place on FP64 fields): along xi the tile keeps the increment,
+  // added to the field by one bulk FP64 reduce-add per line chunk; along
+  // eta/zeta the lanes of both halves add the originals to the 16 columns
+  // (coalesced 128-byte rows, still in L2), then the chunks are stored
+  if (OP == 1 && DIR != 1) {
+    if (has) {
+      const TT* g = in + base + li;
+      TT* col = s + li;
+      const int lo = half == 0 ? 0 : h, hi = half == 0 ? h : L;
+      int i = lo;
+      for (; i + 16 <= hi; i += 16) {
+        TT v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) col[(i + k) * kHalf] = v[k] + col[(i + k) * kHalf];
+      }
+      for (; i < hi; ++i) col[i * kHalf] = __ldg(g + (long long)i * pstride) + col[i * kHalf];
+    }
+    __syncwarp();
+  }
   if (OP == 1 && DIR == 1 && (L & 1)) s[li * P + L] = TT(0);  // the 16-byte tail's pad element adds 0
   fence_proxy_async();
   __syncwarp();
   for (int c = 0; c < NC; ++c) {
     const int lo = c * CR, len = chunk_len(c);
-    if (OP == 1) {
-      if (DIR == 1) {
-        if (lane < nval) {
-          bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
-                           (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
-        }
-      } else {
-        // one reduce-add per row (nval columns rounded up to 16 bytes: the
-        // extra column is the row's pad, whose increment is 0)
-        const uint32_t rb = (uint32_t)((nval + 1) / 2 * 2 * sizeof(TT));
-        for (int r = lo + lane; r < lo + len; r += kLanes)
-          bulk_s2g_add_f64(out + base + (long long)r * pstride, s + r * kHalf, rb);
-      }
-    } else if (DIR == 1) {
+    if (DIR == 1) {
       if (lane < nval) {
-        bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo,
-                 (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
+        const uint32_t nb = (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT));
+        if (OP == 1) bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
+        else bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
       }
     } else if (lane == 0) {
       if (DIR == 2) tma_store_3d(map_out, x0, lo, fix, s + lo * kHalf);
@@ -1415,6 +1492,14 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   }
   bulk_commit();
   bulk_wait_read0();
+  TRACE(7)
+#ifdef CANARD_TRACE
+  if (threadIdx.x == 0) {
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    g_trace[(long long)blockIdx.x * 8 + 6] = smid;
+  }
+#endif
 }
 
 // ---------------------------------------------------------------------------
