@@ -126,9 +126,12 @@ int split_row(int L, int dir, int nt, int c0, int es = 4) {
 // E0, E1 = the homogeneous backward solutions started at rows h, h+1 (index
 // h-1-row); each L + 8 entries of type T; returns the lengths beyond which
 // every entry stays below thr (set to zero): 1e-12 for the FP32
-// eliminations, 1e-18 for the FP64 ones.
+// eliminations, 1e-18 for the FP64 ones; kf: the same length for the
+// forward homogeneous solutions G0, G1 themselves (index row - h), which the
+// split kernel forms by their recurrence in registers.
 template <class T>
-void split_tables(const std::vector<double>& lu, int L, int h, double thr, std::vector<T>& out, int& kg, int& ke) {
+void split_tables(const std::vector<double>& lu, int L, int h, double thr, std::vector<T>& out, int& kg, int& ke,
+                  int& kf) {
   const double* l1 = lu.data();
   const double* l2 = l1 + L;
   const double* u1 = l1 + 2 * L;
@@ -175,6 +178,10 @@ void split_tables(const std::vector<double>& lu, int L, int h, double thr, std::
   };
   kg = std::max(2, len(H0, H1, L - h));  // c(h), c(h+1) always read H at 0 and 1
   ke = len(E0, E1, h);
+  {
+    std::vector<double> g0(G0.begin() + h, G0.end()), g1(G1.begin() + h, G1.end());
+    kf = len(g0, g1, L - h);
+  }
   const int LT = L + 8;  // padded: the kernel reads the tables in blocks of eight
   out.assign((size_t)4 * LT, T(0));
   for (int j = 0; j < kg; ++j) { out[j] = (T)H0[j]; out[LT + j] = (T)H1[j]; }
@@ -216,7 +223,7 @@ struct BlockState {
   // mixed precision: FP32 work fields, factors and line-end buffers
   float* arena32 = nullptr;
   float* lu32[2][3] = {};   // FP32 factors (5 L) followed by the split-solve tables (4 (L + 8))
-  int h32[2][3] = {}, kg32[2][3] = {}, ke32[2][3] = {};
+  int h32[2][3] = {}, kg32[2][3] = {}, ke32[2][3] = {}, kf32[2][3] = {};
   float luc32[2][3][5] = {};  // bitwise-constant interior FP32 factors
   int luc032[2][3] = {};      // first row of that range
   float* recv32[3] = {};  // derivative receive buffers of the FP32 fields
@@ -225,7 +232,7 @@ struct BlockState {
   // FP64 factors (5 L) followed by the FP64 split-solve tables (4 (L + 8)):
   // the fast FP64 mode's line kind, also a filter candidate of the mixed path
   double* lu64s[2][3] = {};
-  int h64[2][3] = {}, kg64[2][3] = {}, ke64[2][3] = {};
+  int h64[2][3] = {}, kg64[2][3] = {}, ke64[2][3] = {}, kf64[2][3] = {};
   double* recv_ptr(int nt, int dir, int m, int side) const {
     const int nc = nt == 0 ? 2 : 3;
     return recv[nt][dir] + ((size_t)(m - 1) * 2 + side) * nc * g.nbs[dir];
@@ -464,7 +471,7 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.m = m;
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
-  t.h = t.kg = t.ke = 0;
+  t.h = t.kg = t.ke = t.kf = 0;
   if (!f64solve) {  // FP32 elimination: rounded factors and their constant range
     t.cl1 = B.luc32[nt][dir][0]; t.cl2 = B.luc32[nt][dir][1]; t.cu1 = B.luc32[nt][dir][2];
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
@@ -474,10 +481,12 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
     t.h = B.h64[nt][dir];
     t.kg = B.kg64[nt][dir];
     t.ke = B.ke64[nt][dir];
+    t.kf = B.kf64[nt][dir];
   } else if (tile_lanes(kind) == kHalf) {
     t.h = B.h32[nt][dir];
     t.kg = B.kg32[nt][dir];
     t.ke = B.ke32[nt][dir];
+    t.kf = B.kf32[nt][dir];
   }
   chunking_dir(dir, t.L, t.nbox, t.by, nc_req);
   if (kind == LK_F64_TM) {  // 32-row boxes streamed through the ring
@@ -1793,7 +1802,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
           for (int k = 0; k < 5; ++k) B.luc32[nt][dir][k] = lu32[(size_t)k * L + e];
           B.luc032[nt][dir] = c0f;
           const int h = split_row(L, dir, nt, c0f);
-          split_tables(lu, L, h, 1e-12, hom, B.kg32[nt][dir], B.ke32[nt][dir]);
+          split_tables(lu, L, h, 1e-12, hom, B.kg32[nt][dir], B.ke32[nt][dir], B.kf32[nt][dir]);
           B.h32[nt][dir] = h;
           lu32.insert(lu32.end(), hom.begin(), hom.end());
           B.lu32[nt][dir] = dupload(lu32, c->st);
@@ -1815,7 +1824,7 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
         {  // the split FP64 solve: factors followed by FP64 correction tables
           std::vector<double> lus(lu), hom;
           const int h = split_row(L, dir, nt, i0, (int)sizeof(double));
-          split_tables(lu, L, h, 1e-18, hom, B.kg64[nt][dir], B.ke64[nt][dir]);
+          split_tables(lu, L, h, 1e-18, hom, B.kg64[nt][dir], B.ke64[nt][dir], B.kf64[nt][dir]);
           B.h64[nt][dir] = h;
           lus.insert(lus.end(), hom.begin(), hom.end());
           B.lu64s[nt][dir] = dupload(lus, c->st);

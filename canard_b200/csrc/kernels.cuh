@@ -96,6 +96,7 @@ struct LineTask {
   int L, nbs, m, ndf0, ndf1;
   int selfp;               // derivative of a line periodic onto itself: contraction formed in the kernel
   int h, kg, ke;           // split solves: first row of the second half; homogeneous table lengths
+  int kf;                  // split solves: rows the forward homogeneous solutions from h span
   int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
   int nbox, by;            // chunks per tile and positions per chunk
 };
@@ -804,8 +805,9 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   TT* s = reinterpret_cast<TT*>(smem_raw + 128);
   const int lane = threadIdx.x;
   TRACE(0)
-  if (error_pending(err)) return;
+  // the tile's task and the error flag load together (independent)
   const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
+  if (error_pending(err)) return;
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -995,6 +997,7 @@ struct SplitTab {
   const RS* __restrict__ e0;
   const RS* __restrict__ e1;
   int kh, ke;
+  int kf;  // rows the forward homogeneous solutions from h span (register recurrence)
 };
 using SplitTables = SplitTab<float>;
 
@@ -1280,16 +1283,36 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
   const RS A0 = __shfl_sync(full, am2, src), A1 = __shfl_sync(full, am1, src);
   __syncwarp();
   TRACE(3)
-  // the correction tables' first entries load under the back substitution
-  const RS* t0 = half == 0 ? H.e0 : H.h0;
-  const RS* t1 = half == 0 ? H.e1 : H.h1;
-  RS g0[8], g1[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    g0[k] = __ldg(t0 + k);
-    g1[k] = __ldg(t1 + k);
+  // ---- second half: its forward values from the zero start plus the
+  // homogeneous forward solution g(i) = -l1 g(i-2) - l2 g(i-1) started from
+  // the first half's a(h-2), a(h-1), over the rows where it has not decayed
+  // (the recurrence in registers: no table reads); its back substitution
+  // below then runs on the true forward values
+  if (half == 1) {
+    RS g2 = A0, g1 = A1;
+    const int ie = min(h + H.kf, L);
+    int i = h;
+    for (; i < min(ie, c0); ++i) {  // rows below the constant range (short lines)
+      const RS g = -(cf.L1(i) * g2) - cf.L2(i) * g1;
+      s[i * ST] = TT(RS(s[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
+#pragma unroll 4
+    for (; i < min(ie, c1 + 1); ++i) {  // the constant interior factors
+      const RS g = -(cc.L1(i) * g2) - cc.L2(i) * g1;
+      s[i * ST] = TT(RS(s[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
+    for (; i < ie; ++i) {
+      const RS g = -(cf.L1(i) * g2) - cf.L2(i) * g1;
+      s[i * ST] = TT(RS(s[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
   }
-  const RS hh00 = __ldg(H.h0), hh01 = __ldg(H.h0 + 1), hh10 = __ldg(H.h1), hh11 = __ldg(H.h1 + 1);
+  __syncwarp();
   // ---- back substitution: two end rows (second half), then the shared loop
   RS cp1 = 0, cp2 = 0;
   if (half == 1) {
@@ -1301,44 +1324,34 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
     cp1 = c;
   }
   bwd3<ST, TT, RS>(s, half == 0 ? h - 1 : N - 2, half == 0 ? 0 : h, c0, c1, cf, cc, cp1, cp2);
-  // the second half's true c(h), c(h+1), needed by the first half's correction
   TRACE(4)
-  RS ch0 = 0, ch1 = 0;
-  if (half == 1) {
-    ch0 = cp1 + (hh00 * A0 + hh10 * A1);
-    ch1 = cp2 + (hh01 * A0 + hh11 * A1);
-  }
-  const RS C0 = __shfl_sync(full, ch0, src + kHalf), C1 = __shfl_sync(full, ch1, src + kHalf);
+  // the second half's c(h), c(h+1) are final: the first half adds the
+  // homogeneous backward solution e(i) = -u2 e(i+1) - u3 e(i+2) started from
+  // them to its rows from the zero start, down to where it has decayed
+  const RS C0 = __shfl_sync(full, cp1, src + kHalf), C1 = __shfl_sync(full, cp2, src + kHalf);
   __syncwarp();
-  // ---- both corrections in one loop: first half rows h-1, h-2, ... with
-  // (E0, E1; c(h), c(h+1)), second half rows h, h+1, ... with (H0, H1;
-  // a(h-2), a(h-1)); the next block's table entries load during the current
-  // block (the tables hold L + 8 entries, zero past their length)
-  {
-    const RS s0 = half == 0 ? C0 : A0, s1 = half == 0 ? C1 : A1;
-    const int cnt = half == 0 ? min(H.ke, h) : min(H.kh, L - h);
-    const int i0 = half == 0 ? h - 1 : h, di = half == 0 ? -1 : 1;
-    const int kmax = max(min(H.ke, h), min(H.kh, L - h));
-    for (int j0 = 0; j0 < kmax; j0 += 8) {
-      RS n0[8], n1[8];
-      const bool more = j0 + 8 < kmax;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        n0[k] = more ? __ldg(t0 + j0 + 8 + k) : RS(0);
-        n1[k] = more ? __ldg(t1 + j0 + 8 + k) : RS(0);
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (j0 + k < cnt) {
-          const int i = i0 + di * (j0 + k);
-          s[i * ST] = TT(RS(s[i * ST]) + (g0[k] * s0 + g1[k] * s1));
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        g0[k] = n0[k];
-        g1[k] = n1[k];
-      }
+  if (half == 0) {
+    RS e1 = C0, e2 = C1;
+    const int ib = max(h - H.ke, 0);
+    int i = h - 1;
+    for (; i > c1 && i >= ib; --i) {  // rows above the constant range (short lines)
+      const RS e = -(cf.U2(i) * e1) - cf.U3(i) * e2;
+      s[i * ST] = TT(RS(s[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
+    }
+#pragma unroll 4
+    for (; i >= max(ib, c0); --i) {  // the constant interior factors
+      const RS e = -(cc.U2(i) * e1) - cc.U3(i) * e2;
+      s[i * ST] = TT(RS(s[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
+    }
+    for (; i >= ib; --i) {
+      const RS e = -(cf.U2(i) * e1) - cf.U3(i) * e2;
+      s[i * ST] = TT(RS(s[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
     }
   }
   __syncwarp();
@@ -1360,8 +1373,9 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   const int lane = threadIdx.x;
   const int half = lane >> 4, li = lane & (kHalf - 1);
   TRACE(0)
-  if (error_pending(err)) return;
+  // the tile's task and the error flag load together (independent)
   const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
+  if (error_pending(err)) return;
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -1421,7 +1435,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   const CoefTable<RS> cf{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
   const RS* hb = lu + 5 * L;  // correction tables follow the factors
   const int LT = L + 8;
-  const SplitTab<RS> H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke};
+  const SplitTab<RS> H{hb, hb + LT, hb + 2 * LT, hb + 3 * LT, T.kg, T.ke, T.kf};
   const TT* recv = static_cast<const TT*>(T.recv);
   // interface sums received by the own end
   TT q0 = 0, q1 = 0, q2 = 0;
@@ -2063,9 +2077,11 @@ __global__ void k_flux(const BlockDev* __restrict__ bd, const StageParams* __res
 // 9-field round trip through memory. Same operations in the same order, so
 // the results are bit-identical to k_viscous_assemble followed by k_flux
 // (de(:,1) = ss(:,1) is read from ss directly).
+// FP32: at most 64 registers, so four 256-thread blocks (32 warps) keep
+// enough 128-byte requests in flight per SM
 template <class R>
-__global__ void k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
-                            const CaseConst* __restrict__ cc) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1)
+    k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp, const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
