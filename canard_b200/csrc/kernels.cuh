@@ -2078,9 +2078,9 @@ __global__ void k_flux(const BlockDev* __restrict__ bd, const StageParams* __res
 // the results are bit-identical to k_viscous_assemble followed by k_flux
 // (de(:,1) = ss(:,1) is read from ss directly).
 // FP32: at most 64 registers, so four 256-thread blocks (32 warps) keep
-// enough 128-byte requests in flight per SM
+// enough 128-byte requests in flight per SM; FP64: two blocks
 template <class R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp, const CaseConst* __restrict__ cc) {
   FOR_POINTS(bd[blockIdx.y]) {
     const Work<R> W = work<R>(B);

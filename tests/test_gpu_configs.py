@@ -15,7 +15,8 @@ the oracle's by an ulp) and the fast FP64 mode, <= 1e-5 for FP32-mixed.
   curved and straight interfaces and a sponge, 12 steps; FP32-mixed against
   FP64 after 200 steps on the device.
 * C4: the isentropic vortex through a GCBC outflow on a 96 x 64 x 32 copy,
-  50 steps.
+  after 50, 200 and 1000 steps; at the stated size FP32-mixed and the fast
+  mode against FP64 after 1000 steps.
 
 The oracle runs on every host thread; C2 takes it a couple of minutes.
 """
@@ -95,5 +96,37 @@ def test_c3_fp32_mixed_against_fp64_after_200_steps():
     assert max(max(e) for e in errs) <= 1e-5, errs
 
 
-def test_c4_vortex_small_copy_50_steps():
-    check(cases.vortex(96, 64, 32), 50, 0.5)
+def test_c4_vortex_small_copy_50_200_1000_steps():
+    """The C4 study's rows on a 96 x 64 x 32 copy: after 50, 200 and 1000
+    steps against the oracle (the vortex leaves through the outflow and its
+    sponge within them)."""
+    cs = cases.vortex(96, 64, 32)
+    o = po.Oracle(cs, threads=os.cpu_count() or 1)
+    gs = {name: api.Context(cs, precision=prec) for name, prec in
+          (("fp64", api.FP64), ("fast", api.FP64_FAST), ("fp32", api.FP32_MIXED))}
+    tol = {"fp64": 1e-10, "fast": 1e-10, "fp32": 1e-5}
+    done = 0
+    for n in (50, 200, 1000):
+        o.step(n - done)
+        ref = o.state(0)
+        for name, g in gs.items():
+            g.step(n - done)
+            e = errors(g.state(0), ref, 0.5)
+            print(cs.name, name, n, "steps", e)
+            assert max(e) <= tol[name], (name, n, e)
+        done = n
+    for g in gs.values():
+        g.close()
+
+
+def test_c4_fp32_mixed_against_fp64_after_1000_steps():
+    """The stated 384 x 256 x 128 case: FP32-mixed and the fast FP64 mode
+    against the bit-exact FP64 path after 1000 steps (the oracle would take
+    hours at this size; the FP64 path follows it to 1e-10)."""
+    cs = cases.vortex()
+    a = run_device(cs, 1000, api.FP64)
+    for prec, tol in ((api.FP32_MIXED, 1e-5), (api.FP64_FAST, 1e-10)):
+        b = run_device(cs, 1000, prec)
+        e = errors(b[0], a[0], 0.5)
+        print("C4 after 1000 steps against FP64, precision", prec, e)
+        assert np.isfinite(b[0]).all() and max(e) <= tol, e
