@@ -347,22 +347,25 @@ def kernels_mode(args, api, cases, torch):
     # fp32-stream: the mixed filter that streams the FP64 state into FP32
     # right-hand sides (an autotuner candidate), pinned for the comparison
     for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP64_FAST, "fp64-fast"),
-                       (api.FP32_MIXED, "fp32"), (api.FP32_MIXED, "fp32-stream")):
+                       (api.FP64_FAST, "fp64-quad"), (api.FP32_MIXED, "fp32"), (api.FP32_MIXED, "fp32-quad"),
+                       (api.FP32_MIXED, "fp32-stream")):
         ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
         for op in (0, 1):
-            if name == "fp32-stream" and op == 0:
+            if (name == "fp32-stream" and op == 0) or (name.endswith("quad") and op == 1):
                 continue
             for nn in (1, 2, 3):
                 if name == "fp64-tmem" and nn > 1:
                     ctx.set_line_kind("flux" if op == 0 else "filter", "xi eta zeta".split()[nn - 1], "fp64-tmem")
                 if name == "fp32-stream":
                     ctx.set_line_kind("filter", "xi eta zeta".split()[nn - 1], "fp64-stream/fp32-split")
+                if name.endswith("quad"):
+                    ctx.set_line_kind("flux", "xi eta zeta".split()[nn - 1], name)
                 # xi runs on the shared-memory tiles here too: the filter's interface calls
                 # advance the send chains of all directions in the oracle's order
                 out, ms = ctx.line_bench(op, nn, fields, reps=args.steps)
                 if name == "fp64-tmem" and nn == 1:
                     continue
-                es = 4 if (name.startswith("fp32") and op == 0) else 8
+                es = 4 if (name in ("fp32", "fp32-quad") and op == 0) else 8
                 gbs = 5 * blk.npts * 2 * es / (ms / 1e3) / 1e9
                 r = ref[(op, nn)]
                 err = float(np.linalg.norm((out - r).ravel()) / np.linalg.norm(r.ravel()))

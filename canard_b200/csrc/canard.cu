@@ -89,14 +89,33 @@ enum LineKind {
   LK_F64_TILE_F32_SOLVE_1L = 4,
   LK_F64_TM = 5,               // FP64, elimination results in TMEM (eta/zeta, 16 <= L <= 257)
   LK_F64_STREAM_F32 = 6,       // filter: FP64 field streamed into FP32 right-hand sides, split FP32 solve
-  LK_F64_SPLIT = 7             // FP64 fields, split FP64 solve with FMA (fast FP64 mode)
+  LK_F64_SPLIT = 7,            // FP64 fields, split FP64 solve with FMA (fast FP64 mode)
+  LK_F64_QUAD = 8,             // derivative: FP64 fields, four lanes per line, FP64 solve with FMA
+  LK_F32_QUAD = 9              // derivative: FP32 fields, four lanes per line
 };
-inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L; }
+inline bool kind_quad(int kind) { return kind == LK_F64_QUAD || kind == LK_F32_QUAD; }
+inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L || kind == LK_F32_QUAD; }
 inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
 inline int tile_lanes(int kind) {
+  if (kind_quad(kind)) return kQuad;
   return (kind == LK_F32 || kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_STREAM_F32 || kind == LK_F64_SPLIT)
              ? kHalf
              : kLanes;
+}
+
+// Segment boundaries of the quad split along a line of L points: four
+// segments of about L/4 rows, each at least the decay lengths kf, ke of the
+// homogeneous solutions plus two rows, so that the segments' end values are
+// final without a chain across segments. Returns false where L is too short.
+bool quad_rows(int L, int kf, int ke, int& q1, int& q2, int& q3) {
+  const int need = std::max(kf, ke) + 2;
+  q1 = (L + 2) / 4;
+  q2 = L / 2;
+  q3 = (3 * L) / 4;
+  const int len[4] = {q1, q2 - q1, q3 - q2, L - q3};
+  for (int k = 0; k < 4; ++k)
+    if (len[k] < std::max(need, 16)) return false;
+  return true;
 }
 
 // First row of the second half of a split solve: balances the two halves'
@@ -453,8 +472,8 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
   t.out = out;
-  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM || kind == LK_F64_SPLIT;
-  t.lu = kind == LK_F64_SPLIT ? static_cast<const void*>(B.lu64s[nt][dir])
+  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM || kind == LK_F64_SPLIT || kind == LK_F64_QUAD;
+  t.lu = (kind == LK_F64_SPLIT || kind == LK_F64_QUAD) ? static_cast<const void*>(B.lu64s[nt][dir])
          : f64solve          ? static_cast<const void*>(B.lu[nt][dir])
                              : static_cast<const void*>(B.lu32[nt][dir]);
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
@@ -471,13 +490,19 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.m = m;
   t.ndf0 = bc_interface(g.nbc[dir][0]) ? 1 : 0;
   t.ndf1 = bc_interface(g.nbc[dir][1]) ? 1 : 0;
-  t.h = t.kg = t.ke = t.kf = 0;
+  t.h = t.kg = t.ke = t.kf = t.q2 = t.q3 = 0;
   if (!f64solve) {  // FP32 elimination: rounded factors and their constant range
     t.cl1 = B.luc32[nt][dir][0]; t.cl2 = B.luc32[nt][dir][1]; t.cu1 = B.luc32[nt][dir][2];
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
     t.c0 = B.luc032[nt][dir];
   }
-  if (kind == LK_F64_SPLIT) {
+  if (kind_quad(kind)) {
+    const bool q64 = kind == LK_F64_QUAD;
+    t.kf = q64 ? B.kf64[nt][dir] : B.kf32[nt][dir];
+    t.ke = q64 ? B.ke64[nt][dir] : B.ke32[nt][dir];
+    if (!quad_rows(t.L, t.kf, t.ke, t.h, t.q2, t.q3))
+      throw ApiError(CANARD_ERR_ARG, "lines too short for the quad split solve");
+  } else if (kind == LK_F64_SPLIT) {
     t.h = B.h64[nt][dir];
     t.kg = B.kg64[nt][dir];
     t.ke = B.ke64[nt][dir];
@@ -492,6 +517,17 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   if (kind == LK_F64_TM) {  // 32-row boxes streamed through the ring
     t.by = kTmChunk;
     t.nbox = (t.L + kTmChunk - 1) / kTmChunk;
+  }
+  if (dir != 0) {
+    // every chunk's box starts 128-byte aligned in shared memory (a tensor
+    // copy's requirement): rows of lanes x element bytes, so FP32 tiles of
+    // 8 lanes (32-byte rows) take chunks of a multiple of 4 rows
+    const int rb = tile_lanes(kind) * (int)tile_elem(kind);
+    const int m = rb >= 128 ? 1 : 128 / rb;
+    if (t.by % m) {
+      t.by = (t.by + m - 1) / m * m;
+      t.nbox = (t.L + t.by - 1) / t.by;
+    }
   }
   const int lanes = tile_lanes(kind);
   if (dir == 0) {
@@ -687,6 +723,14 @@ void launch_line_tm_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
+template <int DIR, class TT, class RS>
+void launch_line4_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, T_DERIV_XI + DIR - 1, T.bytes);
+  launch_line4_t<DIR, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  CK(cudaGetLastError());
+}
+
 template <int DIR>
 void launch_filt2s_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
@@ -705,6 +749,8 @@ void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   else if (OP == 1 && T.kind == LK_F64_TILE_F32_SOLVE_1L) launch_line_dir<DIR, 1, double, float>(c, T);
   else if (OP == 1 && T.kind == LK_F64_STREAM_F32) launch_filt2s_dir<DIR>(c, T);
   else if (T.kind == LK_F64_SPLIT) launch_line2_dir<DIR, OP, double, double>(c, T);
+  else if (OP == 0 && T.kind == LK_F64_QUAD) launch_line4_dir<DIR, double, double>(c, T);
+  else if (OP == 0 && T.kind == LK_F32_QUAD) launch_line4_dir<DIR, float, float>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -759,6 +805,12 @@ void set_line_smem_limits() {
   CK((line2_smem_limit<1, 1, double, double>(lim)));
   CK((line2_smem_limit<2, 1, double, double>(lim)));
   CK((line2_smem_limit<3, 1, double, double>(lim)));
+  CK((line4_smem_limit<1, double, double>(lim)));
+  CK((line4_smem_limit<2, double, double>(lim)));
+  CK((line4_smem_limit<3, double, double>(lim)));
+  CK((line4_smem_limit<1, float, float>(lim)));
+  CK((line4_smem_limit<2, float, float>(lim)));
+  CK((line4_smem_limit<3, float, float>(lim)));
   CK((filt2s_smem_limit<1>(lim)));
   CK((filt2s_smem_limit<2>(lim)));
   CK((filt2s_smem_limit<3>(lim)));
@@ -1236,6 +1288,20 @@ bool tm_ok(const canard_ctx* c, int dir) {
   for (const auto& b : c->blocks) {
     const int L = b.g.ijk[0][dir] + 1;
     if (L < kTmMinL || L > kTmMaxL) return false;
+  }
+  return true;
+}
+
+// the quad split solve takes derivative lines long enough for its four
+// segments in every block (FP64 or FP32 decay lengths)
+bool quad_ok(const canard_ctx* c, int dir, int kind) {
+  if (c->blocks.empty()) return false;
+  for (const auto& b : c->blocks) {
+    const int L = b.g.ijk[0][dir] + 1;
+    const bool q64 = kind == LK_F64_QUAD;
+    const int kf = q64 ? b.kf64[0][dir] : b.kf32[0][dir], ke = q64 ? b.ke64[0][dir] : b.ke32[0][dir];
+    int q1, q2, q3;
+    if (!quad_rows(L, kf, ke, q1, q2, q3)) return false;
   }
   return true;
 }
@@ -2438,6 +2504,8 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         std::vector<std::pair<int, int>> cand;  // (kind, nc)
         std::vector<int> kinds{default_kind(c, grp, dir)};
         if (c->fast()) kinds.push_back(LK_F64);  // the one-lane FP64 sweeps compete in the fast mode
+        if (grp != 0 && c->fast() && quad_ok(c, dir, LK_F64_QUAD)) kinds.push_back(LK_F64_QUAD);
+        if (grp != 0 && c->f32() && quad_ok(c, dir, LK_F32_QUAD)) kinds.push_back(LK_F32_QUAD);
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
         if (c->f32() && grp == 0) kinds.push_back(LK_F64_STREAM_F32);
         else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
@@ -2482,17 +2550,18 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
 
 int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
   return guarded(c, [&] {
-    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_SPLIT || chunks < 0 ||
+    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F32_QUAD || chunks < 0 ||
         chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
       throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
     if (kind >= 0) {
       bool fits;
       if (!c->f32())
-        fits = kind == LK_F64 || kind == LK_F64_SPLIT || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0);
+        fits = kind == LK_F64 || kind == LK_F64_SPLIT || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0) ||
+               (kind == LK_F64_QUAD && group != 0 && quad_ok(c, dir, kind));
       else if (group == 0)
         fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64 ||
                kind == LK_F64_SPLIT || (kind == LK_F64_STREAM_F32 && chunks == 0);
-      else fits = kind == LK_F32 || kind == LK_F32_1L;
+      else fits = kind == LK_F32 || kind == LK_F32_1L || (kind == LK_F32_QUAD && quad_ok(c, dir, kind));
       if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
     }
     CK(cudaStreamSynchronize(c->st));

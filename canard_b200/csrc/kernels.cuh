@@ -97,6 +97,7 @@ struct LineTask {
   int selfp;               // derivative of a line periodic onto itself: contraction formed in the kernel
   int h, kg, ke;           // split solves: first row of the second half; homogeneous table lengths
   int kf;                  // split solves: rows the forward homogeneous solutions from h span
+  int q2, q3;              // quad split: first rows of the third and fourth segments (h: of the second)
   int tile0, ntiles, ntx;  // first global tile, tiles, x-tiles per row (dir 2/3)
   int nbox, by;            // chunks per tile and positions per chunk
 };
@@ -1477,12 +1478,24 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
       TT* col = s + li;
       const int lo = half == 0 ? 0 : h, hi = half == 0 ? h : L;
       int i = lo;
-      for (; i + 16 <= hi; i += 16) {
+      // two batches of 16 rows in flight: the next batch loads while the
+      // current one is added (the originals have usually left L2 by now)
+      if (i + 16 <= hi) {
         TT v[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+        for (; i + 32 <= hi; i += 16) {
+          TT w[16];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) w[k] = __ldg(g + (long long)(i + 16 + k) * pstride);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) col[(i + k) * kHalf] = v[k] + col[(i + k) * kHalf];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) v[k] = w[k];
+        }
 #pragma unroll
         for (int k = 0; k < 16; ++k) col[(i + k) * kHalf] = v[k] + col[(i + k) * kHalf];
+        i += 16;
       }
       for (; i < hi; ++i) col[i * kHalf] = __ldg(g + (long long)i * pstride) + col[i * kHalf];
     }
@@ -1514,6 +1527,290 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
     g_trace[(long long)blockIdx.x * 8 + 6] = smid;
   }
 #endif
+}
+
+// ---------------------------------------------------------------------------
+// Quad split derivative: 8 lines per warp, four lanes per line. Lane (seg =
+// lane / 8, li = lane % 8) owns rows [q_seg, q_seg+1) of line li (q_0 = 0,
+// q_4 = L; q_1..q_3 from the task). Every segment eliminates forward from its
+// own start (the first from its closure rows, the others from a zero start)
+// and substitutes backward from its own end (the last from the true end, the
+// others from a zero start). By linearity segment s then adds to its forward
+// values the homogeneous forward solution started from segment s-1's last two
+// forward values, and to its results the homogeneous backward solution
+// started from segment s+1's first two results, both as register recurrences
+// (as in the two-lane split solve). The host places the boundaries so that
+// every segment is longer than both solutions take to fall below the solve
+// type's rounding, so a segment's end values are final without a chain across
+// segments and the four segments correct at once.
+constexpr int kQuad = 8;
+
+template <int DIR, class TT, class RS>
+__global__ void __maxnreg__(168) k_line4(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
+                                              int ntasks, const CUtensorMap* __restrict__ maps,
+                                              int* __restrict__ err) {
+  constexpr int kVec = 16 / (int)sizeof(TT);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  TT* s = reinterpret_cast<TT*>(smem_raw + 128);
+  const int lane = threadIdx.x;
+  const int seg = lane >> 3, li = lane & (kQuad - 1);
+  const unsigned full = 0xffffffffu;
+  TRACE(0)
+  const int ti = __ldg(tile_task + blockIdx.x);
+  if (error_pending(err)) return;
+  const LineTask& T = tasks[ti];
+  const TT* in = static_cast<const TT*>(T.in);
+  TT* out = static_cast<TT*>(T.out);
+  const int lt = blockIdx.x - T.tile0;
+  const int L = T.L, N = L - 1;
+  const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
+  const int NC = T.nbox, CR = T.by;
+  int nval, x0 = 0, r0 = 0, fix = 0;
+  if (DIR == 1) {
+    r0 = lt * kQuad;
+    nval = min(kQuad, Y * Z - r0);
+  } else {
+    fix = lt / T.ntx;
+    x0 = (lt % T.ntx) * kQuad;
+    nval = min(kQuad, X - x0);
+  }
+  const int P = dir1_pitch<TT>(L);
+  const long long base = (DIR == 1) ? (long long)r0 * Xp
+                                    : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
+  const CUtensorMap* map_in = maps + 2 * ti;
+  const CUtensorMap* map_out = maps + 2 * ti + 1;
+  auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
+  if (lane == 0)
+    for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+  __syncwarp();
+  for (int c = 0; c < NC; ++c) {
+    if (DIR == 1) {
+      const uint32_t bytes = (uint32_t)((chunk_len(c) + kVec - 1) / kVec * kVec * sizeof(TT));
+      if (lane == 0) mbar_expect_tx(bars + c, bytes * nval);
+      __syncwarp();
+      if (lane < nval) bulk_g2s(s + lane * P + c * CR, in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
+    } else if (lane == 0) {
+      mbar_expect_tx(bars + c, (uint32_t)(CR * kQuad * sizeof(TT)));
+      if (DIR == 2) tma_load_3d(s + c * CR * kQuad, map_in, x0, c * CR, fix, bars + c);
+      else tma_load_3d(s + c * CR * kQuad, map_in, x0, fix, c * CR, bars + c);
+    }
+  }
+  TRACE(1)
+  bool ok = true;
+  for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
+  if (!ok) {
+    if (lane == 0) atomicExch(err, kErrTimeout);
+    return;
+  }
+  __syncwarp();
+  TRACE(2)
+  constexpr int ST = (DIR == 1) ? 1 : kQuad;
+  TT* sl = (DIR == 1) ? s + li * P : s + li;
+  const bool has = li < nval;
+  int jk = 0;
+  if (DIR == 1) jk = r0 + li;
+  else if (DIR == 2) jk = (x0 + li) * Z + fix;
+  else jk = fix * X + x0 + li;
+  const int nbs = T.nbs;
+  const RS* lu = static_cast<const RS*>(T.lu);
+  const CoefTable<RS> cf{lu, lu + L, lu + 2 * L, lu + 3 * L, lu + 4 * L};
+  const CoefConst<RS> cc{RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3)};
+  const int c0 = T.c0, c1 = L - 4;
+  const int q1 = T.h, q2 = T.q2, q3 = T.q3;
+  const int lo = seg == 0 ? 0 : (seg == 1 ? q1 : (seg == 2 ? q2 : q3));
+  const int hi = seg == 0 ? q1 : (seg == 1 ? q2 : (seg == 2 ? q3 : L));
+  const DevScheme* __restrict__ sc = T.sc;
+  const TT* recv = static_cast<const TT*>(T.recv);
+  // interface sums received by the own end (first and last segment)
+  TT q0v = 0, q1v = 0;
+  if (T.selfp) {
+    // periodic onto itself: the contraction the other end would send (see k_line)
+    if (seg == 0 || seg == 3) {
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const TT v = seg == 0 ? sl[(N - 1 - i) * ST] : sl[(1 + i) * ST];
+        q0v = q0v + TT(sc->pbco[0][0][i]) * v;
+        q1v = q1v + TT(sc->pbco[0][1][i]) * v;
+      }
+    }
+  } else if (has) {
+    if (seg == 0 && T.ndf0) { q0v = recv[jk]; q1v = recv[nbs + jk]; }
+    if (seg == 3 && T.ndf1) { q0v = recv[2 * nbs + jk]; q1v = recv[3 * nbs + jk]; }
+  }
+  // ---- reads of the original line, before any row is overwritten
+  TT b[2] = {0, 0};  // closure right-hand sides of the own end (last segment: bn, bn1)
+  TT x[2] = {0, 0};  // originals at hi, hi + 1 (the stencil of the own last two rows)
+  TT w0, w1, w2, w3;
+  if (seg == 0) {
+    if (T.ndf0 == 0) {
+      const TT s0 = sl[0], s1 = sl[ST], s2 = sl[2 * ST], s3 = sl[3 * ST], s4 = sl[4 * ST];
+      b[0] = ((TT(CA_A01) * (s1 - s0) + TT(CA_A02) * (s2 - s0)) + TT(CA_A03) * (s3 - s0)) + TT(CA_A04) * (s4 - s0);
+      b[1] = ((TT(CA_A10) * (s0 - s1) + TT(CA_A12) * (s2 - s1)) + TT(CA_A13) * (s3 - s1)) + TT(CA_A14) * (s4 - s1);
+    } else {
+      TT t0 = 0, t1 = 0;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const TT v = sl[i * ST];
+        t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+        t1 = t1 + TT(sc->pbci[0][1][i]) * v;
+      }
+      b[0] = t0 + q0v;
+      b[1] = t1 + q1v;
+    }
+    w0 = sl[0]; w1 = sl[ST]; w2 = sl[2 * ST]; w3 = sl[3 * ST];
+  } else {
+    if (seg == 3) {
+      if (T.ndf1 == 0) {
+        const TT e0 = sl[N * ST], e1 = sl[(N - 1) * ST], e2 = sl[(N - 2) * ST], e3 = sl[(N - 3) * ST],
+                 e4 = sl[(N - 4) * ST];
+        b[0] = ((TT(CA_A01) * (e0 - e1) + TT(CA_A02) * (e0 - e2)) + TT(CA_A03) * (e0 - e3)) + TT(CA_A04) * (e0 - e4);
+        b[1] = ((TT(CA_A10) * (e1 - e0) + TT(CA_A12) * (e1 - e2)) + TT(CA_A13) * (e1 - e3)) + TT(CA_A14) * (e1 - e4);
+      } else {
+        TT t0 = 0, t1 = 0;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const TT v = sl[(N - i) * ST];
+          t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+          t1 = t1 + TT(sc->pbci[0][1][i]) * v;
+        }
+        b[0] = -t0 - q0v;
+        b[1] = -t1 - q1v;
+      }
+    }
+    w0 = sl[(lo - 2) * ST]; w1 = sl[(lo - 1) * ST]; w2 = sl[lo * ST]; w3 = sl[(lo + 1) * ST];
+  }
+  if (seg != 3) {
+    x[0] = sl[hi * ST];
+    x[1] = sl[(hi + 1) * ST];
+  }
+  __syncwarp();
+  // ---- forward elimination: the first segment's closure rows, the interior
+  // rows of every segment, then its last two rows (right-hand sides from x or,
+  // in the last segment, the closures)
+  RS am2 = 0, am1 = 0;
+  if (seg == 0) {
+    am2 = RS(b[0]);
+    am1 = RS(b[1]) - cf.L2(1) * am2;
+    sl[0] = TT(am2);
+    sl[ST] = TT(am1);
+  }
+  const int fb = seg == 0 ? 2 : lo;
+  const int fe = seg == 3 ? N - 1 : hi - 2;
+  {
+    TT w4 = 0, w5 = 0;
+    fwd3<0, ST, TT, RS>(sl, fb, fe, c0, c1, cf, cc, TT(0), TT(0), TT(0), w0, w1, w2, w3, w4, w5, am2, am1);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int i = fe + k;
+    TT rhs;
+    {
+      const TT w4n = x[k];
+      rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4n - w0);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4n;
+    }
+    if (seg == 3) rhs = b[1 - k];
+    const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
+    sl[i * ST] = TT(a);
+    am2 = am1;
+    am1 = a;
+  }
+  // ---- the previous segment's last two forward values start each segment's
+  // homogeneous forward correction
+  const int srcp = (lane + 24) & 31, srcn = (lane + 8) & 31;
+  const RS A0 = __shfl_sync(full, am2, srcp), A1 = __shfl_sync(full, am1, srcp);
+  __syncwarp();
+  TRACE(3)
+  if (seg >= 1) {
+    RS g2 = A0, g1 = A1;
+    const int ie = min(lo + T.kf, hi);
+    int i = lo;
+    for (; i < min(ie, c0); ++i) {
+      const RS g = -(cf.L1(i) * g2) - cf.L2(i) * g1;
+      sl[i * ST] = TT(RS(sl[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
+#pragma unroll 4
+    for (; i < min(ie, c1 + 1); ++i) {
+      const RS g = -(cc.L1(i) * g2) - cc.L2(i) * g1;
+      sl[i * ST] = TT(RS(sl[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
+    for (; i < ie; ++i) {
+      const RS g = -(cf.L1(i) * g2) - cf.L2(i) * g1;
+      sl[i * ST] = TT(RS(sl[i * ST]) + g);
+      g2 = g1;
+      g1 = g;
+    }
+  }
+  __syncwarp();
+  // ---- back substitution: the last segment from the true end, the others
+  // from a zero start at their own end
+  RS cp1 = 0, cp2 = 0;
+  if (seg == 3) {
+    cp1 = cf.U1(N) * RS(sl[N * ST]);
+    sl[N * ST] = TT(cp1);
+    const RS c = cf.U1(N - 1) * RS(sl[(N - 1) * ST]) - cf.U2(N - 1) * cp1;
+    sl[(N - 1) * ST] = TT(c);
+    cp2 = cp1;
+    cp1 = c;
+  }
+  bwd3<ST, TT, RS>(sl, seg == 3 ? N - 2 : hi - 1, lo, c0, c1, cf, cc, cp1, cp2);
+  TRACE(4)
+  // ---- the next segment's first two results start each segment's
+  // homogeneous backward correction
+  const RS C0 = __shfl_sync(full, cp1, srcn), C1 = __shfl_sync(full, cp2, srcn);
+  __syncwarp();
+  if (seg <= 2) {
+    RS e1 = C0, e2 = C1;
+    const int ib = max(hi - T.ke, lo);
+    int i = hi - 1;
+    for (; i > c1 && i >= ib; --i) {
+      const RS e = -(cf.U2(i) * e1) - cf.U3(i) * e2;
+      sl[i * ST] = TT(RS(sl[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
+    }
+#pragma unroll 4
+    for (; i >= max(ib, c0); --i) {
+      const RS e = -(cc.U2(i) * e1) - cc.U3(i) * e2;
+      sl[i * ST] = TT(RS(sl[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
+    }
+    for (; i >= ib; --i) {
+      const RS e = -(cf.U2(i) * e1) - cf.U3(i) * e2;
+      sl[i * ST] = TT(RS(sl[i * ST]) + e);
+      e2 = e1;
+      e1 = e;
+    }
+  }
+  __syncwarp();
+  TRACE(5)
+  if (has && T.drva) {
+    TT* drva = static_cast<TT*>(T.drva);
+    if (seg == 0) drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+    if (seg == 3) drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[N * ST];
+  }
+  fence_proxy_async();
+  __syncwarp();
+  for (int c = 0; c < NC; ++c) {
+    const int clo = c * CR, len = chunk_len(c);
+    if (DIR == 1) {
+      if (lane < nval)
+        bulk_s2g(out + base + (long long)lane * Xp + clo, s + lane * P + clo,
+                 (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT)));
+    } else if (lane == 0) {
+      if (DIR == 2) tma_store_3d(map_out, x0, clo, fix, s + clo * kQuad);
+      else tma_store_3d(map_out, x0, fix, clo, s + clo * kQuad);
+    }
+  }
+  bulk_commit();
+  bulk_wait_read0();
+  TRACE(7)
 }
 
 // ---------------------------------------------------------------------------
@@ -2440,6 +2737,15 @@ template <int DIR, int OP, class TT, class RS = float>
 void launch_line2_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
                     const CUtensorMap* maps, int* err) {
   k_line2<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, class TT, class RS>
+void launch_line4_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
+                    const CUtensorMap* maps, int* err) {
+  k_line4<DIR, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, class TT, class RS>
+cudaError_t line4_smem_limit(int bytes) {
+  return cudaFuncSetAttribute(k_line4<DIR, TT, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 template <int DIR>
 void launch_filt2s_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt, int* err) {

@@ -66,6 +66,19 @@ CANARD_F64S_LINE(1, 1)
 CANARD_F64S_LINE(2, 1)
 CANARD_F64S_LINE(3, 1)
 #undef CANARD_F64S_LINE
+// quad split derivatives (four lanes per line): FP64 for the fast mode, FP32
+// for the mixed path
+#define CANARD_QUAD_LINE(DIR, TT)                                                                              \
+  CANARD_F32_EXTERN template void launch_line4_t<DIR, TT, TT>(int, size_t, cudaStream_t, const LineTask*,        \
+                                                              const int*, int, const CUtensorMap*, int*);       \
+  CANARD_F32_EXTERN template cudaError_t line4_smem_limit<DIR, TT, TT>(int);
+CANARD_QUAD_LINE(1, double)
+CANARD_QUAD_LINE(2, double)
+CANARD_QUAD_LINE(3, double)
+CANARD_QUAD_LINE(1, float)
+CANARD_QUAD_LINE(2, float)
+CANARD_QUAD_LINE(3, float)
+#undef CANARD_QUAD_LINE
 // one-lane sweeps with an FP32 elimination (the autotuner's alternative)
 #define CANARD_F32_LINE1(DIR, OP, TT)                                                                         \
   CANARD_F32_EXTERN template void launch_line_t<DIR, OP, TT, float>(int, size_t, cudaStream_t, const LineTask*, \

@@ -302,7 +302,10 @@ int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax)
  * results in tensor memory (eta/zeta, 16..257 points per line), 6 the filter
  * of the FP64 state streamed into FP32 right-hand sides (mixed precision), 7
  * FP64 split solve with FMA (FP64 and fast FP64 contexts; the fast mode's
- * default); -1 restores the precision's default. Kinds 0 and 5 give results
+ * default), 8 and 9 the derivative's quad split solve (four lanes per line) on
+ * FP64 fields (FP64 and fast FP64 contexts) and on FP32 fields (mixed
+ * precision), for lines of at least about 4 x 60 points (FP64) or 4 x 40
+ * (FP32); -1 restores the precision's default. Kinds 0 and 5 give results
  * bit-identical to the reference's operation order; kind 7 differs from them
  * at the rounding level. A kind
  * the context's precision or line lengths do not admit returns
