@@ -646,12 +646,9 @@ def main():
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for _ in range(args.e2e_steps):
-        for ci, bi, _, qn in hosts:
-            ctx.set_state(bi, qn, ci)
-        ctx.step(1)
-        for ci, bi, _, qn in hosts:
-            ctx.get_state_into(bi, qn, ci)
+    # every step: the state in from pinned host memory, the step, its result
+    # back out (canard_step_host pipelines the two directions in chunks)
+    ctx.step_host(args.e2e_steps, [h[3] for h in hosts], [(h[0], h[1]) for h in hosts])
     f1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0

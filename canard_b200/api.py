@@ -84,6 +84,8 @@ def lib():
         L.canard_get_field.argtypes = [vp, i32, i32, i32, _DP, ctypes.c_int64]
         L.canard_set_field.argtypes = [vp, i32, i32, i32, _DP, ctypes.c_int64]
         L.canard_step.argtypes = [vp, i32]
+        L.canard_step_host.argtypes = [vp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
         L.canard_phase.argtypes = [vp, i32, i32]
         L.canard_phase_with.argtypes = [vp, i32, i32, ctypes.c_double, _DP, _DP]
         L.canard_get_time.argtypes = [vp, i32, _DP]
@@ -453,6 +455,22 @@ class Context:
 
     def step(self, n=1):
         self._check(lib().canard_step(self.h, n))
+
+    def step_host(self, n, arrays, blocks=None):
+        """n steps through host memory: arrays[k] (float64, the reference
+        layout of block blocks[k] = (case, block), default (0, k)) is the
+        step's input before every step and receives its result after it; the
+        copies are pipelined in both directions (canard_step_host)."""
+        if blocks is None:
+            blocks = [(0, k) for k in range(len(arrays))]
+        for a in arrays:
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("host states must be C-contiguous float64 arrays")
+        nb = len(arrays)
+        ic = (ctypes.c_int32 * nb)(*[c for c, _ in blocks])
+        ib = (ctypes.c_int32 * nb)(*[b for _, b in blocks])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * nb)(*[_dp(a) for a in arrays])
+        self._check(lib().canard_step_host(self.h, n, nb, ic, ib, ptrs))
 
     def phase(self, ph, nk=0):
         self._check(lib().canard_phase(self.h, ph, nk))

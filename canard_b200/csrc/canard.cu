@@ -311,6 +311,10 @@ struct canard_ctx {
   long long graph_launches[2] = {0, 0};
   bool use_graphs = true;
   double* stage = nullptr;  // contiguous staging of host copies (reference layout)
+  // canard_step_host: staging of every listed block's state and the two copy streams
+  double* hs_stage = nullptr;
+  size_t hs_n = 0;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
   size_t stage_n = 0;
   int* derr = nullptr;
   bool setup_done = false;
@@ -1775,6 +1779,9 @@ void destroy(canard_ctx* c) {
     cudaFree(A->snap);
   }
   free_transient(c);
+  cudaFree(c->hs_stage);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->own) cudaStreamDestroy(c->own);
 }
 
@@ -2163,6 +2170,102 @@ int canard_step(canard_ctx* c, int32_t nsteps) {
     if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_step before canard_setup");
     if (nsteps < 0) throw ApiError(CANARD_ERR_ARG, "negative step count");
     for (int i = 0; i < nsteps; ++i) one_step(c);
+    sync_check(c);
+  });
+}
+
+// Steps through host memory, pipelined: each listed block's state is cut into
+// chunks of rows of the reference layout; a chunk of step n's result goes out
+// on s_out as soon as it is packed, and the same chunk of step n+1's input
+// (the caller's array, which the call owns meanwhile) goes back in on s_in
+// right after, so the two directions of the host link overlap. Same results
+// as nsteps x (set_state, step, get_state).
+int canard_step_host(canard_ctx* c, int32_t nsteps, int32_t nblocks, const int32_t* icase, const int32_t* iblock,
+                     double* const* host) {
+  return guarded(c, [&] {
+    if (!c->setup_done) throw ApiError(CANARD_ERR_STATE, "canard_step_host before canard_setup");
+    if (nsteps < 0 || nblocks < 1 || !icase || !iblock || !host) throw ApiError(CANARD_ERR_ARG, "bad argument");
+    std::vector<int> bs((size_t)nblocks);
+    std::vector<size_t> off((size_t)nblocks);
+    size_t tot = 0;
+    for (int k = 0; k < nblocks; ++k) {
+      if (!host[k]) throw ApiError(CANARD_ERR_ARG, "null host state");
+      bs[k] = block_index(c, icase[k], iblock[k]);
+      for (int q = 0; q < k; ++q)
+        if (bs[q] == bs[k]) throw ApiError(CANARD_ERR_ARG, "a block is listed twice");
+      off[k] = tot;
+      const BlockGeom& g = c->blocks[bs[k]].g;
+      tot += (size_t)5 * g.X * g.Y * g.Z;
+    }
+    if (nsteps == 0) return;
+    if (c->hs_n < tot) {
+      CK(cudaStreamSynchronize(c->st));
+      cudaFree(c->hs_stage);
+      c->hs_stage = nullptr;
+      c->hs_n = 0;
+      c->hs_stage = dalloc<double>(tot, c->st);
+      c->hs_n = tot;
+    }
+    if (!c->s_in) CK(cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+    if (!c->s_out) CK(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+    struct Chunk { int k; long long r0, r1; };
+    std::vector<Chunk> ch;
+    constexpr int kChunks = 16;
+    for (int k = 0; k < nblocks; ++k) {
+      const BlockGeom& g = c->blocks[bs[k]].g;
+      const long long rows = 5LL * g.Y * g.Z, per = (rows + kChunks - 1) / kChunks;
+      for (long long r0 = 0; r0 < rows; r0 += per) ch.push_back({k, r0, std::min(rows, r0 + per)});
+    }
+    const size_t nc = ch.size();
+    std::vector<cudaEvent_t> ev(3 * nc + 1, nullptr);
+    struct EvGuard {
+      std::vector<cudaEvent_t>& v;
+      ~EvGuard() {
+        for (auto e : v)
+          if (e) cudaEventDestroy(e);
+      }
+    } guard{ev};
+    for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaEvent_t* ev_in = ev.data();
+    cudaEvent_t* ev_pack = ev.data() + nc;
+    cudaEvent_t* ev_out = ev.data() + 2 * nc;
+    auto grid_for = [](long long n) { return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16)); };
+    for (int st = 0; st < nsteps; ++st) {
+      for (size_t j = 0; j < nc; ++j) {
+        const Chunk& q = ch[j];
+        BlockState& B = c->blocks[bs[q.k]];
+        const BlockGeom& g = B.g;
+        double* sg = c->hs_stage + off[q.k] + q.r0 * g.X;
+        const long long nr = q.r1 - q.r0;
+        // the chunk's previous result has left the staging and landed in the host array
+        if (st > 0) CK(cudaStreamWaitEvent(c->s_in, ev_out[j], 0));
+        CK(cudaMemcpyAsync(sg, host[q.k] + q.r0 * g.X, (size_t)nr * g.X * sizeof(double), cudaMemcpyHostToDevice,
+                           c->s_in));
+        CK(cudaEventRecord(ev_in[j], c->s_in));
+        CK(cudaStreamWaitEvent(c->st, ev_in[j], 0));
+        k_rows_repack<<<grid_for(nr * g.X), 256, 0, c->st>>>(sg, g.X, fptr(B, F_QA) + q.r0 * g.Xp, g.Xp, g.X, nr);
+        CK(cudaGetLastError());
+      }
+      one_step(c);
+      for (size_t j = 0; j < nc; ++j) {
+        const Chunk& q = ch[j];
+        BlockState& B = c->blocks[bs[q.k]];
+        const BlockGeom& g = B.g;
+        double* sg = c->hs_stage + off[q.k] + q.r0 * g.X;
+        const long long nr = q.r1 - q.r0;
+        k_rows_repack<<<grid_for(nr * g.X), 256, 0, c->st>>>(fptr(B, F_QA) + q.r0 * g.Xp, g.Xp, sg, g.X, g.X, nr);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev_pack[j], c->st));
+        CK(cudaStreamWaitEvent(c->s_out, ev_pack[j], 0));
+        CK(cudaMemcpyAsync(host[q.k] + q.r0 * g.X, sg, (size_t)nr * g.X * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->s_out));
+        CK(cudaEventRecord(ev_out[j], c->s_out));
+      }
+    }
+    // the context's stream ends after the last copy out
+    CK(cudaEventRecord(ev[3 * nc], c->s_out));
+    CK(cudaStreamWaitEvent(c->st, ev[3 * nc], 0));
+    c->launches += 2LL * (long long)nc * nsteps;
     sync_check(c);
   });
 }

@@ -150,6 +150,19 @@ int canard_set_field(canard_ctx* ctx, int32_t icase, int32_t iblock, int32_t fie
  * time6 = (n, ndt, dt, dts, dte, timo) of one case. */
 int canard_step(canard_ctx* ctx, int32_t nsteps);
 int canard_phase(canard_ctx* ctx, int32_t phase, int32_t nk);
+/* nsteps time steps through host memory (no counterpart in the reference; a
+ * driver that keeps the state on the host between steps, e.g. for a coupled
+ * host-side code): before every step the state of each listed block (case
+ * icase[k], block iblock[k]) is read from host[k], reference layout (0:lmx,5)
+ * (pinned memory reaches the full link bandwidth), and after it the step's
+ * result is written back to host[k]. The same as nsteps x (canard_set_state,
+ * canard_step(1), canard_get_state), but the copies are pipelined: each block's
+ * state moves in chunks on two streams of the context, and a chunk of one
+ * step's result goes back in as the next step's input as soon as it has landed,
+ * so both directions of the host link run at once. The arrays belong to the
+ * call until it returns. */
+int canard_step_host(canard_ctx* ctx, int32_t nsteps, int32_t nblocks, const int32_t* icase,
+                     const int32_t* iblock, double* const* host);
 /* The fluxes, GCBC, RK update or wall phase of stage nk with the stage's
  * scalars given by the caller, as the reference's routines receive them
  * (calc_fluxes reads this%umf, src/mo_physics.f90:319-321; gcbc_update takes

@@ -127,6 +127,14 @@ module mo_canard_gpu
          type(c_ptr), value :: ctx
          integer(c_int32_t), value :: nsteps
       end function
+      integer(c_int) function canard_step_host(ctx, nsteps, nblocks, icase, iblock, host) &
+            bind(C, name="canard_step_host")
+         import
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: nsteps, nblocks
+         integer(c_int32_t), intent(in) :: icase(*), iblock(*)
+         type(c_ptr), intent(in) :: host(*)          ! c_loc of each listed block's qa(0:lmx,5)
+      end function
       integer(c_int) function canard_phase(ctx, phase, nk) bind(C, name="canard_phase")
          import
          type(c_ptr), value :: ctx
