@@ -72,6 +72,10 @@ def parse():
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the line-tile autotuner (by default every timed context is tuned first; the "
                         "per-case baseline of the batched comparison never is)")
+    p.add_argument("--tune-file", default="",
+                   help="line-kernel choices of the timed context: read from this JSON file when it exists "
+                        "(no autotuning), else autotuned and written to it, so that a second run (a profiler's "
+                        "launch list, for one) launches the same kernels")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the FP32-mixed and batched comparison lines added to the default run")
     return p.parse_args()
@@ -109,6 +113,25 @@ def time_steps(ctx, steps, stream, torch):
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b)
+
+
+def tune_context(ctx, args):
+    """The timed context's line kernels: autotuned (the default), read from
+    --tune-file when that exists, or none (--no-autotune)."""
+    if args.no_autotune:
+        return None
+    if args.tune_file and os.path.exists(args.tune_file):
+        with open(args.tune_file) as f:
+            tuning = json.load(f)
+        for t in tuning:
+            ch = t["chunks"] if isinstance(t["chunks"], int) else 0
+            ctx.set_line_kind(t["group"], t["dir"], t["kind"], ch)
+        return tuning
+    tuning = ctx.autotune(reps=3)
+    if args.tune_file:
+        with open(args.tune_file, "w") as f:
+            json.dump(tuning, f)
+    return tuning
 
 
 def precision_extra(args, api, cases, torch, stream, prec):
@@ -348,7 +371,7 @@ def kernels_mode(args, api, cases, torch):
     # right-hand sides (an autotuner candidate), pinned for the comparison
     for prec, name in ((api.FP64, "fp64"), (api.FP64, "fp64-tmem"), (api.FP64_FAST, "fp64-fast"),
                        (api.FP64_FAST, "fp64-quad"), (api.FP32_MIXED, "fp32"), (api.FP32_MIXED, "fp32-quad"),
-                       (api.FP32_MIXED, "fp32-stream")):
+                       (api.FP32_MIXED, "fp32-stream"), (api.FP64_FAST, "fp64-twist"), (api.FP32_MIXED, "fp32-twist")):
         ctx = api.Context(cs, precision=prec, setup=False, upload_state=False)
         for op in (0, 1):
             if (name == "fp32-stream" and op == 0) or (name.endswith("quad") and op == 1):
@@ -360,12 +383,15 @@ def kernels_mode(args, api, cases, torch):
                     ctx.set_line_kind("filter", "xi eta zeta".split()[nn - 1], "fp64-stream/fp32-split")
                 if name.endswith("quad"):
                     ctx.set_line_kind("flux", "xi eta zeta".split()[nn - 1], name)
+                if name.endswith("twist"):  # two-ended solve (two warps per 32 lines)
+                    kt = name if (op == 0 or name == "fp64-twist") else "fp64-tile/fp32-twist"
+                    ctx.set_line_kind("flux" if op == 0 else "filter", "xi eta zeta".split()[nn - 1], kt)
                 # xi runs on the shared-memory tiles here too: the filter's interface calls
                 # advance the send chains of all directions in the oracle's order
                 out, ms = ctx.line_bench(op, nn, fields, reps=args.steps)
                 if name == "fp64-tmem" and nn == 1:
                     continue
-                es = 4 if (name in ("fp32", "fp32-quad") and op == 0) else 8
+                es = 4 if (name in ("fp32", "fp32-quad", "fp32-twist") and op == 0) else 8
                 gbs = 5 * blk.npts * 2 * es / (ms / 1e3) / 1e9
                 r = ref[(op, nn)]
                 err = float(np.linalg.norm((out - r).ravel()) / np.linalg.norm(r.ravel()))
@@ -553,7 +579,7 @@ def main():
     case_list, all_cases, workload = workload_cases(args, cases, world, rank)
     prec = {"fp32": api.FP32_MIXED, "fast": api.FP64_FAST}.get(args.precision, api.FP64)
     ctx = api.Context(case_list, precision=prec)
-    tuning = None if args.no_autotune else ctx.autotune(reps=3)
+    tuning = tune_context(ctx, args)
     # a non-default stream: the library launches on it and the CUDA events
     # below are recorded on it (handle 0 would mean the context's own stream)
     stream = torch.cuda.Stream()
@@ -640,6 +666,9 @@ def main():
             qh = torch.empty((5,) + b.shape, dtype=torch.float64, pin_memory=True)
             qh.copy_(torch.from_numpy(ctx.state(bi, ci)))
             hosts.append((ci, bi, qh, qh.numpy()))
+    # one untimed step through the same call: its first use sets up the
+    # staging buffer and copy streams
+    ctx.step_host(1, [h[3] for h in hosts], [(h[0], h[1]) for h in hosts])
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()

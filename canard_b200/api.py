@@ -384,7 +384,7 @@ class Context:
             self._check(-k)
         kinds = {0: "fp64", 1: "fp32-split", 2: "fp64-tile/fp32-split", 3: "fp32-one-lane",
                  4: "fp64-tile/fp32-one-lane", 5: "fp64-tmem", 6: "fp64-stream/fp32-split", 7: "fp64-split",
-                 8: "fp64-quad", 9: "fp32-quad"}
+                 8: "fp64-quad", 9: "fp32-quad", 10: "fp64-twist", 11: "fp32-twist", 12: "fp64-tile/fp32-twist"}
         out = []
         for i in range(k):
             g, d, kd, nc, best, dflt = rep[6 * i:6 * i + 6]
@@ -395,7 +395,7 @@ class Context:
 
     LINE_KINDS = {"default": -1, "fp64": 0, "fp32-split": 1, "fp64-tile/fp32-split": 2, "fp32-one-lane": 3,
                   "fp64-tile/fp32-one-lane": 4, "fp64-tmem": 5, "fp64-stream/fp32-split": 6, "fp64-split": 7,
-                  "fp64-quad": 8, "fp32-quad": 9}
+                  "fp64-quad": 8, "fp32-quad": 9, "fp64-twist": 10, "fp32-twist": 11, "fp64-tile/fp32-twist": 12}
 
     def set_line_kind(self, group, direction, kind, chunks=0):
         """Pins the line kernel of a group ("filter", "viscous", "flux") and

@@ -91,10 +91,18 @@ enum LineKind {
   LK_F64_STREAM_F32 = 6,       // filter: FP64 field streamed into FP32 right-hand sides, split FP32 solve
   LK_F64_SPLIT = 7,            // FP64 fields, split FP64 solve with FMA (fast FP64 mode)
   LK_F64_QUAD = 8,             // derivative: FP64 fields, four lanes per line, FP64 solve with FMA
-  LK_F32_QUAD = 9              // derivative: FP32 fields, four lanes per line
+  LK_F32_QUAD = 9,             // derivative: FP32 fields, four lanes per line
+  LK_F64_TWIST = 10,           // FP64 fields, two-ended FP64 solve with FMA (two warps per 32 lines)
+  LK_F32_TWIST = 11,           // derivative: FP32 fields, two-ended FP32 solve
+  LK_F64_TILE_F32_TWIST = 12   // filter: FP64 field, two-ended FP32 solve
 };
 inline bool kind_quad(int kind) { return kind == LK_F64_QUAD || kind == LK_F32_QUAD; }
-inline bool kind_f32_fields(int kind) { return kind == LK_F32 || kind == LK_F32_1L || kind == LK_F32_QUAD; }
+inline bool kind_twist(int kind) {
+  return kind == LK_F64_TWIST || kind == LK_F32_TWIST || kind == LK_F64_TILE_F32_TWIST;
+}
+inline bool kind_f32_fields(int kind) {
+  return kind == LK_F32 || kind == LK_F32_1L || kind == LK_F32_QUAD || kind == LK_F32_TWIST;
+}
 inline size_t tile_elem(int kind) { return kind_f32_fields(kind) ? sizeof(float) : sizeof(double); }
 inline int tile_lanes(int kind) {
   if (kind_quad(kind)) return kQuad;
@@ -207,6 +215,81 @@ void split_tables(const std::vector<double>& lu, int L, int h, double thr, std::
   for (int j = 0; j < ke; ++j) { out[2 * LT + j] = (T)E0[j]; out[3 * LT + j] = (T)E1[j]; }
 }
 
+// First row of the reversed half of a two-ended solve: the middle of the line.
+int twist_row(int L) { return L / 2; }
+// the two-ended solve needs halves of at least 16 rows
+constexpr int kTwistMinL = 32;
+
+// First row of the range [c0, L-4] over which a factor table's five factors
+// are bit-identical to those of row L-4 (as T), and those factors.
+template <class T>
+int constant_rows(const std::vector<T>& lu, int L, T* cst) {
+  const int e = L - 4;
+  if (e < 0) return L - 3;
+  auto same = [&](int r) {
+    for (int k = 0; k < 5; ++k)
+      if (std::memcmp(&lu[(size_t)k * L + r], &lu[(size_t)k * L + e], sizeof(T)) != 0) return false;
+    return true;
+  };
+  int c0 = e;
+  while (c0 - 1 >= 3 && same(c0 - 1)) --c0;
+  for (int k = 0; k < 5; ++k) cst[k] = lu[(size_t)k * L + e];
+  return c0;
+}
+
+// Factor table of the two-ended solve (k_line2t), as T: the line's factors
+// (5 L, from lu), the reversed line's (the system with its ends swapped,
+// U1 negated for the derivative, whose right-hand sides change sign on the
+// reversed line), the 4 x 4 inverse of the meeting equations times the U1
+// factors of their rows, and the reversed factors' constant interior values.
+// Returns the first row of that constant range (reversed rows), or -1 where
+// the meeting equations are singular.
+template <class T>
+int twist_tables(const Scheme& sch, const std::vector<double>& lu, int L, int n0, int n1, int nt, int h,
+                 std::vector<T>& out) {
+  std::vector<double> rl((size_t)5 * L);
+  sch.lu(L, n1, n0, nt, rl.data());
+  if (nt == 0)
+    for (int i = 0; i < L; ++i) rl[(size_t)2 * L + i] = -rl[(size_t)2 * L + i];
+  const int N = L - 1;
+  auto U1 = [&](const std::vector<double>& f, int i) { return f[(size_t)2 * L + i]; };
+  auto U2 = [&](const std::vector<double>& f, int i) { return f[(size_t)3 * L + i]; };
+  auto U3 = [&](const std::vector<double>& f, int i) { return f[(size_t)4 * L + i]; };
+  // unknowns x(h-2), x(h-1), x(h), x(h+1): rows h-2, h-1 of U, and rows N-h,
+  // N-h-1 of the reversed U (the rows of x(h), x(h+1))
+  double M[4][8] = {{1, U2(lu, h - 2), U3(lu, h - 2), 0},
+                    {0, 1, U2(lu, h - 1), U3(lu, h - 1)},
+                    {U3(rl, N - h), U2(rl, N - h), 1, 0},
+                    {0, U3(rl, N - h - 1), U2(rl, N - h - 1), 1}};
+  const double D[4] = {U1(lu, h - 2), U1(lu, h - 1), U1(rl, N - h), U1(rl, N - h - 1)};
+  for (int r = 0; r < 4; ++r)
+    for (int k = 0; k < 4; ++k) M[r][4 + k] = r == k ? 1.0 : 0.0;
+  for (int col = 0; col < 4; ++col) {  // Gauss-Jordan with partial pivoting
+    int p = col;
+    for (int r = col + 1; r < 4; ++r)
+      if (std::fabs(M[r][col]) > std::fabs(M[p][col])) p = r;
+    if (std::fabs(M[p][col]) < 1e-12) return -1;  // not for this system (the kind is then unavailable)
+    if (p != col)
+      for (int k = 0; k < 8; ++k) std::swap(M[p][k], M[col][k]);
+    const double inv = 1.0 / M[col][col];
+    for (int k = 0; k < 8; ++k) M[col][k] *= inv;
+    for (int r = 0; r < 4; ++r)
+      if (r != col) {
+        const double f = M[r][col];
+        for (int k = 0; k < 8; ++k) M[r][k] -= f * M[col][k];
+      }
+  }
+  out.assign(lu.begin(), lu.end());
+  out.insert(out.end(), rl.begin(), rl.end());
+  for (int r = 0; r < 4; ++r)
+    for (int k = 0; k < 4; ++k) out.push_back((T)(M[r][4 + k] * D[k]));
+  std::vector<T> rt(rl.begin(), rl.end());
+  T cst[5];
+  const int c0 = constant_rows(rt, L, cst);
+  for (int k = 0; k < 5; ++k) out.push_back(cst[k]);
+  return c0;
+}
+
 struct CaseState {
   canard_case_desc d;
   Scheme sch;
@@ -252,6 +335,12 @@ struct BlockState {
   // the fast FP64 mode's line kind, also a filter candidate of the mixed path
   double* lu64s[2][3] = {};
   int h64[2][3] = {}, kg64[2][3] = {}, ke64[2][3] = {}, kf64[2][3] = {};
+  // two-ended solves: factor tables (twist_tables) in FP64 and FP32, the first
+  // row of the reversed half (0: unavailable for this system) and the first
+  // row of the reversed factors' constant range
+  double* lu64t[2][3] = {};
+  float* lu32t[2][3] = {};
+  int ht[2][3] = {}, c0r64[2][3] = {}, c0r32[2][3] = {};
   double* recv_ptr(int nt, int dir, int m, int side) const {
     const int nc = nt == 0 ? 2 : 3;
     return recv[nt][dir] + ((size_t)(m - 1) * 2 + side) * nc * g.nbs[dir];
@@ -476,10 +565,13 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
   t.selfp = (allow_selfp && nt == 0 && self_periodic(g, dir)) ? 1 : 0;
   t.in = in;
   t.out = out;
-  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM || kind == LK_F64_SPLIT || kind == LK_F64_QUAD;
+  const bool f64solve = kind == LK_F64 || kind == LK_F64_TM || kind == LK_F64_SPLIT || kind == LK_F64_QUAD ||
+                        kind == LK_F64_TWIST;
   t.lu = (kind == LK_F64_SPLIT || kind == LK_F64_QUAD) ? static_cast<const void*>(B.lu64s[nt][dir])
-         : f64solve          ? static_cast<const void*>(B.lu[nt][dir])
-                             : static_cast<const void*>(B.lu32[nt][dir]);
+         : kind == LK_F64_TWIST                        ? static_cast<const void*>(B.lu64t[nt][dir])
+         : kind_twist(kind)                            ? static_cast<const void*>(B.lu32t[nt][dir])
+         : f64solve                                    ? static_cast<const void*>(B.lu[nt][dir])
+                                                       : static_cast<const void*>(B.lu32[nt][dir]);
   t.cl1 = B.luc[nt][dir][0]; t.cl2 = B.luc[nt][dir][1]; t.cu1 = B.luc[nt][dir][2];
   t.cu2 = B.luc[nt][dir][3]; t.cu3 = B.luc[nt][dir][4];
   t.c0 = B.luc0[nt][dir];
@@ -500,7 +592,11 @@ void fill_line_task(const canard_ctx* c, const BlockState& B, int dir /*0..2*/, 
     t.cu2 = B.luc32[nt][dir][3]; t.cu3 = B.luc32[nt][dir][4];
     t.c0 = B.luc032[nt][dir];
   }
-  if (kind_quad(kind)) {
+  if (kind_twist(kind)) {
+    if (!B.ht[nt][dir] || !t.lu) throw ApiError(CANARD_ERR_ARG, "lines too short for the two-ended solve");
+    t.h = B.ht[nt][dir];
+    t.kg = kind == LK_F64_TWIST ? B.c0r64[nt][dir] : B.c0r32[nt][dir];
+  } else if (kind_quad(kind)) {
     const bool q64 = kind == LK_F64_QUAD;
     t.kf = q64 ? B.kf64[nt][dir] : B.kf32[nt][dir];
     t.ke = q64 ? B.ke64[nt][dir] : B.ke32[nt][dir];
@@ -727,6 +823,14 @@ void launch_line_tm_dir(canard_ctx* c, const Table<LineTask>& T) {
   CK(cudaGetLastError());
 }
 
+template <int DIR, int OP, class TT, class RS>
+void launch_line2t_dir(canard_ctx* c, const Table<LineTask>& T) {
+  if (T.ntasks == 0 || T.total == 0) return;
+  Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
+  launch_line2t_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  CK(cudaGetLastError());
+}
+
 template <int DIR, class TT, class RS>
 void launch_line4_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
@@ -755,6 +859,9 @@ void launch_line_kind(canard_ctx* c, const Table<LineTask>& T) {
   else if (T.kind == LK_F64_SPLIT) launch_line2_dir<DIR, OP, double, double>(c, T);
   else if (OP == 0 && T.kind == LK_F64_QUAD) launch_line4_dir<DIR, double, double>(c, T);
   else if (OP == 0 && T.kind == LK_F32_QUAD) launch_line4_dir<DIR, float, float>(c, T);
+  else if (T.kind == LK_F64_TWIST) launch_line2t_dir<DIR, OP, double, double>(c, T);
+  else if (OP == 0 && T.kind == LK_F32_TWIST) launch_line2t_dir<DIR, 0, float, float>(c, T);
+  else if (OP == 1 && T.kind == LK_F64_TILE_F32_TWIST) launch_line2t_dir<DIR, 1, double, float>(c, T);
   else throw ApiError(CANARD_ERR_ARG, "line table of an unsupported element type");
 }
 
@@ -809,6 +916,18 @@ void set_line_smem_limits() {
   CK((line2_smem_limit<1, 1, double, double>(lim)));
   CK((line2_smem_limit<2, 1, double, double>(lim)));
   CK((line2_smem_limit<3, 1, double, double>(lim)));
+  CK((line2t_smem_limit<1, 0, double, double>(lim)));
+  CK((line2t_smem_limit<2, 0, double, double>(lim)));
+  CK((line2t_smem_limit<3, 0, double, double>(lim)));
+  CK((line2t_smem_limit<1, 1, double, double>(lim)));
+  CK((line2t_smem_limit<2, 1, double, double>(lim)));
+  CK((line2t_smem_limit<3, 1, double, double>(lim)));
+  CK((line2t_smem_limit<1, 0, float, float>(lim)));
+  CK((line2t_smem_limit<2, 0, float, float>(lim)));
+  CK((line2t_smem_limit<3, 0, float, float>(lim)));
+  CK((line2t_smem_limit<1, 1, double, float>(lim)));
+  CK((line2t_smem_limit<2, 1, double, float>(lim)));
+  CK((line2t_smem_limit<3, 1, double, float>(lim)));
   CK((line4_smem_limit<1, double, double>(lim)));
   CK((line4_smem_limit<2, double, double>(lim)));
   CK((line4_smem_limit<3, double, double>(lim)));
@@ -1310,10 +1429,26 @@ bool quad_ok(const canard_ctx* c, int dir, int kind) {
   return true;
 }
 
+// the two-ended solve has its tables for direction dir in every block (lines
+// of at least kTwistMinL points; FP32 tables in mixed-precision contexts)
+bool twist_ok(const canard_ctx* c, int dir, int kind) {
+  if (c->blocks.empty()) return false;
+  for (const auto& b : c->blocks)
+    for (int nt = 0; nt < 2; ++nt) {
+      if (!b.ht[nt][dir]) return false;
+      if (kind != LK_F64_TWIST && !b.lu32t[nt][dir]) return false;
+    }
+  return true;
+}
+
+// Defaults without autotuning: the filter's two-ended solve where the lines
+// admit it (measured 15-18 % faster than the split and one-lane filters at
+// 257 points), the split solve for the derivatives of the fast and mixed modes
 int default_kind(const canard_ctx* c, int grp, int dir) {
-  if (c->fast()) return LK_F64_SPLIT;
+  if (c->fast()) return (grp == 0 && twist_ok(c, dir, LK_F64_TWIST)) ? LK_F64_TWIST : LK_F64_SPLIT;
   if (!c->f32()) return LK_F64;
-  return grp == 0 ? LK_F64_TILE_F32_SOLVE : LK_F32;
+  if (grp == 0) return twist_ok(c, dir, LK_F64_TILE_F32_TWIST) ? LK_F64_TILE_F32_TWIST : LK_F64_TILE_F32_SOLVE;
+  return LK_F32;
 }
 
 int group_kind(const canard_ctx* c, int grp, int dir) {
@@ -1750,7 +1885,12 @@ void destroy(canard_ctx* c) {
     for (int d = 0; d < 3; ++d) { cudaFree(b.chain[d]); cudaFree(b.drva[d]); cudaFree(b.drvb[d]); cudaFree(b.cm[d]); }
     cudaFree(b.arena32);
     for (int nt = 0; nt < 2; ++nt)
-      for (int d = 0; d < 3; ++d) { cudaFree(b.lu32[nt][d]); cudaFree(b.lu64s[nt][d]); }
+      for (int d = 0; d < 3; ++d) {
+        cudaFree(b.lu32[nt][d]);
+        cudaFree(b.lu64s[nt][d]);
+        cudaFree(b.lu64t[nt][d]);
+        cudaFree(b.lu32t[nt][d]);
+      }
     for (int d = 0; d < 3; ++d) { cudaFree(b.recv32[d]); cudaFree(b.drva32[d]); cudaFree(b.drvb32[d]); }
     cudaFree(b.gc_pts); cudaFree(b.gc_w); cudaFree(b.sp_pts); cudaFree(b.sp_a); cudaFree(b.sp_b);
   }
@@ -1901,6 +2041,23 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
           B.h64[nt][dir] = h;
           lus.insert(lus.end(), hom.begin(), hom.end());
           B.lu64s[nt][dir] = dupload(lus, c->st);
+        }
+        if (L >= kTwistMinL) {  // the two-ended solve's tables
+          const int h = twist_row(L);
+          std::vector<double> t64;
+          const int r64 = twist_tables(sch, lu, L, n0, n1, nt, h, t64);
+          int r32 = -1;
+          std::vector<float> t32;
+          if (r64 >= 0 && c->f32()) r32 = twist_tables(sch, lu, L, n0, n1, nt, h, t32);
+          if (r64 >= 0 && (!c->f32() || r32 >= 0)) {
+            B.ht[nt][dir] = h;
+            B.c0r64[nt][dir] = r64;
+            B.lu64t[nt][dir] = dupload(t64, c->st);
+            if (c->f32()) {
+              B.c0r32[nt][dir] = r32;
+              B.lu32t[nt][dir] = dupload(t32, c->st);
+            }
+          }
         }
         B.recv[nt][dir] = dalloc<double>((size_t)5 * 2 * (nt == 0 ? 2 : 3) * nbs, c->st);
       }
@@ -2606,17 +2763,32 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
         const int op = grp == 0 ? 1 : 0;
         std::vector<std::pair<int, int>> cand;  // (kind, nc)
         std::vector<int> kinds{default_kind(c, grp, dir)};
-        if (c->fast()) kinds.push_back(LK_F64);  // the one-lane FP64 sweeps compete in the fast mode
+        if (c->fast()) {  // the one-lane and split FP64 sweeps compete in the fast mode
+          kinds.push_back(LK_F64);
+          kinds.push_back(LK_F64_SPLIT);
+        }
         if (grp != 0 && c->fast() && quad_ok(c, dir, LK_F64_QUAD)) kinds.push_back(LK_F64_QUAD);
         if (grp != 0 && c->f32() && quad_ok(c, dir, LK_F32_QUAD)) kinds.push_back(LK_F32_QUAD);
         if (c->f32()) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_SOLVE_1L : LK_F32_1L);
-        if (c->f32() && grp == 0) kinds.push_back(LK_F64_STREAM_F32);
-        else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
+        if (c->fast() && twist_ok(c, dir, LK_F64_TWIST)) kinds.push_back(LK_F64_TWIST);
+        if (c->f32() && twist_ok(c, dir, LK_F32_TWIST)) kinds.push_back(grp == 0 ? LK_F64_TILE_F32_TWIST : LK_F32_TWIST);
+        // the streamed filter reads a row of 32 lines per step: coalesced along
+        // eta/zeta only (along xi each lane's row is a line length away)
+        if (c->f32() && grp == 0) {
+          if (dir != 0) kinds.push_back(LK_F64_STREAM_F32);
+        } else if (tm_ok(c, dir)) kinds.push_back(LK_F64_TM);
         // the filter acts on the FP64 state with an FP64 right-hand side in every
         // kind; the FP64 eliminations (one-lane and split) compete with the FP32 ones there
         if (c->f32() && grp == 0) {
           kinds.push_back(LK_F64);
           kinds.push_back(LK_F64_SPLIT);
+          if (twist_ok(c, dir, LK_F64_TWIST)) kinds.push_back(LK_F64_TWIST);
+        }
+        {  // each kind once, the default first
+          std::vector<int> u;
+          for (int k : kinds)
+            if (std::find(u.begin(), u.end(), k) == u.end()) u.push_back(k);
+          kinds.swap(u);
         }
         for (int k : kinds) {
           cand.push_back({k, 0});
@@ -2653,18 +2825,22 @@ int canard_autotune(canard_ctx* c, int32_t reps, double* report, int32_t nmax) {
 
 int canard_set_line_kind(canard_ctx* c, int32_t group, int32_t dir, int32_t kind, int32_t chunks) {
   return guarded(c, [&] {
-    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F32_QUAD || chunks < 0 ||
+    if (group < 0 || group > 2 || dir < 0 || dir > 2 || kind < -1 || kind > LK_F64_TILE_F32_TWIST || chunks < 0 ||
         chunks == 1 || chunks > kMaxChunks || (dir == 0 && chunks != 0))
       throw ApiError(CANARD_ERR_ARG, "bad line kind argument");
     if (kind >= 0) {
       bool fits;
       if (!c->f32())
         fits = kind == LK_F64 || kind == LK_F64_SPLIT || (kind == LK_F64_TM && tm_ok(c, dir) && chunks == 0) ||
-               (kind == LK_F64_QUAD && group != 0 && quad_ok(c, dir, kind));
+               (kind == LK_F64_QUAD && group != 0 && quad_ok(c, dir, kind)) ||
+               (kind == LK_F64_TWIST && twist_ok(c, dir, kind));
       else if (group == 0)
         fits = kind == LK_F64_TILE_F32_SOLVE || kind == LK_F64_TILE_F32_SOLVE_1L || kind == LK_F64 ||
-               kind == LK_F64_SPLIT || (kind == LK_F64_STREAM_F32 && chunks == 0);
-      else fits = kind == LK_F32 || kind == LK_F32_1L || (kind == LK_F32_QUAD && quad_ok(c, dir, kind));
+               kind == LK_F64_SPLIT || (kind == LK_F64_STREAM_F32 && chunks == 0) ||
+               ((kind == LK_F64_TWIST || kind == LK_F64_TILE_F32_TWIST) && twist_ok(c, dir, kind));
+      else
+        fits = kind == LK_F32 || kind == LK_F32_1L || (kind == LK_F32_QUAD && quad_ok(c, dir, kind)) ||
+               (kind == LK_F32_TWIST && twist_ok(c, dir, kind));
       if (!fits) throw ApiError(CANARD_ERR_ARG, "line kind not available for this precision or line length");
     }
     CK(cudaStreamSynchronize(c->st));

@@ -1530,6 +1530,333 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
 }
 
 // ---------------------------------------------------------------------------
+// Two-ended ("twisted") line solve: two warps per tile of 32 lines, one lane
+// per line in each. Warp 0 runs the LU elimination of the line from row 0 to
+// row h-1. Warp 1 runs the LU elimination of the reversed line (the system
+// with its two ends swapped, factored by the host the same way) from row L-1
+// to row h. The first rows of U are rows of U of the whole system, so the
+// last two forward values of each warp give four equations in x(h-2..h+1),
+// which a 4 x 4 inverse from the host solves; each warp then substitutes back
+// towards its own end. Exact up to rounding: no homogeneous corrections, and
+// each chain is half a line long. Warp 1 works on a reversed view of its
+// lines (negative row stride from row L-1), on which the derivative's
+// right-hand sides change sign; its U1 factors carry that sign.
+
+// Reads of the original line (view rows 0..11 for the closures of the own
+// end, rows hw..hw+2 next to the half), made before either warp writes.
+template <class TT>
+struct TwState {
+  TT b[3];  // closure right-hand sides of the own end
+  TT w[6];  // the window s[0..5] that the forward sweep starts with
+  TT x[3];  // originals at view rows hw, hw+1, hw+2 (the other half's first rows)
+};
+
+template <int OP, int ST, class TT>
+__device__ __forceinline__ void twist_read(const TT* __restrict__ s, int hw, int ndf,
+                                           const DevScheme* __restrict__ sc, TT q0, TT q1, TT q2, TwState<TT>& t) {
+  const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
+  auto fbc = [&](int r, int k) { return TT(sc->fbc[r][k]); };
+  t.b[2] = 0;
+  t.x[2] = 0;
+  t.w[4] = t.w[5] = 0;
+  if (OP == 0) {
+    if (ndf == 0) {
+      const TT s0 = s[0], s1 = s[ST], s2 = s[2 * ST], s3 = s[3 * ST], s4 = s[4 * ST];
+      t.b[0] = ((TT(CA_A01) * (s1 - s0) + TT(CA_A02) * (s2 - s0)) + TT(CA_A03) * (s3 - s0)) + TT(CA_A04) * (s4 - s0);
+      t.b[1] = ((TT(CA_A10) * (s0 - s1) + TT(CA_A12) * (s2 - s1)) + TT(CA_A13) * (s3 - s1)) + TT(CA_A14) * (s4 - s1);
+    } else {
+      TT t0 = 0, t1 = 0;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const TT v = s[i * ST];
+        t0 = t0 + TT(sc->pbci[0][0][i]) * v;
+        t1 = t1 + TT(sc->pbci[0][1][i]) * v;
+      }
+      t.b[0] = t0 + q0;
+      t.b[1] = t1 + q1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t.w[k] = s[k * ST];
+  } else {
+    const TT s0 = s[0], s1 = s[ST], s2 = s[2 * ST], s3 = s[3 * ST], s4 = s[4 * ST], s5 = s[5 * ST];
+    if (ndf == 0) {
+      t.b[0] = (((fbc(0, 0) * (s1 - s0) + fbc(0, 1) * (s2 - s0)) + fbc(0, 2) * (s3 - s0)) + fbc(0, 3) * (s4 - s0)) +
+               fbc(0, 4) * (s5 - s0);
+      t.b[1] = (((fbc(1, 0) * (s0 - s1) + fbc(1, 1) * (s2 - s1)) + fbc(1, 2) * (s3 - s1)) + fbc(1, 3) * (s4 - s1)) +
+               fbc(1, 4) * (s5 - s1);
+      t.b[2] = (((fbc(2, 0) * (s0 - s2) + fbc(2, 1) * (s1 - s2)) + fbc(2, 2) * (s3 - s2)) + fbc(2, 3) * (s4 - s2)) +
+               fbc(2, 4) * (s5 - s2);
+    } else {
+      TT t0 = 0, t1 = 0;
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const TT v = s[i * ST];
+        t0 = t0 + TT(sc->pbci[1][0][i]) * v;
+        t1 = t1 + TT(sc->pbci[1][1][i]) * v;
+      }
+      const TT ra2 = s2 + s2;
+      t.b[0] = t0 + q0;
+      t.b[1] = t1 + q1;
+      t.b[2] = (fa * ((s1 + s3) - ra2) + fb * ((s0 + s4) - ra2)) + fc * ((q2 + s5) - ra2);
+    }
+    t.w[0] = s0; t.w[1] = s1; t.w[2] = s2; t.w[3] = s3; t.w[4] = s4; t.w[5] = s5;
+    t.x[2] = s[(hw + 2) * ST];
+  }
+  t.x[0] = s[hw * ST];
+  t.x[1] = s[(hw + 1) * ST];
+}
+
+// Forward elimination of view rows 0..hw-1: the closure rows, the interior
+// (three segments, as fwd3), then the last NE rows, whose look-ahead rows
+// belong to the other half and come from the values read before.
+template <int OP, int ST, class TT, class RS>
+__device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, const CoefTable<RS>& cf,
+                                          const CoefConst<RS>& cc, int c0, const DevScheme* __restrict__ sc,
+                                          const TwState<TT>& t) {
+  constexpr int NE = OP == 0 ? 2 : 3;
+  const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
+  TT w0 = t.w[0], w1 = t.w[1], w2 = t.w[2], w3 = t.w[3], w4 = t.w[4], w5 = t.w[5];
+  RS am2 = RS(t.b[0]);
+  RS am1 = RS(t.b[1]) - cf.L2(1) * am2;
+  s[0] = TT(am2);
+  s[ST] = TT(am1);
+  if (OP == 1) {
+    const RS a2 = (RS(t.b[2]) - cf.L1(2) * am2) - cf.L2(2) * am1;
+    s[2 * ST] = TT(a2);
+    am2 = am1;
+    am1 = a2;
+  }
+  fwd3<OP, ST, TT, RS>(s, NE, hw - NE, c0, L - 4, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const int i = hw - NE + k;
+    TT rhs;
+    if (OP == 0) {
+      const TT w4n = t.x[k];
+      rhs = TT(CA_AA) * (w3 - w1) + TT(CA_AB) * (w4n - w0);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4n;
+    } else {
+      const TT w6 = t.x[k];
+      const TT rk = w3 + w3;
+      rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    }
+    const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
+    s[i * ST] = TT(a);
+    am2 = am1;
+    am1 = a;
+  }
+}
+
+// Factor table of a twisted solve: the LU factors of the line (5 L), those of
+// the reversed line (5 L, U1 negated for the derivative), the 4 x 4 inverse
+// of the meeting equations with the U1 factors of their rows folded in (row
+// k gives x(h-2+k) from the forward values at rows h-2, h-1, h, h+1), and the
+// reversed system's bitwise-constant interior factors (5).
+constexpr int kTwistExtra = 16 + 5;
+
+// One CTA = two warps = 32 lines. DIR: 1 xi, 2 eta, 3 zeta. OP: 0
+// derivative, 1 filter (in place). TT: field and tile type; RS: elimination
+// type. T.h: first row of the reversed half; T.kg: first row of the reversed
+// system's constant factor range.
+template <int DIR, int OP, class TT, class RS>
+__global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
+                                               int ntasks, const CUtensorMap* __restrict__ maps,
+                                               int* __restrict__ err) {
+  static_assert(OP == 0 || sizeof(TT) == 8, "the filter acts on FP64 fields (reduce-add stores)");
+  constexpr int kVec = 16 / (int)sizeof(TT);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  TT* s = reinterpret_cast<TT*>(smem_raw + 128);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool rev = warp == 1;
+  TRACE(0)
+  const int ti = __ldg(tile_task + blockIdx.x);
+  // one decision for both warps (they meet at CTA barriers below)
+  if (__syncthreads_or(error_pending(err))) return;
+  const LineTask& T = tasks[ti];
+  const TT* in = static_cast<const TT*>(T.in);
+  TT* out = static_cast<TT*>(T.out);
+  const int lt = blockIdx.x - T.tile0;
+  const int L = T.L, h = T.h, N = L - 1;
+  const int X = T.X, Y = T.Y, Z = T.Z, Xp = T.Xp;
+  const int NC = T.nbox, CR = T.by;
+  int nval, x0 = 0, r0 = 0, fix = 0;
+  if (DIR == 1) {
+    r0 = lt * kLanes;
+    nval = min(kLanes, Y * Z - r0);
+  } else {
+    fix = lt / T.ntx;
+    x0 = (lt % T.ntx) * kLanes;
+    nval = min(kLanes, X - x0);
+  }
+  const int P = dir1_pitch<TT>(L);
+  const long long pstride = (DIR == 2) ? (long long)Xp : (long long)Xp * Y;
+  const long long base = (DIR == 1) ? (long long)r0 * Xp
+                                    : ((DIR == 2) ? (long long)fix * Y * Xp + x0 : (long long)fix * Xp + x0);
+  const CUtensorMap* map_in = maps + 2 * ti;
+  const CUtensorMap* map_out = maps + 2 * ti + 1;
+  auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
+  if (threadIdx.x == 0)
+    for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+  __syncthreads();
+  if (!rev) {
+    for (int c = 0; c < NC; ++c) {
+      if (DIR == 1) {
+        const uint32_t bytes = (uint32_t)((chunk_len(c) + kVec - 1) / kVec * kVec * sizeof(TT));
+        if (lane == 0) mbar_expect_tx(bars + c, bytes * nval);
+        __syncwarp();
+        if (lane < nval)
+          bulk_g2s(s + lane * P + c * CR, in + base + (long long)lane * Xp + c * CR, bytes, bars + c);
+      } else if (lane == 0) {
+        mbar_expect_tx(bars + c, (uint32_t)(CR * kLanes * sizeof(TT)));
+        if (DIR == 2) tma_load_3d(s + c * CR * kLanes, map_in, x0, c * CR, fix, bars + c);
+        else tma_load_3d(s + c * CR * kLanes, map_in, x0, fix, c * CR, bars + c);
+      }
+    }
+  }
+  TRACE(1)
+  bool ok = true;
+  for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(err, kErrTimeout);
+    return;
+  }
+  TRACE(2)
+  constexpr int ST = (DIR == 1) ? 1 : kLanes;
+  TT* sl = (DIR == 1) ? s + lane * P : s + lane;
+  TT* sv = rev ? sl + N * ST : sl;  // the warp's view of its line (warp 1: reversed)
+  const bool has = lane < nval;
+  int jk = 0;
+  if (DIR == 1) jk = r0 + lane;
+  else if (DIR == 2) jk = (x0 + lane) * Z + fix;
+  else jk = fix * X + x0 + lane;
+  const int nbs = T.nbs;
+  const RS* lu = static_cast<const RS*>(T.lu);
+  const RS* tb = rev ? lu + 5 * L : lu;
+  const RS* Wt = lu + 10 * L;
+  const CoefTable<RS> cf{tb, tb + L, tb + 2 * L, tb + 3 * L, tb + 4 * L};
+  const CoefConst<RS> cc = rev ? CoefConst<RS>{__ldg(Wt + 16), __ldg(Wt + 17), __ldg(Wt + 18), __ldg(Wt + 19),
+                                               __ldg(Wt + 20)}
+                               : CoefConst<RS>{RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3)};
+  const int c0 = rev ? T.kg : T.c0;
+  const int hw = rev ? L - h : h;  // rows of the warp's half
+  const TT* recv = static_cast<const TT*>(T.recv);
+  // interface sums received by the warp's own end
+  TT q0 = 0, q1 = 0, q2 = 0;
+  if (OP == 0 && T.selfp) {
+    // periodic onto itself: the contraction the other end would send (see k_line)
+    const DevScheme* sc = T.sc;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const TT v = !rev ? sl[(N - 1 - i) * ST] : sl[(1 + i) * ST];
+      q0 = q0 + TT(sc->pbco[0][0][i]) * v;
+      q1 = q1 + TT(sc->pbco[0][1][i]) * v;
+    }
+  } else if (has) {
+    const int nc = OP == 0 ? 2 : 3;
+    if (!rev && T.ndf0) {
+      q0 = recv[jk]; q1 = recv[nbs + jk];
+      if (OP == 1) q2 = recv[2 * nbs + jk];
+    }
+    if (rev && T.ndf1) {
+      q0 = recv[nc * nbs + jk]; q1 = recv[(nc + 1) * nbs + jk];
+      if (OP == 1) q2 = recv[(nc + 2) * nbs + jk];
+    }
+  }
+  TwState<TT> tw;
+  if (!rev) twist_read<OP, ST, TT>(sv, hw, T.ndf0, T.sc, q0, q1, q2, tw);
+  else twist_read<OP, -ST, TT>(sv, hw, T.ndf1, T.sc, q0, q1, q2, tw);
+  __syncthreads();
+  if (!rev) twist_fwd<OP, ST, TT, RS>(sv, L, hw, cf, cc, c0, T.sc, tw);
+  else twist_fwd<OP, -ST, TT, RS>(sv, L, hw, cf, cc, c0, T.sc, tw);
+  __syncthreads();
+  TRACE(3)
+  // the four meeting unknowns; warp 0 keeps x(h-2), x(h-1), warp 1 x(h), x(h+1)
+  RS xa, xb;
+  {
+    const RS y0 = RS(sl[(h - 2) * ST]), y1 = RS(sl[(h - 1) * ST]), z0 = RS(sl[h * ST]), z1 = RS(sl[(h + 1) * ST]);
+    const RS* w = Wt + (rev ? 8 : 0);
+    xa = ((__ldg(w + 0) * y0 + __ldg(w + 1) * y1) + __ldg(w + 2) * z0) + __ldg(w + 3) * z1;
+    xb = ((__ldg(w + 4) * y0 + __ldg(w + 5) * y1) + __ldg(w + 6) * z0) + __ldg(w + 7) * z1;
+  }
+  __syncthreads();
+  if (!rev) {
+    sv[(hw - 2) * ST] = TT(xa);
+    sv[(hw - 1) * ST] = TT(xb);
+    RS cp1 = xa, cp2 = xb;
+    bwd3<ST, TT, RS>(sv, hw - 3, 0, c0, L - 4, cf, cc, cp1, cp2);
+  } else {
+    sv[(hw - 1) * -ST] = TT(xa);
+    sv[(hw - 2) * -ST] = TT(xb);
+    RS cp1 = xb, cp2 = xa;
+    bwd3<-ST, TT, RS>(sv, hw - 3, 0, c0, L - 4, cf, cc, cp1, cp2);
+  }
+  TRACE(4)
+  if (OP == 0 && has && T.drva) {
+    TT* drva = static_cast<TT*>(T.drva);
+    if (!rev) drva[jk + (long long)nbs * (T.m - 1)] = sl[0];
+    else drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[N * ST];
+  }
+  // filter (in place on FP64 fields): along xi the tile keeps the increment,
+  // added to the field by one bulk FP64 reduce-add per line; along eta/zeta
+  // each warp adds the originals to its half of the 32 columns (coalesced
+  // rows), then the chunks are stored
+  if (OP == 1 && DIR != 1 && has) {
+    const TT* g = in + base + lane;
+    TT* col = s + lane;
+    const int lo = !rev ? 0 : h, hi = !rev ? h : L;
+    int i = lo;
+    if (i + 16 <= hi) {
+      TT v[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = __ldg(g + (long long)(i + k) * pstride);
+      for (; i + 32 <= hi; i += 16) {
+        TT w[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) w[k] = __ldg(g + (long long)(i + 16 + k) * pstride);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = w[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) col[(i + k) * kLanes] = v[k] + col[(i + k) * kLanes];
+      i += 16;
+    }
+    for (; i < hi; ++i) col[i * kLanes] = __ldg(g + (long long)i * pstride) + col[i * kLanes];
+  }
+  if (OP == 1 && DIR == 1 && (L & 1) && !rev) s[lane * P + L] = TT(0);  // the 16-byte tail's pad adds 0
+  fence_proxy_async();
+  __syncthreads();
+  TRACE(5)
+  if (rev) return;
+  for (int c = 0; c < NC; ++c) {
+    const int lo = c * CR, len = chunk_len(c);
+    if (DIR == 1) {
+      if (lane < nval) {
+        const uint32_t nb = (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT));
+        if (OP == 1) bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
+        else bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
+      }
+    } else if (lane == 0) {
+      if (DIR == 2) tma_store_3d(map_out, x0, lo, fix, s + lo * kLanes);
+      else tma_store_3d(map_out, x0, fix, lo, s + lo * kLanes);
+    }
+  }
+  bulk_commit();
+  bulk_wait_read0();
+  TRACE(7)
+#ifdef CANARD_TRACE
+  if (threadIdx.x == 0) {
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    g_trace[(long long)blockIdx.x * 8 + 6] = smid;
+  }
+#endif
+}
+
+// ---------------------------------------------------------------------------
 // Quad split derivative: 8 lines per warp, four lanes per line. Lane (seg =
 // lane / 8, li = lane % 8) owns rows [q_seg, q_seg+1) of line li (q_0 = 0,
 // q_4 = L; q_1..q_3 from the task). Every segment eliminates forward from its
@@ -2737,6 +3064,15 @@ template <int DIR, int OP, class TT, class RS = float>
 void launch_line2_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
                     const CUtensorMap* maps, int* err) {
   k_line2<DIR, OP, TT, RS><<<grid, kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, int OP, class TT, class RS>
+void launch_line2t_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,
+                     const CUtensorMap* maps, int* err) {
+  k_line2t<DIR, OP, TT, RS><<<grid, 2 * kLanes, smem, st>>>(t, f, nt, maps, err);
+}
+template <int DIR, int OP, class TT, class RS>
+cudaError_t line2t_smem_limit(int bytes) {
+  return cudaFuncSetAttribute(k_line2t<DIR, OP, TT, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 template <int DIR, class TT, class RS>
 void launch_line4_t(int grid, size_t smem, cudaStream_t st, const LineTask* t, const int* f, int nt,

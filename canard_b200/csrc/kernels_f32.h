@@ -66,6 +66,25 @@ CANARD_F64S_LINE(1, 1)
 CANARD_F64S_LINE(2, 1)
 CANARD_F64S_LINE(3, 1)
 #undef CANARD_F64S_LINE
+// two-ended solves (two warps per 32 lines): FP64 with FMA for the fast
+// mode, FP32 derivatives and FP32 filter eliminations for the mixed path
+#define CANARD_TWIST_LINE(DIR, OP, TT, RS)                                                                     \
+  CANARD_F32_EXTERN template void launch_line2t_t<DIR, OP, TT, RS>(int, size_t, cudaStream_t, const LineTask*, \
+                                                                   const int*, int, const CUtensorMap*, int*); \
+  CANARD_F32_EXTERN template cudaError_t line2t_smem_limit<DIR, OP, TT, RS>(int);
+CANARD_TWIST_LINE(1, 0, double, double)
+CANARD_TWIST_LINE(2, 0, double, double)
+CANARD_TWIST_LINE(3, 0, double, double)
+CANARD_TWIST_LINE(1, 1, double, double)
+CANARD_TWIST_LINE(2, 1, double, double)
+CANARD_TWIST_LINE(3, 1, double, double)
+CANARD_TWIST_LINE(1, 0, float, float)
+CANARD_TWIST_LINE(2, 0, float, float)
+CANARD_TWIST_LINE(3, 0, float, float)
+CANARD_TWIST_LINE(1, 1, double, float)
+CANARD_TWIST_LINE(2, 1, double, float)
+CANARD_TWIST_LINE(3, 1, double, float)
+#undef CANARD_TWIST_LINE
 // quad split derivatives (four lanes per line): FP64 for the fast mode, FP32
 // for the mixed path
 #define CANARD_QUAD_LINE(DIR, TT)                                                                              \

@@ -300,7 +300,8 @@ int canard_line_bench(canard_ctx* ctx, int32_t op, int32_t nn, int32_t nfields, 
  * lines per tile), and for the filter, which filters the FP64 state with an
  * FP64 right-hand side in every kind, the FP64 eliminations (one-lane and
  * split) as well; fast FP64 contexts try the split FP64 solve against the
- * one-lane FP64 sweeps. The
+ * one-lane FP64 sweeps. Where every block's lines along the direction have at
+ * least 32 points, the two-ended solves (kinds 10-12) compete too. The
  * fastest choice is installed in the step tables. Returns the number of groups
  * (9) and fills up to nmax report rows of 6 doubles: group, direction
  * (0..2), chosen kind, chosen chunk count (0 = default), its ms per launch
@@ -318,9 +319,15 @@ int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax)
  * default), 8 and 9 the derivative's quad split solve (four lanes per line) on
  * FP64 fields (FP64 and fast FP64 contexts) and on FP32 fields (mixed
  * precision), for lines of at least about 4 x 60 points (FP64) or 4 x 40
- * (FP32); -1 restores the precision's default. Kinds 0 and 5 give results
- * bit-identical to the reference's operation order; kind 7 differs from them
- * at the rounding level. A kind
+ * (FP32); 10, 11 and 12 the two-ended solve (two warps per tile of 32 lines,
+ * one eliminating from each end of the line, the four unknowns where they
+ * meet from a 4 x 4 inverse; lines of at least 32 points) with FP64 fields and
+ * elimination (FP64 and fast FP64 contexts, and the filter of mixed-precision
+ * ones), FP32 fields (derivatives, mixed precision) and the FP64 state with an
+ * FP32 elimination (filter, mixed precision); -1 restores the precision's
+ * default. Kinds 0 and 5 give results bit-identical to the reference's
+ * operation order; kinds 7, 8 and 10 differ from them at the rounding level.
+ * A kind
  * the context's precision or line lengths do not admit returns
  * CANARD_ERR_ARG. Before canard_setup the choice only applies to
  * canard_line_bench (the step tables are built by canard_setup). */

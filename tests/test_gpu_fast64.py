@@ -1,9 +1,10 @@
 """The fast FP64 mode (CANARD_FP64_FAST) against the FP64 oracle.
 
 A fast FP64 context keeps every value in FP64 but solves each compact line in
-two halves (two lanes per line, the halves joined by tabulated homogeneous
-solutions), with FMA contraction in the eliminations, and filters the five
-fields direction by direction. Its results therefore differ from the
+two halves: the derivatives with two lanes per line, the halves joined by the
+homogeneous solutions, and the filter (on lines of at least 32 points) with the
+two-ended solve, one warp eliminating from each end; both with FMA contraction
+in the eliminations. It filters the five fields direction by direction. Its results therefore differ from the
 reference's operation order at the rounding level only. The bound its steps
 are held to is the specification's: relative L2 error <= 1e-10 per conserved
 variable after 10-12 steps (momenta against ||rho|| * U_ref where that exceeds
