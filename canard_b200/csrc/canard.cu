@@ -650,6 +650,11 @@ size_t line_smem(int dir, const LineTask& t, int kind) {
     return (size_t)kHalf * (dir == 0 ? dir1_pitch<float>(t.L) : t.L) * sizeof(float);
   const size_t es = tile_elem(kind);
   const int lanes = tile_lanes(kind);
+  if (kind_twist(kind)) {  // the tile, then both warps' staged closure factors
+    const size_t rs = kind == LK_F64_TWIST ? sizeof(double) : sizeof(float);
+    const int P = kind_f32_fields(kind) ? dir1_pitch<float>(t.L) : dir1_pitch<double>(t.L);
+    return 128 + twist_tile_bytes(dir, t.L, t.nbox, t.by, es, P) + (size_t)2 * 5 * kTwistSh * rs;
+  }
   if (dir == 0)
     return 128 + (size_t)lanes * (kind_f32_fields(kind) ? dir1_pitch<float>(t.L) : dir1_pitch<double>(t.L)) * es;
   return 128 + (size_t)t.nbox * t.by * lanes * es;

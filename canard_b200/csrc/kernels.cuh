@@ -314,6 +314,21 @@ struct CoefTable {
   __device__ __forceinline__ RS U3(int i) const { return __ldg(u3 + i); }
 };
 
+// per-row factors staged in shared memory (the two-ended solve's closure rows)
+template <class RS>
+struct CoefShared {
+  const RS* l1;
+  const RS* l2;
+  const RS* u1;
+  const RS* u2;
+  const RS* u3;
+  __device__ __forceinline__ RS L1(int i) const { return l1[i]; }
+  __device__ __forceinline__ RS L2(int i) const { return l2[i]; }
+  __device__ __forceinline__ RS U1(int i) const { return u1[i]; }
+  __device__ __forceinline__ RS U2(int i) const { return u2[i]; }
+  __device__ __forceinline__ RS U3(int i) const { return u3[i]; }
+};
+
 // Rows are processed in blocks of eight: the block's inputs, right-hand sides
 // and factors are all formed before its dependent chain, so their latency
 // overlaps the chain. Every row is still evaluated with the reference's
@@ -1542,6 +1557,40 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
 // lines (negative row stride from row L-1), on which the derivative's
 // right-hand sides change sign; its U1 factors carry that sign.
 
+// Rows [ib, ie) in four per-lane segments: shared-memory factors below
+// k0 = min(ks, c0), table factors on [k0, c0), the register constants on
+// [c0, c1], table factors above c1.
+template <int OP, int ST, class TT, class RS>
+__device__ __forceinline__ void fwd4(TT* s, int ib, int ie, int ks, int c0, int c1, const CoefShared<RS>& sh,
+                                     const CoefTable<RS>& ct, const CoefConst<RS>& cc, TT fa, TT fb, TT fc, TT& w0,
+                                     TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+  const int k0 = min(ks, c0);
+  const int a1 = min(ie, k0), b0 = max(ib, k0), b1 = min(ie, c0), m0 = max(ib, c0), m1 = min(ie, c1 + 1),
+            d0 = max(ib, c1 + 1);
+  if (OP == 0) {
+    fwd_rows_deriv<ST, TT, RS>(s, ib, a1, sh, w0, w1, w2, w3, am2, am1);
+    fwd_rows_deriv<ST, TT, RS>(s, b0, b1, ct, w0, w1, w2, w3, am2, am1);
+    fwd_rows_deriv<ST, TT, RS>(s, m0, m1, cc, w0, w1, w2, w3, am2, am1);
+    fwd_rows_deriv<ST, TT, RS>(s, d0, ie, ct, w0, w1, w2, w3, am2, am1);
+  } else {
+    fwd_rows_filter<ST, TT, RS>(s, ib, a1, sh, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS>(s, b0, b1, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS>(s, m0, m1, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS>(s, d0, ie, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  }
+}
+
+// rows ihi down to ilo in the same four segments
+template <int ST, class TT, class RS>
+__device__ __forceinline__ void bwd4(TT* s, int ihi, int ilo, int ks, int c0, int c1, const CoefShared<RS>& sh,
+                                     const CoefTable<RS>& ct, const CoefConst<RS>& cc, RS& cp1, RS& cp2) {
+  const int k0 = min(ks, c0);
+  bwd_rows<ST, TT, RS>(s, ihi, max(ilo, c1 + 1), ct, cp1, cp2);
+  bwd_rows<ST, TT, RS>(s, min(ihi, c1), max(ilo, c0), cc, cp1, cp2);
+  bwd_rows<ST, TT, RS>(s, min(ihi, c0 - 1), max(ilo, k0), ct, cp1, cp2);
+  bwd_rows<ST, TT, RS>(s, min(ihi, k0 - 1), ilo, sh, cp1, cp2);
+}
+
 // Reads of the original line (view rows 0..11 for the closures of the own
 // end, rows hw..hw+2 next to the half), made before either warp writes.
 template <class TT>
@@ -1610,9 +1659,9 @@ __device__ __forceinline__ void twist_read(const TT* __restrict__ s, int hw, int
 // (three segments, as fwd3), then the last NE rows, whose look-ahead rows
 // belong to the other half and come from the values read before.
 template <int OP, int ST, class TT, class RS>
-__device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, const CoefTable<RS>& cf,
-                                          const CoefConst<RS>& cc, int c0, const DevScheme* __restrict__ sc,
-                                          const TwState<TT>& t) {
+__device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, const CoefShared<RS>& sh, int ks,
+                                          const CoefTable<RS>& cf, const CoefConst<RS>& cc, int c0,
+                                          const DevScheme* __restrict__ sc, const TwState<TT>& t) {
   constexpr int NE = OP == 0 ? 2 : 3;
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
   TT w0 = t.w[0], w1 = t.w[1], w2 = t.w[2], w3 = t.w[3], w4 = t.w[4], w5 = t.w[5];
@@ -1626,7 +1675,7 @@ __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, con
     am2 = am1;
     am1 = a2;
   }
-  fwd3<OP, ST, TT, RS>(s, NE, hw - NE, c0, L - 4, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  fwd4<OP, ST, TT, RS>(s, NE, hw - NE, ks, c0, L - 4, sh, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
 #pragma unroll
   for (int k = 0; k < NE; ++k) {
     const int i = hw - NE + k;
@@ -1654,6 +1703,15 @@ __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, con
 // k gives x(h-2+k) from the forward values at rows h-2, h-1, h, h+1), and the
 // reversed system's bitwise-constant interior factors (5).
 constexpr int kTwistExtra = 16 + 5;
+// factor rows per warp staged in shared memory behind the tile: the closure
+// rows below the constant range (at most 64 rows in FP64, 34 in FP32, for the
+// schemes' 8th-order derivative and filter), read there instead of from L2
+constexpr int kTwistSh = 64;
+// shared-memory offset of the staged factors: the tile, rounded up to 16 bytes
+__host__ __device__ __forceinline__ size_t twist_tile_bytes(int dir, int L, int nbox, int by, size_t es, int pitch) {
+  const size_t t = dir == 0 ? (size_t)32 * pitch * es : (size_t)nbox * by * 32 * es;
+  return (t + 15) / 16 * 16;
+}
 
 // One CTA = two warps = 32 lines. DIR: 1 xi, 2 eta, 3 zeta. OP: 0
 // derivative, 1 filter (in place). TT: field and tile type; RS: elimination
@@ -1741,6 +1799,14 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
                                : CoefConst<RS>{RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3)};
   const int c0 = rev ? T.kg : T.c0;
   const int hw = rev ? L - h : h;  // rows of the warp's half
+  // the warp's closure-row factors into shared memory (read below c0 only)
+  const int ks = min(min(c0, hw), kTwistSh);
+  RS* fsh = reinterpret_cast<RS*>(smem_raw + 128 + twist_tile_bytes(DIR - 1, L, NC, CR, sizeof(TT), P)) +
+            warp * 5 * kTwistSh;
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    for (int r = lane; r < ks; r += 32) fsh[k * kTwistSh + r] = __ldg(tb + k * L + r);
+  const CoefShared<RS> sh{fsh, fsh + kTwistSh, fsh + 2 * kTwistSh, fsh + 3 * kTwistSh, fsh + 4 * kTwistSh};
   const TT* recv = static_cast<const TT*>(T.recv);
   // interface sums received by the warp's own end
   TT q0 = 0, q1 = 0, q2 = 0;
@@ -1768,8 +1834,8 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   if (!rev) twist_read<OP, ST, TT>(sv, hw, T.ndf0, T.sc, q0, q1, q2, tw);
   else twist_read<OP, -ST, TT>(sv, hw, T.ndf1, T.sc, q0, q1, q2, tw);
   __syncthreads();
-  if (!rev) twist_fwd<OP, ST, TT, RS>(sv, L, hw, cf, cc, c0, T.sc, tw);
-  else twist_fwd<OP, -ST, TT, RS>(sv, L, hw, cf, cc, c0, T.sc, tw);
+  if (!rev) twist_fwd<OP, ST, TT, RS>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
+  else twist_fwd<OP, -ST, TT, RS>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
   __syncthreads();
   TRACE(3)
   // the four meeting unknowns; warp 0 keeps x(h-2), x(h-1), warp 1 x(h), x(h+1)
@@ -1785,12 +1851,12 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
     sv[(hw - 2) * ST] = TT(xa);
     sv[(hw - 1) * ST] = TT(xb);
     RS cp1 = xa, cp2 = xb;
-    bwd3<ST, TT, RS>(sv, hw - 3, 0, c0, L - 4, cf, cc, cp1, cp2);
+    bwd4<ST, TT, RS>(sv, hw - 3, 0, ks, c0, L - 4, sh, cf, cc, cp1, cp2);
   } else {
     sv[(hw - 1) * -ST] = TT(xa);
     sv[(hw - 2) * -ST] = TT(xb);
     RS cp1 = xb, cp2 = xa;
-    bwd3<-ST, TT, RS>(sv, hw - 3, 0, c0, L - 4, cf, cc, cp1, cp2);
+    bwd4<-ST, TT, RS>(sv, hw - 3, 0, ks, c0, L - 4, sh, cf, cc, cp1, cp2);
   }
   TRACE(4)
   if (OP == 0 && has && T.drva) {
