@@ -272,7 +272,8 @@ def workload_cases(args, cases, world=1, rank=0):
 def config_dict(args, workload, ncases, job_points, npts, world):
     """The bench line's config, the same for the device arm and the reference arm."""
     mode = {"fp64": "FP64, bit-exact with the reference's operation order",
-            "fast": "FP64 fast mode (split line solves with FMA; within 1e-10 of the reference after 10 steps)",
+            "fast": "FP64 fast mode (split and two-ended line solves with FMA; within 1e-10 of the reference "
+                    "after 10 steps)",
             "fp32": "FP32-mixed (FP32 line solves and fluxes; FP64 state, RK update, metrics and LU)"}[args.precision]
     return {"workload": workload, "cases": ncases, "points": job_points, "precision": args.precision,
             "arithmetic": mode,
@@ -650,10 +651,17 @@ def main():
     cands = [(k, v) for k, v in fam.items() if v["launches"] and v["bytes"] > 0
              and (k in kernel_of or k.startswith(("deriv", "filter")))]
     dom_name = max(cands, key=lambda kv: kv[1]["ms"])[0]
-    roofline = family_roofline(dom_name, kernel_of.get(dom_name, "k_line"))
+    def line_kernel(name):
+        """The line kernels of a family: the autotuner's kinds for its groups."""
+        op, d = name.split("_")
+        groups = ("filter",) if op == "filter" else ("viscous", "flux")
+        kinds = sorted({t["kind"] for t in (tuning or []) if t["dir"] == d and t["group"] in groups})
+        return "line solve, " + ("/".join(kinds) if kinds else "default kinds")
+
+    roofline = family_roofline(dom_name, kernel_of.get(dom_name) or line_kernel(dom_name))
     line_fams = {k: v for k, v in fam.items() if k.startswith(("deriv", "filter")) and v["launches"]}
     ln = max(line_fams, key=lambda k: line_fams[k]["ms"])
-    roofline_line = family_roofline(ln, "k_line")
+    roofline_line = family_roofline(ln, line_kernel(ln))
     lb = sum(v["bytes"] for v in line_fams.values())
     lms = sum(v["ms"] for v in line_fams.values())
     roofline_line["all_line_solves_gbs"] = lb / (lms / 1e3) / 1e9
