@@ -60,7 +60,9 @@ def parse():
     p.add_argument("--acc-ny", type=int, default=256)
     p.add_argument("--acc-nz", type=int, default=128)
     p.add_argument("--cpu-steps", type=int, default=5)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=10,
+                   help="steps of the end-to-end measurement through host memory (one canard_step_host call: "
+                        "the first step's copy in and the last one's copy out are not overlapped)")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--mode", default="step", choices=["step", "kernels", "accuracy", "cpu"],
                    help="step: the time-step benchmark (default); kernels: isolated derivative and filter "
