@@ -1438,11 +1438,17 @@ bool quad_ok(const canard_ctx* c, int dir, int kind) {
 // of at least kTwistMinL points; FP32 tables in mixed-precision contexts)
 bool twist_ok(const canard_ctx* c, int dir, int kind) {
   if (c->blocks.empty()) return false;
-  for (const auto& b : c->blocks)
+  for (const auto& b : c->blocks) {
     for (int nt = 0; nt < 2; ++nt) {
       if (!b.ht[nt][dir]) return false;
       if (kind != LK_F64_TWIST && !b.lu32t[nt][dir]) return false;
     }
+    // the whole tile of 32 lines (and the staged factors) in one CTA's shared memory
+    LineTask t{};
+    t.L = b.g.ijk[0][dir] + 1;
+    chunking_dir(dir, t.L, t.nbox, t.by);
+    if (line_smem(dir, t, kind) > (size_t)kLineSmemMax) return false;
+  }
   return true;
 }
 
