@@ -867,6 +867,24 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
     }
   }
   TRACE(1)
+  // the received interface sums load while the tile's copies are in flight
+  // (the periodic contraction below reads the tile instead)
+  const bool has = lane < nval;
+  int jk = 0;
+  if (DIR == 1) jk = r0 + lane;
+  else if (DIR == 2) jk = (x0 + lane) * Z + fix;
+  else jk = fix * X + x0 + lane;
+  const int nbs = T.nbs;
+  const TT* recv = static_cast<const TT*>(T.recv);
+  TT r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
+  if (OP == 0 && !T.selfp) {
+    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; }
+    if (has && T.ndf1) { r01 = recv[2 * nbs + jk]; r11 = recv[3 * nbs + jk]; }
+  }
+  if (OP == 1) {
+    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; r20 = recv[2 * nbs + jk]; }
+    if (has && T.ndf1) { r01 = recv[3 * nbs + jk]; r11 = recv[4 * nbs + jk]; r21 = recv[5 * nbs + jk]; }
+  }
   if (!mbar_wait(bars, 0) || !mbar_wait(bars + NC - 1, 0)) {
     if (lane == 0) atomicExch(err, kErrTimeout);
     // copies may still be landing: wait for the other chunks (bounded) before exit
@@ -915,18 +933,10 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   // every lane runs the sweep (lanes past the tile edge on zero-filled or
   // stale columns) so the chunk hand-offs stay warp-uniform; only lanes with a
   // line read the receive buffers or write drva
-  const bool has = lane < nval;
-  int jk = 0;
-  if (DIR == 1) jk = r0 + lane;
-  else if (DIR == 2) jk = (x0 + lane) * Z + fix;
-  else jk = fix * X + x0 + lane;
-  const int nbs = T.nbs;
   constexpr int ST = (DIR == 1) ? 1 : kLanes;
   TT* sl = (DIR == 1) ? s + lane * P : s + lane;
   const LuRows<RS> F(static_cast<const RS*>(T.lu), L, RS(T.cl1), RS(T.cl2), RS(T.cu1), RS(T.cu2), RS(T.cu3), T.c0);
-  const TT* recv = static_cast<const TT*>(T.recv);
   if (OP == 0) {
-    TT r00 = 0, r10 = 0, r01 = 0, r11 = 0;
     if (T.selfp) {
       // The line is periodic onto itself, so the interface contraction the
       // other end would send (src/mo_numerics.f90:503-518 with n45 = 0) is
@@ -942,9 +952,6 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
         r01 = r01 + TT(sc->pbco[0][0][i]) * w;
         r11 = r11 + TT(sc->pbco[0][1][i]) * w;
       }
-    } else {
-      if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; }
-      if (has && T.ndf1) { r01 = recv[2 * nbs + jk]; r11 = recv[3 * nbs + jk]; }
     }
     ok = sweep_deriv<ST, TT, RS>(sl, L, F, T.ndf0, T.ndf1, T.sc, r00, r10, r01, r11, CI, err, done);
     if (ok && has && T.drva) {
@@ -953,9 +960,6 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
       drva[jk + (long long)nbs * ((T.m - 1) + 5)] = sl[(L - 1) * ST];
     }
   } else {
-    TT r00 = 0, r10 = 0, r20 = 0, r01 = 0, r11 = 0, r21 = 0;
-    if (has && T.ndf0) { r00 = recv[jk]; r10 = recv[nbs + jk]; r20 = recv[2 * nbs + jk]; }
-    if (has && T.ndf1) { r01 = recv[3 * nbs + jk]; r11 = recv[4 * nbs + jk]; r21 = recv[5 * nbs + jk]; }
     // this lane's line of the unfiltered field (lanes without a line read
     // lane 0's, whose results are not stored)
     const TT* og = (DIR == 1) ? in + base + (long long)(has ? lane : 0) * Xp : in + base + (has ? lane : 0);
@@ -1774,13 +1778,8 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
     }
   }
   TRACE(1)
-  bool ok = true;
-  for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicExch(err, kErrTimeout);
-    return;
-  }
-  TRACE(2)
+  // while the tile's copies are in flight: the factors, the staged closure
+  // factors and the received interface sums (none of them read the tile)
   constexpr int ST = (DIR == 1) ? 1 : kLanes;
   TT* sl = (DIR == 1) ? s + lane * P : s + lane;
   TT* sv = rev ? sl + N * ST : sl;  // the warp's view of its line (warp 1: reversed)
@@ -1810,16 +1809,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   const TT* recv = static_cast<const TT*>(T.recv);
   // interface sums received by the warp's own end
   TT q0 = 0, q1 = 0, q2 = 0;
-  if (OP == 0 && T.selfp) {
-    // periodic onto itself: the contraction the other end would send (see k_line)
-    const DevScheme* sc = T.sc;
-#pragma unroll
-    for (int i = 0; i < 12; ++i) {
-      const TT v = !rev ? sl[(N - 1 - i) * ST] : sl[(1 + i) * ST];
-      q0 = q0 + TT(sc->pbco[0][0][i]) * v;
-      q1 = q1 + TT(sc->pbco[0][1][i]) * v;
-    }
-  } else if (has) {
+  if (!(OP == 0 && T.selfp) && has) {
     const int nc = OP == 0 ? 2 : 3;
     if (!rev && T.ndf0) {
       q0 = recv[jk]; q1 = recv[nbs + jk];
@@ -1828,6 +1818,23 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
     if (rev && T.ndf1) {
       q0 = recv[nc * nbs + jk]; q1 = recv[(nc + 1) * nbs + jk];
       if (OP == 1) q2 = recv[(nc + 2) * nbs + jk];
+    }
+  }
+  bool ok = true;
+  for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(err, kErrTimeout);
+    return;
+  }
+  TRACE(2)
+  if (OP == 0 && T.selfp) {
+    // periodic onto itself: the contraction the other end would send (see k_line)
+    const DevScheme* sc = T.sc;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const TT v = !rev ? sl[(N - 1 - i) * ST] : sl[(1 + i) * ST];
+      q0 = q0 + TT(sc->pbco[0][0][i]) * v;
+      q1 = q1 + TT(sc->pbco[0][1][i]) * v;
     }
   }
   TwState<TT> tw;
