@@ -74,6 +74,7 @@ struct Table {
   double bytes = 0;  // algorithmic bytes of one launch
   CUtensorMap* maps = nullptr;  // line tables: TMA descriptors (in, out) per task
   int kind = 0;  // line tables: a LineKind; face tables: 0 FP64 fields, 1 FP32 fields
+  int tdiv = 0;  // line tables: tiles per task when every task has as many (the kernels divide), else 0
 };
 
 // Element types of a line launch: tile (field) type and elimination type.
@@ -748,6 +749,9 @@ Table<LineTask> make_line_table(canard_ctx* c, std::vector<LineTask> v, int dir,
     T.bytes += 2.0 * es * t.X * t.Y * t.Z;  // read the field, write the result
   }
   if (tile_task.empty()) tile_task.push_back(0);
+  T.tdiv = v.empty() ? 0 : v[0].ntiles;
+  for (const LineTask& t : v)
+    if (t.ntiles != T.tdiv) T.tdiv = 0;
   T.ntasks = (int)v.size();
   T.total = tot;
   T.smem = sm;
@@ -796,7 +800,7 @@ template <int DIR, int OP, class TT, class RS>
 void launch_line_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  launch_line_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.tdiv, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -804,7 +808,7 @@ template <int DIR, int OP, class TT, class RS = float>
 void launch_line2_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  launch_line2_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line2_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.tdiv, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -832,7 +836,7 @@ template <int DIR, int OP, class TT, class RS>
 void launch_line2t_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, (OP == 0 ? T_DERIV_XI : T_FILTER_XI) + DIR - 1, T.bytes);
-  launch_line2t_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line2t_t<DIR, OP, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.tdiv, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -840,7 +844,7 @@ template <int DIR, class TT, class RS>
 void launch_line4_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, T_DERIV_XI + DIR - 1, T.bytes);
-  launch_line4_t<DIR, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, T.maps, c->derr);
+  launch_line4_t<DIR, TT, RS>(T.total, T.smem, c->st, T.tasks, T.first, T.tdiv, T.maps, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -848,7 +852,7 @@ template <int DIR>
 void launch_filt2s_dir(canard_ctx* c, const Table<LineTask>& T) {
   if (T.ntasks == 0 || T.total == 0) return;
   Timed tm(c, T_FILTER_XI + DIR - 1, T.bytes);
-  launch_filt2s_t<DIR>(T.total, T.smem, c->st, T.tasks, T.first, T.ntasks, c->derr);
+  launch_filt2s_t<DIR>(T.total, T.smem, c->st, T.tasks, T.first, T.tdiv, c->derr);
   CK(cudaGetLastError());
 }
 
@@ -3111,9 +3115,10 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     const int* d0 = reinterpret_cast<const int*>(base + kNaTiles);  // zeros: tile -> task 0
     const CUtensorMap* dm = reinterpret_cast<const CUtensorMap*>(base + kNaMaps);
     int* de = reinterpret_cast<int*>(base + kNaErr);
-    if (dir == 0) launch_line_t<1, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
-    else if (dir == 1) launch_line_t<2, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
-    else launch_line_t<3, 0, double, double>(t.ntiles, smem, st, dt, d0, 1, dm, de);
+    // one task: every tile's task is tile / ntiles = 0 (the zero table is not read)
+    if (dir == 0) launch_line_t<1, 0, double, double>(t.ntiles, smem, st, dt, d0, t.ntiles, dm, de);
+    else if (dir == 1) launch_line_t<2, 0, double, double>(t.ntiles, smem, st, dt, d0, t.ntiles, dm, de);
+    else launch_line_t<3, 0, double, double>(t.ntiles, smem, st, dt, d0, t.ntiles, dm, de);
     CK(cudaGetLastError());
   } catch (const ApiError& e) {
     return fail(e.code, e.what());

@@ -144,6 +144,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
+// L1 prefetch of one cache line
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 // Bounded wait for phase `parity`; returns false if the limit expired.
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -264,6 +266,19 @@ struct LuRows {
 };
 
 constexpr int kMaxChunks = 8;
+
+// While a tile's copies are in flight: the scheme's coefficients (944 bytes)
+// and the first 16 rows of the five factor tables into L1, which the closures
+// and the first blocks of the sweeps read as soon as the tile has arrived.
+template <class RS>
+__device__ __forceinline__ void prefetch_sweep_start(const DevScheme* sc, const RS* lu, int L, int lane) {
+  if (lane < 8) {
+    prefetch_l1(reinterpret_cast<const char*>(sc) + 128 * lane);
+  } else if (lane < 18) {
+    const int k = (lane - 8) % 5, e = (lane - 8) / 5 ? 15 : 0;
+    prefetch_l1(lu + (size_t)k * L + e);
+  }
+}
 
 #ifdef CANARD_TRACE
 __device__ long long* g_trace;  // per CTA: start, loads issued, data ready, forward done, end, SM id
@@ -781,6 +796,12 @@ __device__ __forceinline__ bool sweep_filter(TT* __restrict__ s, int L, const Lu
 #undef BR_CE
 #undef BR_LO
 
+// The task of this CTA's tile: tdiv > 0 when every task of the launch has
+// tdiv tiles (no table read on the CTA's start-up path), else the table.
+__device__ __forceinline__ int tile_of(const int* __restrict__ tile_task, int tdiv) {
+  return tdiv > 0 ? (int)(blockIdx.x / (unsigned)tdiv) : __ldg(tile_task + blockIdx.x);
+}
+
 __device__ __forceinline__ int find_task(const int* __restrict__ tile0, int ntasks, int tile) {
   int lo = 0, hi = ntasks - 1;
   while (lo < hi) {
@@ -813,7 +834,7 @@ __host__ __device__ __forceinline__ int dir1_pitch(int L) {
 // forward sweep, stores the back substitution.
 template <int DIR, int OP, class TT, class RS>
 __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
-                                             int ntasks, const CUtensorMap* __restrict__ maps,
+                                             int tdiv, const CUtensorMap* __restrict__ maps,
                                              int* __restrict__ err) {
   constexpr int kVec = 16 / (int)sizeof(TT);  // elements per 16 bytes
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -822,7 +843,7 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   const int lane = threadIdx.x;
   TRACE(0)
   // the tile's task and the error flag load together (independent)
-  const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
+  const int ti = tile_of(tile_task, tdiv);
   if (error_pending(err)) return;
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
@@ -866,6 +887,7 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
       else tma_load_3d(s + c * CR * kLanes, map_in, x0, fix, c * CR, bars + c);
     }
   }
+  prefetch_sweep_start(T.sc, static_cast<const RS*>(T.lu), L, lane);
   TRACE(1)
   // the received interface sums load while the tile's copies are in flight
   // (the periodic contraction below reads the tile instead)
@@ -1383,7 +1405,7 @@ __device__ __forceinline__ void sweep2(TT* __restrict__ s, int L, int h, int hal
 // mode, whose factors and correction tables are FP64).
 template <int DIR, int OP, class TT, class RS = float>
 __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
-                                              int ntasks, const CUtensorMap* __restrict__ maps,
+                                              int tdiv, const CUtensorMap* __restrict__ maps,
                                               int* __restrict__ err) {
   static_assert(OP == 0 || sizeof(TT) == 8, "the split filter acts on FP64 fields (reduce-add stores)");
   constexpr int kVec = 16 / (int)sizeof(TT);
@@ -1394,7 +1416,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   const int half = lane >> 4, li = lane & (kHalf - 1);
   TRACE(0)
   // the tile's task and the error flag load together (independent)
-  const int ti = __ldg(tile_task + blockIdx.x);  // tile -> task (ntasks: tasks in the table)
+  const int ti = tile_of(tile_task, tdiv);
   if (error_pending(err)) return;
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
@@ -1434,6 +1456,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
       else tma_load_3d(s + c * CR * kHalf, map_in, x0, fix, c * CR, bars + c);
     }
   }
+  prefetch_sweep_start(T.sc, static_cast<const RS*>(T.lu), L, lane);
   TRACE(1)
   bool ok = true;
   for (int c = 0; c < NC; ++c) ok = mbar_wait(bars + c, 0) && ok;
@@ -1669,12 +1692,13 @@ __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, con
   constexpr int NE = OP == 0 ? 2 : 3;
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
   TT w0 = t.w[0], w1 = t.w[1], w2 = t.w[2], w3 = t.w[3], w4 = t.w[4], w5 = t.w[5];
+  // rows 1 and 2 lie below the constant range, so among the staged factors
   RS am2 = RS(t.b[0]);
-  RS am1 = RS(t.b[1]) - cf.L2(1) * am2;
+  RS am1 = RS(t.b[1]) - sh.L2(1) * am2;
   s[0] = TT(am2);
   s[ST] = TT(am1);
   if (OP == 1) {
-    const RS a2 = (RS(t.b[2]) - cf.L1(2) * am2) - cf.L2(2) * am1;
+    const RS a2 = (RS(t.b[2]) - sh.L1(2) * am2) - sh.L2(2) * am1;
     s[2 * ST] = TT(a2);
     am2 = am1;
     am1 = a2;
@@ -1723,7 +1747,7 @@ __host__ __device__ __forceinline__ size_t twist_tile_bytes(int dir, int L, int 
 // system's constant factor range.
 template <int DIR, int OP, class TT, class RS>
 __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
-                                               int ntasks, const CUtensorMap* __restrict__ maps,
+                                               int tdiv, const CUtensorMap* __restrict__ maps,
                                                int* __restrict__ err) {
   static_assert(OP == 0 || sizeof(TT) == 8, "the filter acts on FP64 fields (reduce-add stores)");
   constexpr int kVec = 16 / (int)sizeof(TT);
@@ -1733,7 +1757,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool rev = warp == 1;
   TRACE(0)
-  const int ti = __ldg(tile_task + blockIdx.x);
+  const int ti = tile_of(tile_task, tdiv);
   // one decision for both warps (they meet at CTA barriers below)
   if (__syncthreads_or(error_pending(err))) return;
   const LineTask& T = tasks[ti];
@@ -1777,6 +1801,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
       }
     }
   }
+  if (lane < 8) prefetch_l1(reinterpret_cast<const char*>(T.sc) + 128 * lane);
   TRACE(1)
   // while the tile's copies are in flight: the factors, the staged closure
   // factors and the received interface sums (none of them read the tile)
@@ -1947,7 +1972,7 @@ constexpr int kQuad = 8;
 
 template <int DIR, class TT, class RS>
 __global__ void __maxnreg__(168) k_line4(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
-                                              int ntasks, const CUtensorMap* __restrict__ maps,
+                                              int tdiv, const CUtensorMap* __restrict__ maps,
                                               int* __restrict__ err) {
   constexpr int kVec = 16 / (int)sizeof(TT);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1957,7 +1982,7 @@ __global__ void __maxnreg__(168) k_line4(const LineTask* __restrict__ tasks, con
   const int seg = lane >> 3, li = lane & (kQuad - 1);
   const unsigned full = 0xffffffffu;
   TRACE(0)
-  const int ti = __ldg(tile_task + blockIdx.x);
+  const int ti = tile_of(tile_task, tdiv);
   if (error_pending(err)) return;
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
@@ -2251,14 +2276,14 @@ __device__ __forceinline__ void fwd_rows_rhs(float* s, int ib, int ie, const CF&
 
 template <int DIR>
 __global__ void __launch_bounds__(32) k_filt2s(const LineTask* __restrict__ tasks, const int* __restrict__ tile_task,
-                                               int ntasks, int* __restrict__ err) {
+                                               int tdiv, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* s = reinterpret_cast<float*>(smem_raw);
   const int lane = threadIdx.x;
   const int half = lane >> 4, li = lane & (kHalf - 1);
   const unsigned full = 0xffffffffu;
   if (error_pending(err)) return;
-  const int ti = __ldg(tile_task + blockIdx.x);
+  const int ti = tile_of(tile_task, tdiv);
   const LineTask& T = tasks[ti];
   const double* __restrict__ in = static_cast<const double*>(T.in);
   double* out = static_cast<double*>(T.out);
