@@ -1456,11 +1456,11 @@ bool twist_ok(const canard_ctx* c, int dir, int kind) {
   return true;
 }
 
-// Defaults without autotuning: the filter's two-ended solve where the lines
-// admit it (measured 15-18 % faster than the split and one-lane filters at
-// 257 points), the split solve for the derivatives of the fast and mixed modes
+// Defaults without autotuning: the two-ended solve where the lines admit it
+// (fast mode: the fastest FP64 filter and derivative at 257 points; mixed
+// precision: the fastest filter), else the split solve
 int default_kind(const canard_ctx* c, int grp, int dir) {
-  if (c->fast()) return (grp == 0 && twist_ok(c, dir, LK_F64_TWIST)) ? LK_F64_TWIST : LK_F64_SPLIT;
+  if (c->fast()) return twist_ok(c, dir, LK_F64_TWIST) ? LK_F64_TWIST : LK_F64_SPLIT;
   if (!c->f32()) return LK_F64;
   if (grp == 0) return twist_ok(c, dir, LK_F64_TILE_F32_TWIST) ? LK_F64_TILE_F32_TWIST : LK_F64_TILE_F32_SOLVE;
   return LK_F32;

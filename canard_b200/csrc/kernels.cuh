@@ -138,8 +138,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// one fence after a thread's initialisations (their visibility to the copies)
+__device__ __forceinline__ void mbar_init_done() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
@@ -172,6 +173,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if ((it & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
+}
+// the error flag's load issued at a kernel's start and decided later (the
+// load's latency then overlaps the task decode and barrier set-up)
+__device__ __forceinline__ int error_flag_early(const int* err) {
+  return (threadIdx.x & 31) == 0 ? *reinterpret_cast<const volatile int*>(err) : 0;
 }
 // a kernel launched after a bounded wait gave up does no work (the host
 // reports the error at its next synchronisation); uniform over the warp
@@ -844,7 +850,7 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   TRACE(0)
   // the tile's task and the error flag load together (independent)
   const int ti = tile_of(tile_task, tdiv);
-  if (error_pending(err)) return;
+  const int eflag = error_flag_early(err);
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -870,7 +876,10 @@ __global__ void __maxnreg__(200) k_line(const LineTask* __restrict__ tasks, cons
   auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
   if (lane == 0) {
     for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+    mbar_init_done();
   }
+  // a kernel launched after a bounded wait gave up does no work
+  if (__shfl_sync(0xffffffffu, eflag, 0) != 0) return;
   __syncwarp();
   // issue the loads: chunk 0, the last chunk, then the middle ones
   for (int k = 0; k < NC; ++k) {
@@ -1417,7 +1426,7 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   TRACE(0)
   // the tile's task and the error flag load together (independent)
   const int ti = tile_of(tile_task, tdiv);
-  if (error_pending(err)) return;
+  const int eflag = error_flag_early(err);
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -1441,8 +1450,12 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
   const CUtensorMap* map_in = maps + 2 * ti;
   const CUtensorMap* map_out = maps + 2 * ti + 1;
   auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
-  if (lane == 0)
+  if (lane == 0) {
     for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+    mbar_init_done();
+  }
+  // a kernel launched after a bounded wait gave up does no work
+  if (__shfl_sync(0xffffffffu, eflag, 0) != 0) return;
   __syncwarp();
   for (int c = 0; c < NC; ++c) {
     if (DIR == 1) {
@@ -1758,8 +1771,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   const bool rev = warp == 1;
   TRACE(0)
   const int ti = tile_of(tile_task, tdiv);
-  // one decision for both warps (they meet at CTA barriers below)
-  if (__syncthreads_or(error_pending(err))) return;
+  const int eflag = error_flag_early(err);
   const LineTask& T = tasks[ti];
   const TT* in = static_cast<const TT*>(T.in);
   TT* out = static_cast<TT*>(T.out);
@@ -1783,9 +1795,13 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   const CUtensorMap* map_in = maps + 2 * ti;
   const CUtensorMap* map_out = maps + 2 * ti + 1;
   auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
-  __syncthreads();
+    mbar_init_done();
+  }
+  // one decision for both warps (they meet at CTA barriers below): a kernel
+  // launched after a bounded wait gave up does no work
+  if (__syncthreads_or(eflag != 0)) return;
   if (!rev) {
     for (int c = 0; c < NC; ++c) {
       if (DIR == 1) {
@@ -2006,8 +2022,10 @@ __global__ void __maxnreg__(168) k_line4(const LineTask* __restrict__ tasks, con
   const CUtensorMap* map_in = maps + 2 * ti;
   const CUtensorMap* map_out = maps + 2 * ti + 1;
   auto chunk_len = [&](int c) { return min(CR, L - c * CR); };
-  if (lane == 0)
+  if (lane == 0) {
     for (int c = 0; c < NC; ++c) mbar_init(bars + c, 1);
+    mbar_init_done();
+  }
   __syncwarp();
   for (int c = 0; c < NC; ++c) {
     if (DIR == 1) {

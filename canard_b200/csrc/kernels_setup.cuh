@@ -316,7 +316,10 @@ __global__ void k_wall_update(const BlockDev* __restrict__ bd, const StageParams
 // a line kernel does when a copy never lands; no fault, no trap.
 __global__ void k_wait_selftest(int* __restrict__ err) {
   __shared__ __align__(8) uint64_t bar;
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_done();
+  }
   __syncwarp();
   const bool ok = mbar_wait(&bar, 0);
   if (!ok && threadIdx.x == 0) atomicExch(err, kErrTimeout);

@@ -526,8 +526,10 @@ __global__ void __launch_bounds__(kTmWarps * 32) k_line_tm(const LineTask* __res
   in.bars = reinterpret_cast<uint64_t*>(smem_raw + kTmBarOff) + w * 8;
   in.ring = reinterpret_cast<double*>(smem_raw + kTmHeader) + (size_t)w * kTmWarpDoubles;
   in.top = in.ring + (size_t)kTmRing * kLanes;
-  if (lane == 0)
+  if (lane == 0) {
     for (int s = 0; s <= kTmTopSlot; ++s) mbar_init(in.bars + s, 1);
+    mbar_init_done();
+  }
   if (w == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tbase)),
                  "r"(512));
