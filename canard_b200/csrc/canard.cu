@@ -2102,6 +2102,8 @@ void create(canard_ctx* c, const canard_case_desc* cases, int ncases, const cana
     std::memcpy(ds.pbcot, cs.sch.pbcot, sizeof(ds.pbcot));
     ds.fa = cs.sch.fa; ds.fb = cs.sch.fb; ds.fc = cs.sch.fc;
     std::memcpy(ds.fbc, cs.sch.fbc, sizeof(ds.fbc));
+    ds.alphf = cs.sch.alphf; ds.betf = cs.sch.betf;
+    std::memcpy(ds.albef, cs.sch.albef, sizeof(ds.albef));
     cs.dsch = dupload(std::vector<DevScheme>{ds}, c->st);
   }
   c->dcc = dupload(ccv, c->st);
@@ -3089,6 +3091,8 @@ extern "C" int canard_deriv_noalloc(const double* d_in, double* d_out, int32_t l
     std::memcpy(ds.pbcot, sch.pbcot, sizeof(ds.pbcot));
     ds.fa = sch.fa; ds.fb = sch.fb; ds.fc = sch.fc;
     std::memcpy(ds.fbc, sch.fbc, sizeof(ds.fbc));
+    ds.alphf = sch.alphf; ds.betf = sch.betf;
+    std::memcpy(ds.albef, sch.albef, sizeof(ds.albef));
     CUtensorMap maps[2];
     std::memset(maps, 0, sizeof(maps));
     if (dir != 0) {

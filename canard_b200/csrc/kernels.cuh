@@ -29,6 +29,8 @@ struct DevScheme {
   double pbcot[2][2];
   double fa, fb, fc;
   double fbc[3][5];       // [row][k]
+  double alphf, betf;     // the filter's interior left-hand side (beta, alpha, 1, alpha, beta)
+  double albef[2][3][5];  // its first three rows [closure kind][row][k+2]: 0 boundary, 1 interface
 };
 
 // Per-case scalars of one RK stage (written by the host before each step).
@@ -273,15 +275,15 @@ struct LuRows {
 
 constexpr int kMaxChunks = 8;
 
-// While a tile's copies are in flight: the scheme's coefficients (944 bytes)
+// While a tile's copies are in flight: the scheme's coefficients (1.2 KB)
 // and the first 16 rows of the five factor tables into L1, which the closures
 // and the first blocks of the sweeps read as soon as the tile has arrived.
 template <class RS>
 __device__ __forceinline__ void prefetch_sweep_start(const DevScheme* sc, const RS* lu, int L, int lane) {
-  if (lane < 8) {
+  if (lane < 10) {
     prefetch_l1(reinterpret_cast<const char*>(sc) + 128 * lane);
-  } else if (lane < 18) {
-    const int k = (lane - 8) % 5, e = (lane - 8) / 5 ? 15 : 0;
+  } else if (lane < 20) {
+    const int k = (lane - 10) % 5, e = (lane - 10) / 5 ? 15 : 0;
     prefetch_l1(lu + (size_t)k * L + e);
   }
 }
@@ -433,9 +435,11 @@ __device__ __forceinline__ void fwd8_deriv(TT* __restrict__ s, int i, const CF& 
 
 // Right-hand sides of the filter's rows i..i+7 (reads rows up to i+10);
 // window w0..w5 = s[i-3..i+2] on entry, s[i+5..i+10] on return
-template <int ST, class TT>
+// DIRECT: the right-hand side of the filtered values themselves, (B x)_i =
+// (A x)_i + ((B - A) x)_i with A's interior row (beta, alpha, 1, alpha, beta)
+template <int ST, class TT, bool DIRECT = false>
 __device__ __forceinline__ void rhs8_filter(const TT* __restrict__ s, int i, TT fa, TT fb, TT fc, TT& w0, TT& w1,
-                                            TT& w2, TT& w3, TT& w4, TT& w5, TT (&r)[8]) {
+                                            TT& w2, TT& w3, TT& w4, TT& w5, TT (&r)[8], TT al = 0, TT be = 0) {
   TT win[14];
   win[0] = w0; win[1] = w1; win[2] = w2; win[3] = w3; win[4] = w4; win[5] = w5;
 #pragma unroll
@@ -445,6 +449,7 @@ __device__ __forceinline__ void rhs8_filter(const TT* __restrict__ s, int i, TT 
     const TT rk = win[k + 3] + win[k + 3];
     r[k] = (fa * ((win[k + 2] + win[k + 4]) - rk) + fb * ((win[k + 1] + win[k + 5]) - rk)) +
            fc * ((win[k] + win[k + 6]) - rk);
+    if (DIRECT) r[k] = r[k] + ((win[k + 3] + al * (win[k + 2] + win[k + 4])) + be * (win[k + 1] + win[k + 5]));
   }
   w0 = win[8]; w1 = win[9]; w2 = win[10]; w3 = win[11]; w4 = win[12]; w5 = win[13];
 }
@@ -1088,22 +1093,23 @@ __device__ __forceinline__ void fwd_rows_deriv(TT* s, int ib, int ie, const CF& 
   }
 }
 
-template <int ST, class TT, class RS, class CF>
+template <int ST, class TT, class RS, class CF, bool DIRECT = false>
 __device__ __forceinline__ void fwd_rows_filter(TT* s, int ib, int ie, const CF& cf, TT fa, TT fb, TT fc, TT& w0,
-                                                TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+                                                TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1,
+                                                TT al = 0, TT be = 0) {
   int i = ib;
   if (i + 7 < ie) {
     F8<RS> nx;
     nx.load(cf, i);
     TT rr[8];
-    rhs8_filter<ST, TT>(s, i, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr);
+    rhs8_filter<ST, TT, DIRECT>(s, i, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr, al, be);
     while (i + 15 < ie) {
       const F8<RS> cu = nx;
       TT rc[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) rc[k] = rr[k];
       nx.load(cf, i + 8);
-      rhs8_filter<ST, TT>(s, i + 8, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr);
+      rhs8_filter<ST, TT, DIRECT>(s, i + 8, fa, fb, fc, w0, w1, w2, w3, w4, w5, rr, al, be);
       chain8_fwd<ST, TT, RS>(s, i, cu, rc, am2, am1);
       i += 8;
     }
@@ -1113,7 +1119,8 @@ __device__ __forceinline__ void fwd_rows_filter(TT* s, int ib, int ie, const CF&
   for (; i < ie; ++i) {
     const TT w6 = s[(i + 3) * ST];
     const TT rk = w3 + w3;
-    const TT rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+    TT rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+    if (DIRECT) rhs = rhs + ((w3 + al * (w2 + w4)) + be * (w1 + w5));
     const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
     s[i * ST] = TT(a);
     w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
@@ -1600,10 +1607,11 @@ __global__ void __launch_bounds__(32) k_line2(const LineTask* __restrict__ tasks
 // Rows [ib, ie) in four per-lane segments: shared-memory factors below
 // k0 = min(ks, c0), table factors on [k0, c0), the register constants on
 // [c0, c1], table factors above c1.
-template <int OP, int ST, class TT, class RS>
+template <int OP, int ST, class TT, class RS, bool DIRECT = false>
 __device__ __forceinline__ void fwd4(TT* s, int ib, int ie, int ks, int c0, int c1, const CoefShared<RS>& sh,
                                      const CoefTable<RS>& ct, const CoefConst<RS>& cc, TT fa, TT fb, TT fc, TT& w0,
-                                     TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1) {
+                                     TT& w1, TT& w2, TT& w3, TT& w4, TT& w5, RS& am2, RS& am1, TT al = 0,
+                                     TT be = 0) {
   const int k0 = min(ks, c0);
   const int a1 = min(ie, k0), b0 = max(ib, k0), b1 = min(ie, c0), m0 = max(ib, c0), m1 = min(ie, c1 + 1),
             d0 = max(ib, c1 + 1);
@@ -1613,10 +1621,14 @@ __device__ __forceinline__ void fwd4(TT* s, int ib, int ie, int ks, int c0, int 
     fwd_rows_deriv<ST, TT, RS>(s, m0, m1, cc, w0, w1, w2, w3, am2, am1);
     fwd_rows_deriv<ST, TT, RS>(s, d0, ie, ct, w0, w1, w2, w3, am2, am1);
   } else {
-    fwd_rows_filter<ST, TT, RS>(s, ib, a1, sh, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
-    fwd_rows_filter<ST, TT, RS>(s, b0, b1, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
-    fwd_rows_filter<ST, TT, RS>(s, m0, m1, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
-    fwd_rows_filter<ST, TT, RS>(s, d0, ie, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+    fwd_rows_filter<ST, TT, RS, CoefShared<RS>, DIRECT>(s, ib, a1, sh, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2,
+                                                        am1, al, be);
+    fwd_rows_filter<ST, TT, RS, CoefTable<RS>, DIRECT>(s, b0, b1, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1,
+                                                       al, be);
+    fwd_rows_filter<ST, TT, RS, CoefConst<RS>, DIRECT>(s, m0, m1, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1,
+                                                       al, be);
+    fwd_rows_filter<ST, TT, RS, CoefTable<RS>, DIRECT>(s, d0, ie, ct, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1,
+                                                       al, be);
   }
 }
 
@@ -1640,7 +1652,7 @@ struct TwState {
   TT x[3];  // originals at view rows hw, hw+1, hw+2 (the other half's first rows)
 };
 
-template <int OP, int ST, class TT>
+template <int OP, int ST, class TT, bool DIRECT = false>
 __device__ __forceinline__ void twist_read(const TT* __restrict__ s, int hw, int ndf,
                                            const DevScheme* __restrict__ sc, TT q0, TT q1, TT q2, TwState<TT>& t) {
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
@@ -1688,6 +1700,12 @@ __device__ __forceinline__ void twist_read(const TT* __restrict__ s, int hw, int
       t.b[1] = t1 + q1;
       t.b[2] = (fa * ((s1 + s3) - ra2) + fb * ((s0 + s4) - ra2)) + fc * ((q2 + s5) - ra2);
     }
+    if (DIRECT) {  // (A x) of the three closure rows: the filtered values' right-hand sides
+      const double* a = &sc->albef[ndf][0][0];
+      t.b[0] = t.b[0] + ((s0 + TT(a[3]) * s1) + TT(a[4]) * s2);
+      t.b[1] = t.b[1] + (((TT(a[6]) * s0 + s1) + TT(a[8]) * s2) + TT(a[9]) * s3);
+      t.b[2] = t.b[2] + ((((TT(a[10]) * s0 + TT(a[11]) * s1) + s2) + TT(a[13]) * s3) + TT(a[14]) * s4);
+    }
     t.w[0] = s0; t.w[1] = s1; t.w[2] = s2; t.w[3] = s3; t.w[4] = s4; t.w[5] = s5;
     t.x[2] = s[(hw + 2) * ST];
   }
@@ -1698,12 +1716,13 @@ __device__ __forceinline__ void twist_read(const TT* __restrict__ s, int hw, int
 // Forward elimination of view rows 0..hw-1: the closure rows, the interior
 // (three segments, as fwd3), then the last NE rows, whose look-ahead rows
 // belong to the other half and come from the values read before.
-template <int OP, int ST, class TT, class RS>
+template <int OP, int ST, class TT, class RS, bool DIRECT = false>
 __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, const CoefShared<RS>& sh, int ks,
                                           const CoefTable<RS>& cf, const CoefConst<RS>& cc, int c0,
                                           const DevScheme* __restrict__ sc, const TwState<TT>& t) {
   constexpr int NE = OP == 0 ? 2 : 3;
   const TT fa = TT(sc->fa), fb = TT(sc->fb), fc = TT(sc->fc);
+  const TT al = DIRECT ? TT(sc->alphf) : TT(0), be = DIRECT ? TT(sc->betf) : TT(0);
   TT w0 = t.w[0], w1 = t.w[1], w2 = t.w[2], w3 = t.w[3], w4 = t.w[4], w5 = t.w[5];
   // rows 1 and 2 lie below the constant range, so among the staged factors
   RS am2 = RS(t.b[0]);
@@ -1716,7 +1735,8 @@ __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, con
     am2 = am1;
     am1 = a2;
   }
-  fwd4<OP, ST, TT, RS>(s, NE, hw - NE, ks, c0, L - 4, sh, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2, am1);
+  fwd4<OP, ST, TT, RS, DIRECT>(s, NE, hw - NE, ks, c0, L - 4, sh, cf, cc, fa, fb, fc, w0, w1, w2, w3, w4, w5, am2,
+                               am1, al, be);
 #pragma unroll
   for (int k = 0; k < NE; ++k) {
     const int i = hw - NE + k;
@@ -1729,6 +1749,7 @@ __device__ __forceinline__ void twist_fwd(TT* __restrict__ s, int L, int hw, con
       const TT w6 = t.x[k];
       const TT rk = w3 + w3;
       rhs = (fa * ((w2 + w4) - rk) + fb * ((w1 + w5) - rk)) + fc * ((w0 + w6) - rk);
+      if (DIRECT) rhs = rhs + ((w3 + al * (w2 + w4)) + be * (w1 + w5));
       w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
     }
     const RS a = (RS(rhs) - cf.L1(i) * am2) - cf.L2(i) * am1;
@@ -1817,7 +1838,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
       }
     }
   }
-  if (lane < 8) prefetch_l1(reinterpret_cast<const char*>(T.sc) + 128 * lane);
+  if (lane < 10) prefetch_l1(reinterpret_cast<const char*>(T.sc) + 128 * lane);
   TRACE(1)
   // while the tile's copies are in flight: the factors, the staged closure
   // factors and the received interface sums (none of them read the tile)
@@ -1878,12 +1899,16 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
       q1 = q1 + TT(sc->pbco[0][1][i]) * v;
     }
   }
+  // FP64 eliminations of the filter solve for the filtered values directly
+  // (right-hand side B x): no originals to add afterwards (the FP32 one keeps
+  // the increment, whose rounding is then relative to the increment)
+  constexpr bool kDirect = OP == 1 && sizeof(RS) == 8;
   TwState<TT> tw;
-  if (!rev) twist_read<OP, ST, TT>(sv, hw, T.ndf0, T.sc, q0, q1, q2, tw);
-  else twist_read<OP, -ST, TT>(sv, hw, T.ndf1, T.sc, q0, q1, q2, tw);
+  if (!rev) twist_read<OP, ST, TT, kDirect>(sv, hw, T.ndf0, T.sc, q0, q1, q2, tw);
+  else twist_read<OP, -ST, TT, kDirect>(sv, hw, T.ndf1, T.sc, q0, q1, q2, tw);
   __syncthreads();
-  if (!rev) twist_fwd<OP, ST, TT, RS>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
-  else twist_fwd<OP, -ST, TT, RS>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
+  if (!rev) twist_fwd<OP, ST, TT, RS, kDirect>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
+  else twist_fwd<OP, -ST, TT, RS, kDirect>(sv, L, hw, sh, ks, cf, cc, c0, T.sc, tw);
   __syncthreads();
   TRACE(3)
   // the four meeting unknowns; warp 0 keeps x(h-2), x(h-1), warp 1 x(h), x(h+1)
@@ -1916,7 +1941,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
   // added to the field by one bulk FP64 reduce-add per line; along eta/zeta
   // each warp adds the originals to its half of the 32 columns (coalesced
   // rows), then the chunks are stored
-  if (OP == 1 && DIR != 1 && has) {
+  if (OP == 1 && !kDirect && DIR != 1 && has) {
     const TT* g = in + base + lane;
     TT* col = s + lane;
     const int lo = !rev ? 0 : h, hi = !rev ? h : L;
@@ -1940,7 +1965,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
     }
     for (; i < hi; ++i) col[i * kLanes] = __ldg(g + (long long)i * pstride) + col[i * kLanes];
   }
-  if (OP == 1 && DIR == 1 && (L & 1) && !rev) s[lane * P + L] = TT(0);  // the 16-byte tail's pad adds 0
+  if (OP == 1 && !kDirect && DIR == 1 && (L & 1) && !rev) s[lane * P + L] = TT(0);  // the 16-byte tail's pad adds 0
   fence_proxy_async();
   __syncthreads();
   TRACE(5)
@@ -1950,7 +1975,7 @@ __global__ void __launch_bounds__(64) k_line2t(const LineTask* __restrict__ task
     if (DIR == 1) {
       if (lane < nval) {
         const uint32_t nb = (uint32_t)((len + kVec - 1) / kVec * kVec * sizeof(TT));
-        if (OP == 1) bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
+        if (OP == 1 && !kDirect) bulk_s2g_add_f64(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
         else bulk_s2g(out + base + (long long)lane * Xp + lo, s + lane * P + lo, nb);
       }
     } else if (lane == 0) {
