@@ -2890,18 +2890,29 @@ __global__ void k_rk_next(const BlockDev* __restrict__ bd, const StageParams* __
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const double r1 = sp[B.case_id].dtk * B.yaco[l];
+    // every input is read before the first store: the compiler cannot tell
+    // that the stores (de, qa) touch nothing the loads read, and a store
+    // between two loads would hold the second behind the first's latency
+    R dv[5];
+    double qo[5];
+    if (sum) {
+      const R* r = W.scr;
+      R f[15];
+#pragma unroll
+      for (int k = 0; k < 15; ++k) f[k] = r[l + k * n];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) dv[c] = (f[3 * c] + f[3 * c + 1]) + f[3 * c + 2];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) dv[c] = W.de[l + c * n];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) qo[c] = B.qo[l + c * n];
     double q[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-      R dv;
-      if (sum) {
-        const R* r = W.scr;
-        dv = (r[l + (3 * c) * n] + r[l + (3 * c + 1) * n]) + r[l + (3 * c + 2) * n];
-        if (sum == 2) W.de[l + c * n] = dv;
-      } else {
-        dv = W.de[l + c * n];
-      }
-      q[c] = B.qo[l + c * n] - r1 * double(dv);
+      if (sum == 2) W.de[l + c * n] = dv[c];
+      q[c] = qo[c] - r1 * double(dv[c]);
       if (STORE_Q) B.qa[l + c * n] = q[c];
     }
     if (prim) prim_point<R>(W, cc[B.case_id], l, n, q[0], q[1], q[2], q[3], q[4]);
@@ -3064,11 +3075,24 @@ __global__ void k_gcbc_update(const BlockDev* __restrict__ bd, const GcbcTask* _
     R v[5];
     for (int c = 0; c < 5; ++c) v[c] = cha[c] - drv[c];
     r2q_apply<R>(e, cm, v, dha);
+    // the five points of the line are distinct: their 25 values load before
+    // any of them is stored (a store between two loads would make the second
+    // wait for the first's latency, since the compiler cannot tell they differ)
+    long long pts[5];
+    R ws[5], dv[5][5];
+#pragma unroll
     for (int ii = 0; ii <= 4; ++ii) {
-      const long long pt = T.pts[(long long)jk * 5 + ii];
-      const R w = R(T.w[(long long)jk * 5 + ii]);
-      for (int c = 0; c < 5; ++c) W.de[pt + c * n] = W.de[pt + c * n] + w * dha[c];
+      pts[ii] = T.pts[(long long)jk * 5 + ii];
+      ws[ii] = R(T.w[(long long)jk * 5 + ii]);
     }
+#pragma unroll
+    for (int ii = 0; ii <= 4; ++ii)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) dv[ii][c] = W.de[pts[ii] + c * n];
+#pragma unroll
+    for (int ii = 0; ii <= 4; ++ii)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) W.de[pts[ii] + c * n] = dv[ii][c] + ws[ii] * dha[c];
   }
 }
 
@@ -3146,10 +3170,17 @@ __global__ void k_rk_faces(const BlockDev* __restrict__ bd, const StageParams* _
     const long long l = tl[t], n = B.npad;
     const double r1 = sp[B.case_id].dtk * B.yaco[l];
     const R* r = W.scr;
+    // inputs first, then the stores (see k_rk_next)
+    R f[15];
+    double qo[5];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) f[k] = r[l + k * n];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) qo[c] = B.qo[l + c * n];
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-      const R dv = (r[l + (3 * c) * n] + r[l + (3 * c + 1) * n]) + r[l + (3 * c + 2) * n];
-      B.qa[l + c * n] = B.qo[l + c * n] - r1 * double(dv);
+      const R dv = (f[3 * c] + f[3 * c + 1]) + f[3 * c + 2];
+      B.qa[l + c * n] = qo[c] - r1 * double(dv);
     }
   }
 }

@@ -93,11 +93,15 @@ __global__ void k_avg_combine(const BlockDev* __restrict__ bd, const int* __rest
     const BlockDev& B = bd[tb[t]];
     const long long l = tl[t];
     const int f = tfirst[t], cnt = tcount[t];
+    // all five components formed before any is stored (the stores cannot
+    // alias the snapshot, but the compiler cannot know that)
+    double out[5];
+#pragma unroll
     for (int c = 0; c < 5; ++c) {
       if (mode == 0) {
         double acc = snap[(long long)f * 5 + c];
         for (int j = 1; j < cnt; ++j) acc = acc + snap[(long long)(f + j) * 5 + c];
-        B.qa[l + c * B.npad] = (1.0 / (double)cnt) * acc;
+        out[c] = (1.0 / (double)cnt) * acc;
       } else {
         double q = B.qa[l + c * B.npad];
         double r1 = 1.0;
@@ -106,9 +110,11 @@ __global__ void k_avg_combine(const BlockDev* __restrict__ bd, const int* __rest
           const double r2 = 1.0 / r1;
           q = r2 * ((r1 - 1.0) * q + snap[(long long)(f + j) * 5 + c]) + 0.0 * q;
         }
-        B.qa[l + c * B.npad] = q;
+        out[c] = q;
       }
     }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) B.qa[l + c * B.npad] = out[c];
   }
 }
 
