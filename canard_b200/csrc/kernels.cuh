@@ -3108,9 +3108,17 @@ __global__ void k_sponge(const BlockDev* __restrict__ bd, const SpongeTask* __re
     const int e = g - T.first;
     const long long l = T.pts[e], n = B.npad;
     const double a = T.asz[e], bb = T.bsz[e];
-    de[l] = R(double(de[l]) + a * (B.qa[l] - 1.0));
-    for (int d = 1; d <= 3; ++d) de[l + d * n] = R(double(de[l + d * n]) + bb * (B.qa[l + d * n] - 0.0));
-    de[l + 4 * n] = R(double(de[l + 4 * n]) + a * (B.qa[l + 4 * n] - (1.0 / kGam) * (1.0 / KGAMM1)));
+    // every input before the first store (see k_rk_next)
+    R dv[5];
+    double q[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      dv[c] = de[l + c * n];
+      q[c] = B.qa[l + c * n];
+    }
+    de[l] = R(double(dv[0]) + a * (q[0] - 1.0));
+    for (int d = 1; d <= 3; ++d) de[l + d * n] = R(double(dv[d]) + bb * (q[d] - 0.0));
+    de[l + 4 * n] = R(double(dv[4]) + a * (q[4] - (1.0 / kGam) * (1.0 / KGAMM1)));
   }
 }
 
