@@ -2727,17 +2727,19 @@ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long l
 
 // flux components rr(:,d,m) of one point into scr field (m-1)*3 + d and
 // de(:,5) = qa(:,5) + p (src/mo_physics.f90:319-382); t as from visc_point
+// pre (FROM_PRIM only): p and 1/rho as loaded by the caller ahead of the
+// viscous terms, so that their loads overlap the others'
 template <class R, bool FROM_PRIM = false>
 __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
-                                           long long l, long long n, const R t[9]) {
+                                           long long l, long long n, const R t[9], const R* pre = nullptr) {
   const double* q = B.qa;
   R* de = W.de;
-  const R p = W.p[l];
+  const R p = (FROM_PRIM && pre) ? pre[0] : W.p[l];
   // FROM_PRIM (FP32 step path): the conserved values come from the primitives
   // in de (1/rho, u, v, w) and p instead of a second read of the FP64 state
   R qv[5];
   if (FROM_PRIM) {
-    const R rho = R(1) / de[l];
+    const R rho = R(1) / (pre ? pre[1] : de[l]);
     const R uu = de[l + n], vv = de[l + 2 * n], ww = de[l + 3 * n];
     qv[0] = rho;
     qv[1] = rho * uu;
@@ -2851,12 +2853,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const bool visc = cc[B.case_id].viscous != 0;
+    // FP32: p and 1/rho load with the viscous terms' inputs
+    const R pre[2] = {sizeof(R) == 4 ? W.p[l] : R(0), sizeof(R) == 4 ? W.de[l] : R(0)};
     R t[9] = {};
     if (visc) {
       R d5;
       visc_point<R>(W, l, n, W.mu[l], t, d5);
     }
-    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t);
+    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, sizeof(R) == 4 ? pre : nullptr);
   }
 }
 
