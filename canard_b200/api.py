@@ -401,7 +401,8 @@ class Context:
         """Pins the line kernel of a group ("filter", "viscous", "flux") and
         direction ("xi", "eta", "zeta"), by name from LINE_KINDS; "fp64",
         "fp64-tmem" give results bit-identical to the reference's order,
-        "fp64-split" (the fast FP64 mode's kind) differs at rounding level."""
+        "fp64-split" and "fp64-twist" (the fast FP64 mode's kinds) differ at
+        rounding level."""
         g = ("filter", "viscous", "flux").index(group)
         d = ("xi", "eta", "zeta").index(direction)
         self._check(lib().canard_set_line_kind(self.h, g, d, self.LINE_KINDS[kind], chunks))

@@ -316,7 +316,7 @@ int canard_autotune(canard_ctx* ctx, int32_t reps, double* report, int32_t nmax)
  * results in tensor memory (eta/zeta, 16..257 points per line), 6 the filter
  * of the FP64 state streamed into FP32 right-hand sides (mixed precision), 7
  * FP64 split solve with FMA (FP64 and fast FP64 contexts; the fast mode's
- * default), 8 and 9 the derivative's quad split solve (four lanes per line) on
+ * default on lines under 32 points), 8 and 9 the derivative's quad split solve (four lanes per line) on
  * FP64 fields (FP64 and fast FP64 contexts) and on FP32 fields (mixed
  * precision), for lines of at least about 4 x 60 points (FP64) or 4 x 40
  * (FP32); 10, 11 and 12 the two-ended solve (two warps per tile of 32 lines,
