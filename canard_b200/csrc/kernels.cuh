@@ -2734,11 +2734,14 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
                                            long long l, long long n, const R t[9], const R* pre = nullptr) {
   const double* q = B.qa;
   R* de = W.de;
-  const R p = (FROM_PRIM && pre) ? pre[0] : W.p[l];
+  const R p = pre ? pre[0] : W.p[l];
   // FROM_PRIM (FP32 step path): the conserved values come from the primitives
   // in de (1/rho, u, v, w) and p instead of a second read of the FP64 state
   R qv[5];
-  if (FROM_PRIM) {
+  if (!FROM_PRIM && pre) {  // the state as loaded by the caller
+#pragma unroll
+    for (int c = 0; c < 5; ++c) qv[c] = pre[2 + c];
+  } else if (FROM_PRIM) {
     const R rho = R(1) / (pre ? pre[1] : de[l]);
     const R uu = de[l + n], vv = de[l + 2 * n], ww = de[l + 3 * n];
     qv[0] = rho;
@@ -2853,14 +2856,21 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const bool visc = cc[B.case_id].viscous != 0;
-    // FP32: p and 1/rho load with the viscous terms' inputs
-    const R pre[2] = {sizeof(R) == 4 ? W.p[l] : R(0), sizeof(R) == 4 ? W.de[l] : R(0)};
+    // p and 1/rho (FP32) or the state (FP64) load with the viscous terms' inputs
+    R pre[7];
+    pre[0] = W.p[l];
+    if (sizeof(R) == 4) {
+      pre[1] = W.de[l];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) pre[2 + c] = R(B.qa[l + c * n]);
+    }
     R t[9] = {};
     if (visc) {
       R d5;
       visc_point<R>(W, l, n, W.mu[l], t, d5);
     }
-    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, sizeof(R) == 4 ? pre : nullptr);
+    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, pre);
   }
 }
 
