@@ -2699,11 +2699,15 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
 // (src/mo_physics.f90:245-299); scr field g*3+d = d/d(xi_d) of u, v, w, T.
 // t = txx tyy tzz txy tyz tzx hxx hyy hzz; d5 = (2/3) div u.
 template <class R>
-__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5) {
+// mt (optional): the nine metric terms [d][c] as loaded by the caller
+__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5,
+                                           const R* mt = nullptr) {
   const R *xi = W.xim, *et = W.etm, *ze = W.zem, *g = W.scr;
+  auto met = [&](int d, int c) {
+    return mt ? mt[3 * d + c] : (d == 0 ? xi : d == 1 ? et : ze)[l + c * n];
+  };
   auto comb = [&](int f, int c) {
-    return (xi[l + c * n] * g[l + (3 * f) * n] + et[l + c * n] * g[l + (3 * f + 1) * n]) +
-           ze[l + c * n] * g[l + (3 * f + 2) * n];
+    return (met(0, c) * g[l + (3 * f) * n] + met(1, c) * g[l + (3 * f + 1) * n]) + met(2, c) * g[l + (3 * f + 2) * n];
   };
   R txx = comb(0, 0), hzz = comb(0, 1), tzx = comb(0, 2);
   R txy = comb(1, 0), tyy = comb(1, 1), hxx = comb(1, 2);
@@ -2731,7 +2735,8 @@ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long l
 // viscous terms, so that their loads overlap the others'
 template <class R, bool FROM_PRIM = false>
 __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
-                                           long long l, long long n, const R t[9], const R* pre = nullptr) {
+                                           long long l, long long n, const R t[9], const R* pre = nullptr,
+                                           const R* mtp = nullptr) {
   const double* q = B.qa;
   R* de = W.de;
   const R p = pre ? pre[0] : W.p[l];
@@ -2759,7 +2764,11 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
   R ssd[3], m[3][3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
+    if (mtp) {
+      m[d][0] = mtp[3 * d]; m[d][1] = mtp[3 * d + 1]; m[d][2] = mtp[3 * d + 2];
+    } else {
+      m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
+    }
     ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
   }
   R* r = W.scr;
@@ -2865,12 +2874,22 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
 #pragma unroll
       for (int c = 0; c < 5; ++c) pre[2 + c] = R(B.qa[l + c * n]);
     }
+    // FP32: the nine metric terms too, once for both parts
+    R mt9[9];
+    if (sizeof(R) == 4) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        mt9[c] = W.xim[l + c * n];
+        mt9[3 + c] = W.etm[l + c * n];
+        mt9[6 + c] = W.zem[l + c * n];
+      }
+    }
     R t[9] = {};
     if (visc) {
       R d5;
-      visc_point<R>(W, l, n, W.mu[l], t, d5);
+      visc_point<R>(W, l, n, W.mu[l], t, d5, sizeof(R) == 4 ? mt9 : nullptr);
     }
-    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, pre);
+    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, pre, sizeof(R) == 4 ? mt9 : nullptr);
   }
 }
 
