@@ -649,7 +649,8 @@ def main():
 
     # the dominant kernel: the single kernel with the largest share of the step
     # (each family is one kernel; the line solves are one kernel per direction)
-    kernel_of = {"flux_components": "k_flux_visc", "rk_update": "k_rk_next", "primitives": "k_prim"}
+    kernel_of = {"flux_components": "k_flux_visc_pairs" if args.precision == "fp32" else "k_flux_visc",
+                 "rk_update": "k_rk_next", "primitives": "k_prim"}
     cands = [(k, v) for k, v in fam.items() if v["launches"] and v["bytes"] > 0
              and (k in kernel_of or k.startswith(("deriv", "filter")))]
     dom_name = max(cands, key=lambda kv: kv[1]["ms"])[0]

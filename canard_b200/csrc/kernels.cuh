@@ -2699,13 +2699,9 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
 // (src/mo_physics.f90:245-299); scr field g*3+d = d/d(xi_d) of u, v, w, T.
 // t = txx tyy tzz txy tyz tzx hxx hyy hzz; d5 = (2/3) div u.
 template <class R>
-// mt (optional): the nine metric terms [d][c] as loaded by the caller
-__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5,
-                                           const R* mt = nullptr) {
+__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5) {
   const R *xi = W.xim, *et = W.etm, *ze = W.zem, *g = W.scr;
-  auto met = [&](int d, int c) {
-    return mt ? mt[3 * d + c] : (d == 0 ? xi : d == 1 ? et : ze)[l + c * n];
-  };
+  auto met = [&](int d, int c) { return (d == 0 ? xi : d == 1 ? et : ze)[l + c * n]; };
   auto comb = [&](int f, int c) {
     return (met(0, c) * g[l + (3 * f) * n] + met(1, c) * g[l + (3 * f + 1) * n]) + met(2, c) * g[l + (3 * f + 2) * n];
   };
@@ -2731,29 +2727,18 @@ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long l
 
 // flux components rr(:,d,m) of one point into scr field (m-1)*3 + d and
 // de(:,5) = qa(:,5) + p (src/mo_physics.f90:319-382); t as from visc_point
-// pre (FROM_PRIM only): p and 1/rho as loaded by the caller ahead of the
-// viscous terms, so that their loads overlap the others'
-template <class R, bool FROM_PRIM = false>
+// pre (optional): p and the five state values as loaded by the caller ahead
+// of the viscous terms, so that their loads overlap the others'
+template <class R>
 __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
-                                           long long l, long long n, const R t[9], const R* pre = nullptr,
-                                           const R* mtp = nullptr) {
+                                           long long l, long long n, const R t[9], const R* pre = nullptr) {
   const double* q = B.qa;
   R* de = W.de;
   const R p = pre ? pre[0] : W.p[l];
-  // FROM_PRIM (FP32 step path): the conserved values come from the primitives
-  // in de (1/rho, u, v, w) and p instead of a second read of the FP64 state
   R qv[5];
-  if (!FROM_PRIM && pre) {  // the state as loaded by the caller
+  if (pre) {
 #pragma unroll
-    for (int c = 0; c < 5; ++c) qv[c] = pre[2 + c];
-  } else if (FROM_PRIM) {
-    const R rho = R(1) / (pre ? pre[1] : de[l]);
-    const R uu = de[l + n], vv = de[l + 2 * n], ww = de[l + 3 * n];
-    qv[0] = rho;
-    qv[1] = rho * uu;
-    qv[2] = rho * vv;
-    qv[3] = rho * ww;
-    qv[4] = p * R(1.0 / KGAMM1) + R(0.5) * rho * ((uu * uu + vv * vv) + ww * ww);
+    for (int c = 0; c < 5; ++c) qv[c] = pre[1 + c];
   } else {
 #pragma unroll
     for (int c = 0; c < 5; ++c) qv[c] = R(q[l + c * n]);
@@ -2764,11 +2749,7 @@ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, 
   R ssd[3], m[3][3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    if (mtp) {
-      m[d][0] = mtp[3 * d]; m[d][1] = mtp[3 * d + 1]; m[d][2] = mtp[3 * d + 2];
-    } else {
-      m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
-    }
+    m[d][0] = mt[d][l]; m[d][1] = mt[d][l + n]; m[d][2] = mt[d][l + 2 * n];
     ssd[d] = (m[d][0] * u + m[d][1] * v) + m[d][2] * w;
   }
   R* r = W.scr;
@@ -2856,40 +2837,159 @@ __global__ void k_flux(const BlockDev* __restrict__ bd, const StageParams* __res
 // 9-field round trip through memory. Same operations in the same order, so
 // the results are bit-identical to k_viscous_assemble followed by k_flux
 // (de(:,1) = ss(:,1) is read from ss directly).
-// FP32: at most 64 registers, so four 256-thread blocks (32 warps) keep
-// enough 128-byte requests in flight per SM; FP64: two blocks
+// FP64, two 256-thread blocks per SM (128 registers); the FP32 step path runs
+// k_flux_visc_pairs.
 template <class R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(256, 2)
     k_flux_visc(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp, const CaseConst* __restrict__ cc) {
+  static_assert(sizeof(R) == 8, "the FP32 step path runs k_flux_visc_pairs");
   FOR_POINTS(bd[blockIdx.y]) {
     const Work<R> W = work<R>(B);
     const long long n = B.npad;
     const bool visc = cc[B.case_id].viscous != 0;
-    // p and 1/rho (FP32) or the state (FP64) load with the viscous terms' inputs
-    R pre[7];
+    // p and the state load with the viscous terms' inputs
+    R pre[6];
     pre[0] = W.p[l];
-    if (sizeof(R) == 4) {
-      pre[1] = W.de[l];
-    } else {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) pre[2 + c] = R(B.qa[l + c * n]);
-    }
-    // FP32: the nine metric terms too, once for both parts
-    R mt9[9];
-    if (sizeof(R) == 4) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        mt9[c] = W.xim[l + c * n];
-        mt9[3 + c] = W.etm[l + c * n];
-        mt9[6 + c] = W.zem[l + c * n];
-      }
-    }
+    for (int c = 0; c < 5; ++c) pre[1 + c] = R(B.qa[l + c * n]);
     R t[9] = {};
     if (visc) {
       R d5;
-      visc_point<R>(W, l, n, W.mu[l], t, d5, sizeof(R) == 4 ? mt9 : nullptr);
+      visc_point<R>(W, l, n, W.mu[l], t, d5);
     }
-    flux_point<R, (sizeof(R) == 4)>(W, B, sp[B.case_id], visc, l, n, t, pre, sizeof(R) == 4 ? mt9 : nullptr);
+    flux_point<R>(W, B, sp[B.case_id], visc, l, n, t, pre);
+  }
+}
+
+// One point of the FP32 fused kernel from values already in registers: the
+// operations of visc_point followed by flux_point<float, true>, in their order.
+// a: 12 gradients, 9 metric terms [d][c], mu, yaco, p, then the primitives
+// in de(:,1:4): 1/rho, u, v, w. out: the 15 flux components, then de(:,5).
+__device__ __forceinline__ void flux_visc_values(const float a[28], bool visc, float um0, float um1, float um2,
+                                                 float out[16]) {
+  const float* g = a;
+  const float* mt = a + 12;
+  const float mu = a[21], yaco = a[22], p = a[23], rhop = a[24], uu = a[25], vv = a[26], ww = a[27];
+  float t[9] = {};
+  if (visc) {
+    auto comb = [&](int f, int c) {
+      return (mt[c] * g[3 * f] + mt[3 + c] * g[3 * f + 1]) + mt[6 + c] * g[3 * f + 2];
+    };
+    float txx = comb(0, 0), hzz = comb(0, 1), tzx = comb(0, 2);
+    float txy = comb(1, 0), tyy = comb(1, 1), hxx = comb(1, 2);
+    float hyy = comb(2, 0), tyz = comb(2, 1), tzz = comb(2, 2);
+    const float s1 = comb(3, 0), s2 = comb(3, 1), s3 = comb(3, 2);
+    const float rr1 = mu * yaco;
+    const float rr2 = float(1.0 / (KGAMM1 * 0.71)) * rr1;
+    const float d5 = float(2.0 / 3.0) * ((txx + tyy) + tzz);
+    txx = rr1 * ((txx + txx) - d5);
+    tyy = rr1 * ((tyy + tyy) - d5);
+    tzz = rr1 * ((tzz + tzz) - d5);
+    txy = rr1 * (txy + hzz);
+    tyz = rr1 * (tyz + hxx);
+    tzx = rr1 * (tzx + hyy);
+    t[0] = txx; t[1] = tyy; t[2] = tzz; t[3] = txy; t[4] = tyz; t[5] = tzx;
+    t[6] = ((rr2 * s1 + uu * txx) + vv * txy) + ww * tzx;
+    t[7] = ((rr2 * s2 + uu * txy) + vv * tyy) + ww * tyz;
+    t[8] = ((rr2 * s3 + uu * tzx) + vv * tyz) + ww * tzz;
+  }
+  const float rho = 1.0f / rhop;
+  float qv[5];
+  qv[0] = rho;
+  qv[1] = rho * uu;
+  qv[2] = rho * vv;
+  qv[3] = rho * ww;
+  qv[4] = p * float(1.0 / KGAMM1) + 0.5f * rho * ((uu * uu + vv * vv) + ww * ww);
+  const float u = uu + um0, v = vv + um1, w = ww + um2;
+  float ssd[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ssd[d] = (mt[3 * d] * u + mt[3 * d + 1] * v) + mt[3 * d + 2] * w;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out[d] = qv[0] * ssd[d];
+  const float tau[3][3] = {{t[0], t[3], t[5]}, {t[3], t[1], t[4]}, {t[5], t[4], t[2]}};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float v1 = qv[c + 1] * ssd[d] + mt[3 * d + c] * p;
+      if (visc) {
+        v1 = v1 - mt[3 * d] * tau[c][0];
+        v1 = v1 - mt[3 * d + 1] * tau[c][1];
+        v1 = v1 - mt[3 * d + 2] * tau[c][2];
+      }
+      out[3 * (c + 1) + d] = v1;
+    }
+  }
+  const float d5 = qv[4] + p;
+  out[15] = d5;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float v1 = d5 * ssd[d] - p * ((um0 * mt[3 * d] + um1 * mt[3 * d + 1]) + um2 * mt[3 * d + 2]);
+    if (visc) {
+      v1 = v1 - mt[3 * d] * t[6];
+      v1 = v1 - mt[3 * d + 1] * t[7];
+      v1 = v1 - mt[3 * d + 2] * t[8];
+    }
+    out[12 + d] = v1;
+  }
+}
+
+// The FP32 fused kernel over pairs of neighbouring points (x even, x + 1):
+// every access is 8 bytes per thread, the width of the FP64 kernel's. The x
+// pitch is a multiple of 4, so a pair never straddles two rows; the second
+// point of a pair at the last x of an odd row is padding, computed and not
+// stored. Each thread reads all 28 inputs of both points before its first
+// store. Two blocks per SM (126 registers, no spill): with three, the spills
+// cost what the wider accesses gain.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_flux_visc_pairs(const BlockDev* __restrict__ bd, const StageParams* __restrict__ sp,
+                      const CaseConst* __restrict__ cc) {
+  const BlockDev& B = bd[blockIdx.y];
+  const Work<float> W = B.f;
+  const long long n = B.npad;
+  const bool visc = cc[B.case_id].viscous != 0;
+  const StageParams& S = sp[B.case_id];
+  const float um0 = float(S.umf[0]), um1 = float(S.umf[1]), um2 = float(S.umf[2]);
+  const long long stride = (long long)gridDim.x * blockDim.x;   // in pairs
+  const int sx = (int)((2 * stride) % B.Xp);
+  long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int x = (int)((2 * j) % B.Xp);
+  for (; 2 * j < n; j += stride, x = (x + sx >= B.Xp) ? x + sx - B.Xp : x + sx) {
+    if (x >= B.X) continue;
+    const long long l = 2 * j;
+    auto ld = [&](const float* f, int c) { return *reinterpret_cast<const float2*>(f + l + c * n); };
+    float2 v[28];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = visc ? ld(W.scr, k) : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v[12 + c] = ld(W.xim, c);
+      v[15 + c] = ld(W.etm, c);
+      v[18 + c] = ld(W.zem, c);
+    }
+    v[21] = visc ? ld(W.mu, 0) : make_float2(0.f, 0.f);
+    v[22] = visc ? ld(W.yaco, 0) : make_float2(0.f, 0.f);
+    v[23] = ld(W.p, 0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) v[24 + c] = ld(W.de, c);
+    float a0[28], a1[28], o0[16], o1[16];
+#pragma unroll
+    for (int k = 0; k < 28; ++k) {
+      a0[k] = v[k].x;
+      a1[k] = v[k].y;
+    }
+    flux_visc_values(a0, visc, um0, um1, um2, o0);
+    flux_visc_values(a1, visc, um0, um1, um2, o1);
+    if (x + 1 < B.X) {
+#pragma unroll
+      for (int k = 0; k < 15; ++k) *reinterpret_cast<float2*>(W.scr + l + k * n) = make_float2(o0[k], o1[k]);
+      *reinterpret_cast<float2*>(W.de + l + 4 * n) = make_float2(o0[15], o1[15]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 15; ++k) W.scr[l + k * n] = o0[k];
+      W.de[l + 4 * n] = o0[15];
+    }
   }
 }
 
@@ -3194,7 +3294,11 @@ void launch_flux(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams*
 }
 template <class R>
 void launch_flux_visc(dim3 g, cudaStream_t st, const BlockDev* bd, const StageParams* sp, const CaseConst* cc) {
-  k_flux_visc<R><<<g, 256, 0, st>>>(bd, sp, cc);
+  if constexpr (sizeof(R) == 4) {
+    k_flux_visc_pairs<2><<<g, 256, 0, st>>>(bd, sp, cc);
+  } else {
+    k_flux_visc<R><<<g, 256, 0, st>>>(bd, sp, cc);
+  }
 }
 template <class R>
 void launch_flux_sum(dim3 g, cudaStream_t st, const BlockDev* bd) {
