@@ -29,6 +29,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -526,7 +527,67 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
+
+
+class NvmlClocks:
+    """SM clock and clock event reasons read through NVML (read-only queries)
+    every `period` seconds on a thread between start() and stop(), so that a
+    timed region shorter than nvidia-smi's sampling interval still gets samples
+    taken under its load. Any NVML failure leaves it without samples, and
+    summary() returns None."""
+
+    # NVML clock event reason bits
+    MASKS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, gpu, period=0.01, nvml=None):
+        self.rows, self.period, self.thread = [], period, None
+        self.stop_ev = threading.Event()
+        self.nv = None
+        try:
+            if nvml is None:
+                import pynvml as nvml
+            nvml.nvmlInit()
+            self.h = nvml.nvmlDeviceGetHandleByIndex(gpu)
+            self.mx = float(nvml.nvmlDeviceGetMaxClockInfo(self.h, nvml.NVML_CLOCK_SM))
+            self.reasons = getattr(nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.nv = nvml
+        except Exception:
+            self.nv = None
+
+    def _poll(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                self.rows.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                  int(self.reasons(self.h))))
+            except Exception:
+                return
+            self.stop_ev.wait(self.period)
+
+    def start(self):
+        if self.nv is not None:
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+
+    def stop(self):
+        if self.thread is not None:
+            self.stop_ev.set()
+            self.thread.join(timeout=2.0)
+        if self.nv is not None:
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
+
+    def summary(self):
+        if not self.rows:
+            return None
+        reasons = sorted(k for k, m in self.MASKS.items() if any(r & m for _, r in self.rows))
+        return {"sm_mhz": float(np.median([s for s, _ in self.rows])), "sm_max_mhz": self.mx,
+                "reasons": reasons, "samples": len(self.rows),
+                "source": f"NVML, every {self.period * 1e3:.0f} ms during the timed steps"}
 
 
 def main():
@@ -602,17 +663,29 @@ def main():
     clk = Clocks(local) if rank == 0 else None
     if clk:
         clk.wait_first()
+    nclk = NvmlClocks(local) if rank == 0 else None
     barrier()
     torch.cuda.synchronize()
     n0 = ctx.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    if nclk:
+        nclk.start()
     e0.record(stream)
     ctx.step(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
+    if nclk:
+        nclk.stop()
     barrier()
     clocks = clk.stop() if clk else None
+    # NVML's samples fall inside the timed steps; nvidia-smi's 200 ms record is
+    # kept when NVML gave none
+    in_region = nclk.summary() if nclk else None
+    if in_region is not None:
+        if clocks is not None:
+            in_region["nvidia_smi"] = clocks
+        clocks = in_region
     ms = e0.elapsed_time(e1)
     launches = ctx.launch_count() - n0
     if dist is not None:
