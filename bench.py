@@ -476,6 +476,24 @@ def accuracy_mode(args, api, cases, torch):
     return out
 
 
+def smi_device(local):
+    """The device that nvidia-smi and NVML should read for CUDA device `local`:
+    its PCI bus id (domain:bus:device.function, as torch reports it), which
+    names the same GPU whatever CUDA_VISIBLE_DEVICES maps, once a one-shot
+    nvidia-smi query accepts it; else the index `local` as a string."""
+    try:
+        import torch
+        pr = torch.cuda.get_device_properties(local)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        r = subprocess.run(["nvidia-smi", "-i", bus, "--query-gpu=index", "--format=csv,noheader"],
+                           capture_output=True, text=True, timeout=10)
+        if r.returncode == 0 and r.stdout.strip():
+            return bus
+    except Exception:
+        pass
+    return str(local)
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -486,7 +504,7 @@ class Clocks:
     def __init__(self, gpu):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}",
+            self.p = subprocess.Popen(["nvidia-smi", "-i", gpu, f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
@@ -540,7 +558,9 @@ class NvmlClocks:
     # NVML clock event reason bits
     MASKS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, gpu, period=0.01, nvml=None):
+    def __init__(self, gpu, index=0, period=0.01, nvml=None):
+        """gpu: a PCI bus id or an index, as smi_device gives it; index: the
+        NVML index read when gpu is not a bus id NVML accepts."""
         self.rows, self.period, self.thread = [], period, None
         self.stop_ev = threading.Event()
         self.nv = None
@@ -548,7 +568,12 @@ class NvmlClocks:
             if nvml is None:
                 import pynvml as nvml
             nvml.nvmlInit()
-            self.h = nvml.nvmlDeviceGetHandleByIndex(gpu)
+            try:
+                self.h = nvml.nvmlDeviceGetHandleByPciBusId(str(gpu)) if ":" in str(gpu) else None
+            except Exception:
+                self.h = None
+            if self.h is None:
+                self.h = nvml.nvmlDeviceGetHandleByIndex(int(index))
             self.mx = float(nvml.nvmlDeviceGetMaxClockInfo(self.h, nvml.NVML_CLOCK_SM))
             self.reasons = getattr(nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
                 nvml.nvmlDeviceGetCurrentClocksThrottleReasons
@@ -660,10 +685,11 @@ def main():
             dist.barrier()
 
     ctx.step(args.warmup)
-    clk = Clocks(local) if rank == 0 else None
+    dev = smi_device(local) if rank == 0 else None
+    clk = Clocks(dev) if rank == 0 else None
     if clk:
         clk.wait_first()
-    nclk = NvmlClocks(local) if rank == 0 else None
+    nclk = NvmlClocks(dev, local) if rank == 0 else None
     barrier()
     torch.cuda.synchronize()
     n0 = ctx.launch_count()

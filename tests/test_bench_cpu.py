@@ -50,6 +50,9 @@ class _FakeNvml:
     def nvmlDeviceGetHandleByIndex(self, i):
         return ("gpu", i)
 
+    def nvmlDeviceGetHandleByPciBusId(self, bus):
+        raise RuntimeError("not found")  # the sampler falls back to the index
+
     def nvmlDeviceGetMaxClockInfo(self, h, kind):
         return 1965
 
@@ -69,7 +72,7 @@ def test_nvml_clock_sampler_summary():
     sys.path.insert(0, ROOT)
     import bench
     nv = _FakeNvml()
-    c = bench.NvmlClocks(0, period=0.001, nvml=nv)
+    c = bench.NvmlClocks("00000000:3B:00.0", 0, period=0.001, nvml=nv)
     c.start()
     time.sleep(0.05)
     c.stop()
@@ -83,7 +86,7 @@ def test_nvml_clock_sampler_summary():
 def test_nvml_clock_sampler_without_nvml():
     sys.path.insert(0, ROOT)
     import bench
-    c = bench.NvmlClocks(0, nvml=_FakeNvml(fail_init=True))
+    c = bench.NvmlClocks("0", 0, nvml=_FakeNvml(fail_init=True))
     c.start()
     c.stop()
     assert c.summary() is None
