@@ -2862,10 +2862,13 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // One point of the FP32 fused kernel from values already in registers: the
-// operations of visc_point followed by flux_point<float, true>, in their order.
+// stresses and heat flux (src/mo_physics.f90:245-299) and the flux components
+// (src/mo_physics.f90:319-382) in the order of visc_point and flux_point, with
+// the conserved values formed from the primitives instead of read.
 // a: 12 gradients, 9 metric terms [d][c], mu, yaco, p, then the primitives
 // in de(:,1:4): 1/rho, u, v, w. out: the 15 flux components, then de(:,5).
-__device__ __forceinline__ void flux_visc_values(const float a[28], bool visc, float um0, float um1, float um2,
+// Host-callable too, so that a CPU test can check it point by point.
+__host__ __device__ __forceinline__ void flux_visc_values(const float a[28], bool visc, float um0, float um1, float um2,
                                                  float out[16]) {
   const float* g = a;
   const float* mt = a + 12;
