@@ -2699,7 +2699,8 @@ __global__ void k_dtmax(const BlockDev* __restrict__ bd, const StageParams* __re
 // (src/mo_physics.f90:245-299); scr field g*3+d = d/d(xi_d) of u, v, w, T.
 // t = txx tyy tzz txy tyz tzx hxx hyy hzz; d5 = (2/3) div u.
 template <class R>
-__device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9], R& d5) {
+__host__ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long long n, R mu, R t[9],
+                                                    R& d5) {
   const R *xi = W.xim, *et = W.etm, *ze = W.zem, *g = W.scr;
   auto met = [&](int d, int c) { return (d == 0 ? xi : d == 1 ? et : ze)[l + c * n]; };
   auto comb = [&](int f, int c) {
@@ -2730,8 +2731,9 @@ __device__ __forceinline__ void visc_point(const Work<R>& W, long long l, long l
 // pre (optional): p and the five state values as loaded by the caller ahead
 // of the viscous terms, so that their loads overlap the others'
 template <class R>
-__device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S, bool visc,
-                                           long long l, long long n, const R t[9], const R* pre = nullptr) {
+__host__ __device__ __forceinline__ void flux_point(const Work<R>& W, const BlockDev& B, const StageParams& S,
+                                                    bool visc, long long l, long long n, const R t[9],
+                                                    const R* pre = nullptr) {
   const double* q = B.qa;
   R* de = W.de;
   const R p = pre ? pre[0] : W.p[l];

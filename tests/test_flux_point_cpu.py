@@ -1,11 +1,13 @@
-"""The FP32 fused flux kernel's point function (canard::flux_visc_values in
-canard_b200/csrc/kernels.cuh, the body of k_flux_visc_pairs), compiled for
-the host and checked against the reference's point formulas in FP64: the
+"""The flux kernels' point functions (canard_b200/csrc/kernels.cuh), compiled
+for the host and checked against the reference's point formulas in FP64: the
 viscous stresses and heat flux of calc_viscous_shear_stress
 (src/mo_physics.f90:245-299) and the flux components of calc_fluxes
-(src/mo_physics.f90:319-382), with the conserved values formed from the
-primitives as the FP32-mixed step path does. Viscous and inviscid points,
-with a moving frame. No GPU: the harness calls no CUDA API."""
+(src/mo_physics.f90:319-382). FP32: flux_visc_values, the point of
+k_flux_visc_pairs, with the conserved values formed from the primitives as
+the FP32-mixed step path does. FP64: visc_point and flux_point as
+k_flux_visc<double> (state preloaded) and k_flux (the phase API) call them.
+Viscous and inviscid points, with a moving frame. No GPU: the harness calls
+no CUDA API."""
 import os
 import shutil
 import subprocess
@@ -28,18 +30,23 @@ def harness(tmp_path_factory):
     return exe
 
 
-def run_harness(exe, a, visc, um):
-    head = np.array([a.shape[0], int(visc)], np.int32).tobytes() + np.asarray(um, np.float32).tobytes()
-    r = subprocess.run([exe], input=head + a.astype(np.float32).tobytes(), capture_output=True, timeout=60)
+def run_harness(exe, a, visc, um, mode=0):
+    """mode 0: FP32 point function on a[:, :28]; 1: FP64 fused form; 2: FP64
+    phase form, both on a[:, :33] (the conserved values in a[:, 28:33])."""
+    dt = np.float32 if mode == 0 else np.float64
+    cols = 28 if mode == 0 else 33
+    head = np.array([mode, a.shape[0], int(visc)], np.int32).tobytes() + np.asarray(um, np.float64).tobytes()
+    r = subprocess.run([exe], input=head + np.ascontiguousarray(a[:, :cols], dt).tobytes(), capture_output=True,
+                       timeout=60)
     assert r.returncode == 0, r.returncode
-    return np.frombuffer(r.stdout, np.float32).reshape(a.shape[0], 16)
+    return np.frombuffer(r.stdout, dt).reshape(a.shape[0], 16)
 
 
-def reference_point(a, visc, um):
+def reference_point(a, visc, um, qa=None):
     """FP64 statement of the reference's point formulas. a[:, 3f + d]: the
     derivative along direction d of variable f (u, v, w, T); a[:, 12 + 3d + c]:
     metric term c of direction d (xim, etm, zem); then mu, yaco, p, 1/rho, u,
-    v, w."""
+    v, w. qa: the conserved values, else formed from the primitives."""
     g = a[:, :12]
     mt = a[:, 12:21].reshape(-1, 3, 3)
     mu, yaco, p, rinv, u, v, w = (a[:, 21 + k] for k in range(7))
@@ -64,8 +71,9 @@ def reference_point(a, visc, um):
         tau[:, 0] = np.stack([txx, txy, tzx], 1)
         tau[:, 1] = np.stack([txy, tyy, tyz], 1)
         tau[:, 2] = np.stack([tzx, tyz, tzz], 1)
-    rho = 1.0 / rinv
-    qa = np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], 1)
+    if qa is None:
+        rho = 1.0 / rinv
+        qa = np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], 1)
     vel = np.stack([u + um[0], v + um[1], w + um[2]], 1)
     ss = np.einsum("ndc,nc->nd", mt, vel)
     out = np.zeros((n, 16))
@@ -95,6 +103,14 @@ def point_inputs(n, seed):
     return a.astype(np.float32).astype(np.float64)
 
 
+def conserved(a):
+    """The five conserved values of the points' primitives (for the FP64 forms,
+    which read the state)."""
+    rho = 1.0 / a[:, 24]
+    u, v, w, p = a[:, 25], a[:, 26], a[:, 27], a[:, 23]
+    return np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], 1)
+
+
 @pytest.mark.parametrize("visc", [1, 0])
 def test_flux_point_matches_reference_formulas(harness, visc):
     um = (0.1, -0.05, 0.02)
@@ -107,3 +123,16 @@ def test_flux_point_matches_reference_formulas(harness, visc):
     if visc:
         # the viscous terms are not negligible in these inputs
         assert np.linalg.norm(ref - reference_point(a, 0, um)) > 0.1 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("visc", [1, 0])
+def test_fp64_flux_point_matches_reference_formulas(harness, visc, mode):
+    um = (0.1, -0.05, 0.02)
+    a = point_inputs(4096, seed=11 + visc)
+    qa = conserved(a)
+    got = run_harness(harness, np.concatenate([a, qa], 1), visc, um, mode)
+    ref = reference_point(a, visc, um, qa)
+    for k in range(16):
+        err = np.linalg.norm(got[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k])
+        assert err <= 1e-14, (k, err)
